@@ -1,0 +1,147 @@
+/*
+ * uegccd.h -- C ABI of the B200 coupled-cluster path for the uniform electron gas.
+ *
+ * The entry points replace the Fortran module procedures of the reference
+ * (shepherd-group/uegccd) on the MP2 / CCD / dRPA hot path.  They take plain
+ * pointers in the reference's own layout so that a Fortran host can bind them
+ * with iso_c_binding (the binding is shown in INTEGRATION.md):
+ *
+ *   amplitude arrays  T(NOcc, NOcc, NOcc+1:NAO), FP64, column-major, i.e. element
+ *                     (i,j,a) (1-based, a > NOcc) at (i-1) + O*(j-1) + O*O*(a-O-1);
+ *   nVec              HEGData%nVec(NAO,3), int32, column-major: (p,d) at (p-1) + NAO*(d-1);
+ *   Eigen             HEGData%Eigen(NAO), FP64.
+ *
+ * Every function returns an int status: 0 ok, > 0 not converged, < 0 error
+ * (the message is in uegccd_last_error()).  The reference calls Stop or prints
+ * "DID NOT CONVERGE" in these places (CCD.f90:107-114, dRPA.f90:100-107); a host
+ * shim maps the statuses back to those messages.
+ *
+ * Calls on one context are serialised on that context's CUDA stream; separate
+ * contexts may be used from separate threads.  All device memory a call needs is
+ * allocated when the context is created (or grown on first use) and freed by
+ * uegccd_ctx_destroy.  There is no CPU fallback: without a CUDA device of compute
+ * capability 10.0 every call fails with UEGCCD_ERR_CUDA.
+ */
+#ifndef UEGCCD_H
+#define UEGCCD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    UEGCCD_OK = 0,
+    UEGCCD_NOT_CONVERGED = 1,        /* MaxRes > FailRatio*TolMax, or MaxIter reached */
+    UEGCCD_ERR_ARG = -1,             /* bad argument (null pointer, size, option)      */
+    UEGCCD_ERR_CUDA = -2,            /* CUDA error or no usable device                 */
+    UEGCCD_ERR_ALLOC = -3,           /* device or host allocation failed               */
+    UEGCCD_ERR_UNSUPPORTED = -4,     /* Input option outside the GPU path (see below)  */
+    UEGCCD_ERR_NUMERIC = -5          /* NaN/Inf in the amplitudes or the energy        */
+};
+
+/* Precision of the residual contractions. */
+enum { UEGCCD_FP64 = 0, UEGCCD_MIXED = 1 };
+/* Iteration scheme: REPLAY reproduces the reference iteration (1/2-damped Jacobi,
+ * CCD.f90:380, with its DIIS that never extrapolates, DIISCC.f90:110-115);
+ * DIIS runs a Pulay extrapolation over ndiis vectors (new in this library). */
+enum { UEGCCD_REPLAY = 0, UEGCCD_DIIS = 1 };
+
+/* The plane-wave system, i.e. the fields of HEGDataType / UEGInfoType
+ * (Types.f90:7-82) that the hot path reads. */
+typedef struct {
+    int32_t nocc;            /* UEGInfo%NOcc                                 */
+    int32_t nao;             /* UEGInfo%NAO                                  */
+    double L;                /* HEGData%L (box length)                       */
+    double madelung;         /* HEGData%Madelung; V(q=0) = -Madelung         */
+    const double *eigen;     /* HEGData%Eigen(NAO)                           */
+    const int32_t *nvec;     /* HEGData%nVec(NAO,3), column-major            */
+} UegccdSystem;
+
+/* Run options; uegccd_default_options() fills the reference's values. */
+typedef struct {
+    int32_t do_ring, do_xring, do_ladder, do_mosaic;   /* Input "Do Rings" ... (IO.f90:170-180)   */
+    int32_t core_n;          /* UEGInfo%CoreN; must be 0 (CAS integrals are outside the GPU path) */
+    double gapii;            /* UEGInfo%GapII; must be <= 0                                     */
+    int32_t range_flags;     /* sum of |"... Range"| Input values; must be 0                    */
+    int32_t max_iter;        /* MaxIter, 1000 (CCD.f90:36)                                      */
+    double tol;              /* TolMax on max|dT|, 1e-8 (HEG.f90:1078)                          */
+    double denom_factor;     /* DenomFactor, 2 (CCD.f90:11)                                     */
+    double fail_ratio;       /* FailRatio, 100 for CCD (HEG.f90:1079), 1e4 for dRPA (dRPA.f90:100) */
+    int32_t scheme;          /* UEGCCD_REPLAY or UEGCCD_DIIS                                    */
+    int32_t ndiis;           /* DIIS vectors for UEGCCD_DIIS (2..16)                            */
+    int32_t precision;       /* UEGCCD_FP64 or UEGCCD_MIXED                                     */
+    int32_t refine_sweeps;   /* MIXED: FP64 residual sweeps kept at the end                     */
+    double *energies;        /* optional: per-iteration energy, as printed to Output            */
+    double *dts;             /* optional: per-iteration max|dT|                                 */
+    int32_t max_rec;         /* capacity of energies/dts                                        */
+} UegccdOptions;
+
+typedef struct {
+    double ecorr;            /* Ec(CCD) / Ec(dRPA) (HEGData%ECorr at exit)                      */
+    double ecorr_sosex;      /* Ec(SOSEX) (dRPA only)                                           */
+    double max_res;          /* max |R| of the final residual (CCD.f90:105)                     */
+    double last_dt;          /* max |dT| of the last iteration                                  */
+    int32_t niter;           /* NIter at exit                                                   */
+    int32_t fail;            /* MaxRes > FailRatio*TolMax                                       */
+    int32_t n_recorded;      /* entries written to energies/dts                                 */
+    int32_t kernel_launches; /* CUDA kernels this call launched                                 */
+    double gpu_ms;           /* device time of the call (CUDA events)                           */
+} UegccdResult;
+
+typedef struct UegccdCtx UegccdCtx;
+
+/* Defaults of FindTol at HEGData%rS = 1 (HEG.f90:1073-1086) and of the Input
+ * switches (all terms on). */
+void uegccd_default_options(UegccdOptions *opt);
+
+/* Builds the momentum-block plan of one system on the current CUDA device and
+ * uploads it.  Replaces the per-call FindIndex lookups (HEG.f90:357-404) and the
+ * scratch set-up SetUpCCScr (CCScr.f90:9-31). */
+int uegccd_ctx_create(const UegccdSystem *sys, UegccdCtx **out);
+int uegccd_ctx_destroy(UegccdCtx *ctx);
+
+/* Replaces the eigenvalues (the twist-averaged-eigenvalue solve, Main.f90:243). */
+int uegccd_ctx_set_eigen(UegccdCtx *ctx, const double *eigen);
+
+/* DrvMBPT (MP2.f90:11-157) without the structure-factor dump: writes the MP2
+ * amplitudes T2aaaa/T2abab/T2abba (each may be NULL) and E(2). */
+int uegccd_mp2(UegccdCtx *ctx, double *t_aaaa, double *t_abab, double *t_abba, double *e2);
+
+/* DrvCCD (CCD.f90:18-183): iterates from the amplitudes given (the MP2 guess in
+ * Main.f90:85-89) and writes the converged amplitudes back in place.  Requires
+ * do_ring == do_xring (the spin-adapted form). */
+int uegccd_ccd(UegccdCtx *ctx, const UegccdOptions *opt, double *t_aaaa, double *t_abab,
+               double *t_abba, UegccdResult *res);
+
+/* DrvdRPA (dRPA.f90:23-174) on one amplitude array (the caller passes T2aaaa of
+ * the MP2 step, Main.f90:91); returns Ec(dRPA) and Ec(SOSEX). */
+int uegccd_drpa(UegccdCtx *ctx, const UegccdOptions *opt, double *t2, UegccdResult *res);
+
+/* One CCD residual G2 of the selected terms (TermsWrapper, CCD.f90:146-181; bit0
+ * drivers, bit1 mosaics, bit2 ladders, bit3 rings, bit4 crossed rings) for
+ * spin-adapted amplitudes t_abab; writes G2abab in the reference layout. */
+int uegccd_ccd_g2(UegccdCtx *ctx, const double *t_abab, int32_t term_mask, double *g_abab);
+
+/* ---- many independent solves in one launch per residual term ---------------- */
+typedef struct UegccdBatch UegccdBatch;
+
+/* A batch of n systems (twists, rs points, basis sizes); each keeps its own
+ * momentum blocks.  Amplitudes stay on the device between calls. */
+int uegccd_batch_create(const UegccdSystem *systems, int32_t n, UegccdBatch **out);
+int uegccd_batch_destroy(UegccdBatch *b);
+/* MP2 start + CCD (or dRPA when drpa != 0) of every system; results[n]. */
+int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2,
+                       UegccdResult *results);
+/* Copies solve s's amplitudes out in the reference layout (T2abab). */
+int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
+
+const char *uegccd_last_error(void);
+/* Library version string. */
+const char *uegccd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,594 @@
+// capi.cu -- the C ABI of include/uegccd.h: contexts, batches and the solve drivers.
+//
+// A context is a batch of one system.  The drivers follow DrvMBPT (MP2.f90:11-157),
+// DrvCCD (CCD.f90:18-183) and DrvdRPA (dRPA.f90:23-174): MP2 guess, then
+// residual -> update -> convergence -> energy per iteration until max|dT| < TolMax
+// or MaxIter, then one final residual for MaxRes.  All amplitudes, index maps
+// and intermediates stay on the device for the whole solve; one small
+// device-to-host read per iteration carries (E, max|dT|, max|R|) of every solve.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/uegccd.h"
+#include "kernels.h"
+#include "plan.h"
+#include "uegccd_internal.h"
+
+using namespace uegccd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CU(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(UEGCCD_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));            \
+    } while (0)
+
+int check_device()
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(UEGCCD_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    cudaDeviceProp p;
+    CU(cudaGetDeviceProperties(&p, dev));
+    if (p.major != 10)
+        return fail(UEGCCD_ERR_CUDA, std::string("the library is built for sm_100a (B200); device is ") + p.name);
+    return 0;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------
+// Batch: plans + device buffers of n systems
+// ----------------------------------------------------------------------------
+struct UegccdBatch {
+    std::vector<SystemHost> sys;
+    std::vector<SolvePlan> plans;
+    std::vector<SolveDev> hsolves;
+    std::vector<int> chunk_begin;
+    DevBatch d;
+    std::vector<void *> allocs;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<double> red;         // host copy: 3 per solve
+    std::vector<uint8_t> active;     // host copy
+    double *dense[3] = {nullptr, nullptr, nullptr};  // reference-layout scratch of the largest solve
+    size_t dense_n = 0;
+    int launches = 0;
+
+    ~UegccdBatch()
+    {
+        for (void *p : allocs) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    int alloc(T *&p, size_t n)
+    {
+        p = nullptr;
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc((void **)&p, n * sizeof(T));
+        if (e != cudaSuccess) return fail(UEGCCD_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(p);
+        return 0;
+    }
+    template <class T>
+    int upload(T *&p, const std::vector<T> &h)
+    {
+        int rc = alloc(p, h.size());
+        if (rc) return rc;
+        if (!h.empty()) CU(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        return 0;
+    }
+};
+
+struct UegccdCtx {
+    std::unique_ptr<UegccdBatch> batch;
+};
+
+namespace {
+
+int read_system(const UegccdSystem *s, SystemHost &h)
+{
+    if (!s || !s->eigen || !s->nvec) return fail(UEGCCD_ERR_ARG, "null system or array");
+    if (s->nocc <= 0 || s->nao <= s->nocc) return fail(UEGCCD_ERR_ARG, "need 0 < NOcc < NAO");
+    if (!(s->L > 0)) return fail(UEGCCD_ERR_ARG, "L must be positive");
+    h.O = s->nocc;
+    h.M = s->nao;
+    h.L = s->L;
+    h.madelung = s->madelung;
+    h.eigen.assign(s->eigen, s->eigen + s->nao);
+    h.n.resize(s->nao);
+    for (int p = 0; p < s->nao; p++)
+        for (int d = 0; d < 3; d++) h.n[p][d] = s->nvec[p + (size_t)s->nao * d];
+    return 0;
+}
+
+int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch> &out)
+{
+    int rc = check_device();
+    if (rc) return rc;
+    if (n <= 0) return fail(UEGCCD_ERR_ARG, "empty batch");
+    auto b = std::make_unique<UegccdBatch>();
+    b->sys.resize(n);
+    b->plans.resize(n);
+    for (int s = 0; s < n; s++) {
+        rc = read_system(&systems[s], b->sys[s]);
+        if (rc) return rc;
+        std::string msg = build_solve_plan(b->sys[s], b->plans[s]);
+        if (!msg.empty()) return fail(UEGCCD_ERR_ARG, "system " + std::to_string(s) + ": " + msg);
+        if (b->plans[s].O > 64) return fail(UEGCCD_ERR_UNSUPPORTED, "NOcc > 64 is outside the hole-hole ladder tiling");
+    }
+    CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&b->ev0));
+    CU(cudaEventCreate(&b->ev1));
+
+    std::vector<SolveDev> solves(n);
+    std::vector<BlockDev> blocks;
+    std::vector<LadderTile> tiles;
+    std::vector<ChunkDev> chunks, rchunks;
+    std::vector<int> chunk_begin(n + 1, 0);
+    std::vector<int2> targets;
+    std::vector<int16_t> pair_i, pair_j, vir;
+    std::vector<int32_t> pos, partner;
+    std::vector<AmpInfo> amps;
+    std::vector<int4> nv4;
+    std::vector<double> eigen, vtab;
+    std::vector<int64_t> hh0;
+    int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0;
+    int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0;
+    for (int s = 0; s < n; s++) {
+        const SolvePlan &P = b->plans[s];
+        const SystemHost &H = b->sys[s];
+        SolveDev &S = solves[s];
+        S.O = P.O; S.V = P.V; S.M = P.M;
+        S.nblk = (int)P.blocks.size();
+        S.blk0 = (int)blocks.size();
+        S.orb0 = orb0;
+        S.vtab0 = vtab0;
+        S.q2max = P.q2max;
+        S.amp0 = amp0;
+        S.namp = (int32_t)P.namp;
+        S.pad0 = 0;
+        S.pos0 = pos0;
+        S.ph0 = ph0;
+        S.jvv0 = jvv0;
+        S.joo0 = joo0;
+        S.denom_factor = 2.0;
+        for (const auto &B : P.blocks) {
+            BlockDev bd;
+            bd.solve = s; bd.o = B.o; bd.v = B.v;
+            bd.pair0 = (int)pair_i.size() + B.pair0;
+            bd.vir0 = (int)vir.size() + B.vir0;
+            bd.t0 = amp0 + B.t0;
+            int bi = (int)blocks.size();
+            blocks.push_back(bd);
+            hh0.push_back(hhoff);
+            hhoff += (int64_t)B.o * B.o;
+            max_o = std::max(max_o, B.o);
+            for (int a0 = 0; a0 < B.v; a0 += 64)
+                for (int p0 = 0; p0 < B.o; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, 0});
+        }
+        pair_i.insert(pair_i.end(), P.pair_i.begin(), P.pair_i.end());
+        pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
+        vir.insert(vir.end(), P.vir.begin(), P.vir.end());
+        for (int32_t x : P.pos) pos.push_back(x >= 0 ? (int32_t)(x + amp0) : -1);
+        for (const AmpInfo &q : P.amps) {
+            amps.push_back(q);
+            int32_t pb = P.pos[((size_t)q.i * P.O + q.j) * P.V + (q.b - P.O)];
+            partner.push_back((int32_t)(pb + amp0));
+        }
+        for (int p = 0; p < P.M; p++) nv4.push_back(make_int4(H.n[p][0], H.n[p][1], H.n[p][2], 0));
+        eigen.insert(eigen.end(), H.eigen.begin(), H.eigen.end());
+        vtab.insert(vtab.end(), P.vtab.begin(), P.vtab.end());
+        chunk_begin[s] = (int)chunks.size();
+        for (int64_t st = 0; st < P.namp; st += kChunk) chunks.push_back(ChunkDev{s, (int32_t)st});
+        for (int64_t st = 0; st < P.ring_entries; st += kChunk) rchunks.push_back(ChunkDev{s, (int32_t)st});
+        for (int x = 0; x < P.V + P.O; x++) targets.push_back(make_int2(s, x));
+        amp0 += P.namp;
+        pos0 += (int64_t)P.O * P.O * P.V;
+        ph0 += P.ring_entries;
+        orb0 += P.M;
+        vtab0 += P.q2max + 1;
+        jvv0 += P.V;
+        joo0 += P.O;
+        if (amp0 >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit packed indices");
+    }
+    chunk_begin[n] = (int)chunks.size();
+
+    DevBatch &d = b->d;
+    d.nsolves = n;
+    d.nblocks = (int)blocks.size();
+    d.ntiles = (int)tiles.size();
+    d.nchunks = (int)chunks.size();
+    d.nrchunks = (int)rchunks.size();
+    d.ntargets = (int)targets.size();
+    d.max_o = max_o;
+    d.namp = amp0;
+    if ((rc = b->upload(d.solves, solves))) return rc;
+    if ((rc = b->upload(d.blocks, blocks))) return rc;
+    if ((rc = b->upload(d.tiles, tiles))) return rc;
+    if ((rc = b->upload(d.chunks, chunks))) return rc;
+    if ((rc = b->upload(d.rchunks, rchunks))) return rc;
+    if ((rc = b->upload(d.chunk_begin, chunk_begin))) return rc;
+    if ((rc = b->upload(d.targets, targets))) return rc;
+    if ((rc = b->upload(d.pair_i, pair_i))) return rc;
+    if ((rc = b->upload(d.pair_j, pair_j))) return rc;
+    if ((rc = b->upload(d.vir, vir))) return rc;
+    if ((rc = b->upload(d.pos, pos))) return rc;
+    if ((rc = b->upload(d.partner, partner))) return rc;
+    if ((rc = b->upload(d.amps, amps))) return rc;
+    if ((rc = b->upload(d.nv4, nv4))) return rc;
+    if ((rc = b->upload(d.eigen, eigen))) return rc;
+    if ((rc = b->upload(d.vtab, vtab))) return rc;
+    if ((rc = b->upload(d.hh0, hh0))) return rc;
+    if ((rc = b->alloc(d.t, amp0))) return rc;
+    if ((rc = b->alloc(d.t_new, amp0))) return rc;
+    if ((rc = b->alloc(d.g, amp0))) return rc;
+    if ((rc = b->alloc(d.S, amp0))) return rc;
+    if ((rc = b->alloc(d.jvv, jvv0))) return rc;
+    if ((rc = b->alloc(d.joo, joo0))) return rc;
+    if ((rc = b->alloc(d.J1, ph0))) return rc;
+    if ((rc = b->alloc(d.J2, ph0))) return rc;
+    if ((rc = b->alloc(d.J3, ph0))) return rc;
+    if ((rc = b->alloc(d.hh, hhoff))) return rc;
+    if ((rc = b->alloc(d.part_e, chunks.size()))) return rc;
+    if ((rc = b->alloc(d.part_dt, chunks.size()))) return rc;
+    if ((rc = b->alloc(d.part_r, chunks.size()))) return rc;
+    if ((rc = b->alloc(d.red, 3 * (size_t)n))) return rc;
+    if ((rc = b->alloc(d.active, n))) return rc;
+    b->hsolves = solves;
+    b->chunk_begin = chunk_begin;
+    b->red.assign(3 * (size_t)n, 0.0);
+    b->active.assign(n, 1);
+    CU(cudaMemcpyAsync(d.active, b->active.data(), n, cudaMemcpyHostToDevice, b->stream));
+    size_t dn = 0;
+    for (int s = 0; s < n; s++) dn = std::max(dn, (size_t)b->plans[s].O * b->plans[s].O * b->plans[s].V);
+    b->dense_n = dn;
+    for (int k = 0; k < 3; k++)
+        if ((rc = b->alloc(b->dense[k], dn))) return rc;
+    CU(cudaStreamSynchronize(b->stream));
+    out = std::move(b);
+    return 0;
+}
+
+int set_active_all(UegccdBatch &b, uint8_t v)
+{
+    std::fill(b.active.begin(), b.active.end(), v);
+    CU(cudaMemcpyAsync(b.d.active, b.active.data(), b.active.size(), cudaMemcpyHostToDevice, b.stream));
+    return 0;
+}
+
+int read_red(UegccdBatch &b)
+{
+    CU(cudaMemcpyAsync(b.red.data(), b.d.red, b.red.size() * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+    CU(cudaGetLastError());
+    return 0;
+}
+
+// Copies one solve's amplitudes from a host reference-layout array into the packed t.
+int pack_from_host(UegccdBatch &b, int s, const double *host_dense)
+{
+    const SolvePlan &P = b.plans[s];
+    size_t n = (size_t)P.O * P.O * P.V;
+    CU(cudaMemcpyAsync(b.dense[0], host_dense, n * sizeof(double), cudaMemcpyHostToDevice, b.stream));
+    launch_pack(b.d, s, (int)P.namp, b.dense[0], b.stream);
+    b.launches++;
+    CU(cudaGetLastError());
+    return 0;
+}
+
+int unpack_to_host(UegccdBatch &b, int s, const double *t_dev, double *ab, double *ba, double *aa)
+{
+    const SolvePlan &P = b.plans[s];
+    size_t n = (size_t)P.O * P.O * P.V;
+    double *h[3] = {ab, ba, aa};
+    for (int k = 0; k < 3; k++)
+        if (h[k]) CU(cudaMemsetAsync(b.dense[k], 0, n * sizeof(double), b.stream));
+    launch_unpack(b.d, s, (int)P.namp, t_dev, ab ? b.dense[0] : nullptr, ba ? b.dense[1] : nullptr,
+                  aa ? b.dense[2] : nullptr, b.stream);
+    b.launches++;
+    CU(cudaGetLastError());
+    for (int k = 0; k < 3; k++)
+        if (h[k]) CU(cudaMemcpyAsync(h[k], b.dense[k], n * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+    return 0;
+}
+
+int validate_options(const UegccdOptions *o, int drpa)
+{
+    if (!o) return fail(UEGCCD_ERR_ARG, "null options");
+    if (o->core_n != 0) return fail(UEGCCD_ERR_UNSUPPORTED, "CoreN > 0 (CAS integrals) is outside the GPU path");
+    if (o->gapii > 0.0) return fail(UEGCCD_ERR_UNSUPPORTED, "GapII > 0 is outside the GPU path");
+    if (o->range_flags != 0) return fail(UEGCCD_ERR_UNSUPPORTED, "range-separated integrals are outside the GPU path");
+    if (!drpa && (o->do_ring != 0) != (o->do_xring != 0))
+        return fail(UEGCCD_ERR_UNSUPPORTED,
+                    "Do Rings and Do XRings must agree: alone, either breaks the spin symmetry the GPU path uses");
+    if (o->max_iter <= 0 || !(o->tol > 0) || !(o->denom_factor != 0)) return fail(UEGCCD_ERR_ARG, "bad iteration options");
+    if (o->scheme != UEGCCD_REPLAY) return fail(UEGCCD_ERR_UNSUPPORTED, "only the replay iteration is built");
+    if (o->precision != UEGCCD_FP64) return fail(UEGCCD_ERR_UNSUPPORTED, "only FP64 is built");
+    return 0;
+}
+
+// Runs the iteration for all solves of the batch from the amplitudes in d.t.
+// drpa: 0 CCD, 1 dRPA.  Per-solve results in res[]; records of solve 0 in opt.
+int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult *res)
+{
+    DevBatch &d = b.d;
+    const int n = d.nsolves;
+    TermFlags f;
+    f.drpa = drpa;
+    f.do_driver = 1;
+    f.do_mosaic = opt->do_mosaic ? 1 : 0;
+    f.do_ladder = (!drpa && opt->do_ladder) ? 1 : 0;
+    f.do_ring = opt->do_ring ? 1 : 0;
+    f.do_xring = (!drpa && opt->do_xring) ? 1 : 0;
+    for (int s = 0; s < n; s++) b.hsolves[s].denom_factor = opt->denom_factor;
+    CU(cudaMemcpyAsync(d.solves, b.hsolves.data(), n * sizeof(SolveDev), cudaMemcpyHostToDevice, b.stream));
+    int rc = set_active_all(b, 1);
+    if (rc) return rc;
+    b.launches = 0;
+    CU(cudaEventRecord(b.ev0, b.stream));
+    // CCEnergy of the start amplitudes and dT = max|T| (CCD.f90:63-64, dRPA.f90:68-69)
+    launch_energy(d, drpa ? 1 : 0, 0.0, b.stream);
+    launch_reduce(d, b.stream);
+    b.launches += 2;
+    if ((rc = read_red(b))) return rc;
+    std::vector<double> e(n), dt(n), rmax(n, 0.0);
+    std::vector<int> niter(n, 1);
+    for (int s = 0; s < n; s++) {
+        e[s] = b.red[3 * s];
+        dt[s] = b.red[3 * s + 1];
+    }
+    int nrec = 0;
+    auto record = [&](double en, double dtv) {
+        if (opt->max_rec > 0 && nrec < opt->max_rec) {
+            if (opt->energies) opt->energies[nrec] = en;
+            if (opt->dts) opt->dts[nrec] = dtv;
+            nrec++;
+        }
+    };
+    record(e[0], dt[0]);
+    int nactive = 0;
+    for (int s = 0; s < n; s++) {
+        b.active[s] = (dt[s] >= opt->tol && niter[s] < opt->max_iter) ? 1 : 0;
+        nactive += b.active[s];
+    }
+    CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
+    int status = 0;
+    while (nactive > 0) {
+        b.launches += launch_residual(d, f, 0, nullptr, b.stream);
+        CU(cudaGetLastError());
+        std::swap(d.t, d.t_new);
+        if ((rc = read_red(b))) return rc;
+        nactive = 0;
+        for (int s = 0; s < n; s++) {
+            if (!b.active[s]) continue;
+            niter[s]++;
+            e[s] = b.red[3 * s];
+            dt[s] = b.red[3 * s + 1];
+            if (s == 0) record(e[s], dt[s]);
+            if (!std::isfinite(e[s]) || !std::isfinite(dt[s])) {
+                b.active[s] = 0;
+                status = UEGCCD_ERR_NUMERIC;
+                continue;
+            }
+            if (dt[s] >= opt->tol && niter[s] < opt->max_iter) {
+                nactive++;
+            } else {
+                b.active[s] = 0;
+            }
+        }
+        CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
+    }
+    // final residual (CCD.f90:103-107, dRPA.f90:98-101)
+    if ((rc = set_active_all(b, 1))) return rc;
+    b.launches += launch_residual(d, f, 1, nullptr, b.stream);
+    if ((rc = read_red(b))) return rc;
+    for (int s = 0; s < n; s++) rmax[s] = b.red[3 * s + 2];
+    std::vector<double> esosex(n, 0.0);
+    if (drpa) {
+        launch_energy(d, 1, 1.0, b.stream);
+        launch_reduce(d, b.stream);
+        b.launches += 2;
+        if ((rc = read_red(b))) return rc;
+        for (int s = 0; s < n; s++) esosex[s] = b.red[3 * s];
+    }
+    CU(cudaEventRecord(b.ev1, b.stream));
+    CU(cudaEventSynchronize(b.ev1));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, b.ev0, b.ev1));
+    for (int s = 0; s < n; s++) {
+        UegccdResult &r = res[s];
+        r.ecorr = e[s];
+        r.max_res = rmax[s];
+        r.last_dt = dt[s];
+        r.niter = niter[s];
+        r.fail = rmax[s] > opt->fail_ratio * opt->tol;
+        r.ecorr_sosex = (drpa && !r.fail) ? esosex[s] : 0.0;
+        r.n_recorded = (s == 0) ? nrec : 0;
+        r.kernel_launches = b.launches;
+        r.gpu_ms = ms;
+        if (status == 0 && (r.fail || niter[s] >= opt->max_iter)) status = UEGCCD_NOT_CONVERGED;
+    }
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *uegccd_last_error(void) { return g_last_error.c_str(); }
+const char *uegccd_version(void) { return "uegccd_b200 0.1 (sm_100a)"; }
+
+void uegccd_default_options(UegccdOptions *o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->do_ring = o->do_xring = o->do_ladder = o->do_mosaic = 1;
+    o->max_iter = 1000;
+    o->tol = 1.0e-8;
+    o->denom_factor = 2.0;
+    o->fail_ratio = 100.0;
+    o->scheme = UEGCCD_REPLAY;
+    o->ndiis = 6;
+    o->precision = UEGCCD_FP64;
+    o->refine_sweeps = 2;
+}
+
+int uegccd_ctx_create(const UegccdSystem *sys, UegccdCtx **out)
+{
+    if (!out) return fail(UEGCCD_ERR_ARG, "null out");
+    *out = nullptr;
+    std::unique_ptr<UegccdBatch> b;
+    int rc = build_batch(sys, 1, b);
+    if (rc) return rc;
+    auto *c = new UegccdCtx;
+    c->batch = std::move(b);
+    *out = c;
+    return 0;
+}
+
+int uegccd_ctx_destroy(UegccdCtx *c)
+{
+    delete c;
+    return 0;
+}
+
+int uegccd_ctx_set_eigen(UegccdCtx *c, const double *eigen)
+{
+    if (!c || !eigen) return fail(UEGCCD_ERR_ARG, "null argument");
+    UegccdBatch &b = *c->batch;
+    b.sys[0].eigen.assign(eigen, eigen + b.sys[0].M);
+    CU(cudaMemcpyAsync(b.d.eigen, eigen, b.sys[0].M * sizeof(double), cudaMemcpyHostToDevice, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+    return 0;
+}
+
+int uegccd_mp2(UegccdCtx *c, double *t_aaaa, double *t_abab, double *t_abba, double *e2)
+{
+    if (!c) return fail(UEGCCD_ERR_ARG, "null context");
+    UegccdBatch &b = *c->batch;
+    launch_mp2(b.d, b.stream);
+    launch_reduce(b.d, b.stream);
+    CU(cudaGetLastError());
+    int rc = read_red(b);
+    if (rc) return rc;
+    if (e2) *e2 = b.red[0];
+    if (t_aaaa || t_abab || t_abba) {
+        rc = unpack_to_host(b, 0, b.d.t, t_abab, t_abba, t_aaaa);
+        if (rc) return rc;
+    }
+    return std::isfinite(b.red[0]) ? 0 : fail(UEGCCD_ERR_NUMERIC, "non-finite MP2 energy");
+}
+
+int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t_abab, double *t_abba,
+               UegccdResult *res)
+{
+    if (!c || !t_abab || !res) return fail(UEGCCD_ERR_ARG, "null argument");
+    int rc = validate_options(opt, 0);
+    if (rc) return rc;
+    UegccdBatch &b = *c->batch;
+    if ((rc = pack_from_host(b, 0, t_abab))) return rc;
+    int st = run_solves(b, opt, 0, res);
+    if (st < 0) return st;
+    if ((rc = unpack_to_host(b, 0, b.d.t, t_abab, t_abba, t_aaaa))) return rc;
+    return st;
+}
+
+int uegccd_drpa(UegccdCtx *c, const UegccdOptions *opt, double *t2, UegccdResult *res)
+{
+    if (!c || !t2 || !res) return fail(UEGCCD_ERR_ARG, "null argument");
+    int rc = validate_options(opt, 1);
+    if (rc) return rc;
+    UegccdBatch &b = *c->batch;
+    if ((rc = pack_from_host(b, 0, t2))) return rc;
+    int st = run_solves(b, opt, 1, res);
+    if (st < 0) return st;
+    if ((rc = unpack_to_host(b, 0, b.d.t, t2, nullptr, nullptr))) return rc;
+    return st;
+}
+
+int uegccd_ccd_g2(UegccdCtx *c, const double *t_abab, int32_t mask, double *g_abab)
+{
+    if (!c || !t_abab || !g_abab) return fail(UEGCCD_ERR_ARG, "null argument");
+    UegccdBatch &b = *c->batch;
+    int rc = pack_from_host(b, 0, t_abab);
+    if (rc) return rc;
+    if ((rc = set_active_all(b, 1))) return rc;
+    TermFlags f;
+    f.do_driver = (mask & 1) ? 1 : 0;
+    f.do_mosaic = (mask & 2) ? 1 : 0;
+    f.do_ladder = (mask & 4) ? 1 : 0;
+    f.do_ring = (mask & 8) ? 1 : 0;
+    f.do_xring = (mask & 16) ? 1 : 0;
+    // g_out reuses t_new (mode 1 does not write the update)
+    launch_residual(b.d, f, 1, b.d.t_new, b.stream);
+    CU(cudaGetLastError());
+    return unpack_to_host(b, 0, b.d.t_new, g_abab, nullptr, nullptr);
+}
+
+int uegccd_batch_create(const UegccdSystem *systems, int32_t n, UegccdBatch **out)
+{
+    if (!out || !systems) return fail(UEGCCD_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::unique_ptr<UegccdBatch> b;
+    int rc = build_batch(systems, n, b);
+    if (rc) return rc;
+    *out = b.release();
+    return 0;
+}
+
+int uegccd_batch_destroy(UegccdBatch *b)
+{
+    delete b;
+    return 0;
+}
+
+int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2, UegccdResult *results)
+{
+    if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
+    int rc = validate_options(opt, drpa);
+    if (rc) return rc;
+    launch_mp2(b->d, b->stream);
+    launch_reduce(b->d, b->stream);
+    if ((rc = read_red(*b))) return rc;
+    if (e2)
+        for (int s = 0; s < b->d.nsolves; s++) e2[s] = b->red[3 * s];
+    if (drpa) {
+        // the reference starts dRPA from T2aaaa of the MP2 step (Main.f90:85-91)
+        launch_to_aaaa(b->d, b->stream);
+        std::swap(b->d.t, b->d.t_new);
+    }
+    return run_solves(*b, opt, drpa, results);
+}
+
+int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab)
+{
+    if (!b || !t_abab || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
+    return unpack_to_host(*b, s, b->d.t, t_abab, nullptr, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,55 @@
+// kernels.h -- device buffers of a batch and the kernel launch wrappers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "uegccd_internal.h"
+
+namespace uegccd {
+
+// Raw device pointers of one batch (owned by the Batch object in capi.cu).
+struct DevBatch {
+    int nsolves = 0, nblocks = 0, ntiles = 0, nchunks = 0, nrchunks = 0, ntargets = 0;
+    int max_o = 0;
+    int64_t namp = 0;
+    SolveDev *solves = nullptr;
+    BlockDev *blocks = nullptr;
+    LadderTile *tiles = nullptr;
+    ChunkDev *chunks = nullptr;      // amplitude chunks
+    ChunkDev *rchunks = nullptr;     // ring-intermediate chunks over (i, x, l)
+    int *chunk_begin = nullptr;      // nsolves+1: first chunk of each solve
+    int2 *targets = nullptr;         // mosaic targets (solve, id)
+    int16_t *pair_i = nullptr, *pair_j = nullptr, *vir = nullptr;
+    int32_t *pos = nullptr;          // dense (i,j,a) -> global packed index or -1
+    int32_t *partner = nullptr;      // packed -> packed index of (i,j,b)
+    AmpInfo *amps = nullptr;
+    int4 *nv4 = nullptr;
+    double *eigen = nullptr, *vtab = nullptr;
+    double *t = nullptr, *t_new = nullptr, *g = nullptr, *S = nullptr;
+    double *jvv = nullptr, *joo = nullptr;
+    double *J1 = nullptr, *J2 = nullptr, *J3 = nullptr;
+    int64_t *hh0 = nullptr;          // per block: offset of H_K in hh
+    double *hh = nullptr;
+    double *part_e = nullptr, *part_dt = nullptr, *part_r = nullptr;
+    double *red = nullptr;           // 3 per solve: sum e, max dt, max |r|
+    uint8_t *active = nullptr;       // per solve
+};
+
+struct TermFlags {
+    int do_driver = 1, do_mosaic = 1, do_ladder = 1, do_pp = 1, do_hh = 1, do_ring = 1, do_xring = 1;
+    int drpa = 0;
+};
+
+void launch_mp2(const DevBatch &d, cudaStream_t st);
+void launch_reduce(const DevBatch &d, cudaStream_t st);
+void launch_energy(const DevBatch &d, int kind, double csosex, cudaStream_t st);
+// d.t_new = T2aaaa of d.t (t(ij,a) - t(ij,b))
+void launch_to_aaaa(const DevBatch &d, cudaStream_t st);
+// Residual of the selected terms for d.t; mode 0 also updates into d.t_new.  Returns launches.
+int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st);
+void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
+void launch_unpack(const DevBatch &d, int s, int namp, const double *t, double *ab, double *ba, double *aa,
+                   cudaStream_t st);
+
+}  // namespace uegccd

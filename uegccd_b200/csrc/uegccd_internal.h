@@ -1,0 +1,60 @@
+// uegccd_internal.h -- device data model shared by the host planner and the kernels.
+//
+// Amplitudes are stored block-packed by total crystal momentum K = n_i + n_j
+// (n_p the integer plane-wave vector of orbital p).  Block K holds o_K ordered
+// occupied pairs (i,j) as rows and v_K virtuals a (whose partner
+// b = K - a is also a virtual of the basis) as columns, row-major, one block
+// after another.  Only momentum-allowed amplitudes are stored; the reference's
+// dense T(NOcc,NOcc,NOcc+1:NAO) holds the same values with zeros elsewhere.
+//
+// The stored amplitude is the spin-adapted t(ij,a) = T2abab(i,j,a); the
+// reference's other channels follow from it: T2abba(i,j,a) = -t(ij,b) and
+// T2aaaa(i,j,a) = t(ij,a) - t(ij,b).
+//
+// Many independent solves (twists, rs values, basis sizes) live in one batch:
+// every per-solve array is concatenated and addressed through SolveDev offsets.
+#pragma once
+#include <cstdint>
+
+namespace uegccd {
+
+constexpr int kChunk = 256;  // amplitudes per element-wise work chunk
+
+struct SolveDev {
+    int O, V, M;            // occupied, virtual, orbitals
+    int nblk, blk0;         // K blocks of this solve: [blk0, blk0+nblk)
+    int orb0;               // offset of this solve's orbitals in nvec/eigen
+    int vtab0, q2max;       // Coulomb table: vtab[vtab0 + |q|^2], |q|^2 <= q2max
+    int64_t amp0;           // first packed amplitude (global index)
+    int32_t namp;           // number of stored amplitudes
+    int32_t pad0;
+    int64_t pos0;           // offset of the dense (i,j,a) -> packed map (O*O*V entries)
+    int64_t ph0;            // offset of the ring intermediates (O*V*O entries each)
+    int32_t jvv0, joo0;     // offsets of the mosaic intermediates (V and O entries)
+    double denom_factor;    // SolveCC damping (CCD.f90:380), 2 in the reference
+};
+
+struct BlockDev {
+    int solve;              // owning solve
+    int o, v;               // o_K rows (ordered occupied pairs), v_K columns (virtuals)
+    int pair0;              // offset into pair_i/pair_j
+    int vir0;               // offset into vir (absolute orbital indices, local to the solve)
+    int64_t t0;             // global packed index of element (row 0, col 0)
+};
+
+// One tile of the particle-particle ladder: rows [p0, p0+P) x columns [a0, a0+A) of block blk.
+struct LadderTile {
+    int blk, a0, p0, pad;
+};
+
+// Per-amplitude record: orbital indices local to the solve (a, b absolute, >= O).
+struct AmpInfo {
+    int16_t i, j, a, b;
+};
+
+struct ChunkDev {
+    int solve;
+    int32_t start;          // first amplitude of the chunk, local to the solve
+};
+
+}  // namespace uegccd

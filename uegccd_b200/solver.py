@@ -1,0 +1,120 @@
+"""Python face of the C ABI: one system (context) or many (batch).
+
+Mirrors the reference's driver entry points on the hot path:
+    DrvMBPT  (MP2.f90:11)   -> Context.mp2
+    DrvCCD   (CCD.f90:18)   -> Context.ccd
+    DrvdRPA  (dRPA.f90:23)  -> Context.drpa
+Amplitude arrays use the reference layout T(NOcc,NOcc,NOcc+1:NAO) column-major,
+which is a C-ordered numpy array of shape (V, O, O) indexed [a-O-1, j-1, i-1].
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi as capi
+
+
+class Context:
+    """uegccd_ctx_*: the momentum-block plan of one system, resident on the GPU."""
+
+    def __init__(self, nocc: int, L: float, madelung: float, eigen, nvec):
+        self.nocc = int(nocc)
+        self.nao = int(len(eigen))
+        self.nvir = self.nao - self.nocc
+        self._sys = capi.make_system(nocc, L, madelung, eigen, nvec)
+        h = C.c_void_p()
+        capi.check(capi.lib().uegccd_ctx_create(C.byref(self._sys), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.lib().uegccd_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def zeros_t(self) -> np.ndarray:
+        return np.zeros((self.nvir, self.nocc, self.nocc))
+
+    def set_eigen(self, eigen) -> None:
+        e = np.ascontiguousarray(eigen, dtype=np.float64)
+        capi.check(capi.lib().uegccd_ctx_set_eigen(self._h, capi.dptr(e)))
+
+    def mp2(self):
+        """DrvMBPT: returns (E2, T2aaaa, T2abab, T2abba)."""
+        ta, tb, tc = self.zeros_t(), self.zeros_t(), self.zeros_t()
+        e2 = C.c_double()
+        capi.check(capi.lib().uegccd_mp2(self._h, capi.dptr(ta), capi.dptr(tb), capi.dptr(tc), C.byref(e2)))
+        return e2.value, ta, tb, tc
+
+    def ccd(self, t_aaaa, t_abab, t_abba, max_rec: int = 1100, **opts):
+        """DrvCCD: iterates in place; returns (status, result dict, energies, dts)."""
+        en, dts = np.zeros(max_rec), np.zeros(max_rec)
+        o = capi.default_options(**opts)
+        o.energies, o.dts, o.max_rec = capi.dptr(en), capi.dptr(dts), max_rec
+        r = capi.Result()
+        rc = capi.check(capi.lib().uegccd_ccd(self._h, C.byref(o), capi.dptr(t_aaaa), capi.dptr(t_abab),
+                                              capi.dptr(t_abba), C.byref(r)))
+        return rc, r.as_dict(), en[: r.n_recorded].copy(), dts[: r.n_recorded].copy()
+
+    def drpa(self, t2, max_rec: int = 1100, **opts):
+        """DrvdRPA on one amplitude array (T2aaaa of the MP2 step)."""
+        en, dts = np.zeros(max_rec), np.zeros(max_rec)
+        o = capi.default_options(**opts)
+        o.fail_ratio = opts.get("fail_ratio", 1.0e4)
+        o.energies, o.dts, o.max_rec = capi.dptr(en), capi.dptr(dts), max_rec
+        r = capi.Result()
+        rc = capi.check(capi.lib().uegccd_drpa(self._h, C.byref(o), capi.dptr(t2), C.byref(r)))
+        return rc, r.as_dict(), en[: r.n_recorded].copy(), dts[: r.n_recorded].copy()
+
+    def ccd_g2(self, t_abab, mask: int = 31) -> np.ndarray:
+        g = self.zeros_t()
+        t = np.ascontiguousarray(t_abab, dtype=np.float64)
+        capi.check(capi.lib().uegccd_ccd_g2(self._h, capi.dptr(t), mask, capi.dptr(g)))
+        return g
+
+
+class Batch:
+    """uegccd_batch_*: many independent systems solved together."""
+
+    def __init__(self, systems):
+        """systems: iterable of (nocc, L, madelung, eigen, nvec)."""
+        self._systems = [capi.make_system(*s) for s in systems]
+        arr = (capi.System * len(self._systems))(*self._systems)
+        self._arr = arr
+        h = C.c_void_p()
+        capi.check(capi.lib().uegccd_batch_create(arr, len(self._systems), C.byref(h)))
+        self._h = h
+        self.n = len(self._systems)
+        self._shapes = [(s.nao - s.nocc, s.nocc, s.nocc) for s in self._systems]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.lib().uegccd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, drpa: bool = False, **opts):
+        o = capi.default_options(**opts)
+        if drpa and "fail_ratio" not in opts:
+            o.fail_ratio = 1.0e4
+        e2 = np.zeros(self.n)
+        res = (capi.Result * self.n)()
+        rc = capi.check(capi.lib().uegccd_batch_solve(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2), res))
+        return rc, e2, [r.as_dict() for r in res]
+
+    def amplitudes(self, s: int) -> np.ndarray:
+        t = np.zeros(self._shapes[s])
+        capi.check(capi.lib().uegccd_batch_get_amplitudes(self._h, s, capi.dptr(t)))
+        return t
