@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: batched twist-averaged CCD solves per second on the B200.
+
+Workload ("ccd-twist-batch", the batched twist-average configuration):
+  N=54 electrons (27 occupied), rs=1.0, per twist k_s ~ U[-0.5,0.5)^3 (units of 2*pi/L,
+  numpy default_rng seed 2024): occupy the 27 lowest |n+k_s|^2, basis = the 485
+  lowest from the |n|^2 <= 30 pool (fcut 6.857 -> NAO 485); HF eigenvalues; MP2 start;
+  CCD iterated exactly as the reference does (1/2-damped Jacobi, DIIS inert,
+  max|dT| < 1e-8, FP64) to convergence.  One step = MP2 + CCD of every twist.
+  Inputs are synthetic: the reference publishes no dataset, only this recipe.
+
+Metric: CCD solves/s (whole job; N GPUs each solve their own twist batch, weak scaling).
+  value  device-timed (CUDA events on the library's stream), inputs resident;
+  e2e    the same through the C ABI with host buffers: batch create (plan + uploads),
+         solve, amplitudes copied back to host, every step.
+--impl reference times the oracle (C restatement of the reference Fortran) on the
+host cores: one process per core, each running CCD iterations of its own twist.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ELECTRONS = 54
+RS = 1.0
+MAXK = 30          # candidate pool |n|^2 <= 30 (739 plane waves)
+FCUT = 6.857       # round(fcut^1.5 * 27) = 485 orbitals
+SEED = 2024
+# Mean CCD iteration count of this workload in the reference's iteration (replay mode
+# reproduces the reference's iterations exactly); measured by the GPU arm, which
+# checks it every run.  Used to turn the oracle's time per iteration into a time per solve.
+REF_ITERS_PER_SOLVE = None  # filled from the GPU arm's own run when available
+
+
+def twists(n: int, seed: int = SEED, rank: int = 0):
+    import numpy as np
+
+    rng = np.random.default_rng(seed + 7919 * rank)
+    return rng.random((n, 3)) - 0.5
+
+
+def build_systems(tw):
+    from uegccd_b200 import heg
+
+    inp = heg.default_input(nelectron=N_ELECTRONS, maxkpoint=MAXK, rsmin=RS, rsmax=RS, fcut=FCUT)
+    h = heg.Heg(inp)
+    out = []
+    for t in tw:
+        h.change_twist(t)
+        out.append(h.system())
+    return out
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in r.stdout.strip().split(",")]
+                if len(f) >= 7:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------- GPU arm
+def ladder_flops(batch_systems):
+    """Algorithmic FLOPs of one particle-particle ladder pass: 2 * sum_K o_K v_K^2."""
+    from collections import defaultdict
+
+    import numpy as np
+
+    tot = 0
+    for (nocc, L, mad, eig, nv) in batch_systems:
+        O = nocc
+        idx = {tuple(v): p for p, v in enumerate(nv)}
+        blocks = defaultdict(lambda: [0, None])
+        for i in range(O):
+            for j in range(O):
+                K = tuple(nv[i] + nv[j])
+                blocks[K][0] += 1
+                if blocks[K][1] is None:
+                    cnt = 0
+                    for a in range(O, len(nv)):
+                        b = idx.get(tuple(np.array(K) - nv[a]), -1)
+                        if b >= O:
+                            cnt += 1
+                    blocks[K][1] = cnt
+        tot += sum(2 * o * v * v for o, v in blocks.values())
+    return tot
+
+
+def run_gpu(args, rank, world):
+    import numpy as np
+
+    from uegccd_b200 import Batch
+
+    tw = twists(args.twists, rank=rank)
+    systems = build_systems(tw)
+    batch = Batch(systems)
+    # warm-up (untimed)
+    for _ in range(args.warmup):
+        rc, e2, res = batch.solve()
+    batch.set_profiling(True)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    if dist:
+        dist.barrier()
+    step_ms = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for _ in range(args.steps):
+            rc, e2, res = batch.solve()
+            step_ms.append(res[0]["gpu_ms"])
+    stats = batch.kernel_stats()
+    batch.set_profiling(False)
+    niters = [r["niter"] for r in res]
+    fails = sum(r["fail"] for r in res)
+    total_ms = float(sum(step_ms))
+    # e2e: through the C ABI with host buffers, every step
+    e2e_ms = []
+    h2d = d2h = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        b2 = Batch(systems)
+        rc2, e2b, res2 = b2.solve()
+        amps = [b2.amplitudes(s) for s in range(b2.n)]
+        hb, db = b2.transfer_bytes()
+        b2.close()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        h2d, d2h = hb, db
+    e_max = total_ms
+    if dist:
+        import torch
+
+        t = torch.tensor([total_ms, float(np.mean(e2e_ms))], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_max, e2e_mean = float(t[0]), float(t[1])
+    else:
+        e2e_mean = float(np.mean(e2e_ms))
+    solves_total = args.twists * world * args.steps
+    value = solves_total / (e_max / 1e3)
+    e2e_value = args.twists * world / (e2e_mean / 1e3)
+    out = {
+        "value": value, "ms_per_step": e_max / args.steps, "e2e_value": e2e_value, "h2d": h2d, "d2h": d2h,
+        "niter_mean": float(np.mean(niters)), "niter_min": int(min(niters)), "niter_max": int(max(niters)),
+        "fails": int(fails), "rc": rc, "stats": stats, "clocks": clk.summary(),
+        "ecorr_first": res[0]["ecorr"], "e2_first": float(e2[0]), "launches_per_step": res[0]["kernel_launches"],
+        "systems": systems,
+    }
+    return out
+
+
+# ------------------------------------------------------------------- oracle arm
+def _oracle_iter_worker(q):
+    """Runs `iters` CCD iterations of one twist in the oracle; returns seconds per iteration."""
+    tw, iters = q
+    sys.path.insert(0, ROOT)
+    import numpy as np  # noqa: F401
+
+    from oracle.oracle import Oracle, parse_input_text
+
+    vals = parse_input_text("")
+    vals.update({"# Electrons": str(N_ELECTRONS), "Momentum Cutoff": str(MAXK), "rSMin": str(RS),
+                 "rSMax": str(RS), "fcut": str(FCUT), "NTwist": " ".join(str(x) for x in tw)})
+    o = Oracle(vals)
+    e2, ta, tb, tc, _ = o.mp2()
+    t0 = time.perf_counter()
+    o.ccd(ta, tb, tc, max_iter=iters + 1)  # iters updates + the final residual
+    dt = time.perf_counter() - t0
+    return dt / (iters + 1)
+
+
+def oracle_rate(ncores: int, iters: int, iters_per_solve: float, rank: int = 0):
+    """Solves/s of the oracle on ncores processes (one twist each), from a bounded sample."""
+    import multiprocessing as mp
+
+    tw = twists(max(ncores, 1), rank=rank)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(ncores) as pool:
+        per_iter = pool.map(_oracle_iter_worker, [(tuple(t), iters) for t in tw[:ncores]])
+    wall = time.perf_counter() - t0
+    sec_per_solve = statistics.mean(per_iter) * iters_per_solve
+    return ncores / sec_per_solve, per_iter, wall
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--twists", type=int, default=100)
+    ap.add_argument("--cpu-iters", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--iters-per-solve", type=float, default=None)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    metric = "CCD solves/s (N=54 rs=1 twist batch, FP64 replay to max|dT|<1e-8)"
+    config = {"workload": "ccd-twist-batch", "n_electrons": N_ELECTRONS, "rs": RS, "nao": 485,
+              "twists_per_gpu": args.twists, "twist_seed": SEED, "maxkpoint_pool": MAXK, "fcut": FCUT,
+              "iteration": "reference replay (1/2-damped Jacobi, DIIS inert, tol 1e-8)",
+              "l2": "inputs larger than L2 (each step reads >1 GB of amplitudes and tables)",
+              "parallelism": f"independent solves, {world} GPU(s)"}
+    ips = args.iters_per_solve or 21.0
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ncores = os.cpu_count() or 1
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            r, per_iter, wall = oracle_rate(ncores, args.cpu_iters, ips)
+            vals.append(r)
+        v = statistics.mean(vals[args.warmup:]) if args.steps > 0 else vals[-1]
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": "solves/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": ncores, "kind": "port",
+                                 "sample": f"{args.cpu_iters} CCD iteration(s) of one twist per core, "
+                                           f"x {ips} iterations per solve"},
+                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        from datetime import timedelta
+
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+    g = run_gpu(args, rank, world)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    stats = g["stats"]
+    top = max((k for k in stats if k not in ("k_mp2",)), key=lambda k: stats[k][0])
+    top_ms, top_launch = stats[top]
+    flops_pp = ladder_flops(g["systems"][:min(10, len(g["systems"]))]) * (len(g["systems"]) / min(10, len(g["systems"])))
+    roof = {"kernel": top, "launches": top_launch, "avg_ms": top_ms / max(top_launch, 1)}
+    roof.update({"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None, "traffic": None})
+    line = {"metric": metric, "value": g["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": g["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+            "e2e": {"value": g["e2e_value"], "unit": "solves/s", "h2d_bytes_per_step": g["h2d"],
+                    "d2h_bytes_per_step": g["d2h"]},
+            "gpu_launches": int(g["launches_per_step"]) * args.steps,
+            "clocks": g["clocks"], "roofline": roof,
+            "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in stats.items()},
+            "check": {"niter_mean": g["niter_mean"], "niter_min": g["niter_min"], "niter_max": g["niter_max"],
+                      "not_converged": g["fails"], "ecorr_twist0": g["ecorr_first"], "e2_twist0": g["e2_first"],
+                      "pp_ladder_gflop_per_iter": flops_pp / 1e9}}
+    if world == 1 and not args.no_cpu_baseline:
+        ncores = 1
+        r, per_iter, wall = oracle_rate(ncores, args.cpu_iters, g["niter_mean"])
+        line["cpu_baseline"] = {"value": r, "unit": "solves/s", "cores": ncores, "kind": "port",
+                                "sample": f"{args.cpu_iters} CCD iteration(s) of twist 0 in the oracle, "
+                                          f"x {g['niter_mean']:.2f} mean iterations per solve ({per_iter[0]:.2f} s/iter)"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

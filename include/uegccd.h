@@ -137,6 +137,15 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
 /* Copies solve s's amplitudes out in the reference layout (T2abab). */
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
 
+/* Live kernel timing: when on, every kernel of a batch solve is bracketed by CUDA
+ * events on the batch's stream; stats return per-kernel total ms and launches. */
+int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on);
+int32_t uegccd_batch_kernel_stats(UegccdBatch *b, int32_t max, const char **names, double *ms,
+                                  int64_t *launches);
+
+/* Host<->device bytes the batch has moved since its creation (its upload included). */
+int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h);
+
 const char *uegccd_last_error(void);
 /* Library version string. */
 const char *uegccd_version(void);

@@ -117,7 +117,8 @@ def test_drpa_g1_golden(goldens):
     ctx = _ctx(o)
     e2, ta, tb, tc = ctx.mp2()
     assert abs(e2 - g["e2"]) < 5e-13
-    rc, r, en, dts = ctx.drpa(ta.copy())
+    # G1's Input has "Do Mosaics: F"
+    rc, r, en, dts = ctx.drpa(ta.copy(), do_mosaic=0)
     assert rc == 0 and not r["fail"]
     assert r["niter"] == g["niter"] == 22
     assert abs(r["ecorr"] - g["ec_drpa"]) < 1e-11
@@ -142,3 +143,18 @@ def test_ccd_n54_three_iterations_match_oracle():
     np.testing.assert_allclose(en, en_o, atol=1e-12, rtol=0)
     np.testing.assert_allclose(dts, dts_o, atol=1e-13, rtol=0)
     assert np.abs(tb - tb2).max() < 1e-13
+
+
+def test_drpa_with_mosaics_matches_oracle(goldens):
+    g = goldens["G1"]
+    vals = parse_input_text(g["input_text"])
+    vals["Do Mosaics"] = "T"
+    o = Oracle(vals)
+    ctx = _ctx(o)
+    e2, ta, tb, tc = ctx.mp2()
+    rc, r, en, dts = ctx.drpa(ta.copy(), do_mosaic=1)
+    e2o, ta2, tb2, tc2, _ = o.mp2()
+    st, en_o, _ = o.drpa(ta2.copy())
+    assert r["niter"] == st.niter
+    np.testing.assert_allclose(en, en_o, atol=1e-12, rtol=0)
+    assert abs(r["ecorr_sosex"] - st.ecorr_sosex) < 1e-12

@@ -59,7 +59,8 @@ EXPORTS = [
     "uegccd_default_options", "uegccd_ctx_create", "uegccd_ctx_destroy", "uegccd_ctx_set_eigen",
     "uegccd_mp2", "uegccd_ccd", "uegccd_drpa", "uegccd_ccd_g2", "uegccd_batch_create",
     "uegccd_batch_destroy", "uegccd_batch_solve", "uegccd_batch_get_amplitudes", "uegccd_last_error",
-    "uegccd_version",
+    "uegccd_version", "uegccd_batch_set_profiling", "uegccd_batch_kernel_stats",
+    "uegccd_batch_transfer_bytes",
 ]
 
 _lib = None
@@ -85,11 +86,11 @@ def lib() -> C.CDLL:
         L.uegccd_batch_destroy.argtypes = [vp]
         L.uegccd_batch_solve.argtypes = [vp, P(Options), C.c_int32, dp, P(Result)]
         L.uegccd_batch_get_amplitudes.argtypes = [vp, C.c_int32, dp]
+        L.uegccd_batch_set_profiling.argtypes = [vp, C.c_int32]
+        L.uegccd_batch_kernel_stats.argtypes = [vp, C.c_int32, P(C.c_char_p), dp, P(C.c_int64)]
+        L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
         L.uegccd_last_error.restype = C.c_char_p
         L.uegccd_version.restype = C.c_char_p
-        for f in EXPORTS:
-            if getattr(L, f).restype is C.c_int or f in ("uegccd_ctx_create",):
-                getattr(L, f).restype = C.c_int
         _lib = L
     return _lib
 

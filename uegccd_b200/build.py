@@ -18,7 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libuegccd.so")
 OBJDIR = os.path.join(PKG, "_build")
 
-SOURCES = ["capi.cu", "kernels_fp64.cu", "plan.cpp"]
+SOURCES = ["capi.cu", "kernels_fp64.cu", "plan.cpp", "heg_host.cpp"]
 HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -41,7 +41,7 @@ def _stale(target: str, deps) -> bool:
 def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
     os.makedirs(OBJDIR, exist_ok=True)
     nvcc = _nvcc()
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "uegccd.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", f) for f in ("uegccd.h", "uegccd_host.h")]
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)

@@ -68,18 +68,25 @@ struct UegccdBatch {
     DevBatch d;
     std::vector<void *> allocs;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_solve0 = nullptr, ev_solve1 = nullptr;
     std::vector<double> red;         // host copy: 3 per solve
     std::vector<uint8_t> active;     // host copy
     double *dense[3] = {nullptr, nullptr, nullptr};  // reference-layout scratch of the largest solve
     size_t dense_n = 0;
     int launches = 0;
+    int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the calls so far
+    KernelTimer kt;
+    bool kt_events = false;
 
     ~UegccdBatch()
     {
+        if (kt_events)
+            for (auto &e : kt.ev) cudaEventDestroy(e);
         for (void *p : allocs) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_solve0) cudaEventDestroy(ev_solve0);
+        if (ev_solve1) cudaEventDestroy(ev_solve1);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -99,6 +106,7 @@ struct UegccdBatch {
         int rc = alloc(p, h.size());
         if (rc) return rc;
         if (!h.empty()) CU(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        h2d_bytes += (int64_t)(h.size() * sizeof(T));
         return 0;
     }
 };
@@ -143,6 +151,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&b->ev0));
     CU(cudaEventCreate(&b->ev1));
+    CU(cudaEventCreate(&b->ev_solve0));
+    CU(cudaEventCreate(&b->ev_solve1));
 
     std::vector<SolveDev> solves(n);
     std::vector<BlockDev> blocks;
@@ -277,14 +287,17 @@ int set_active_all(UegccdBatch &b, uint8_t v)
 {
     std::fill(b.active.begin(), b.active.end(), v);
     CU(cudaMemcpyAsync(b.d.active, b.active.data(), b.active.size(), cudaMemcpyHostToDevice, b.stream));
+    b.h2d_bytes += (int64_t)b.active.size();
     return 0;
 }
 
 int read_red(UegccdBatch &b)
 {
     CU(cudaMemcpyAsync(b.red.data(), b.d.red, b.red.size() * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+    b.d2h_bytes += (int64_t)(b.red.size() * sizeof(double));
     CU(cudaStreamSynchronize(b.stream));
     CU(cudaGetLastError());
+    b.kt.collect();
     return 0;
 }
 
@@ -294,6 +307,7 @@ int pack_from_host(UegccdBatch &b, int s, const double *host_dense)
     const SolvePlan &P = b.plans[s];
     size_t n = (size_t)P.O * P.O * P.V;
     CU(cudaMemcpyAsync(b.dense[0], host_dense, n * sizeof(double), cudaMemcpyHostToDevice, b.stream));
+    b.h2d_bytes += (int64_t)(n * sizeof(double));
     launch_pack(b.d, s, (int)P.namp, b.dense[0], b.stream);
     b.launches++;
     CU(cudaGetLastError());
@@ -312,7 +326,10 @@ int unpack_to_host(UegccdBatch &b, int s, const double *t_dev, double *ab, doubl
     b.launches++;
     CU(cudaGetLastError());
     for (int k = 0; k < 3; k++)
-        if (h[k]) CU(cudaMemcpyAsync(h[k], b.dense[k], n * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+        if (h[k]) {
+            CU(cudaMemcpyAsync(h[k], b.dense[k], n * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+            b.d2h_bytes += (int64_t)(n * sizeof(double));
+        }
     CU(cudaStreamSynchronize(b.stream));
     return 0;
 }
@@ -379,7 +396,7 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
     int status = 0;
     while (nactive > 0) {
-        b.launches += launch_residual(d, f, 0, nullptr, b.stream);
+        b.launches += launch_residual(d, f, 0, nullptr, b.stream, &b.kt);
         CU(cudaGetLastError());
         std::swap(d.t, d.t_new);
         if ((rc = read_red(b))) return rc;
@@ -405,7 +422,7 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     }
     // final residual (CCD.f90:103-107, dRPA.f90:98-101)
     if ((rc = set_active_all(b, 1))) return rc;
-    b.launches += launch_residual(d, f, 1, nullptr, b.stream);
+    b.launches += launch_residual(d, f, 1, nullptr, b.stream, &b.kt);
     if ((rc = read_red(b))) return rc;
     for (int s = 0; s < n; s++) rmax[s] = b.red[3 * s + 2];
     std::vector<double> esosex(n, 0.0);
@@ -572,7 +589,10 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
     if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
     int rc = validate_options(opt, drpa);
     if (rc) return rc;
+    CU(cudaEventRecord(b->ev_solve0, b->stream));
+    b->kt.begin(KID_MP2, b->stream);
     launch_mp2(b->d, b->stream);
+    b->kt.end(b->stream);
     launch_reduce(b->d, b->stream);
     if ((rc = read_red(*b))) return rc;
     if (e2)
@@ -582,7 +602,48 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
         launch_to_aaaa(b->d, b->stream);
         std::swap(b->d.t, b->d.t_new);
     }
-    return run_solves(*b, opt, drpa, results);
+    int st = run_solves(*b, opt, drpa, results);
+    if (st < 0) return st;
+    CU(cudaEventRecord(b->ev_solve1, b->stream));
+    CU(cudaEventSynchronize(b->ev_solve1));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, b->ev_solve0, b->ev_solve1));
+    for (int s = 0; s < b->d.nsolves; s++) results[s].gpu_ms = ms;
+    return st;
+}
+
+int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    if (on && !b->kt_events) {
+        for (auto &e : b->kt.ev) CU(cudaEventCreate(&e));
+        b->kt_events = true;
+    }
+    b->kt.on = on != 0;
+    for (int k = 0; k < KID_COUNT; k++) { b->kt.ms[k] = 0.0; b->kt.launches[k] = 0; }
+    return 0;
+}
+
+int32_t uegccd_batch_kernel_stats(UegccdBatch *b, int32_t max, const char **names, double *ms, int64_t *launches)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    int n = 0;
+    for (int k = 0; k < KID_COUNT && n < max; k++) {
+        if (b->kt.launches[k] == 0) continue;
+        if (names) names[n] = kKernelNames[k];
+        if (ms) ms[n] = b->kt.ms[k];
+        if (launches) launches[n] = b->kt.launches[k];
+        n++;
+    }
+    return n;
+}
+
+int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    if (h2d) *h2d = b->h2d_bytes;
+    if (d2h) *d2h = b->d2h_bytes;
+    return 0;
 }
 
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab)

@@ -1,0 +1,401 @@
+// heg_host.cpp -- host side of the drop-in: the Input file reader and the
+// plane-wave set-up that the reference's Fortran host runs before it calls the
+// hot path.  Restates IO.f90 ReadInput/ParseLine (IO.f90:14-391) and, from
+// HEG.f90, init_HEG (16-43), CalcMadelung (89-148), SetupBasis (150-324),
+// FcutToBasisFn (326-342), change_rs (494-533), ChangeTwist (551-578), print_HF
+// (581-615) and FindTol (1073-1086).  Floating-point expressions keep the
+// Fortran evaluation order, so the eigenvalues equal the reference's printout.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/uegccd.h"
+#include "../../include/uegccd_host.h"
+
+namespace {
+
+constexpr double kPi = 3.1415926535897932384626433833;  // Constants.f90:7
+thread_local std::string g_host_error;
+
+int herr(int code, const std::string &m)
+{
+    g_host_error = m;
+    return code;
+}
+
+struct G1Entry {
+    int n[3];
+    int n2;
+    double nt[3];
+    double nt2;
+};
+
+}  // namespace
+
+struct UegccdHeg {
+    UegccdInput in;
+    int nel = 0, nocc = 0, nao = 0, cell = 0, maxkpoint = 0, coren = 0;
+    double exchangefactor = 1.0;
+    double L = 0, rS = 1.0, omega = 0, madelung = 0, density = 0, kf = 0, screening = 0;
+    double ntwist[3] = {0, 0, 0};
+    double ehf = 0, xhf = 0;
+    std::vector<double> kvec;   // NAO x 3 row-major (p, d)
+    std::vector<double> eigen;  // NAO
+    std::vector<int32_t> nvec;  // NAO x 3 column-major (Fortran nVec(NAO,3))
+};
+
+namespace {
+
+int fcut_to_basis_fn(double fcut, int nel)
+{
+    int m = (int)(std::pow(fcut, 3.0 / 2.0) * nel / 2);
+    double target = std::pow(fcut, 3.0 / 2.0) * nel / 2;
+    if (std::fabs(m - target) > std::fabs(m + 1 - target)) m = m + 1;
+    return m;
+}
+
+double calc_madelung(double omega, double L)
+{
+    double kappa = 2.8 / std::pow(omega, 1.0 / 3.0);
+    double term2 = -kPi / (std::pow(kappa, 2.0) * std::pow(L, 3.0));
+    double term4 = -2.0 * kappa / std::sqrt(kPi);
+    const int l4 = 10;  // only the last pass of the l4 loop survives its reset
+    double recip = 0.0;
+    for (int l1 = -l4; l1 <= l4; l1++)
+        for (int l2 = -l4; l2 <= l4; l2++)
+            for (int l3 = -l4; l3 <= l4; l3++) {
+                int n2 = l1 * l1 + l2 * l2 + l3 * l3;
+                if (n2 == 0) continue;
+                double k2 = (1.0 / std::pow(L, 2.0)) * (double)n2;
+                double ek2 = (1.0 / std::pow(L, 3.0)) * (1.0 / (kPi * k2)) *
+                             std::exp(-(std::pow(kPi, 2.0) * k2) / std::pow(kappa, 2.0));
+                recip = recip + ek2;
+            }
+    double real = 0.0;
+    for (int l1 = -l4; l1 <= l4; l1++)
+        for (int l2 = -l4; l2 <= l4; l2++)
+            for (int l3 = -l4; l3 <= l4; l3++) {
+                double modr = L * std::sqrt((double)(l1 * l1 + l2 * l2 + l3 * l3));
+                if (modr != 0.0) real = real + std::erfc(kappa * modr) / modr;
+            }
+    return real + recip + term2 + term4;
+}
+
+void form_eigen(UegccdHeg &h)
+{
+    for (int p = 0; p < h.nao; p++) {
+        const double *k = &h.kvec[3 * p];
+        double e = 0.5 * (k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+        for (int q = 0; q < h.nel / 2; q++) {
+            if (q != p) {
+                const double *kq = &h.kvec[3 * q];
+                double q1 = k[0] - kq[0], q2 = k[1] - kq[1], q3 = k[2] - kq[2];
+                e = e - (1.0 / h.omega) * (4.0 * kPi / (q1 * q1 + q2 * q2 + q3 * q3)) * h.exchangefactor;
+            } else {
+                e = e + h.madelung - h.in.gap;
+            }
+        }
+        h.eigen[p] = e;
+    }
+}
+
+void hf_energy(UegccdHeg &h)
+{
+    double ehf = 0.0, xhf = 0.0;
+    for (int p = 0; p < h.nel / 2; p++) {
+        const double *k = &h.kvec[3 * p];
+        ehf = ehf + 0.5 * (k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+        for (int q = 0; q < h.nel / 2; q++) {
+            if (q == p) continue;
+            const double *kq = &h.kvec[3 * q];
+            double q1 = k[0] - kq[0], q2 = k[1] - kq[1], q3 = k[2] - kq[2];
+            double qq = q1 * q1 + q2 * q2 + q3 * q3;
+            ehf = ehf - 0.5 * (1.0 / h.omega) * (4.0 * kPi / qq);
+            xhf = xhf - 0.5 * (1.0 / h.omega) * (4.0 * kPi / qq);
+        }
+    }
+    ehf = ehf * 2.0;
+    h.xhf = xhf * 2.0;
+    h.ehf = ehf + h.madelung * 0.5 * h.nel;
+}
+
+int setup_basis(UegccdHeg &h)
+{
+    const int cell = h.cell;
+    std::vector<G1Entry> g1;
+    g1.reserve((size_t)(2 * cell + 1) * (2 * cell + 1) * (2 * cell + 1));
+    for (int l1 = -cell; l1 <= cell; l1++)
+        for (int l2 = -cell; l2 <= cell; l2++)
+            for (int l3 = -cell; l3 <= cell; l3++) {
+                G1Entry g;
+                g.n[0] = l1; g.n[1] = l2; g.n[2] = l3;
+                g.n2 = l1 * l1 + l2 * l2 + l3 * l3;
+                g.nt[0] = l1 + h.ntwist[0];
+                g.nt[1] = l2 + h.ntwist[1];
+                g.nt[2] = l3 + h.ntwist[2];
+                g.nt2 = g.nt[0] * g.nt[0] + g.nt[1] * g.nt[1] + g.nt[2] * g.nt[2];
+                if (g.n2 <= h.maxkpoint) g1.push_back(g);
+            }
+    int nbasis = (int)g1.size();
+    // stable ascending sort by twisted |n+k|^2 (the reference's bubble sort)
+    for (;;) {
+        bool swapped = false;
+        for (int l1 = 1; l1 < nbasis; l1++)
+            if (g1[l1].nt2 < g1[l1 - 1].nt2) {
+                std::swap(g1[l1], g1[l1 - 1]);
+                swapped = true;
+            }
+        if (!swapped) break;
+    }
+    int mfcut = (int)(std::pow(h.in.fcut, 3.0 / 2.0) * h.nel / 2);
+    double mtarget = std::pow(h.in.fcut, 3.0 / 2.0) * h.nel / 2;
+    if (std::fabs(mfcut - mtarget) > std::fabs(mfcut + 1 - mtarget)) mfcut = mfcut + 1;
+    if (mfcut < nbasis) nbasis = mfcut;
+    int mcore = fcut_to_basis_fn(h.in.corefcut, h.nel);
+    if ((h.in.corefcut - 1.0) < 1e-6 && mcore != h.nel / 2)
+        return herr(UEGCCD_ERR_ARG, "ERROR in setup_basis: corefcut is less than 1 rather than equal to 1");
+    nbasis = nbasis - mcore + h.nel / 2;
+    if (nbasis <= h.nel / 2) return herr(UEGCCD_ERR_ARG, "basis has no virtual orbitals");
+    h.nao = nbasis;
+    h.kvec.assign((size_t)nbasis * 3, 0.0);
+    h.eigen.assign(nbasis, 0.0);
+    h.nvec.assign((size_t)nbasis * 3, 0);
+    for (int p = 0; p < nbasis; p++) {
+        int off = (p + 1 > h.nel / 2) ? mcore - h.nel / 2 : 0;
+        const G1Entry &g = g1[p + off];
+        for (int d = 0; d < 3; d++) {
+            h.kvec[3 * p + d] = g.nt[d] * (2.0 * kPi / h.L);
+            h.nvec[p + (size_t)nbasis * d] = g.n[d];
+        }
+    }
+    form_eigen(h);
+    hf_energy(h);
+    return 0;
+}
+
+bool parse_bool(const std::string &v)
+{
+    std::string s;
+    for (char c : v)
+        if (!isspace((unsigned char)c)) s += (char)toupper((unsigned char)c);
+    if (!s.empty() && s[0] == '.') s = s.substr(1);
+    return !s.empty() && s[0] == 'T';
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *uegccd_host_last_error(void) { return g_host_error.c_str(); }
+
+void uegccd_default_input(UegccdInput *in)
+{
+    std::memset(in, 0, sizeof(*in));
+    in->nelectron = 14;
+    in->maxkpoint = 2;
+    in->rsmin = in->rsmax = 1.0;
+    in->num_rs_points = 1;
+    in->do_ring = in->do_xring = in->do_ladder = in->do_mosaic = 1;
+    in->madelung_factor = 1.0;
+    in->fcut = 10.0;
+    in->corefcut = 1.0;
+    in->gapii = -0.01;
+    in->do_single_calc = 1;
+    in->do_skip_ta = 1;
+}
+
+// ReadInput (IO.f90:14-348): "Key: Value" lines, '!' comments; every key of the
+// reference's list must be set exactly once (IO.f90:329-335); unknown keys stop.
+int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
+{
+    static const char *kNames[] = {
+        "# Electrons", "Momentum Cutoff", "rSMin", "rSMax", "# rS Points", "Safe ERI", "Do Rings", "Do XRings",
+        "Do Ladders", "Do Mosaics", "Rings Range", "XRings Range", "Ladders Range", "Mosaics Range",
+        "DriverDir Range", "DriverEx Range", "Energy Range", "LinRings Range", "QuadRings Range", "DRings Range",
+        "ExRings Range", "LinLadd Range", "QuadLadd Range", "DLadders Range", "ExLadders Range", "CoreFactor",
+        "TACalcN", "DoCalcTACCD", "DodRPASOSEX", "DoTruncCoulombHF", "DoTruncCoulombAll", "DoKS", "MadelungFactor",
+        "DoSingleCalc", "Gap", "fcut", "corefcut", "fcut2ecut", "GapII", "DoSFCalcMP2", "DoSFCalcCCD", "DoSkipTA",
+        "DoOnlyMP2Grid", "EndInput"};
+    const int nparams = (int)(sizeof(kNames) / sizeof(kNames[0]));
+    if (!in || !path) return herr(UEGCCD_ERR_ARG, "null argument");
+    uegccd_default_input(in);
+    std::ifstream f(path);
+    if (!f) return herr(UEGCCD_ERR_ARG, "No Input file");
+    std::map<std::string, int> count;
+    std::string line;
+    int lineno = 0;
+    int fcut2ecut = 0;
+    while (std::getline(f, line)) {
+        lineno++;
+        size_t c = line.find('!');
+        if (c != std::string::npos) line = line.substr(0, c);
+        for (char &ch : line)
+            if ((unsigned char)ch <= 31) ch = ' ';
+        if (line.find_first_not_of(' ') == std::string::npos) continue;
+        size_t colon = line.find(':');
+        std::string key = colon == std::string::npos ? line : line.substr(0, colon);
+        std::string val = colon == std::string::npos ? "" : line.substr(colon + 1);
+        size_t a = key.find_first_not_of(' '), b = key.find_last_not_of(' ');
+        key = (a == std::string::npos) ? "" : key.substr(a, b - a + 1);
+        std::istringstream vs(val);
+        count[key]++;
+        if (key == "# Electrons") {
+            vs >> in->nelectron;
+            if (in->nelectron < 0) return herr(UEGCCD_ERR_ARG, "Must have positive number of electrons");
+            if (in->nelectron % 2 == 1) return herr(UEGCCD_ERR_ARG, "Must have closed shell");
+        } else if (key == "Momentum Cutoff") vs >> in->maxkpoint;
+        else if (key == "rSMin") vs >> in->rsmin;
+        else if (key == "rSMax") vs >> in->rsmax;
+        else if (key == "# rS Points") {
+            vs >> in->num_rs_points;
+            if (in->num_rs_points > 1) return herr(UEGCCD_ERR_ARG, "Cannot have more than one rs point");
+        } else if (key == "Safe ERI") in->safe_eri = parse_bool(val);
+        else if (key == "Do Rings") in->do_ring = parse_bool(val);
+        else if (key == "Do XRings") in->do_xring = parse_bool(val);
+        else if (key == "Do Ladders") in->do_ladder = parse_bool(val);
+        else if (key == "Do Mosaics") in->do_mosaic = parse_bool(val);
+        else if (key.size() > 6 && key.compare(key.size() - 5, 5, "Range") == 0) {
+            int r = 0;
+            vs >> r;
+            in->range_flags += std::abs(r);
+        } else if (key == "NTwist") vs >> in->ntwist[0] >> in->ntwist[1] >> in->ntwist[2];
+        else if (key == "CoreFactor") vs >> in->core_factor;
+        else if (key == "TACalcN") vs >> in->tacalcn;
+        else if (key == "DoCalcTACCD") in->do_calc_ta_ccd = parse_bool(val);
+        else if (key == "DodRPASOSEX") in->do_drpa_sosex = parse_bool(val);
+        else if (key == "DoTruncCoulombHF") {
+            if (parse_bool(val)) return herr(UEGCCD_ERR_ARG, "Not Implemented");
+        } else if (key == "DoTruncCoulombAll") {
+            if (parse_bool(val)) return herr(UEGCCD_ERR_ARG, "Not Implemented");
+        } else if (key == "DoKS") in->do_ks = parse_bool(val);
+        else if (key == "MadelungFactor") vs >> in->madelung_factor;
+        else if (key == "DoSingleCalc") in->do_single_calc = parse_bool(val);
+        else if (key == "DoSFCalcMP2" || key == "DoSFCalcCCD" || key == "DoOnlyMP2Grid") {
+            if (parse_bool(val)) in->diagnostics_requested = 1;
+        } else if (key == "DoSkipTA") in->do_skip_ta = parse_bool(val);
+        else if (key == "Gap") vs >> in->gap;
+        else if (key == "fcut") vs >> in->fcut;
+        else if (key == "corefcut") vs >> in->corefcut;
+        else if (key == "fcut2ecut") fcut2ecut = parse_bool(val);
+        else if (key == "GapII") vs >> in->gapii;
+        else if (key == "EndInput") {
+            if (!parse_bool(val)) return herr(UEGCCD_ERR_ARG, "EndInput must be T");
+        } else {
+            return herr(UEGCCD_ERR_ARG, "Error: Line number " + std::to_string(lineno) + " of Input not recognized");
+        }
+    }
+    in->fcut2ecut = fcut2ecut;
+    if (require_all) {
+        for (int k = 2; k < nparams; k++)
+            if (count[kNames[k]] == 0) return herr(UEGCCD_ERR_ARG, std::string("Error: Parameter ") + kNames[k] + " not set.");
+        for (auto &kv : count)
+            if (kv.second > 1) return herr(UEGCCD_ERR_ARG, "Error: Parameter " + kv.first + " multiply set.");
+    }
+    return 0;
+}
+
+int uegccd_heg_create(const UegccdInput *in, UegccdHeg **out)
+{
+    if (!in || !out) return herr(UEGCCD_ERR_ARG, "null argument");
+    *out = nullptr;
+    auto *h = new UegccdHeg;
+    h->in = *in;
+    h->nel = in->nelectron;
+    h->nocc = in->nelectron / 2;
+    h->maxkpoint = in->maxkpoint;
+    h->coren = (int)(in->nelectron / 2 * in->core_factor);
+    h->exchangefactor = in->do_ks ? 0.0 : 1.0;
+    if (in->fcut2ecut) {  // IO.f90:291-300
+        double nfermi = std::pow((double)in->nelectron, 2.0 / 3.0) / 4.0;
+        double mult = in->fcut < 2.0 ? 2.0 : in->fcut;
+        h->maxkpoint = (int)(nfermi * mult * 2.0);
+        if (nfermi < 10) h->maxkpoint = (int)(10 * mult * 2.0);
+    }
+    for (int d = 0; d < 3; d++) h->ntwist[d] = in->ntwist[d];
+    // init_HEG at rS = 1
+    h->rS = 1.0;
+    h->L = h->rS * std::pow(4.0 / 3.0 * kPi * h->nel, 1.0 / 3.0);
+    h->omega = h->L * h->L * h->L;
+    h->madelung = calc_madelung(h->omega, h->L) * in->madelung_factor;
+    h->cell = (int)std::sqrt((double)h->maxkpoint) + 3;
+    int rc = setup_basis(*h);
+    if (rc) { delete h; return rc; }
+    // change_rs to rSMin (Main.f90:78-79)
+    double rescale = in->rsmin / h->rS;
+    h->L = h->L * rescale;
+    h->omega = h->omega * std::pow(rescale, 3.0);
+    for (double &k : h->kvec) k = k * (1.0 / rescale);
+    h->madelung = calc_madelung(h->omega, h->L) * in->madelung_factor;
+    form_eigen(*h);
+    hf_energy(*h);
+    *out = h;
+    return 0;
+}
+
+void uegccd_heg_destroy(UegccdHeg *h) { delete h; }
+
+int uegccd_heg_change_twist(UegccdHeg *h, const double twist[3])
+{
+    if (!h || !twist) return herr(UEGCCD_ERR_ARG, "null argument");
+    int nao = h->nao;
+    for (int d = 0; d < 3; d++) h->ntwist[d] = twist[d];
+    int rc = setup_basis(*h);
+    if (rc) return rc;
+    if (h->nao != nao) return herr(UEGCCD_ERR_ARG, "basis size changed with the twist");
+    return 0;
+}
+
+int uegccd_heg_set_eigen(UegccdHeg *h, const double *eigen)
+{
+    if (!h || !eigen) return herr(UEGCCD_ERR_ARG, "null argument");
+    h->eigen.assign(eigen, eigen + h->nao);
+    return 0;
+}
+
+int uegccd_heg_system(const UegccdHeg *h, UegccdSystem *sys)
+{
+    if (!h || !sys) return herr(UEGCCD_ERR_ARG, "null argument");
+    sys->nocc = h->nocc;
+    sys->nao = h->nao;
+    sys->L = h->L;
+    sys->madelung = h->madelung;
+    sys->eigen = h->eigen.data();
+    sys->nvec = h->nvec.data();
+    return 0;
+}
+
+int uegccd_heg_info(const UegccdHeg *h, UegccdHegInfo *info)
+{
+    if (!h || !info) return herr(UEGCCD_ERR_ARG, "null argument");
+    info->nocc = h->nocc;
+    info->nao = h->nao;
+    info->maxkpoint = h->maxkpoint;
+    info->cell = h->cell;
+    info->core_n = h->coren;
+    info->L = h->L;
+    info->omega = h->omega;
+    info->madelung = h->madelung;
+    info->ehf = h->ehf;
+    for (int d = 0; d < 3; d++) info->twist[d] = h->ntwist[d];
+    return 0;
+}
+
+// FindTol (HEG.f90:1073-1086), fed HEGData%rS as the reference does (always 1).
+void uegccd_find_tol(double rs, double *tolmax, double *failratio, double *denomfactor)
+{
+    *tolmax = 1.0e-8;
+    *failratio = 100;
+    if (rs > 5.1) *tolmax = 1.0e-6;
+    if (rs > 5.1) *denomfactor = 5.0;
+    if (rs > 9.9) *tolmax = 1.0e-5;
+    if (rs > 80.0) *tolmax = 1.0e-3;
+    if (rs < 0.95) *failratio = 1e6;
+}
+
+}  // extern "C"

@@ -36,6 +36,42 @@ struct DevBatch {
     uint8_t *active = nullptr;       // per solve
 };
 
+// Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
+enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
+                KID_UPDATE, KID_REDUCE, KID_PACK, KID_COUNT };
+struct KernelTimer {
+    bool on = false;
+    cudaEvent_t ev[2 * 64];
+    int kid[64];
+    int n = 0;
+    double ms[KID_COUNT] = {};
+    long long launches[KID_COUNT] = {};
+    void begin(int id, cudaStream_t st)
+    {
+        if (!on || n >= 64) return;
+        kid[n] = id;
+        cudaEventRecord(ev[2 * n], st);
+    }
+    void end(cudaStream_t st)
+    {
+        if (!on || n >= 64) return;
+        cudaEventRecord(ev[2 * n + 1], st);
+        n++;
+    }
+    // call after the stream is synchronised
+    void collect()
+    {
+        for (int k = 0; k < n; k++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]);
+            ms[kid[k]] += t;
+            launches[kid[k]]++;
+        }
+        n = 0;
+    }
+};
+extern const char *kKernelNames[KID_COUNT];
+
 struct TermFlags {
     int do_driver = 1, do_mosaic = 1, do_ladder = 1, do_pp = 1, do_hh = 1, do_ring = 1, do_xring = 1;
     int drpa = 0;
@@ -47,7 +83,8 @@ void launch_energy(const DevBatch &d, int kind, double csosex, cudaStream_t st);
 // d.t_new = T2aaaa of d.t (t(ij,a) - t(ij,b))
 void launch_to_aaaa(const DevBatch &d, cudaStream_t st);
 // Residual of the selected terms for d.t; mode 0 also updates into d.t_new.  Returns launches.
-int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st);
+int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
+                    KernelTimer *kt = nullptr);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
 void launch_unpack(const DevBatch &d, int s, int namp, const double *t, double *ab, double *ba, double *aa,
                    cudaStream_t st);

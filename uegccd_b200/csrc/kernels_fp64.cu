@@ -656,29 +656,45 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
     k_to_aaaa<<<(unsigned)((d.namp + 255) / 256), 256, 0, st>>>(d.namp, d.partner, d.t, d.t_new);
 }
 
-int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st)
+const char *kKernelNames[KID_COUNT] = {"k_mp2", "k_energy", "k_hh_w", "k_ladder", "k_mosaic_s",
+                                      "k_mosaic_reduce", "k_ring_int", "k_update", "k_reduce_solves", "k_pack"};
+
+int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
+                    KernelTimer *kt)
 {
+    KernelTimer dummy;
+    if (!kt) kt = &dummy;
     int n = 0;
     if (f.do_ladder && d.nblocks > 0) {
         if (f.do_hh) {
             size_t smem = (size_t)(2 * d.max_o * kHhC) * sizeof(double) + (size_t)d.max_o * sizeof(int4);
+            kt->begin(KID_HH_W, st);
             k_hh_w<<<d.nblocks, 256, smem, st>>>(d.blocks, d.solves, d.pair_i, d.vir, d.nv4, d.vtab, d.t, d.hh0,
                                                  d.hh, d.active);
+            kt->end(st);
             n++;
         }
+        kt->begin(KID_LADDER, st);
         k_ladder<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.nv4, d.vtab, d.t, d.hh0, d.hh,
                                            f.do_pp, f.do_hh, d.g, d.active);
+        kt->end(st);
         n++;
     }
     if (f.do_mosaic) {
+        kt->begin(KID_MOSAIC_S, st);
         k_mosaic_s<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.amps, d.partner, d.nv4, d.vtab, d.t, f.drpa,
                                                  d.S, d.active);
+        kt->end(st);
+        kt->begin(KID_MOSAIC_RED, st);
         k_mosaic_reduce<<<d.ntargets, 256, 0, st>>>(d.targets, d.solves, d.pos, d.S, d.jvv, d.joo, d.active);
+        kt->end(st);
         n += 2;
     }
     if (f.do_ring || f.do_xring) {
+        kt->begin(KID_RING_INT, st);
         k_ring_int<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.amps, d.partner, d.pos, d.nv4, d.vtab, d.t,
                                                   f.drpa, d.J1, d.J2, d.J3, d.active);
+        kt->end(st);
         n++;
     }
     UpdateArgs A;
@@ -688,9 +704,13 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
+    kt->begin(KID_UPDATE, st);
     k_update<<<d.nchunks, kChunk, 0, st>>>(A);
+    kt->end(st);
     n++;
+    kt->begin(KID_REDUCE, st);
     k_reduce_solves<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, d.part_e, d.part_dt, d.part_r, d.red);
+    kt->end(st);
     n++;
     return n;
 }

@@ -114,6 +114,23 @@ class Batch:
         rc = capi.check(capi.lib().uegccd_batch_solve(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2), res))
         return rc, e2, [r.as_dict() for r in res]
 
+    def set_profiling(self, on: bool) -> None:
+        capi.check(capi.lib().uegccd_batch_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_stats(self) -> dict:
+        n = 16
+        names = (C.c_char_p * n)()
+        ms = np.zeros(n)
+        la = np.zeros(n, dtype=np.int64)
+        k = capi.lib().uegccd_batch_kernel_stats(self._h, n, names, capi.dptr(ms),
+                                                   la.ctypes.data_as(C.POINTER(C.c_int64)))
+        return {names[i].decode(): (float(ms[i]), int(la[i])) for i in range(k)}
+
+    def transfer_bytes(self):
+        h, d = C.c_int64(), C.c_int64()
+        capi.check(capi.lib().uegccd_batch_transfer_bytes(self._h, C.byref(h), C.byref(d)))
+        return h.value, d.value
+
     def amplitudes(self, s: int) -> np.ndarray:
         t = np.zeros(self._shapes[s])
         capi.check(capi.lib().uegccd_batch_get_amplitudes(self._h, s, capi.dptr(t)))
