@@ -89,6 +89,8 @@ def lib():
         L.uo_drpa.restype = C.c_int
         L.uo_drpa.argtypes = [C.c_void_p, dp, C.c_int, P(UoSolveStats), dp, dp, C.c_int]
         L.uo_ccd_g2.argtypes = [C.c_void_p, dp, dp, C.c_int, dp, dp]
+        L.uo_set_tol_override.argtypes = [C.c_double]
+        L.uo_set_tol_override.restype = None
         L.uo_drpa_g2.argtypes = [C.c_void_p, dp, C.c_int, dp]
         L.uo_ccd_energy.restype = C.c_double
         L.uo_ccd_energy.argtypes = [C.c_void_p, dp, dp, dp]
@@ -243,12 +245,15 @@ class Oracle:
         e = self.L.uo_mp2(self.h, _ptr(ta), _ptr(tb), _ptr(tc), _ptr(conn, C.c_int))
         return e, ta, tb, tc, conn
 
-    def ccd(self, t_aaaa, t_abab, t_abba, max_iter: int = 0, max_rec: int = 1100):
+    def ccd(self, t_aaaa, t_abab, t_abba, max_iter: int = 0, max_rec: int = 1100, tol: float = 0.0):
+        """DrvCCD; tol > 0 replaces TolMax (tight-mode parity only)."""
         st = UoSolveStats()
+        self.L.uo_set_tol_override(tol)
         en = np.zeros(max_rec)
         dts = np.zeros(max_rec)
         rc = self.L.uo_ccd(self.h, _ptr(t_aaaa), _ptr(t_abab), _ptr(t_abba), max_iter, C.byref(st),
                            _ptr(en), _ptr(dts), max_rec)
+        self.L.uo_set_tol_override(0.0)
         if rc != 0:
             raise RuntimeError(self.L.uo_last_error().decode())
         return st, en[: st.n_recorded].copy(), dts[: st.n_recorded].copy()

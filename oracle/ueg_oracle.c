@@ -1006,6 +1006,10 @@ static double cnvrg_channel(const double *t2, double *old, size_t n, int ndiis)
 }
 
 /* DrvCCD (CCD.f90:18-183) */
+static double g_tol_override = 0.0;
+/* Test hook: a TolMax below the reference's (tight-mode parity); <= 0 restores FindTol. */
+void uo_set_tol_override(double tol) { g_tol_override = tol; }
+
 int uo_ccd(UoCtx *c, double *t_aaaa, double *t_abab, double *t_abba, int max_iter_override, UoSolveStats *st,
            double *energies, double *dts, int max_rec)
 {
@@ -1014,6 +1018,7 @@ int uo_ccd(UoCtx *c, double *t_aaaa, double *t_abab, double *t_abba, int max_ite
     size_t n = (size_t)O * O * (M - O);
     double tolmax = 1.0e-8, failratio = 100;
     find_tol(c->heg.rS, &tolmax, &failratio, &c->denom_factor_ccd);
+    if (g_tol_override > 0.0) tolmax = g_tol_override;
     const int max_iter = max_iter_override > 0 ? max_iter_override : 1000;
     double *g_abab = (double *)calloc(n, sizeof(double));
     double *g_abba = (double *)calloc(n, sizeof(double));

@@ -88,6 +88,8 @@ double uo_mp2(UoCtx *c, double *t_aaaa, double *t_abab, double *t_abba, int *con
 /* DrvCCD (CCD.f90:18-183).  energies/dts (may be NULL) get one entry per printed line. */
 int    uo_ccd(UoCtx *c, double *t_aaaa, double *t_abab, double *t_abba,
               int max_iter_override, UoSolveStats *st, double *energies, double *dts, int max_rec);
+/* Test hook: TolMax for uo_ccd below the reference's 1e-8 (tight-mode parity); <= 0 restores it. */
+void   uo_set_tol_override(double tol);
 /* DrvdRPA (dRPA.f90:23-174) on one amplitude array. */
 int    uo_drpa(UoCtx *c, double *t2, int max_iter_override, UoSolveStats *st,
                double *energies, double *dts, int max_rec);

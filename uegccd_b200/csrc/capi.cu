@@ -77,6 +77,9 @@ struct UegccdBatch {
     int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the calls so far
     KernelTimer kt;
     bool kt_events = false;
+    // Pulay DIIS history (allocated on first use)
+    int diis_cap = 0;
+    double *hist_t = nullptr, *hist_e = nullptr, *diis_part = nullptr, *diis_brow = nullptr, *diis_coef = nullptr;
 
     ~UegccdBatch()
     {
@@ -156,7 +159,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
 
     std::vector<SolveDev> solves(n);
     std::vector<BlockDev> blocks;
-    std::vector<LadderTile> tiles;
+    std::vector<LadderTile> tiles, htiles;
     std::vector<ChunkDev> chunks, rchunks;
     std::vector<int> chunk_begin(n + 1, 0);
     std::vector<int2> targets;
@@ -166,8 +169,12 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int4> nv4;
     std::vector<double> eigen, vtab;
     std::vector<int64_t> hh0;
-    int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0;
-    int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0;
+    std::vector<ChunkDev> phchunks;
+    std::vector<RingTile> rtiles;
+    std::vector<int16_t> ph_i, ph_x;
+    std::vector<int32_t> phrow_of;
+    int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0;
+    int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_occ = 0;
     for (int s = 0; s < n; s++) {
         const SolvePlan &P = b->plans[s];
         const SystemHost &H = b->sys[s];
@@ -186,6 +193,19 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         S.jvv0 = jvv0;
         S.joo0 = joo0;
         S.denom_factor = 2.0;
+        S.phr0 = phr0;
+        max_occ = std::max(max_occ, P.O);
+        ph_i.insert(ph_i.end(), P.ph_i.begin(), P.ph_i.end());
+        ph_x.insert(ph_x.end(), P.ph_x.begin(), P.ph_x.end());
+        phrow_of.insert(phrow_of.end(), P.phrow_of.begin(), P.phrow_of.end());
+        for (int r = 0; r < P.O * P.V; r += kPhRows) phchunks.push_back(ChunkDev{s, r});
+        for (const auto &G : P.groups) {
+            if (G.partner < 0) continue;
+            const auto &H2 = P.groups[G.partner];
+            for (int a0 = 0; a0 < G.n; a0 += 16)
+                for (int b0 = 0; b0 < H2.n; b0 += 16)
+                    rtiles.push_back(RingTile{s, G.r0 + a0, std::min(16, G.n - a0), H2.r0 + b0, std::min(16, H2.n - b0)});
+        }
         for (const auto &B : P.blocks) {
             BlockDev bd;
             bd.solve = s; bd.o = B.o; bd.v = B.v;
@@ -197,8 +217,12 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             hh0.push_back(hhoff);
             hhoff += (int64_t)B.o * B.o;
             max_o = std::max(max_o, B.o);
-            for (int a0 = 0; a0 < B.v; a0 += 64)
-                for (int p0 = 0; p0 < B.o; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, 0});
+            // row tile NP follows o_K (8, 16, 32); columns in tiles of 128 (4 warps x 32)
+            const int np = B.o <= 8 ? 8 : B.o <= 16 ? 16 : 32;
+            for (int a0 = 0; a0 < B.v; a0 += 128)
+                for (int p0 = 0; p0 < B.o; p0 += np) tiles.push_back(LadderTile{bi, a0, p0, np});
+            for (int q0 = 0; q0 < B.o; q0 += 128)
+                for (int p0 = 0; p0 < B.o; p0 += np) htiles.push_back(LadderTile{bi, q0, p0, np});
         }
         pair_i.insert(pair_i.end(), P.pair_i.begin(), P.pair_i.end());
         pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
@@ -223,6 +247,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         vtab0 += P.q2max + 1;
         jvv0 += P.V;
         joo0 += P.O;
+        phr0 += (int64_t)P.O * P.V;
         if (amp0 >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit packed indices");
     }
     chunk_begin[n] = (int)chunks.size();
@@ -231,14 +256,19 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.nsolves = n;
     d.nblocks = (int)blocks.size();
     d.ntiles = (int)tiles.size();
+    d.nhtiles = (int)htiles.size();
     d.nchunks = (int)chunks.size();
     d.nrchunks = (int)rchunks.size();
     d.ntargets = (int)targets.size();
     d.max_o = max_o;
+    d.max_occ = max_occ;
     d.namp = amp0;
+    d.nphchunks = (int)phchunks.size();
+    d.nrtiles = (int)rtiles.size();
     if ((rc = b->upload(d.solves, solves))) return rc;
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;
+    if ((rc = b->upload(d.htiles, htiles))) return rc;
     if ((rc = b->upload(d.chunks, chunks))) return rc;
     if ((rc = b->upload(d.rchunks, rchunks))) return rc;
     if ((rc = b->upload(d.chunk_begin, chunk_begin))) return rc;
@@ -253,6 +283,19 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.eigen, eigen))) return rc;
     if ((rc = b->upload(d.vtab, vtab))) return rc;
     if ((rc = b->upload(d.hh0, hh0))) return rc;
+    if ((rc = b->upload(d.phchunks, phchunks))) return rc;
+    if ((rc = b->upload(d.rtiles, rtiles))) return rc;
+    if ((rc = b->upload(d.ph_i, ph_i))) return rc;
+    if ((rc = b->upload(d.ph_x, ph_x))) return rc;
+    if ((rc = b->upload(d.phrow_of, phrow_of))) return rc;
+    if ((rc = b->alloc(d.X, ph0))) return rc;
+    if ((rc = b->alloc(d.Y, ph0))) return rc;
+    if ((rc = b->alloc(d.Ex, ph0))) return rc;
+    if ((rc = b->alloc(d.Ey, ph0))) return rc;
+    if ((rc = b->alloc(d.Sx, phr0))) return rc;
+    if ((rc = b->alloc(d.Sy, phr0))) return rc;
+    if ((rc = b->alloc(d.g_rq, amp0))) return rc;
+    if ((rc = b->alloc(d.g_xq, amp0))) return rc;
     if ((rc = b->alloc(d.t, amp0))) return rc;
     if ((rc = b->alloc(d.t_new, amp0))) return rc;
     if ((rc = b->alloc(d.g, amp0))) return rc;
@@ -344,9 +387,67 @@ int validate_options(const UegccdOptions *o, int drpa)
         return fail(UEGCCD_ERR_UNSUPPORTED,
                     "Do Rings and Do XRings must agree: alone, either breaks the spin symmetry the GPU path uses");
     if (o->max_iter <= 0 || !(o->tol > 0) || !(o->denom_factor != 0)) return fail(UEGCCD_ERR_ARG, "bad iteration options");
-    if (o->scheme != UEGCCD_REPLAY) return fail(UEGCCD_ERR_UNSUPPORTED, "only the replay iteration is built");
+    if (o->scheme != UEGCCD_REPLAY && o->scheme != UEGCCD_DIIS) return fail(UEGCCD_ERR_ARG, "unknown scheme");
+    if (o->scheme == UEGCCD_DIIS && (o->ndiis < 2 || o->ndiis > kDiisMax))
+        return fail(UEGCCD_ERR_ARG, "ndiis must be in [2, 16]");
     if (o->precision != UEGCCD_FP64) return fail(UEGCCD_ERR_UNSUPPORTED, "only FP64 is built");
     return 0;
+}
+
+int diis_alloc(UegccdBatch &b, int ndiis)
+{
+    if (b.diis_cap >= ndiis) return 0;
+    int rc;
+    if ((rc = b.alloc(b.hist_t, (size_t)ndiis * b.d.namp))) return rc;
+    if ((rc = b.alloc(b.hist_e, (size_t)ndiis * b.d.namp))) return rc;
+    if ((rc = b.alloc(b.diis_part, (size_t)b.d.nchunks * kDiisMax))) return rc;
+    if ((rc = b.alloc(b.diis_brow, (size_t)b.d.nsolves * kDiisMax))) return rc;
+    if ((rc = b.alloc(b.diis_coef, (size_t)b.d.nsolves * kDiisMax))) return rc;
+    b.diis_cap = ndiis;
+    return 0;
+}
+
+// Pulay coefficients: minimise |sum c_j e_j|^2 subject to sum c_j = 1, i.e.
+// [B 1; 1 0] [c; lambda] = [0; 1] with B_jk = e_j . e_k (scaled by max diag).
+// Returns false when the system is numerically singular.
+bool pulay_solve(const std::vector<double> &Bfull, int nvec, double *c)
+{
+    const int n = nvec + 1;
+    double scale = 0.0;
+    for (int j = 0; j < nvec; j++) scale = std::max(scale, Bfull[j * kDiisMax + j]);
+    if (!(scale > 0.0) || !std::isfinite(scale)) return false;
+    std::vector<double> A((size_t)n * n, 0.0), r(n, 0.0);
+    for (int j = 0; j < nvec; j++) {
+        for (int k = 0; k < nvec; k++) A[j * n + k] = Bfull[j * kDiisMax + k] / scale;
+        A[j * n + nvec] = 1.0;
+        A[nvec * n + j] = 1.0;
+    }
+    r[nvec] = 1.0;
+    for (int k = 0; k < n; k++) {
+        int piv = k;
+        for (int i = k + 1; i < n; i++)
+            if (std::fabs(A[i * n + k]) > std::fabs(A[piv * n + k])) piv = i;
+        if (std::fabs(A[piv * n + k]) < 1e-14) return false;
+        if (piv != k) {
+            for (int j = 0; j < n; j++) std::swap(A[k * n + j], A[piv * n + j]);
+            std::swap(r[k], r[piv]);
+        }
+        for (int i = k + 1; i < n; i++) {
+            double f = A[i * n + k] / A[k * n + k];
+            for (int j = k; j < n; j++) A[i * n + j] -= f * A[k * n + j];
+            r[i] -= f * r[k];
+        }
+    }
+    for (int k = n - 1; k >= 0; k--) {
+        double x = r[k];
+        for (int j = k + 1; j < n; j++) x -= A[k * n + j] * r[j];
+        r[k] = x / A[k * n + k];
+    }
+    for (int j = 0; j < nvec; j++) {
+        if (!std::isfinite(r[j])) return false;
+        c[j] = r[j];
+    }
+    return true;
 }
 
 // Runs the iteration for all solves of the batch from the amplitudes in d.t.
@@ -395,11 +496,33 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     }
     CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
     int status = 0;
+    const bool diis = opt->scheme == UEGCCD_DIIS;
+    const int ndiis = diis ? opt->ndiis : 0;
+    std::vector<double> Bm, brow, coef;
+    if (diis) {
+        if ((rc = diis_alloc(b, ndiis))) return rc;
+        Bm.assign((size_t)n * kDiisMax * kDiisMax, 0.0);
+        brow.assign((size_t)n * kDiisMax, 0.0);
+        coef.assign((size_t)n * kDiisMax, 0.0);
+    }
+    int it = 0;
     while (nactive > 0) {
         b.launches += launch_residual(d, f, 0, nullptr, b.stream, &b.kt);
         CU(cudaGetLastError());
-        std::swap(d.t, d.t_new);
+        int slot = 0, nvec = 0;
+        if (diis) {
+            slot = it % ndiis;
+            nvec = std::min(it + 1, ndiis);
+            launch_diis_push(d, slot, nvec, b.hist_t, b.hist_e, b.diis_part, b.diis_brow, b.stream);
+            b.launches += 2;
+            CU(cudaMemcpyAsync(brow.data(), b.diis_brow, brow.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               b.stream));
+            b.d2h_bytes += (int64_t)(brow.size() * sizeof(double));
+        } else {
+            std::swap(d.t, d.t_new);
+        }
         if ((rc = read_red(b))) return rc;
+        std::vector<uint8_t> next = b.active;
         nactive = 0;
         for (int s = 0; s < n; s++) {
             if (!b.active[s]) continue;
@@ -407,18 +530,37 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
             e[s] = b.red[3 * s];
             dt[s] = b.red[3 * s + 1];
             if (s == 0) record(e[s], dt[s]);
+            bool go = true;
             if (!std::isfinite(e[s]) || !std::isfinite(dt[s])) {
-                b.active[s] = 0;
+                go = false;
                 status = UEGCCD_ERR_NUMERIC;
-                continue;
+            } else if (!(dt[s] >= opt->tol && niter[s] < opt->max_iter)) {
+                go = false;
             }
-            if (dt[s] >= opt->tol && niter[s] < opt->max_iter) {
-                nactive++;
-            } else {
-                b.active[s] = 0;
+            if (diis) {
+                double *B = &Bm[(size_t)s * kDiisMax * kDiisMax];
+                for (int j = 0; j < nvec; j++) B[slot * kDiisMax + j] = B[j * kDiisMax + slot] = brow[s * kDiisMax + j];
+                double *c = &coef[(size_t)s * kDiisMax];
+                for (int j = 0; j < kDiisMax; j++) c[j] = 0.0;
+                // converged, failed or first step: keep the plain step t = t'
+                if (!go || nvec < 2 || !pulay_solve(std::vector<double>(B, B + kDiisMax * kDiisMax), nvec, c)) {
+                    for (int j = 0; j < kDiisMax; j++) c[j] = 0.0;
+                    c[slot] = 1.0;
+                }
             }
+            if (go) nactive++;
+            else next[s] = 0;
         }
+        if (diis) {
+            CU(cudaMemcpyAsync(b.diis_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               b.stream));
+            b.h2d_bytes += (int64_t)(coef.size() * sizeof(double));
+            launch_diis_extrap(d, b.hist_t, b.diis_coef, nvec, b.stream);
+            b.launches++;
+        }
+        b.active = next;
         CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
+        it++;
     }
     // final residual (CCD.f90:103-107, dRPA.f90:98-101)
     if ((rc = set_active_all(b, 1))) return rc;

@@ -11,11 +11,14 @@ namespace uegccd {
 // Raw device pointers of one batch (owned by the Batch object in capi.cu).
 struct DevBatch {
     int nsolves = 0, nblocks = 0, ntiles = 0, nchunks = 0, nrchunks = 0, ntargets = 0;
-    int max_o = 0;
+    int max_o = 0;      // largest o_K
+    int max_occ = 0;    // largest NOcc
     int64_t namp = 0;
     SolveDev *solves = nullptr;
     BlockDev *blocks = nullptr;
-    LadderTile *tiles = nullptr;
+    LadderTile *tiles = nullptr;     // particle-particle (+hole-hole apply) tiles; pad = row tile NP
+    LadderTile *htiles = nullptr;    // hole-hole intermediate tiles
+    int nhtiles = 0;
     ChunkDev *chunks = nullptr;      // amplitude chunks
     ChunkDev *rchunks = nullptr;     // ring-intermediate chunks over (i, x, l)
     int *chunk_begin = nullptr;      // nsolves+1: first chunk of each solve
@@ -34,11 +37,23 @@ struct DevBatch {
     double *part_e = nullptr, *part_dt = nullptr, *part_r = nullptr;
     double *red = nullptr;           // 3 per solve: sum e, max dt, max |r|
     uint8_t *active = nullptr;       // per solve
+    // particle-hole form of the ring terms
+    int nphchunks = 0, nrtiles = 0;
+    ChunkDev *phchunks = nullptr;    // kPhRows rows of one solve per chunk
+    RingTile *rtiles = nullptr;
+    int16_t *ph_i = nullptr, *ph_x = nullptr;
+    int32_t *phrow_of = nullptr;
+    double *X = nullptr, *Y = nullptr, *Ex = nullptr, *Ey = nullptr;  // O*V*O each (A1..A3 live in J1..J3)
+    double *Sx = nullptr, *Sy = nullptr;                              // O*V each
+    double *g_rq = nullptr, *g_xq = nullptr;                          // per amplitude
 };
+
+constexpr int kPhRows = 8;
+constexpr int kDiisMax = 16;   // DIIS history capacity (k_diis_* use the same bound)   // ph rows per CTA of k_ph_build (one warp each)
 
 // Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
 enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
-                KID_UPDATE, KID_REDUCE, KID_PACK, KID_COUNT };
+                KID_UPDATE, KID_REDUCE, KID_PACK, KID_PH_BUILD, KID_RING_QUAD, KID_COUNT };
 struct KernelTimer {
     bool on = false;
     cudaEvent_t ev[2 * 64];
@@ -86,6 +101,10 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st);
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt = nullptr);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
+// Pulay DIIS: store (t_new, t_new - t) in slot, dot products with nvec stored errors -> brow
+void launch_diis_push(const DevBatch &d, int slot, int nvec, double *hist_t, double *hist_e, double *part,
+                      double *brow, cudaStream_t st);
+void launch_diis_extrap(const DevBatch &d, const double *hist_t, const double *coef, int nvec, cudaStream_t st);
 void launch_unpack(const DevBatch &d, int s, int namp, const double *t, double *ab, double *ba, double *aa,
                    cudaStream_t st);
 

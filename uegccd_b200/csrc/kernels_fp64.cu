@@ -172,175 +172,144 @@ __global__ void k_reduce_solves(const int *__restrict__ chunk_begin, const doubl
 // particle-particle (CCD.f90:660-681): W_K[c][a] = v(c-a) over the block's virtuals;
 // hole-hole (CCD.f90:611-657): H_K[p][q] = v(i_p - k_q) + sum_c t_K[p][c] v(c - k_q),
 // p = (i,j), q = (k,l), after the pair-swap re-indexing t(kl,b) = t(lk,a).
-// k_hh_w builds H_K; k_ladder writes G (it overwrites, so it runs first).
+// k_ladder2 in mode 1 builds H_K; in mode 0 it writes G (overwriting, so it runs first).
 // ----------------------------------------------------------------------------
-constexpr int kHhC = 32;
-__global__ void k_hh_w(const BlockDev *__restrict__ blocks, const SolveDev *__restrict__ solves,
-                       const int16_t *__restrict__ pair_i, const int16_t *__restrict__ vir,
-                       const int4 *__restrict__ nv4, const double *__restrict__ vtab,
-                       const double *__restrict__ t, const int64_t *__restrict__ hh0, double *__restrict__ hh,
-                       const uint8_t *__restrict__ active)
+constexpr int kVtabSmem = 1024;  // |q|^2 table entries staged in shared memory
+
+// Ladder tiles v3: FP64 tensor-core MMA (mma.sync m8n8k4 f64; tcgen05 has no f64
+// kind).  One warp owns a 32 (a) x NP (p) output tile as 4 x NP/8 fragments of 8x8;
+// a CTA of 4 warps covers 128 columns.  Each lane generates its own element of the
+// Coulomb fragment, A[a][c] = v(n_a - n_c), from the |q|^2 table, so the Coulomb
+// tile never passes through shared memory; the t fragment is read from L1/L2.
+//   mode 0: G^T[a][p] = sum_c v(a-c) t[p][c] (+ sum_q t[q][a] H[p][q] when do_hh)
+//   mode 1: H^T[q][p] = v(i_p - k_q) + sum_c v(k_q - c) t[p][c]   (columns = pairs)
+// Fragment layouts (PTX ISA, m8n8k4 .f64): A row = lane/4, col = lane%4;
+// B row (k) = lane%4, col = lane/4; C row = lane/4, cols 2*(lane%4) + {0,1}.
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b)
 {
-    const BlockDev B = blocks[blockIdx.x];
-    if (!active[B.solve]) return;
-    const SolveDev s = solves[B.solve];
-    extern __shared__ double sm[];
-    const int o = B.o, v = B.v;
-    double *Ts = sm;                    // o x kHhC
-    double *Us = Ts + o * kHhC;         // kHhC x o
-    int4 *nk = (int4 *)(Us + kHhC * o); // o
-    for (int q = threadIdx.x; q < o; q += blockDim.x) nk[q] = nv4[s.orb0 + pair_i[B.pair0 + q]];
-    const int nent = o * o;
-    constexpr int kPer = 16;  // entries per thread (o <= 64 -> 4096 entries <= 256*16)
-    double acc[kPer];
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <int NP>
+__device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
+                                             const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
+                                             const int4 *__restrict__ nv4, const double *__restrict__ vtab,
+                                             const double *__restrict__ t, const double *__restrict__ H, int mode,
+                                             int do_pp, int do_hh, double *__restrict__ out, const double *sv,
+                                             bool vsm)
+{
+    constexpr int NN = NP / 8;  // n fragments
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int v = B.v, o = B.o;
+    const int ncol = mode == 0 ? v : o;
+    const int colbase = T.a0 + warp * 32;
+    if (colbase >= ncol) return;  // no barriers below
+    // n-vectors of this lane's A-fragment rows (one per m fragment)
+    int4 na[4];
 #pragma unroll
-    for (int r = 0; r < kPer; r++) acc[r] = 0.0;
-    __syncthreads();
-    for (int c0 = 0; c0 < v; c0 += kHhC) {
-        for (int e = threadIdx.x; e < o * kHhC; e += blockDim.x) {
-            int pp = e / kHhC, cc = e % kHhC;
-            Ts[pp * kHhC + cc] = (c0 + cc < v) ? t[B.t0 + (int64_t)pp * v + c0 + cc] : 0.0;
-        }
-        for (int e = threadIdx.x; e < o * kHhC; e += blockDim.x) {
-            int cc = e / o, qq = e % o;
-            double u = 0.0;
-            if (c0 + cc < v) {
-                int4 nc = nv4[s.orb0 + vir[B.vir0 + c0 + cc]];
-                u = vtab[s.vtab0 + q2_of(nc, nk[qq])];
-            }
-            Us[cc * o + qq] = u;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < kPer; r++) {
-            int e = threadIdx.x + r * blockDim.x;
-            if (e < nent) {
-                int pp = e / o, qq = e % o;
-                double a = acc[r];
-                for (int cc = 0; cc < kHhC; cc++) a += Ts[pp * kHhC + cc] * Us[cc * o + qq];
-                acc[r] = a;
-            }
-        }
-        __syncthreads();
+    for (int m = 0; m < 4; m++) {
+        int col = colbase + m * 8 + gid;
+        na[m] = make_int4(0, 0, 0, 0);
+        if (col < ncol) na[m] = nv4[s.orb0 + (mode == 0 ? vir[B.vir0 + col] : pair_i[B.pair0 + col])];
     }
-    double *H = hh + hh0[blockIdx.x];
+    double acc[4][NN][2];
 #pragma unroll
-    for (int r = 0; r < kPer; r++) {
-        int e = threadIdx.x + r * blockDim.x;
-        if (e < nent) {
-            int pp = e / o, qq = e % o;
-            int ip = pair_i[B.pair0 + pp];
-            int4 ni = nv4[s.orb0 + ip];
-            H[pp * o + qq] = vtab[s.vtab0 + q2_of(ni, nk[qq])] + acc[r];
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+        for (int n = 0; n < NN; n++) acc[m][n][0] = acc[m][n][1] = 0.0;
+    const double *trow[NN];
+    bool prow[NN];
+#pragma unroll
+    for (int n = 0; n < NN; n++) {
+        int p = T.p0 + n * 8 + gid;
+        prow[n] = p < o;
+        trow[n] = t + B.t0 + (int64_t)(prow[n] ? p : 0) * v;
+    }
+    if (do_pp || mode == 1) {
+        for (int c0 = 0; c0 < v; c0 += 4) {
+            const int c = c0 + tig;
+            const bool cok = c < v;
+            const int4 nc = cok ? nv4[s.orb0 + vir[B.vir0 + c]] : make_int4(0, 0, 0, 0);
+            double bf[NN];
+#pragma unroll
+            for (int n = 0; n < NN; n++) bf[n] = (cok && prow[n]) ? __ldg(trow[n] + c) : 0.0;
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                int q2 = q2_of(na[m], nc);
+                double af = cok ? (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2])) : 0.0;
+#pragma unroll
+                for (int n = 0; n < NN; n++) dmma_884(acc[m][n][0], acc[m][n][1], af, bf[n]);
+            }
         }
+    }
+    if (mode == 0 && do_hh) {
+        // acc[a][p] += sum_q t[q][a] H[p][q]
+        for (int q0 = 0; q0 < o; q0 += 4) {
+            const int q = q0 + tig;
+            const bool qok = q < o;
+            double bf[NN];
+#pragma unroll
+            for (int n = 0; n < NN; n++) {
+                int p = T.p0 + n * 8 + gid;
+                bf[n] = (qok && p < o) ? H[(int64_t)p * o + q] : 0.0;
+            }
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                int col = colbase + m * 8 + gid;
+                double af = (qok && col < v) ? __ldg(&t[B.t0 + (int64_t)q * v + col]) : 0.0;
+#pragma unroll
+                for (int n = 0; n < NN; n++) dmma_884(acc[m][n][0], acc[m][n][1], af, bf[n]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const int col = colbase + m * 8 + gid;
+        if (col >= ncol) continue;
+#pragma unroll
+        for (int n = 0; n < NN; n++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int p = T.p0 + n * 8 + 2 * tig + h;
+                if (p >= o) continue;
+                if (mode == 0) {
+                    out[B.t0 + (int64_t)p * v + col] = acc[m][n][h];
+                } else {
+                    const int4 ni = nv4[s.orb0 + pair_i[B.pair0 + p]];
+                    const int q2 = q2_of(ni, na[m]);
+                    out[(int64_t)p * o + col] = (vsm ? sv[q2] : vtab[s.vtab0 + q2]) + acc[m][n][h];
+                }
+            }
     }
 }
 
-// G tile [a0, a0+64) x [p0, p0+32) of block blk.  128 threads, 4 (a) x 4 (p) each.
-constexpr int kLA = 64, kLP = 32, kLC = 16;
-__global__ void __launch_bounds__(128) k_ladder(const LadderTile *__restrict__ tiles,
-                                               const BlockDev *__restrict__ blocks,
-                                               const SolveDev *__restrict__ solves,
-                                               const int16_t *__restrict__ vir, const int4 *__restrict__ nv4,
-                                               const double *__restrict__ vtab, const double *__restrict__ t,
-                                               const int64_t *__restrict__ hh0, const double *__restrict__ hh,
-                                               int do_pp, int do_hh, double *__restrict__ g,
-                                               const uint8_t *__restrict__ active)
+__global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ tiles,
+                                                const BlockDev *__restrict__ blocks,
+                                                const SolveDev *__restrict__ solves,
+                                                const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
+                                                const int4 *__restrict__ nv4, const double *__restrict__ vtab,
+                                                const double *__restrict__ t, const int64_t *__restrict__ hh0,
+                                                double *__restrict__ hh, int mode, int do_pp, int do_hh,
+                                                double *__restrict__ g, const uint8_t *__restrict__ active)
 {
     const LadderTile T = tiles[blockIdx.x];
     const BlockDev B = blocks[T.blk];
     if (!active[B.solve]) return;
     const SolveDev s = solves[B.solve];
-    __shared__ double Ws[kLC][kLA + 2];
-    __shared__ double Ts[kLC][kLP + 2];
-    __shared__ int4 na[kLA];
-    __shared__ int4 nc[kLC];
-    const int tid = threadIdx.x;
-    const int ta = tid >> 3;  // 0..15 -> a = 4*ta..4*ta+3
-    const int tp = tid & 7;   // 0..7  -> p = 4*tp..4*tp+3
-    const int v = B.v, o = B.o;
-    for (int x = tid; x < kLA; x += blockDim.x) {
-        int a = T.a0 + x;
-        na[x] = (a < v) ? nv4[s.orb0 + vir[B.vir0 + a]] : make_int4(0, 0, 0, 0);
-    }
-    double acc[4][4];
-#pragma unroll
-    for (int x = 0; x < 4; x++)
-#pragma unroll
-        for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+    __shared__ double sv[kVtabSmem];
+    const bool vsm = s.q2max < kVtabSmem;
+    if (vsm)
+        for (int q = threadIdx.x; q <= s.q2max; q += blockDim.x) sv[q] = vtab[s.vtab0 + q];
     __syncthreads();
-    if (do_pp) {
-        for (int c0 = 0; c0 < v; c0 += kLC) {
-            if (tid < kLC) {
-                int c = c0 + tid;
-                nc[tid] = (c < v) ? nv4[s.orb0 + vir[B.vir0 + c]] : make_int4(0, 0, 0, 0);
-            }
-            __syncthreads();
-            for (int e = tid; e < kLC * kLA; e += blockDim.x) {
-                int cc = e / kLA, aa = e % kLA;
-                bool ok = (c0 + cc < v) && (T.a0 + aa < v);
-                Ws[cc][aa] = ok ? vtab[s.vtab0 + q2_of(nc[cc], na[aa])] : 0.0;
-            }
-            for (int e = tid; e < kLC * kLP; e += blockDim.x) {
-                int pp = e / kLC, cc = e % kLC;
-                int p = T.p0 + pp, c = c0 + cc;
-                Ts[cc][pp] = (p < o && c < v) ? t[B.t0 + (int64_t)p * v + c] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int cc = 0; cc < kLC; cc++) {
-                double wa[4], tp4[4];
-#pragma unroll
-                for (int x = 0; x < 4; x++) wa[x] = Ws[cc][ta * 4 + x];
-#pragma unroll
-                for (int y = 0; y < 4; y++) tp4[y] = Ts[cc][tp * 4 + y];
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] = fma(wa[x], tp4[y], acc[x][y]);
-            }
-            __syncthreads();
-        }
-    }
-    if (do_hh) {
-        // acc[a][p] += sum_q t[q][a] * H[p][q]
-        const double *H = hh + hh0[T.blk];
-        for (int q0 = 0; q0 < o; q0 += kLC) {
-            for (int e = tid; e < kLC * kLA; e += blockDim.x) {
-                int qq = e / kLA, aa = e % kLA;
-                int q = q0 + qq, a = T.a0 + aa;
-                Ws[qq][aa] = (q < o && a < v) ? t[B.t0 + (int64_t)q * v + a] : 0.0;
-            }
-            for (int e = tid; e < kLC * kLP; e += blockDim.x) {
-                int pp = e / kLC, qq = e % kLC;
-                int p = T.p0 + pp, q = q0 + qq;
-                Ts[qq][pp] = (p < o && q < o) ? H[p * o + q] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int qq = 0; qq < kLC; qq++) {
-                double wa[4], tp4[4];
-#pragma unroll
-                for (int x = 0; x < 4; x++) wa[x] = Ws[qq][ta * 4 + x];
-#pragma unroll
-                for (int y = 0; y < 4; y++) tp4[y] = Ts[qq][tp * 4 + y];
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] = fma(wa[x], tp4[y], acc[x][y]);
-            }
-            __syncthreads();
-        }
-    }
-#pragma unroll
-    for (int y = 0; y < 4; y++) {
-        int p = T.p0 + tp * 4 + y;
-        if (p >= o) continue;
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-            int a = T.a0 + ta * 4 + x;
-            if (a < v) g[B.t0 + (int64_t)p * v + a] = acc[x][y];
-        }
+    double *H = hh + hh0[T.blk];
+    double *out = mode == 0 ? g : H;
+    switch (T.pad) {
+    case 8: ladder3_tile<8>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm); break;
+    case 16: ladder3_tile<16>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm); break;
+    default: ladder3_tile<32>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm); break;
     }
 }
 
@@ -461,6 +430,159 @@ __global__ void k_ring_int(const ChunkDev *__restrict__ rchunks, const SolveDev 
 }
 
 // ----------------------------------------------------------------------------
+// Rings and crossed rings in particle-hole form (CCD).
+// For every ph row (i,x), x virtual, with c = partner of (i,k,x):
+//   X[k] = t(ik,x),  Y[k] = t(ik,c)                 (= t(ki,x) by the pair swap)
+//   Sx = sum_k X, Sy = sum_k Y
+//   Ex[j] = sum_k v(k-j) X[k],  Ey[j] = sum_k v(k-j) Y[k]
+//   XW[l] = sum_k X[k] v(i+k-x-l), YW[l] = sum_k Y[k] v(i+k-x-l)
+// and the quadratic-ring intermediates of CCD.f90:774-797 / 902-925 become
+//   A1 = J1 + J2 = 2 vd (2Sx - Sy) - 2 XW + YW,  A2 = J2 = vd (2Sx - Sy) - XW,  A3 = J3 = YW,
+// vd = v(i-x).  Then, for the amplitude (i,j,a) with partner b (rows ia, jb, ib, ja):
+//   linear rings   (CCD.f90:716-763): 2 v(i-a)(Sx_ia + Sx_jb) - v(i-a)(Sy_ia + Sy_jb) - Ex_ia[j] - Ex_jb[i]
+//   linear xrings  (CCD.f90:845-892): -Ey_ib[j] - Ey_ja[i]
+//   quadratic rings  (CCD.f90:801-808): A1_ia . X_jb - A2_ia . Y_jb
+//   quadratic xrings (CCD.f90:927-934): A3_ib . Y_ja
+// The quadratic products pair the rows of momentum Q with those of -Q, which is
+// what k_ring_quad does, group by group; every amplitude receives exactly one
+// ring and one crossed-ring product, so no atomics are needed.
+// Row layout: row r (local) of solve s: scalars at s.phr0 + r, vectors at s.ph0 + r * O (O entries).
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * kPhRows) k_ph_build(
+    const ChunkDev *__restrict__ phchunks, const SolveDev *__restrict__ solves, const int16_t *__restrict__ ph_i,
+    const int16_t *__restrict__ ph_x, const int32_t *__restrict__ pos, const int32_t *__restrict__ partner,
+    const int4 *__restrict__ nv4, const double *__restrict__ vtab, const double *__restrict__ t,
+    double *__restrict__ X, double *__restrict__ Y, double *__restrict__ Ex, double *__restrict__ Ey,
+    double *__restrict__ A1, double *__restrict__ A2, double *__restrict__ A3, double *__restrict__ Sx,
+    double *__restrict__ Sy, const uint8_t *__restrict__ active)
+{
+    const ChunkDev ch = phchunks[blockIdx.x];
+    if (!active[ch.solve]) return;
+    const SolveDev s = solves[ch.solve];
+    const int O = s.O, V = s.V;
+    __shared__ int4 nocc[64];
+    __shared__ double xs[kPhRows][64], ys[kPhRows][64];
+    for (int k = threadIdx.x; k < O; k += blockDim.x) nocc[k] = nv4[s.orb0 + k];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = ch.start + warp;
+    if (r >= O * V) return;  // no barrier below this point
+    const int64_t row = s.phr0 + r;
+    const int64_t vrow = s.ph0 + (int64_t)r * O;
+    const int i = ph_i[row], x = ph_x[row];
+    const int4 ni = nv4[s.orb0 + i], nx = nv4[s.orb0 + x];
+    double sx = 0.0, sy = 0.0;
+    for (int k = lane; k < O; k += 32) {
+        int p = posmap(s, pos, i, k, x);
+        double xv = 0.0, yv = 0.0;
+        if (p >= 0) {
+            xv = t[p];
+            yv = t[partner[p]];
+        }
+        xs[warp][k] = xv;
+        ys[warp][k] = yv;
+        sx += xv;
+        sy += yv;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    __syncwarp();
+    const double vd = vtab[s.vtab0 + q2_of(ni, nx)];
+    const double base = vd * (2.0 * sx - sy);
+    const int bx = ni.x - nx.x, by = ni.y - nx.y, bz = ni.z - nx.z;  // n_i - n_x
+    for (int j = lane; j < O; j += 32) {
+        const int4 nj = nocc[j];
+        double ex = 0.0, ey = 0.0, xw = 0.0, yw = 0.0;
+        for (int k = 0; k < O; k++) {
+            const int4 nk = nocc[k];
+            const double xk = xs[warp][k], yk = ys[warp][k];
+            const double vkj = vtab[s.vtab0 + q2_of(nk, nj)];
+            const int qx = bx + nk.x - nj.x, qy = by + nk.y - nj.y, qz = bz + nk.z - nj.z;
+            // n_i + n_k - n_x lies in the basis exactly when (i,k,x) is allowed; otherwise
+            // X[k] = Y[k] = 0 and |q|^2 may exceed the table, so the term is skipped.
+            const int q2 = qx * qx + qy * qy + qz * qz;
+            const double ve = (q2 <= s.q2max) ? vtab[s.vtab0 + q2] : 0.0;
+            ex = fma(vkj, xk, ex);
+            ey = fma(vkj, yk, ey);
+            xw = fma(xk, ve, xw);
+            yw = fma(yk, ve, yw);
+        }
+        const int64_t o = vrow + j;
+        X[o] = xs[warp][j];
+        Y[o] = ys[warp][j];
+        Ex[o] = ex;
+        Ey[o] = ey;
+        A1[o] = 2.0 * base - 2.0 * xw + yw;
+        A2[o] = base - xw;
+        A3[o] = yw;
+    }
+    if (lane == 0) {
+        Sx[row] = sx;
+        Sy[row] = sy;
+    }
+}
+
+// 16 x 16 output pairs per CTA (256 threads); rows staged in shared memory.
+constexpr int kRT = 16;
+__global__ void __launch_bounds__(kRT * kRT) k_ring_quad(
+    const RingTile *__restrict__ tiles, const SolveDev *__restrict__ solves, const int16_t *__restrict__ ph_i,
+    const int16_t *__restrict__ ph_x, const int32_t *__restrict__ pos, const double *__restrict__ X,
+    const double *__restrict__ Y, const double *__restrict__ A1, const double *__restrict__ A2,
+    const double *__restrict__ A3, int do_ring, int do_xring, double *__restrict__ g_rq,
+    double *__restrict__ g_xq, const uint8_t *__restrict__ active)
+{
+    const RingTile T = tiles[blockIdx.x];
+    if (!active[T.solve]) return;
+    const SolveDev s = solves[T.solve];
+    const int O = s.O;
+    const int ld = O + 1;
+    extern __shared__ double sm[];
+    double *a1 = sm, *a2 = a1 + kRT * ld, *a3 = a2 + kRT * ld, *xr = a3 + kRT * ld, *yr = xr + kRT * ld;
+    for (int e = threadIdx.x; e < kRT * O; e += blockDim.x) {
+        const int rr = e / O, l = e % O;
+        double v1 = 0.0, v2 = 0.0, v3 = 0.0, vx = 0.0, vy = 0.0;
+        if (rr < T.n1) {
+            const int64_t o = s.ph0 + (int64_t)(T.r1 + rr) * O + l;
+            v1 = A1[o];
+            v2 = A2[o];
+            v3 = A3[o];
+        }
+        if (rr < T.n2) {
+            const int64_t o = s.ph0 + (int64_t)(T.r2 + rr) * O + l;
+            vx = X[o];
+            vy = Y[o];
+        }
+        a1[rr * ld + l] = v1;
+        a2[rr * ld + l] = v2;
+        a3[rr * ld + l] = v3;
+        xr[rr * ld + l] = vx;
+        yr[rr * ld + l] = vy;
+    }
+    __syncthreads();
+    const int ty = threadIdx.x / kRT, tx = threadIdx.x % kRT;
+    if (ty >= T.n1 || tx >= T.n2) return;
+    double ring = 0.0, xring = 0.0;
+    for (int l = 0; l < O; l++) {
+        const double yv = yr[tx * ld + l];
+        ring = fma(a1[ty * ld + l], xr[tx * ld + l], ring);
+        ring = fma(-a2[ty * ld + l], yv, ring);
+        xring = fma(a3[ty * ld + l], yv, xring);
+    }
+    const int64_t r1 = s.phr0 + T.r1 + ty, r2 = s.phr0 + T.r2 + tx;
+    const int i = ph_i[r1], x1 = ph_x[r1], j = ph_i[r2], x2 = ph_x[r2];
+    if (do_ring) {
+        const int p = posmap(s, pos, i, j, x1);  // amplitude (i,j,a=x1), partner x2
+        if (p >= 0) g_rq[p] = ring;
+    }
+    if (do_xring) {
+        const int p = posmap(s, pos, i, j, x2);  // amplitude (i,j,a=x2), partner x1
+        if (p >= 0) g_xq[p] = xring;
+    }
+}
+
+// ----------------------------------------------------------------------------
 // Fused residual / update / convergence / energy, one thread per amplitude.
 //   G = ladders (from k_ladder) + drivers + mosaics + rings + crossed rings
 //   R = -G + D t                          (GetRes, CCD.f90:417)
@@ -485,6 +607,8 @@ struct UpdateArgs {
     const double *J1, *J2, *J3;
     double *part_e, *part_dt, *part_r;
     double *g_out;            // optional: full G per amplitude (term checks)
+    const int32_t *phrow_of;
+    const double *Sx, *Sy, *Ex, *Ey, *g_rq, *g_xq;
     const uint8_t *active;
     int do_ladder, do_mosaic, do_ring, do_xring, do_driver, drpa, mode;
 };
@@ -528,51 +652,20 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
                 }
             }
         } else {
+            const int V = s.V;
+            const int64_t pr = s.phr0, pv = s.ph0;
+            const int r_ia = A.phrow_of[pr + i * V + (a - O)];
+            const int r_jb = A.phrow_of[pr + j * V + (b - O)];
             if (A.do_ring) {
-                // linear rings (CCD.f90:716-763), c = partner of (i,k,a) / (j,k,b):
-                //   (2v(i-a) - v(k-j)) t(ik,a) - v(i-a) t(ik,c)
-                // + (2v(a-i) - v(k-i)) t(jk,b) - v(a-i) t(jk,c')
-                double acc = 0.0;
-                for (int k = 0; k < O; k++) {
-                    int p1 = posmap(s, A.pos, i, k, a);
-                    if (p1 >= 0) {
-                        double tx = A.t[p1], ty = A.t[A.partner[p1]];
-                        acc += (2.0 * via - vpq(s, A.nv4, A.vtab, k, j)) * tx - via * ty;
-                    }
-                    int p2 = posmap(s, A.pos, j, k, b);
-                    if (p2 >= 0) {
-                        double tx = A.t[p2], ty = A.t[A.partner[p2]];
-                        acc += (2.0 * via - vpq(s, A.nv4, A.vtab, k, i)) * tx - via * ty;
-                    }
-                }
-                // quadratic rings (CCD.f90:801-808): sum_l (J1+J2)(i,a,l) t(lj,d) - J2(i,a,l) t(lj,b)
-                const int64_t jr = s.ph0 + ((int64_t)i * s.V + (a - O)) * O;
-                for (int l = 0; l < O; l++) {
-                    int pb = posmap(s, A.pos, l, j, b);  // (l,j,b) exists iff d is a virtual
-                    if (pb < 0) continue;
-                    double tb = A.t[pb], td = A.t[A.partner[pb]];
-                    double j2 = A.J2[jr + l];
-                    acc += (A.J1[jr + l] + j2) * td - j2 * tb;
-                }
-                g += acc;
+                // linear rings (CCD.f90:716-763) and quadratic rings (CCD.f90:771-811)
+                g += 2.0 * via * (A.Sx[pr + r_ia] + A.Sx[pr + r_jb]) - via * (A.Sy[pr + r_ia] + A.Sy[pr + r_jb]) -
+                     A.Ex[pv + (int64_t)r_ia * O + j] - A.Ex[pv + (int64_t)r_jb * O + i] + A.g_rq[p];
             }
             if (A.do_xring) {
-                // linear crossed rings (CCD.f90:851-889): -v(j-k) t(ki,b) - v(i-k) t(kj,a)
-                double acc = 0.0;
-                for (int k = 0; k < O; k++) {
-                    int p3 = posmap(s, A.pos, k, i, b);
-                    if (p3 >= 0) acc -= vpq(s, A.nv4, A.vtab, j, k) * A.t[p3];
-                    int p4 = posmap(s, A.pos, k, j, a);
-                    if (p4 >= 0) acc -= vpq(s, A.nv4, A.vtab, i, k) * A.t[p4];
-                }
-                // quadratic crossed rings (CCD.f90:927-934): sum_l J3(i,b,l) t(lj,a)
-                const int64_t jr = s.ph0 + ((int64_t)i * s.V + (b - O)) * O;
-                for (int l = 0; l < O; l++) {
-                    int pa = posmap(s, A.pos, l, j, a);
-                    if (pa < 0) continue;
-                    acc += A.J3[jr + l] * A.t[pa];
-                }
-                g += acc;
+                // linear crossed rings (CCD.f90:845-892) and quadratic crossed rings (CCD.f90:899-937)
+                const int r_ib = A.phrow_of[pr + i * V + (b - O)];
+                const int r_ja = A.phrow_of[pr + j * V + (a - O)];
+                g += -A.Ey[pv + (int64_t)r_ib * O + j] - A.Ey[pv + (int64_t)r_ja * O + i] + A.g_xq[p];
             }
         }
         if (A.g_out) A.g_out[p] = g;
@@ -596,6 +689,87 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
         A.part_dt[blockIdx.x] = dtmax;
         A.part_r[blockIdx.x] = rmax;
     }
+}
+
+// ----------------------------------------------------------------------------
+// Pulay DIIS (new in this library; the reference's GetTFromDIIS, DIISCC.f90:52-131,
+// builds a singular matrix and never extrapolates).  Error vector e = t' - t of
+// the (damped) Jacobi step; history of ndiis (t', e) pairs per solve.
+// k_diis_push stores slot `slot` and forms the dot products e . e_j of every
+// stored j (per-chunk partials, reduced per solve in chunk order).
+// ----------------------------------------------------------------------------
+constexpr int kMaxDiis = 16;
+__global__ void __launch_bounds__(kChunk) k_diis_push(const ChunkDev *__restrict__ chunks,
+                                                      const SolveDev *__restrict__ solves, int64_t namp,
+                                                      const double *__restrict__ t, const double *__restrict__ t_new,
+                                                      double *__restrict__ hist_t, double *__restrict__ hist_e,
+                                                      int slot, int nvec, double *__restrict__ part,
+                                                      const uint8_t *__restrict__ active)
+{
+    const ChunkDev ch = chunks[blockIdx.x];
+    const SolveDev s = solves[ch.solve];
+    const int loc = ch.start + threadIdx.x;
+    const bool on = active[ch.solve] && loc < s.namp;
+    double e = 0.0;
+    int64_t p = 0;
+    if (on) {
+        p = s.amp0 + loc;
+        const double tn = t_new[p];
+        e = tn - t[p];
+        hist_t[(int64_t)slot * namp + p] = tn;
+        hist_e[(int64_t)slot * namp + p] = e;
+    }
+    for (int jv = 0; jv < nvec; jv++) {
+        double d = on ? e * hist_e[(int64_t)jv * namp + p] : 0.0;
+        d = block_sum<kChunk>(d);
+        if (threadIdx.x == 0) part[(int64_t)blockIdx.x * kMaxDiis + jv] = d;
+        __syncthreads();
+    }
+}
+
+// brow[s*kMaxDiis + j] = sum over the solve's chunks of part[chunk][j]
+__global__ void k_diis_rows(const int *__restrict__ chunk_begin, const double *__restrict__ part, int nvec,
+                            double *__restrict__ brow)
+{
+    const int s = blockIdx.x;
+    const int c0 = chunk_begin[s], c1 = chunk_begin[s + 1];
+    for (int jv = 0; jv < nvec; jv++) {
+        double acc = 0.0;
+        for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) acc += part[(int64_t)c * kMaxDiis + jv];
+        acc = block_sum<256>(acc);
+        if (threadIdx.x == 0) brow[s * kMaxDiis + jv] = acc;
+        __syncthreads();
+    }
+}
+
+// t = sum_j coef[s][j] hist_t[j]  (active solves)
+__global__ void k_diis_extrap(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                              int64_t namp, const double *__restrict__ hist_t, const double *__restrict__ coef,
+                              int nvec, double *__restrict__ t, const uint8_t *__restrict__ active)
+{
+    const ChunkDev ch = chunks[blockIdx.x];
+    if (!active[ch.solve]) return;
+    const SolveDev s = solves[ch.solve];
+    const int loc = ch.start + threadIdx.x;
+    if (loc >= s.namp) return;
+    const int64_t p = s.amp0 + loc;
+    const double *c = coef + ch.solve * kMaxDiis;
+    double x = 0.0;
+    for (int jv = 0; jv < nvec; jv++) x = fma(c[jv], hist_t[(int64_t)jv * namp + p], x);
+    t[p] = x;
+}
+
+void launch_diis_push(const DevBatch &d, int slot, int nvec, double *hist_t, double *hist_e, double *part,
+                      double *brow, cudaStream_t st)
+{
+    k_diis_push<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, d.t, d.t_new, hist_t, hist_e, slot, nvec,
+                                              part, d.active);
+    k_diis_rows<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, part, nvec, brow);
+}
+
+void launch_diis_extrap(const DevBatch &d, const double *hist_t, const double *coef, int nvec, cudaStream_t st)
+{
+    k_diis_extrap<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, hist_t, coef, nvec, d.t, d.active);
 }
 
 // ----------------------------------------------------------------------------
@@ -656,8 +830,9 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
     k_to_aaaa<<<(unsigned)((d.namp + 255) / 256), 256, 0, st>>>(d.namp, d.partner, d.t, d.t_new);
 }
 
-const char *kKernelNames[KID_COUNT] = {"k_mp2", "k_energy", "k_hh_w", "k_ladder", "k_mosaic_s",
-                                      "k_mosaic_reduce", "k_ring_int", "k_update", "k_reduce_solves", "k_pack"};
+const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh", "k_ladder",
+                                      "k_mosaic_s", "k_mosaic_reduce", "k_ring_int", "k_update",
+                                      "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad"};
 
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt)
@@ -667,16 +842,15 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     int n = 0;
     if (f.do_ladder && d.nblocks > 0) {
         if (f.do_hh) {
-            size_t smem = (size_t)(2 * d.max_o * kHhC) * sizeof(double) + (size_t)d.max_o * sizeof(int4);
             kt->begin(KID_HH_W, st);
-            k_hh_w<<<d.nblocks, 256, smem, st>>>(d.blocks, d.solves, d.pair_i, d.vir, d.nv4, d.vtab, d.t, d.hh0,
-                                                 d.hh, d.active);
+            k_ladder3<<<d.nhtiles, 128, 0, st>>>(d.htiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t,
+                                                 d.hh0, d.hh, 1, f.do_pp, f.do_hh, d.g, d.active);
             kt->end(st);
             n++;
         }
         kt->begin(KID_LADDER, st);
-        k_ladder<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.nv4, d.vtab, d.t, d.hh0, d.hh,
-                                           f.do_pp, f.do_hh, d.g, d.active);
+        k_ladder3<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t, d.hh0,
+                                            d.hh, 0, f.do_pp, f.do_hh, d.g, d.active);
         kt->end(st);
         n++;
     }
@@ -690,12 +864,26 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         kt->end(st);
         n += 2;
     }
-    if (f.do_ring || f.do_xring) {
+    if ((f.do_ring || f.do_xring) && f.drpa) {
         kt->begin(KID_RING_INT, st);
         k_ring_int<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.amps, d.partner, d.pos, d.nv4, d.vtab, d.t,
                                                   f.drpa, d.J1, d.J2, d.J3, d.active);
         kt->end(st);
         n++;
+    }
+    if ((f.do_ring || f.do_xring) && !f.drpa) {
+        kt->begin(KID_PH_BUILD, st);
+        k_ph_build<<<d.nphchunks, 32 * kPhRows, 0, st>>>(d.phchunks, d.solves, d.ph_i, d.ph_x, d.pos, d.partner,
+                                                          d.nv4, d.vtab, d.t, d.X, d.Y, d.Ex, d.Ey, d.J1, d.J2,
+                                                          d.J3, d.Sx, d.Sy, d.active);
+        kt->end(st);
+        kt->begin(KID_RING_QUAD, st);
+        size_t smem = (size_t)5 * kRT * (d.max_occ + 1) * sizeof(double);
+        k_ring_quad<<<d.nrtiles, kRT * kRT, smem, st>>>(d.rtiles, d.solves, d.ph_i, d.ph_x, d.pos, d.X, d.Y, d.J1,
+                                                         d.J2, d.J3, f.do_ring, f.do_xring, d.g_rq, d.g_xq,
+                                                         d.active);
+        kt->end(st);
+        n += 2;
     }
     UpdateArgs A;
     A.chunks = d.chunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.pos = d.pos;
@@ -704,6 +892,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
+    A.phrow_of = d.phrow_of; A.Sx = d.Sx; A.Sy = d.Sy; A.Ex = d.Ex; A.Ey = d.Ey; A.g_rq = d.g_rq; A.g_xq = d.g_xq;
     kt->begin(KID_UPDATE, st);
     k_update<<<d.nchunks, kChunk, 0, st>>>(A);
     kt->end(st);

@@ -119,6 +119,31 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
     p.namp = t0;
     if (p.namp >= (int64_t)1 << 31) return "too many amplitudes for 32-bit packed indices";
     p.ring_entries = (int64_t)O * V * O;
+
+    // particle-hole rows (i,x) grouped by their momentum Q = n_x - n_i
+    std::map<std::array<int, 3>, std::vector<std::pair<int, int>>> qrows;
+    for (int i = 0; i < O; i++)
+        for (int x = O; x < M; x++) {
+            std::array<int, 3> Q{sys.n[x][0] - sys.n[i][0], sys.n[x][1] - sys.n[i][1], sys.n[x][2] - sys.n[i][2]};
+            qrows[Q].emplace_back(i, x);
+        }
+    p.phrow_of.assign((size_t)O * V, -1);
+    std::map<std::array<int, 3>, int> gidx;
+    for (auto &kv : qrows) {
+        SolvePlan::PhGroup g{(int)p.ph_i.size(), (int)kv.second.size(), -1};
+        gidx[kv.first] = (int)p.groups.size();
+        p.groups.push_back(g);
+        for (auto &r : kv.second) {
+            p.phrow_of[(size_t)r.first * V + (r.second - O)] = (int32_t)p.ph_i.size();
+            p.ph_i.push_back((int16_t)r.first);
+            p.ph_x.push_back((int16_t)r.second);
+        }
+    }
+    for (auto &kv : qrows) {
+        std::array<int, 3> mQ{-kv.first[0], -kv.first[1], -kv.first[2]};
+        auto it = gidx.find(mQ);
+        if (it != gidx.end()) p.groups[gidx[kv.first]].partner = it->second;
+    }
     return "";
 }
 

@@ -30,6 +30,11 @@ struct SolvePlan {
     std::vector<AmpInfo> amps;              // packed index -> (i,j,a,b)
     int64_t namp = 0;
     int64_t ring_entries = 0;               // O*V*O
+    // particle-hole rows (i,x), x virtual, sorted by Q = n_x - n_i
+    std::vector<int16_t> ph_i, ph_x;        // row -> (i, x)
+    std::vector<int32_t> phrow_of;          // i*V + (x-O) -> row
+    struct PhGroup { int r0, n, partner; }; // partner: index of the -Q group or -1
+    std::vector<PhGroup> groups;
 };
 
 // Builds the plan of one system.  Returns "" on success, else a message.

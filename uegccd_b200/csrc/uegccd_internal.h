@@ -32,6 +32,7 @@ struct SolveDev {
     int64_t ph0;            // offset of the ring intermediates (O*V*O entries each)
     int32_t jvv0, joo0;     // offsets of the mosaic intermediates (V and O entries)
     double denom_factor;    // SolveCC damping (CCD.f90:380), 2 in the reference
+    int64_t phr0;           // offset of the particle-hole row arrays (O*V entries: one per row (i,x))
 };
 
 struct BlockDev {
@@ -50,6 +51,13 @@ struct LadderTile {
 // Per-amplitude record: orbital indices local to the solve (a, b absolute, >= O).
 struct AmpInfo {
     int16_t i, j, a, b;
+};
+
+// One output tile of the ring/crossed-ring quadratic products: rows [r1, r1+n1) of the
+// ph group of momentum Q against rows [r2, r2+n2) of the group of -Q (rows local to the solve).
+struct RingTile {
+    int solve;
+    int r1, n1, r2, n2;
 };
 
 struct ChunkDev {
