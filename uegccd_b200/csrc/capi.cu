@@ -169,10 +169,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int4> nv4;
     std::vector<double> eigen, vtab;
     std::vector<int64_t> hh0;
-    std::vector<ChunkDev> phchunks;
-    std::vector<RingTile> rtiles;
+    std::vector<RingPairDev> rpairs;
     std::vector<int16_t> ph_i, ph_x;
-    std::vector<int32_t> phrow_of;
+    size_t rings_smem = 0;
     int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0;
     int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_occ = 0;
     for (int s = 0; s < n; s++) {
@@ -197,14 +196,12 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         max_occ = std::max(max_occ, P.O);
         ph_i.insert(ph_i.end(), P.ph_i.begin(), P.ph_i.end());
         ph_x.insert(ph_x.end(), P.ph_x.begin(), P.ph_x.end());
-        phrow_of.insert(phrow_of.end(), P.phrow_of.begin(), P.phrow_of.end());
-        for (int r = 0; r < P.O * P.V; r += kPhRows) phchunks.push_back(ChunkDev{s, r});
-        for (const auto &G : P.groups) {
-            if (G.partner < 0) continue;
+        for (size_t gi = 0; gi < P.groups.size(); gi++) {
+            const auto &G = P.groups[gi];
+            if (G.partner < 0 || G.partner < (int)gi) continue;  // each {Q, -Q} once
             const auto &H2 = P.groups[G.partner];
-            for (int a0 = 0; a0 < G.n; a0 += 16)
-                for (int b0 = 0; b0 < H2.n; b0 += 16)
-                    rtiles.push_back(RingTile{s, G.r0 + a0, std::min(16, G.n - a0), H2.r0 + b0, std::min(16, H2.n - b0)});
+            rpairs.push_back(RingPairDev{s, G.r0, G.n, H2.r0, H2.n});
+            rings_smem = std::max(rings_smem, rings_smem_bytes(P.O, G.n + H2.n));
         }
         for (const auto &B : P.blocks) {
             BlockDev bd;
@@ -263,8 +260,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.max_o = max_o;
     d.max_occ = max_occ;
     d.namp = amp0;
-    d.nphchunks = (int)phchunks.size();
-    d.nrtiles = (int)rtiles.size();
+    d.nrpairs = (int)rpairs.size();
+    d.rings_smem = rings_smem;
+    if (rings_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ring group pair exceeds shared memory");
+    set_rings_smem_limit(rings_smem);
     if ((rc = b->upload(d.solves, solves))) return rc;
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;
@@ -283,17 +282,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.eigen, eigen))) return rc;
     if ((rc = b->upload(d.vtab, vtab))) return rc;
     if ((rc = b->upload(d.hh0, hh0))) return rc;
-    if ((rc = b->upload(d.phchunks, phchunks))) return rc;
-    if ((rc = b->upload(d.rtiles, rtiles))) return rc;
+    if ((rc = b->upload(d.rpairs, rpairs))) return rc;
     if ((rc = b->upload(d.ph_i, ph_i))) return rc;
     if ((rc = b->upload(d.ph_x, ph_x))) return rc;
-    if ((rc = b->upload(d.phrow_of, phrow_of))) return rc;
-    if ((rc = b->alloc(d.X, ph0))) return rc;
-    if ((rc = b->alloc(d.Y, ph0))) return rc;
-    if ((rc = b->alloc(d.Ex, ph0))) return rc;
-    if ((rc = b->alloc(d.Ey, ph0))) return rc;
-    if ((rc = b->alloc(d.Sx, phr0))) return rc;
-    if ((rc = b->alloc(d.Sy, phr0))) return rc;
     if ((rc = b->alloc(d.g_rq, amp0))) return rc;
     if ((rc = b->alloc(d.g_xq, amp0))) return rc;
     if ((rc = b->alloc(d.t, amp0))) return rc;

@@ -38,22 +38,22 @@ struct DevBatch {
     double *red = nullptr;           // 3 per solve: sum e, max dt, max |r|
     uint8_t *active = nullptr;       // per solve
     // particle-hole form of the ring terms
-    int nphchunks = 0, nrtiles = 0;
-    ChunkDev *phchunks = nullptr;    // kPhRows rows of one solve per chunk
-    RingTile *rtiles = nullptr;
-    int16_t *ph_i = nullptr, *ph_x = nullptr;
-    int32_t *phrow_of = nullptr;
-    double *X = nullptr, *Y = nullptr, *Ex = nullptr, *Ey = nullptr;  // O*V*O each (A1..A3 live in J1..J3)
-    double *Sx = nullptr, *Sy = nullptr;                              // O*V each
-    double *g_rq = nullptr, *g_xq = nullptr;                          // per amplitude
+    int16_t *ph_i = nullptr, *ph_x = nullptr;   // row -> (i, x), rows grouped by Q
+    double *g_rq = nullptr, *g_xq = nullptr;    // per amplitude: ring and crossed-ring G
+    RingPairDev *rpairs = nullptr;              // {Q, -Q} group pairs
+    int nrpairs = 0;
+    size_t rings_smem = 0;
 };
+// dynamic shared memory of k_rings for NOcc = O and R rows of a group pair
+size_t rings_smem_bytes(int O, int R);
+void set_rings_smem_limit(size_t bytes);
 
 constexpr int kPhRows = 8;
 constexpr int kDiisMax = 16;   // DIIS history capacity (k_diis_* use the same bound)   // ph rows per CTA of k_ph_build (one warp each)
 
 // Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
 enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
-                KID_UPDATE, KID_REDUCE, KID_PACK, KID_PH_BUILD, KID_RING_QUAD, KID_COUNT };
+                KID_UPDATE, KID_REDUCE, KID_PACK, KID_PH_BUILD, KID_RING_QUAD, KID_RINGS, KID_COUNT };
 struct KernelTimer {
     bool on = false;
     cudaEvent_t ev[2 * 64];

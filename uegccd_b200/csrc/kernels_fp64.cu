@@ -448,138 +448,171 @@ __global__ void k_ring_int(const ChunkDev *__restrict__ rchunks, const SolveDev 
 // ring and one crossed-ring product, so no atomics are needed.
 // Row layout: row r (local) of solve s: scalars at s.phr0 + r, vectors at s.ph0 + r * O (O entries).
 // ----------------------------------------------------------------------------
-__global__ void __launch_bounds__(32 * kPhRows) k_ph_build(
-    const ChunkDev *__restrict__ phchunks, const SolveDev *__restrict__ solves, const int16_t *__restrict__ ph_i,
-    const int16_t *__restrict__ ph_x, const int32_t *__restrict__ pos, const int32_t *__restrict__ partner,
-    const int4 *__restrict__ nv4, const double *__restrict__ vtab, const double *__restrict__ t,
-    double *__restrict__ X, double *__restrict__ Y, double *__restrict__ Ex, double *__restrict__ Ey,
-    double *__restrict__ A1, double *__restrict__ A2, double *__restrict__ A3, double *__restrict__ Sx,
-    double *__restrict__ Sy, const uint8_t *__restrict__ active)
+// ----------------------------------------------------------------------------
+// Fused rings: one CTA per pair of ph groups {Q, -Q}.  Everything of the formulas
+// above happens in shared memory: X, Y rows of both groups, the exchange kernels
+// W_Q[k][l] = v(n_k - n_l - Q) and W_-Q, the direct occupied kernel
+// Vocc[j][k] = v(n_k - n_j), the A rows (chunk by chunk) and the products.  Each
+// pair of rows (r1 in one group, r2 in the other) owns two amplitudes:
+//   ring  amplitude (i1, i2, a = x1):  lin + A1_r1 . X_r2 - A2_r1 . Y_r2
+//   xring amplitude (i1, i2, a = x2):  xlin + A3_r1 . Y_r2
+// with lin = 2 vd_r1 (Sx_r1 + Sx_r2) - vd_r1 (Sy_r1 + Sy_r2) - Ex_r1[i2] - Ex_r2[i1]
+// and xlin = -Ey_r1[i2] - Ey_r2[i1]; Ex/Ey elements are formed where used.
+// ----------------------------------------------------------------------------
+constexpr int kRingCh = 16;  // A rows per chunk
+
+__global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ pairs,
+                                               const SolveDev *__restrict__ solves,
+                                               const int16_t *__restrict__ ph_i, const int16_t *__restrict__ ph_x,
+                                               const int32_t *__restrict__ pos, const int32_t *__restrict__ partner,
+                                               const int4 *__restrict__ nv4, const double *__restrict__ vtab,
+                                               const double *__restrict__ t, int do_ring, int do_xring,
+                                               double *__restrict__ g_rq, double *__restrict__ g_xq,
+                                               const uint8_t *__restrict__ active)
 {
-    const ChunkDev ch = phchunks[blockIdx.x];
-    if (!active[ch.solve]) return;
-    const SolveDev s = solves[ch.solve];
-    const int O = s.O, V = s.V;
-    __shared__ int4 nocc[64];
-    __shared__ double xs[kPhRows][64], ys[kPhRows][64];
-    for (int k = threadIdx.x; k < O; k += blockDim.x) nocc[k] = nv4[s.orb0 + k];
+    const RingPairDev P = pairs[blockIdx.x];
+    if (!active[P.solve]) return;
+    const SolveDev s = solves[P.solve];
+    const int O = s.O;
+    const int R = P.n1 + P.n2;
+    // shared-memory strides are odd so that consecutive threads hit distinct banks
+    const int ld = O | 1, lr = R | 1;
+    extern __shared__ double smem[];
+    double *sv = smem;                                   // kVtabSmem
+    double *Vo = sv + kVtabSmem;                         // O x ld : Vo[k*ld + j] = v(n_k - n_j)
+    double *W1 = Vo + O * ld;                            // O x ld : W_Q[k][l]
+    double *W2 = W1 + O * ld;                            // O x ld : W_-Q[k][l]
+    double *XT = W2 + O * ld;                            // O x lr : X[r][k] at k*lr + r
+    double *YT = XT + O * lr;                            // O x lr
+    double *A1 = YT + O * lr;                            // kRingCh x ld
+    double *A2 = A1 + kRingCh * ld;
+    double *A3 = A2 + kRingCh * ld;
+    double *Sx = A3 + kRingCh * ld;                      // R
+    double *Sy = Sx + R;                                 // R
+    double *Vd = Sy + R;                                 // R
+    int *ri = (int *)(Vd + R);                           // R
+    int *rx = ri + R;                                    // R
+    int4 *no = (int4 *)(((uintptr_t)(rx + R) + 15) & ~(uintptr_t)15);  // O occupied n-vectors
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const bool vsm = s.q2max < kVtabSmem;
+    if (vsm)
+        for (int q = tid; q <= s.q2max; q += nt) sv[q] = vtab[s.vtab0 + q];
+    for (int k = tid; k < O; k += nt) no[k] = nv4[s.orb0 + k];
+    for (int r = tid; r < R; r += nt) {
+        const int64_t row = s.phr0 + (r < P.n1 ? P.r1 + r : P.r2 + r - P.n1);
+        ri[r] = ph_i[row];
+        rx[r] = ph_x[row];
+    }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = ch.start + warp;
-    if (r >= O * V) return;  // no barrier below this point
-    const int64_t row = s.phr0 + r;
-    const int64_t vrow = s.ph0 + (int64_t)r * O;
-    const int i = ph_i[row], x = ph_x[row];
-    const int4 ni = nv4[s.orb0 + i], nx = nv4[s.orb0 + x];
-    double sx = 0.0, sy = 0.0;
-    for (int k = lane; k < O; k += 32) {
-        int p = posmap(s, pos, i, k, x);
+    auto V = [&](int q2) -> double { return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : vtab[s.vtab0 + q2]); };
+    // Q of group 1 = n_x - n_i of its first row
+    const int4 qa = nv4[s.orb0 + rx[0]], qb = nv4[s.orb0 + ri[0]];
+    const int Qx = qa.x - qb.x, Qy = qa.y - qb.y, Qz = qa.z - qb.z;
+    for (int e = tid; e < O * O; e += nt) {
+        const int k = e / O, l = e % O;
+        const int4 nk = no[k], nl = no[l];
+        const int dx = nk.x - nl.x, dy = nk.y - nl.y, dz = nk.z - nl.z;
+        Vo[k * ld + l] = V(dx * dx + dy * dy + dz * dz);
+        const int ax = dx - Qx, ay = dy - Qy, az = dz - Qz;
+        W1[k * ld + l] = V(ax * ax + ay * ay + az * az);
+        const int bx = dx + Qx, by = dy + Qy, bz = dz + Qz;
+        W2[k * ld + l] = V(bx * bx + by * by + bz * bz);
+    }
+    // X, Y rows (stored transposed)
+    for (int e = tid; e < R * O; e += nt) {
+        const int k = e / R, r = e % R;
+        const int p = posmap(s, pos, ri[r], k, rx[r]);
         double xv = 0.0, yv = 0.0;
         if (p >= 0) {
             xv = t[p];
             yv = t[partner[p]];
         }
-        xs[warp][k] = xv;
-        ys[warp][k] = yv;
-        sx += xv;
-        sy += yv;
+        XT[k * lr + r] = xv;
+        YT[k * lr + r] = yv;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        sx += __shfl_xor_sync(0xffffffffu, sx, o);
-        sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    }
-    __syncwarp();
-    const double vd = vtab[s.vtab0 + q2_of(ni, nx)];
-    const double base = vd * (2.0 * sx - sy);
-    const int bx = ni.x - nx.x, by = ni.y - nx.y, bz = ni.z - nx.z;  // n_i - n_x
-    for (int j = lane; j < O; j += 32) {
-        const int4 nj = nocc[j];
-        double ex = 0.0, ey = 0.0, xw = 0.0, yw = 0.0;
+    __syncthreads();
+    for (int r = tid; r < R; r += nt) {
+        double sx = 0.0, sy = 0.0;
         for (int k = 0; k < O; k++) {
-            const int4 nk = nocc[k];
-            const double xk = xs[warp][k], yk = ys[warp][k];
-            const double vkj = vtab[s.vtab0 + q2_of(nk, nj)];
-            const int qx = bx + nk.x - nj.x, qy = by + nk.y - nj.y, qz = bz + nk.z - nj.z;
-            // n_i + n_k - n_x lies in the basis exactly when (i,k,x) is allowed; otherwise
-            // X[k] = Y[k] = 0 and |q|^2 may exceed the table, so the term is skipped.
-            const int q2 = qx * qx + qy * qy + qz * qz;
-            const double ve = (q2 <= s.q2max) ? vtab[s.vtab0 + q2] : 0.0;
-            ex = fma(vkj, xk, ex);
-            ey = fma(vkj, yk, ey);
-            xw = fma(xk, ve, xw);
-            yw = fma(yk, ve, yw);
+            sx += XT[k * lr + r];
+            sy += YT[k * lr + r];
         }
-        const int64_t o = vrow + j;
-        X[o] = xs[warp][j];
-        Y[o] = ys[warp][j];
-        Ex[o] = ex;
-        Ey[o] = ey;
-        A1[o] = 2.0 * base - 2.0 * xw + yw;
-        A2[o] = base - xw;
-        A3[o] = yw;
+        Sx[r] = sx;
+        Sy[r] = sy;
+        const int4 ni = nv4[s.orb0 + ri[r]], nx = nv4[s.orb0 + rx[r]];
+        Vd[r] = V(q2_of(ni, nx));
     }
-    if (lane == 0) {
-        Sx[row] = sx;
-        Sy[row] = sy;
+    __syncthreads();
+    // two directions: rows of group 1 against group 2, then the reverse
+    for (int dir = 0; dir < 2; dir++) {
+        const int a0 = dir == 0 ? 0 : P.n1, na = dir == 0 ? P.n1 : P.n2;
+        const int b0 = dir == 0 ? P.n1 : 0, nb = dir == 0 ? P.n2 : P.n1;
+        const double *W = dir == 0 ? W1 : W2;
+        for (int c0 = 0; c0 < na; c0 += kRingCh) {
+            const int nc = min(kRingCh, na - c0);
+            // A rows of the chunk: XW, YW with the chunk group's exchange kernel
+            for (int e = tid; e < nc * O; e += nt) {
+                const int rr = e / O, l = e % O;
+                const int r = a0 + c0 + rr;
+                double xw = 0.0, yw = 0.0;
+                for (int k = 0; k < O; k++) {
+                    const double w = W[k * ld + l];
+                    xw = fma(XT[k * lr + r], w, xw);
+                    yw = fma(YT[k * lr + r], w, yw);
+                }
+                const double base = Vd[r] * (2.0 * Sx[r] - Sy[r]);
+                A1[rr * ld + l] = 2.0 * base - 2.0 * xw + yw;
+                A2[rr * ld + l] = base - xw;
+                A3[rr * ld + l] = yw;
+            }
+            __syncthreads();
+            for (int e = tid; e < nc * nb; e += nt) {
+                const int rr = e / nb, r2 = b0 + e % nb;
+                const int r1 = a0 + c0 + rr;
+                const int i1 = ri[r1], i2 = ri[r2];
+                double quad = 0.0, xquad = 0.0, ex12 = 0.0, ex21 = 0.0, ey12 = 0.0, ey21 = 0.0;
+                for (int l = 0; l < O; l++) {
+                    const double x2 = XT[l * lr + r2], y2 = YT[l * lr + r2];
+                    quad = fma(A1[rr * ld + l], x2, quad);
+                    quad = fma(-A2[rr * ld + l], y2, quad);
+                    xquad = fma(A3[rr * ld + l], y2, xquad);
+                    const double vo12 = Vo[l * ld + i2], vo21 = Vo[l * ld + i1];
+                    ex12 = fma(vo12, XT[l * lr + r1], ex12);   // Ex_r1[i2]
+                    ey12 = fma(vo12, YT[l * lr + r1], ey12);   // Ey_r1[i2]
+                    ex21 = fma(vo21, x2, ex21);                // Ex_r2[i1]
+                    ey21 = fma(vo21, y2, ey21);                // Ey_r2[i1]
+                }
+                if (do_ring) {
+                    const double vd = Vd[r1];
+                    const double lin = 2.0 * vd * (Sx[r1] + Sx[r2]) - vd * (Sy[r1] + Sy[r2]) - ex12 - ex21;
+                    const int p = posmap(s, pos, i1, i2, rx[r1]);
+                    if (p >= 0) g_rq[p] = lin + quad;
+                }
+                if (do_xring) {
+                    const int p = posmap(s, pos, i1, i2, rx[r2]);
+                    if (p >= 0) g_xq[p] = -ey12 - ey21 + xquad;
+                }
+            }
+            __syncthreads();
+        }
     }
 }
 
-// 16 x 16 output pairs per CTA (256 threads); rows staged in shared memory.
-constexpr int kRT = 16;
-__global__ void __launch_bounds__(kRT * kRT) k_ring_quad(
-    const RingTile *__restrict__ tiles, const SolveDev *__restrict__ solves, const int16_t *__restrict__ ph_i,
-    const int16_t *__restrict__ ph_x, const int32_t *__restrict__ pos, const double *__restrict__ X,
-    const double *__restrict__ Y, const double *__restrict__ A1, const double *__restrict__ A2,
-    const double *__restrict__ A3, int do_ring, int do_xring, double *__restrict__ g_rq,
-    double *__restrict__ g_xq, const uint8_t *__restrict__ active)
+void set_rings_smem_limit(size_t bytes)
 {
-    const RingTile T = tiles[blockIdx.x];
-    if (!active[T.solve]) return;
-    const SolveDev s = solves[T.solve];
-    const int O = s.O;
-    const int ld = O + 1;
-    extern __shared__ double sm[];
-    double *a1 = sm, *a2 = a1 + kRT * ld, *a3 = a2 + kRT * ld, *xr = a3 + kRT * ld, *yr = xr + kRT * ld;
-    for (int e = threadIdx.x; e < kRT * O; e += blockDim.x) {
-        const int rr = e / O, l = e % O;
-        double v1 = 0.0, v2 = 0.0, v3 = 0.0, vx = 0.0, vy = 0.0;
-        if (rr < T.n1) {
-            const int64_t o = s.ph0 + (int64_t)(T.r1 + rr) * O + l;
-            v1 = A1[o];
-            v2 = A2[o];
-            v3 = A3[o];
-        }
-        if (rr < T.n2) {
-            const int64_t o = s.ph0 + (int64_t)(T.r2 + rr) * O + l;
-            vx = X[o];
-            vy = Y[o];
-        }
-        a1[rr * ld + l] = v1;
-        a2[rr * ld + l] = v2;
-        a3[rr * ld + l] = v3;
-        xr[rr * ld + l] = vx;
-        yr[rr * ld + l] = vy;
+    // keep the largest limit ever requested: batches of different sizes coexist
+    static size_t current = 0;
+    if (bytes > current) {
+        cudaFuncSetAttribute(k_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        current = bytes;
     }
-    __syncthreads();
-    const int ty = threadIdx.x / kRT, tx = threadIdx.x % kRT;
-    if (ty >= T.n1 || tx >= T.n2) return;
-    double ring = 0.0, xring = 0.0;
-    for (int l = 0; l < O; l++) {
-        const double yv = yr[tx * ld + l];
-        ring = fma(a1[ty * ld + l], xr[tx * ld + l], ring);
-        ring = fma(-a2[ty * ld + l], yv, ring);
-        xring = fma(a3[ty * ld + l], yv, xring);
-    }
-    const int64_t r1 = s.phr0 + T.r1 + ty, r2 = s.phr0 + T.r2 + tx;
-    const int i = ph_i[r1], x1 = ph_x[r1], j = ph_i[r2], x2 = ph_x[r2];
-    if (do_ring) {
-        const int p = posmap(s, pos, i, j, x1);  // amplitude (i,j,a=x1), partner x2
-        if (p >= 0) g_rq[p] = ring;
-    }
-    if (do_xring) {
-        const int p = posmap(s, pos, i, j, x2);  // amplitude (i,j,a=x2), partner x1
-        if (p >= 0) g_xq[p] = xring;
-    }
+}
+
+size_t rings_smem_bytes(int O, int R)
+{
+    const int ld = O | 1, lr = R | 1;
+    return sizeof(double) * ((size_t)kVtabSmem + 3 * O * ld + 2 * O * lr + 3 * kRingCh * ld + 3 * R) +
+           sizeof(int) * 2 * R + 16 + sizeof(int4) * O;
 }
 
 // ----------------------------------------------------------------------------
@@ -607,8 +640,7 @@ struct UpdateArgs {
     const double *J1, *J2, *J3;
     double *part_e, *part_dt, *part_r;
     double *g_out;            // optional: full G per amplitude (term checks)
-    const int32_t *phrow_of;
-    const double *Sx, *Sy, *Ex, *Ey, *g_rq, *g_xq;
+    const double *g_rq, *g_xq;
     const uint8_t *active;
     int do_ladder, do_mosaic, do_ring, do_xring, do_driver, drpa, mode;
 };
@@ -652,21 +684,8 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
                 }
             }
         } else {
-            const int V = s.V;
-            const int64_t pr = s.phr0, pv = s.ph0;
-            const int r_ia = A.phrow_of[pr + i * V + (a - O)];
-            const int r_jb = A.phrow_of[pr + j * V + (b - O)];
-            if (A.do_ring) {
-                // linear rings (CCD.f90:716-763) and quadratic rings (CCD.f90:771-811)
-                g += 2.0 * via * (A.Sx[pr + r_ia] + A.Sx[pr + r_jb]) - via * (A.Sy[pr + r_ia] + A.Sy[pr + r_jb]) -
-                     A.Ex[pv + (int64_t)r_ia * O + j] - A.Ex[pv + (int64_t)r_jb * O + i] + A.g_rq[p];
-            }
-            if (A.do_xring) {
-                // linear crossed rings (CCD.f90:845-892) and quadratic crossed rings (CCD.f90:899-937)
-                const int r_ib = A.phrow_of[pr + i * V + (b - O)];
-                const int r_ja = A.phrow_of[pr + j * V + (a - O)];
-                g += -A.Ey[pv + (int64_t)r_ib * O + j] - A.Ey[pv + (int64_t)r_ja * O + i] + A.g_xq[p];
-            }
+            if (A.do_ring) g += A.g_rq[p];   // rings, linear + quadratic (CCD.f90:716-811)
+            if (A.do_xring) g += A.g_xq[p];  // crossed rings (CCD.f90:845-937)
         }
         if (A.g_out) A.g_out[p] = g;
         const double *ev = A.eigen + s.orb0;
@@ -832,7 +851,7 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
 
 const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh", "k_ladder",
                                       "k_mosaic_s", "k_mosaic_reduce", "k_ring_int", "k_update",
-                                      "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad"};
+                                      "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad", "k_rings"};
 
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt)
@@ -872,18 +891,12 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         n++;
     }
     if ((f.do_ring || f.do_xring) && !f.drpa) {
-        kt->begin(KID_PH_BUILD, st);
-        k_ph_build<<<d.nphchunks, 32 * kPhRows, 0, st>>>(d.phchunks, d.solves, d.ph_i, d.ph_x, d.pos, d.partner,
-                                                          d.nv4, d.vtab, d.t, d.X, d.Y, d.Ex, d.Ey, d.J1, d.J2,
-                                                          d.J3, d.Sx, d.Sy, d.active);
+        kt->begin(KID_RINGS, st);
+        k_rings<<<d.nrpairs, 256, d.rings_smem, st>>>(d.rpairs, d.solves, d.ph_i, d.ph_x, d.pos, d.partner, d.nv4,
+                                                       d.vtab, d.t, f.do_ring, f.do_xring, d.g_rq, d.g_xq,
+                                                       d.active);
         kt->end(st);
-        kt->begin(KID_RING_QUAD, st);
-        size_t smem = (size_t)5 * kRT * (d.max_occ + 1) * sizeof(double);
-        k_ring_quad<<<d.nrtiles, kRT * kRT, smem, st>>>(d.rtiles, d.solves, d.ph_i, d.ph_x, d.pos, d.X, d.Y, d.J1,
-                                                         d.J2, d.J3, f.do_ring, f.do_xring, d.g_rq, d.g_xq,
-                                                         d.active);
-        kt->end(st);
-        n += 2;
+        n++;
     }
     UpdateArgs A;
     A.chunks = d.chunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.pos = d.pos;
@@ -892,7 +905,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
-    A.phrow_of = d.phrow_of; A.Sx = d.Sx; A.Sy = d.Sy; A.Ex = d.Ex; A.Ey = d.Ey; A.g_rq = d.g_rq; A.g_xq = d.g_xq;
+    A.g_rq = d.g_rq; A.g_xq = d.g_xq;
     kt->begin(KID_UPDATE, st);
     k_update<<<d.nchunks, kChunk, 0, st>>>(A);
     kt->end(st);

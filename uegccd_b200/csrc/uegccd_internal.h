@@ -53,11 +53,13 @@ struct AmpInfo {
     int16_t i, j, a, b;
 };
 
-// One output tile of the ring/crossed-ring quadratic products: rows [r1, r1+n1) of the
-// ph group of momentum Q against rows [r2, r2+n2) of the group of -Q (rows local to the solve).
-struct RingTile {
+// One pair of particle-hole groups {Q, -Q}: rows [r1, r1+n1) have n_x - n_i = Q,
+// rows [r2, r2+n2) have -Q (rows local to the solve).  All ring and crossed-ring
+// products between the two groups are formed by one CTA.
+struct RingPairDev {
     int solve;
-    int r1, n1, r2, n2;
+    int r1, n1;
+    int r2, n2;
 };
 
 struct ChunkDev {
