@@ -68,6 +68,22 @@ def twists(n: int, seed: int = SEED, rank: int = 0):
     return rng.random((n, 3)) - 0.5
 
 
+def reduce_max(values):
+    """Max over ranks of each value (gloo/NCCL all-reduce); identity on one process."""
+    try:
+        import torch.distributed as dist
+
+        if not (dist.is_available() and dist.is_initialized()):
+            return list(values)
+        import torch
+
+        t = torch.tensor(list(values), dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return [float(x) for x in t]
+    except ImportError:
+        return list(values)
+
+
 def build_systems(tw):
     from uegccd_b200 import heg
 
@@ -229,15 +245,7 @@ def run_gpu(args, rank, world):
         b2.close()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         h2d, d2h = hb, db
-    e_max = total_ms
-    if dist:
-        import torch
-
-        t = torch.tensor([total_ms, float(np.mean(e2e_ms))], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_max, e2e_mean = float(t[0]), float(t[1])
-    else:
-        e2e_mean = float(np.mean(e2e_ms))
+    e_max, e2e_mean = reduce_max([total_ms, float(np.mean(e2e_ms))])
     solves_total = args.twists * world * args.steps
     value = solves_total / (e_max / 1e3)
     e2e_value = args.twists * world / (e2e_mean / 1e3)

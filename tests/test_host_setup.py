@@ -1,0 +1,71 @@
+"""The product's host set-up (include/uegccd_host.h: ReadInput, init_HEG, change_rs,
+ChangeTwist) reproduces the reference -- checked against the oracle and the goldens."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, parse_input_text
+from uegccd_b200 import _capi, heg
+
+
+def _write(tmp_path, text, name="Input"):
+    p = tmp_path / name
+    p.write_text(text)
+    return str(p)
+
+
+def _g5_input_text(g):
+    lines = [f"{k}: {v}" for k, v in g["G5"]["keys"].items()]
+    return "\n".join(lines) + "\n"
+
+
+def test_read_input_benchmark_key_set(goldens, tmp_path):
+    inp = heg.read_input(_write(tmp_path, goldens["G1"]["input_text"]), require_all=False)
+    assert (inp.nelectron, inp.maxkpoint, inp.do_drpa_sosex, inp.do_mosaic) == (14, 5, 1, 0)
+    with pytest.raises(_capi.UegccdError, match="not set"):
+        heg.read_input(_write(tmp_path, goldens["G1"]["input_text"]), require_all=True)
+
+
+def test_read_input_errors(tmp_path):
+    with pytest.raises(_capi.UegccdError, match="closed shell"):
+        heg.read_input(_write(tmp_path, "# Electrons: 13\n"), require_all=False)
+    with pytest.raises(_capi.UegccdError, match="not recognized"):
+        heg.read_input(_write(tmp_path, "# Electrons: 14\nBogus Key: 3\n"), require_all=False)
+    with pytest.raises(_capi.UegccdError, match="No Input file"):
+        heg.read_input(str(tmp_path / "missing"), require_all=False)
+
+
+@pytest.mark.parametrize("which", ["G1", "G3", "G5"])
+def test_setup_matches_oracle_bitwise(goldens, which):
+    if which == "G5":
+        vals = parse_input_text("")
+        vals.update(goldens["G5"]["keys"])
+        inp = heg.default_input(nelectron=24, fcut2ecut=1, fcut=2.0, rsmin=5.0, rsmax=5.0,
+                                ntwist=(0.1, 0.2, 0.45))
+    else:
+        vals = parse_input_text(goldens[which]["input_text"])
+        inp = heg.default_input(nelectron=int(vals["# Electrons"]), maxkpoint=int(vals["Momentum Cutoff"]),
+                                rsmin=float(vals["rSMin"]), rsmax=float(vals["rSMax"]),
+                                ntwist=[float(x) for x in vals["NTwist"].split()])
+    o = Oracle(vals)
+    h = heg.Heg(inp)
+    nocc, L, mad, eig, nv = h.system()
+    sc = o.scalars()
+    assert (nocc, len(eig)) == (o.nocc, o.nao)
+    assert (L, mad, h.info()["ehf"]) == (sc["L"], sc["madelung"], sc["ehf"])
+    np.testing.assert_array_equal(eig, o.eigen())
+    np.testing.assert_array_equal(nv, o.nvec())
+    if which == "G5":
+        np.testing.assert_array_equal(eig, np.array(goldens["G5"]["eigen"]))
+        for tw in goldens["G5"]["ta_twists"][:4]:
+            h.change_twist(tw)
+            o.change_twist(tw)
+            np.testing.assert_array_equal(h.system()[3], o.eigen())
+            assert h.info()["ehf"] == o.scalars()["ehf"]
+
+
+def test_find_tol():
+    assert heg.find_tol(1.0) == (1e-8, 100.0, 2.0)     # HEG.f90:1078-1079
+    assert heg.find_tol(5.5) == (1e-6, 100.0, 5.0)
+    assert heg.find_tol(0.5)[1] == 1e6
