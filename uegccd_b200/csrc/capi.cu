@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/uegccd.h"
@@ -26,6 +27,22 @@ using namespace uegccd;
 namespace {
 
 thread_local std::string g_last_error;
+
+// Runs f(0..n-1) on up to nthreads host threads (static interleaved split).
+template <class F>
+void parallel_for(int n, int nthreads, F f)
+{
+    if (nthreads <= 1 || n <= 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++)
+        th.emplace_back([&, t]() {
+            for (int i = t; i < n; i += nthreads) f(i);
+        });
+    for (auto &x : th) x.join();
+}
 
 int fail(int code, const std::string &msg)
 {
@@ -77,12 +94,27 @@ struct UegccdBatch {
     int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the calls so far
     KernelTimer kt;
     bool kt_events = false;
-    // Pulay DIIS history (allocated on first use)
+    // device-side iteration control (allocated on first solve; DIIS history grows on demand)
+    CtlBuffers ctl;
     int diis_cap = 0;
-    double *hist_t = nullptr, *hist_e = nullptr, *diis_part = nullptr, *diis_brow = nullptr, *diis_coef = nullptr;
+    // CUDA graphs of one iteration: plain and with kernel timers, keyed by the options
+    struct GraphKey {
+        int do_ring, do_xring, do_ladder, do_mosaic, drpa, ndiis, max_iter;
+        double tol;
+        bool operator==(const GraphKey &o) const
+        {
+            return do_ring == o.do_ring && do_xring == o.do_xring && do_ladder == o.do_ladder &&
+                   do_mosaic == o.do_mosaic && drpa == o.drpa && ndiis == o.ndiis && max_iter == o.max_iter &&
+                   tol == o.tol;
+        }
+    } gkey{};
+    bool have_graph = false;
+    cudaGraphExec_t gexec = nullptr;
+    int g_launches = 0;          // kernels per iteration
 
     ~UegccdBatch()
     {
+        if (gexec) cudaGraphExecDestroy(gexec);
         if (kt_events)
             for (auto &e : kt.ev) cudaEventDestroy(e);
         for (void *p : allocs) cudaFree(p);
@@ -147,8 +179,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     for (int s = 0; s < n; s++) {
         rc = read_system(&systems[s], b->sys[s]);
         if (rc) return rc;
-        std::string msg = build_solve_plan(b->sys[s], b->plans[s]);
-        if (!msg.empty()) return fail(UEGCCD_ERR_ARG, "system " + std::to_string(s) + ": " + msg);
+    }
+    // plans of different systems are independent: build them on parallel host threads
+    const int nthreads = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
+    std::vector<std::string> msgs(n);
+    parallel_for(n, nthreads, [&](int s) { msgs[s] = build_solve_plan(b->sys[s], b->plans[s]); });
+    for (int s = 0; s < n; s++) {
+        if (!msgs[s].empty()) return fail(UEGCCD_ERR_ARG, "system " + std::to_string(s) + ": " + msgs[s]);
         if (b->plans[s].O > 64) return fail(UEGCCD_ERR_UNSUPPORTED, "NOcc > 64 is outside the hole-hole ladder tiling");
     }
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
@@ -174,6 +211,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     size_t rings_smem = 0;
     int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0;
     int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_occ = 0;
+    // offsets of each solve in the large concatenated arrays (filled in parallel below)
+    std::vector<int64_t> s_amp0(n), s_pos0(n), s_phr0(n);
     for (int s = 0; s < n; s++) {
         const SolvePlan &P = b->plans[s];
         const SystemHost &H = b->sys[s];
@@ -194,8 +233,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         S.denom_factor = 2.0;
         S.phr0 = phr0;
         max_occ = std::max(max_occ, P.O);
-        ph_i.insert(ph_i.end(), P.ph_i.begin(), P.ph_i.end());
-        ph_x.insert(ph_x.end(), P.ph_x.begin(), P.ph_x.end());
+        s_amp0[s] = amp0;
+        s_pos0[s] = pos0;
+        s_phr0[s] = phr0;
         for (size_t gi = 0; gi < P.groups.size(); gi++) {
             const auto &G = P.groups[gi];
             if (G.partner < 0 || G.partner < (int)gi) continue;  // each {Q, -Q} once
@@ -224,12 +264,6 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         pair_i.insert(pair_i.end(), P.pair_i.begin(), P.pair_i.end());
         pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
         vir.insert(vir.end(), P.vir.begin(), P.vir.end());
-        for (int32_t x : P.pos) pos.push_back(x >= 0 ? (int32_t)(x + amp0) : -1);
-        for (const AmpInfo &q : P.amps) {
-            amps.push_back(q);
-            int32_t pb = P.pos[((size_t)q.i * P.O + q.j) * P.V + (q.b - P.O)];
-            partner.push_back((int32_t)(pb + amp0));
-        }
         for (int p = 0; p < P.M; p++) nv4.push_back(make_int4(H.n[p][0], H.n[p][1], H.n[p][2], 0));
         eigen.insert(eigen.end(), H.eigen.begin(), H.eigen.end());
         vtab.insert(vtab.end(), P.vtab.begin(), P.vtab.end());
@@ -248,6 +282,24 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         if (amp0 >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit packed indices");
     }
     chunk_begin[n] = (int)chunks.size();
+    pos.resize(pos0);
+    amps.resize(amp0);
+    partner.resize(amp0);
+    ph_i.resize(phr0);
+    ph_x.resize(phr0);
+    parallel_for(n, nthreads, [&](int s) {
+        const SolvePlan &P = b->plans[s];
+        const int64_t a0 = s_amp0[s];
+        int32_t *pdst = pos.data() + s_pos0[s];
+        for (size_t k = 0; k < P.pos.size(); k++) pdst[k] = P.pos[k] >= 0 ? (int32_t)(P.pos[k] + a0) : -1;
+        for (size_t k = 0; k < P.amps.size(); k++) {
+            const AmpInfo &q = P.amps[k];
+            amps[a0 + k] = q;
+            partner[a0 + k] = (int32_t)(P.pos[((size_t)q.i * P.O + q.j) * P.V + (q.b - P.O)] + a0);
+        }
+        std::copy(P.ph_i.begin(), P.ph_i.end(), ph_i.begin() + s_phr0[s]);
+        std::copy(P.ph_x.begin(), P.ph_x.end(), ph_x.begin() + s_phr0[s]);
+    });
 
     DevBatch &d = b->d;
     d.nsolves = n;
@@ -385,66 +437,61 @@ int validate_options(const UegccdOptions *o, int drpa)
     return 0;
 }
 
-int diis_alloc(UegccdBatch &b, int ndiis)
+int ctl_alloc(UegccdBatch &b, int ndiis, int max_rec)
 {
-    if (b.diis_cap >= ndiis) return 0;
+    CtlBuffers &c = b.ctl;
+    const int n = b.d.nsolves;
     int rc;
-    if ((rc = b.alloc(b.hist_t, (size_t)ndiis * b.d.namp))) return rc;
-    if ((rc = b.alloc(b.hist_e, (size_t)ndiis * b.d.namp))) return rc;
-    if ((rc = b.alloc(b.diis_part, (size_t)b.d.nchunks * kDiisMax))) return rc;
-    if ((rc = b.alloc(b.diis_brow, (size_t)b.d.nsolves * kDiisMax))) return rc;
-    if ((rc = b.alloc(b.diis_coef, (size_t)b.d.nsolves * kDiisMax))) return rc;
-    b.diis_cap = ndiis;
+    if (!c.state) {
+        if ((rc = b.alloc(c.state, n))) return rc;
+        if ((rc = b.alloc(c.active_next, n))) return rc;
+        if ((rc = b.alloc(c.count, 1))) return rc;
+        if ((rc = b.alloc(c.Bm, (size_t)n * kDiisMax * kDiisMax))) return rc;
+        if ((rc = b.alloc(c.coef, (size_t)n * kDiisMax))) return rc;
+        if ((rc = b.alloc(c.brow, (size_t)n * kDiisMax))) return rc;
+        if ((rc = b.alloc(c.part, (size_t)b.d.nchunks * kDiisMax))) return rc;
+    }
+    if (max_rec > c.max_rec) {
+        if ((rc = b.alloc(c.rec_e, (size_t)n * max_rec))) return rc;
+        if ((rc = b.alloc(c.rec_dt, (size_t)n * max_rec))) return rc;
+        c.max_rec = max_rec;
+    }
+    if (ndiis > b.diis_cap) {
+        if ((rc = b.alloc(c.hist_t, (size_t)ndiis * b.d.namp))) return rc;
+        if ((rc = b.alloc(c.hist_e, (size_t)ndiis * b.d.namp))) return rc;
+        b.diis_cap = ndiis;
+    }
     return 0;
 }
 
-// Pulay coefficients: minimise |sum c_j e_j|^2 subject to sum c_j = 1, i.e.
-// [B 1; 1 0] [c; lambda] = [0; 1] with B_jk = e_j . e_k (scaled by max diag).
-// Returns false when the system is numerically singular.
-bool pulay_solve(const std::vector<double> &Bfull, int nvec, double *c)
+// Captures one iteration as a CUDA graph.
+int capture_iteration(UegccdBatch &b, const TermFlags &f, double tol, int max_iter, int ndiis)
 {
-    const int n = nvec + 1;
-    double scale = 0.0;
-    for (int j = 0; j < nvec; j++) scale = std::max(scale, Bfull[j * kDiisMax + j]);
-    if (!(scale > 0.0) || !std::isfinite(scale)) return false;
-    std::vector<double> A((size_t)n * n, 0.0), r(n, 0.0);
-    for (int j = 0; j < nvec; j++) {
-        for (int k = 0; k < nvec; k++) A[j * n + k] = Bfull[j * kDiisMax + k] / scale;
-        A[j * n + nvec] = 1.0;
-        A[nvec * n + j] = 1.0;
-    }
-    r[nvec] = 1.0;
-    for (int k = 0; k < n; k++) {
-        int piv = k;
-        for (int i = k + 1; i < n; i++)
-            if (std::fabs(A[i * n + k]) > std::fabs(A[piv * n + k])) piv = i;
-        if (std::fabs(A[piv * n + k]) < 1e-14) return false;
-        if (piv != k) {
-            for (int j = 0; j < n; j++) std::swap(A[k * n + j], A[piv * n + j]);
-            std::swap(r[k], r[piv]);
-        }
-        for (int i = k + 1; i < n; i++) {
-            double f = A[i * n + k] / A[k * n + k];
-            for (int j = k; j < n; j++) A[i * n + j] -= f * A[k * n + j];
-            r[i] -= f * r[k];
-        }
-    }
-    for (int k = n - 1; k >= 0; k--) {
-        double x = r[k];
-        for (int j = k + 1; j < n; j++) x -= A[k * n + j] * r[j];
-        r[k] = x / A[k * n + k];
-    }
-    for (int j = 0; j < nvec; j++) {
-        if (!std::isfinite(r[j])) return false;
-        c[j] = r[j];
-    }
-    return true;
+    UegccdBatch::GraphKey key{f.do_ring, f.do_xring, f.do_ladder, f.do_mosaic, f.drpa, ndiis, max_iter, tol};
+    if (b.have_graph && b.gkey == key) return 0;
+    if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+    int nl = launch_iteration(b.d, b.ctl, f, tol, max_iter, ndiis, b.stream, nullptr);
+    cudaError_t e = cudaStreamEndCapture(b.stream, &g);
+    if (e != cudaSuccess) return fail(UEGCCD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b.gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(UEGCCD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    b.g_launches = nl;
+    b.gkey = key;
+    b.have_graph = true;
+    return 0;
 }
 
 // Runs the iteration for all solves of the batch from the amplitudes in d.t.
-// drpa: 0 CCD, 1 dRPA.  Per-solve results in res[]; records of solve 0 in opt.
+// Iteration control lives on the device; the host replays a captured iteration
+// graph kPoll times between polls of the number of active solves.  With kernel
+// timing on, the last iteration of each round runs as direct launches between
+// CUDA events: that iteration is the sample the per-kernel times come from.
 int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult *res)
 {
+    constexpr int kPoll = 4;
     DevBatch &d = b.d;
     const int n = d.nsolves;
     TermFlags f;
@@ -454,111 +501,50 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     f.do_ladder = (!drpa && opt->do_ladder) ? 1 : 0;
     f.do_ring = opt->do_ring ? 1 : 0;
     f.do_xring = (!drpa && opt->do_xring) ? 1 : 0;
+    const int ndiis = opt->scheme == UEGCCD_DIIS ? opt->ndiis : 0;
+    const int max_rec = std::min(opt->max_iter, 1100);
+    int rc = ctl_alloc(b, ndiis, max_rec);
+    if (rc) return rc;
     for (int s = 0; s < n; s++) b.hsolves[s].denom_factor = opt->denom_factor;
     CU(cudaMemcpyAsync(d.solves, b.hsolves.data(), n * sizeof(SolveDev), cudaMemcpyHostToDevice, b.stream));
-    int rc = set_active_all(b, 1);
-    if (rc) return rc;
+    std::vector<IterState> st0(n, IterState{1, 0, 0.0, 0.0});
+    CU(cudaMemcpyAsync(b.ctl.state, st0.data(), n * sizeof(IterState), cudaMemcpyHostToDevice, b.stream));
+    CU(cudaMemsetAsync(b.ctl.Bm, 0, (size_t)n * kDiisMax * kDiisMax * sizeof(double), b.stream));
+    if ((rc = set_active_all(b, 1))) return rc;
+    if ((rc = capture_iteration(b, f, opt->tol, opt->max_iter, ndiis))) return rc;
     b.launches = 0;
     CU(cudaEventRecord(b.ev0, b.stream));
     // CCEnergy of the start amplitudes and dT = max|T| (CCD.f90:63-64, dRPA.f90:68-69)
     launch_energy(d, drpa ? 1 : 0, 0.0, b.stream);
     launch_reduce(d, b.stream);
-    b.launches += 2;
-    if ((rc = read_red(b))) return rc;
-    std::vector<double> e(n), dt(n), rmax(n, 0.0);
-    std::vector<int> niter(n, 1);
-    for (int s = 0; s < n; s++) {
-        e[s] = b.red[3 * s];
-        dt[s] = b.red[3 * s + 1];
-    }
-    int nrec = 0;
-    auto record = [&](double en, double dtv) {
-        if (opt->max_rec > 0 && nrec < opt->max_rec) {
-            if (opt->energies) opt->energies[nrec] = en;
-            if (opt->dts) opt->dts[nrec] = dtv;
-            nrec++;
+    launch_control(d, b.ctl, opt->tol, opt->max_iter, ndiis, 1, b.stream);
+    launch_active_swap(d, b.ctl, b.stream);
+    b.launches += 4;
+    int count = n, rounds = 0;
+    const int max_rounds = opt->max_iter / kPoll + 2;
+    while (count > 0 && rounds < max_rounds) {
+        for (int k = 0; k < kPoll; k++) {
+            if (b.kt.on && k == kPoll - 1) {
+                // the sampled iteration of the round: direct launches between CUDA events
+                b.launches += launch_iteration(d, b.ctl, f, opt->tol, opt->max_iter, ndiis, b.stream, &b.kt);
+            } else {
+                CU(cudaGraphLaunch(b.gexec, b.stream));
+                b.launches += b.g_launches;
+            }
         }
-    };
-    record(e[0], dt[0]);
-    int nactive = 0;
-    for (int s = 0; s < n; s++) {
-        b.active[s] = (dt[s] >= opt->tol && niter[s] < opt->max_iter) ? 1 : 0;
-        nactive += b.active[s];
-    }
-    CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
-    int status = 0;
-    const bool diis = opt->scheme == UEGCCD_DIIS;
-    const int ndiis = diis ? opt->ndiis : 0;
-    std::vector<double> Bm, brow, coef;
-    if (diis) {
-        if ((rc = diis_alloc(b, ndiis))) return rc;
-        Bm.assign((size_t)n * kDiisMax * kDiisMax, 0.0);
-        brow.assign((size_t)n * kDiisMax, 0.0);
-        coef.assign((size_t)n * kDiisMax, 0.0);
-    }
-    int it = 0;
-    while (nactive > 0) {
-        b.launches += launch_residual(d, f, 0, nullptr, b.stream, &b.kt);
+        CU(cudaMemcpyAsync(&count, b.ctl.count, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+        b.d2h_bytes += sizeof(int);
+        CU(cudaStreamSynchronize(b.stream));
         CU(cudaGetLastError());
-        int slot = 0, nvec = 0;
-        if (diis) {
-            slot = it % ndiis;
-            nvec = std::min(it + 1, ndiis);
-            launch_diis_push(d, slot, nvec, b.hist_t, b.hist_e, b.diis_part, b.diis_brow, b.stream);
-            b.launches += 2;
-            CU(cudaMemcpyAsync(brow.data(), b.diis_brow, brow.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                               b.stream));
-            b.d2h_bytes += (int64_t)(brow.size() * sizeof(double));
-        } else {
-            std::swap(d.t, d.t_new);
-        }
-        if ((rc = read_red(b))) return rc;
-        std::vector<uint8_t> next = b.active;
-        nactive = 0;
-        for (int s = 0; s < n; s++) {
-            if (!b.active[s]) continue;
-            niter[s]++;
-            e[s] = b.red[3 * s];
-            dt[s] = b.red[3 * s + 1];
-            if (s == 0) record(e[s], dt[s]);
-            bool go = true;
-            if (!std::isfinite(e[s]) || !std::isfinite(dt[s])) {
-                go = false;
-                status = UEGCCD_ERR_NUMERIC;
-            } else if (!(dt[s] >= opt->tol && niter[s] < opt->max_iter)) {
-                go = false;
-            }
-            if (diis) {
-                double *B = &Bm[(size_t)s * kDiisMax * kDiisMax];
-                for (int j = 0; j < nvec; j++) B[slot * kDiisMax + j] = B[j * kDiisMax + slot] = brow[s * kDiisMax + j];
-                double *c = &coef[(size_t)s * kDiisMax];
-                for (int j = 0; j < kDiisMax; j++) c[j] = 0.0;
-                // converged, failed or first step: keep the plain step t = t'
-                if (!go || nvec < 2 || !pulay_solve(std::vector<double>(B, B + kDiisMax * kDiisMax), nvec, c)) {
-                    for (int j = 0; j < kDiisMax; j++) c[j] = 0.0;
-                    c[slot] = 1.0;
-                }
-            }
-            if (go) nactive++;
-            else next[s] = 0;
-        }
-        if (diis) {
-            CU(cudaMemcpyAsync(b.diis_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice,
-                               b.stream));
-            b.h2d_bytes += (int64_t)(coef.size() * sizeof(double));
-            launch_diis_extrap(d, b.hist_t, b.diis_coef, nvec, b.stream);
-            b.launches++;
-        }
-        b.active = next;
-        CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
-        it++;
+        b.kt.collect();
+        rounds++;
     }
     // final residual (CCD.f90:103-107, dRPA.f90:98-101)
     if ((rc = set_active_all(b, 1))) return rc;
     b.launches += launch_residual(d, f, 1, nullptr, b.stream, &b.kt);
     if ((rc = read_red(b))) return rc;
+    std::vector<double> rmax(n), esosex(n, 0.0);
     for (int s = 0; s < n; s++) rmax[s] = b.red[3 * s + 2];
-    std::vector<double> esosex(n, 0.0);
     if (drpa) {
         launch_energy(d, 1, 1.0, b.stream);
         launch_reduce(d, b.stream);
@@ -566,23 +552,40 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
         if ((rc = read_red(b))) return rc;
         for (int s = 0; s < n; s++) esosex[s] = b.red[3 * s];
     }
+    std::vector<IterState> st(n);
+    CU(cudaMemcpyAsync(st.data(), b.ctl.state, n * sizeof(IterState), cudaMemcpyDeviceToHost, b.stream));
+    int nrec = 0;
+    if (opt->max_rec > 0 && (opt->energies || opt->dts)) {
+        nrec = std::min(std::min(st[0].niter, max_rec), opt->max_rec);
+        std::vector<double> re(nrec), rd(nrec);
+        CU(cudaMemcpyAsync(re.data(), b.ctl.rec_e, nrec * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+        CU(cudaMemcpyAsync(rd.data(), b.ctl.rec_dt, nrec * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+        CU(cudaStreamSynchronize(b.stream));
+        for (int k = 0; k < nrec; k++) {
+            if (opt->energies) opt->energies[k] = re[k];
+            if (opt->dts) opt->dts[k] = rd[k];
+        }
+    }
     CU(cudaEventRecord(b.ev1, b.stream));
     CU(cudaEventSynchronize(b.ev1));
     float ms = 0.f;
     CU(cudaEventElapsedTime(&ms, b.ev0, b.ev1));
+    int status = 0;
     for (int s = 0; s < n; s++) {
         UegccdResult &r = res[s];
-        r.ecorr = e[s];
+        r.ecorr = st[s].e;
         r.max_res = rmax[s];
-        r.last_dt = dt[s];
-        r.niter = niter[s];
+        r.last_dt = st[s].dt;
+        r.niter = st[s].niter;
         r.fail = rmax[s] > opt->fail_ratio * opt->tol;
         r.ecorr_sosex = (drpa && !r.fail) ? esosex[s] : 0.0;
         r.n_recorded = (s == 0) ? nrec : 0;
         r.kernel_launches = b.launches;
         r.gpu_ms = ms;
-        if (status == 0 && (r.fail || niter[s] >= opt->max_iter)) status = UEGCCD_NOT_CONVERGED;
+        if (st[s].status == 3) status = UEGCCD_ERR_NUMERIC;
+        if (status == 0 && (r.fail || st[s].status == 2)) status = UEGCCD_NOT_CONVERGED;
     }
+    if (status == UEGCCD_ERR_NUMERIC) fail(status, "non-finite amplitudes or energy");
     return status;
 }
 
@@ -754,6 +757,7 @@ int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on)
     }
     b->kt.on = on != 0;
     for (int k = 0; k < KID_COUNT; k++) { b->kt.ms[k] = 0.0; b->kt.launches[k] = 0; }
+    b->have_graph = false;  // re-capture with (or without) the timer events
     return 0;
 }
 

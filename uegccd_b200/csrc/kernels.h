@@ -78,14 +78,35 @@ struct KernelTimer {
     {
         for (int k = 0; k < n; k++) {
             float t = 0.f;
-            cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]);
-            ms[kid[k]] += t;
-            launches[kid[k]]++;
+            if (cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]) == cudaSuccess) {
+                ms[kid[k]] += t;
+                launches[kid[k]]++;
+            } else {
+                cudaGetLastError();  // a missing sample is not an error of the solve
+            }
         }
         n = 0;
     }
 };
 extern const char *kKernelNames[KID_COUNT];
+
+// Per-solve iteration state kept on the device (see k_control).
+struct IterState {
+    int niter;      // NIter of the reference (1 before the first update)
+    int status;     // 0 running, 1 converged, 2 MaxIter reached, 3 non-finite
+    double e, dt;   // energy and max|dT| of the latest iteration
+};
+
+// Buffers of the device-side iteration control.
+struct CtlBuffers {
+    IterState *state = nullptr;
+    uint8_t *active_next = nullptr;
+    int *count = nullptr;
+    double *Bm = nullptr, *coef = nullptr, *brow = nullptr, *part = nullptr;
+    double *hist_t = nullptr, *hist_e = nullptr;
+    double *rec_e = nullptr, *rec_dt = nullptr;
+    int max_rec = 0;
+};
 
 struct TermFlags {
     int do_driver = 1, do_mosaic = 1, do_ladder = 1, do_pp = 1, do_hh = 1, do_ring = 1, do_xring = 1;
@@ -101,10 +122,12 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st);
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt = nullptr);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
-// Pulay DIIS: store (t_new, t_new - t) in slot, dot products with nvec stored errors -> brow
-void launch_diis_push(const DevBatch &d, int slot, int nvec, double *hist_t, double *hist_e, double *part,
-                      double *brow, cudaStream_t st);
-void launch_diis_extrap(const DevBatch &d, const double *hist_t, const double *coef, int nvec, cudaStream_t st);
+// Device-side iteration control
+void launch_control(const DevBatch &d, const CtlBuffers &c, double tol, int max_iter, int ndiis, int init,
+                    cudaStream_t st);
+void launch_active_swap(const DevBatch &d, const CtlBuffers &c, cudaStream_t st);
+int launch_iteration(const DevBatch &d, const CtlBuffers &c, const TermFlags &f, double tol, int max_iter,
+                     int ndiis, cudaStream_t st, KernelTimer *kt);
 void launch_unpack(const DevBatch &d, int s, int namp, const double *t, double *ab, double *ba, double *aa,
                    cudaStream_t st);
 

@@ -714,21 +714,157 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
 // Pulay DIIS (new in this library; the reference's GetTFromDIIS, DIISCC.f90:52-131,
 // builds a singular matrix and never extrapolates).  Error vector e = t' - t of
 // the (damped) Jacobi step; history of ndiis (t', e) pairs per solve.
-// k_diis_push stores slot `slot` and forms the dot products e . e_j of every
-// stored j (per-chunk partials, reduced per solve in chunk order).
+// k_diis_push2 stores the solve's current slot and forms the dot products e . e_j
+// of every stored j (per-chunk partials, reduced per solve in chunk order).
 // ----------------------------------------------------------------------------
 constexpr int kMaxDiis = 16;
-__global__ void __launch_bounds__(kChunk) k_diis_push(const ChunkDev *__restrict__ chunks,
-                                                      const SolveDev *__restrict__ solves, int64_t namp,
-                                                      const double *__restrict__ t, const double *__restrict__ t_new,
-                                                      double *__restrict__ hist_t, double *__restrict__ hist_e,
-                                                      int slot, int nvec, double *__restrict__ part,
-                                                      const uint8_t *__restrict__ active)
+// ----------------------------------------------------------------------------
+// Device-side iteration control.  Every solve of a batch carries its own state;
+// one iteration is a fixed sequence of launches (residual terms -> update ->
+// per-solve reduction -> [DIIS push] -> k_control -> commit -> k_active_swap),
+// so it can be captured once as a CUDA graph and replayed.  Converged solves stop
+// being updated (their CTAs return at once) while the others continue.
+// ----------------------------------------------------------------------------
+// Pulay system [B 1; 1 0][c; l] = [0; 1] over nvec vectors, B scaled by its max
+// diagonal; Gaussian elimination with partial pivoting.  Returns false if singular.
+__device__ bool pulay_device(const double *B, int nvec, double *c)
+{
+    constexpr int N = kMaxDiis + 1;
+    double A[N][N + 1];
+    const int n = nvec + 1;
+    double scale = 0.0;
+    for (int j = 0; j < nvec; j++) scale = fmax(scale, B[j * kMaxDiis + j]);
+    if (!(scale > 0.0) || !isfinite(scale)) return false;
+    for (int j = 0; j < n; j++)
+        for (int k = 0; k <= n; k++) A[j][k] = 0.0;
+    for (int j = 0; j < nvec; j++) {
+        for (int k = 0; k < nvec; k++) A[j][k] = B[j * kMaxDiis + k] / scale;
+        A[j][nvec] = 1.0;
+        A[nvec][j] = 1.0;
+    }
+    A[nvec][n] = 1.0;
+    for (int k = 0; k < n; k++) {
+        int piv = k;
+        for (int i = k + 1; i < n; i++)
+            if (fabs(A[i][k]) > fabs(A[piv][k])) piv = i;
+        if (fabs(A[piv][k]) < 1e-14) return false;
+        if (piv != k)
+            for (int j = 0; j <= n; j++) {
+                double tmp = A[k][j];
+                A[k][j] = A[piv][j];
+                A[piv][j] = tmp;
+            }
+        for (int i = k + 1; i < n; i++) {
+            const double f = A[i][k] / A[k][k];
+            for (int j = k; j <= n; j++) A[i][j] -= f * A[k][j];
+        }
+    }
+    for (int k = n - 1; k >= 0; k--) {
+        double x = A[k][n];
+        for (int j = k + 1; j < n; j++) x -= A[k][j] * A[j][n];
+        A[k][n] = x / A[k][k];
+    }
+    for (int j = 0; j < nvec; j++) {
+        if (!isfinite(A[j][n])) return false;
+        c[j] = A[j][n];
+    }
+    return true;
+}
+
+// One thread per solve.  init = 1: record the start energy and decide whether to iterate.
+__global__ void k_control(int nsolves, const double *__restrict__ red, const double *__restrict__ brow,
+                          IterState *__restrict__ st, double *__restrict__ Bm, double *__restrict__ coef,
+                          double *__restrict__ rec_e, double *__restrict__ rec_dt, int max_rec,
+                          const uint8_t *__restrict__ active, uint8_t *__restrict__ active_next, double tol,
+                          int max_iter, int ndiis, int init)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsolves) return;
+    IterState S = st[s];
+    if (!init && !active[s]) {
+        active_next[s] = 0;
+        return;
+    }
+    const double e = red[3 * s], dt = red[3 * s + 1];
+    if (!init) S.niter += 1;
+    const int r = S.niter - 1;
+    if (r >= 0 && r < max_rec) {
+        rec_e[(int64_t)s * max_rec + r] = e;
+        rec_dt[(int64_t)s * max_rec + r] = dt;
+    }
+    S.e = e;
+    S.dt = dt;
+    const bool finite = isfinite(e) && isfinite(dt);
+    const bool go = finite && dt >= tol && S.niter < max_iter;
+    if (!finite) S.status = 3;
+    if (!init && ndiis > 0) {
+        // this iteration pushed slot (niter_before - 1) % ndiis with nvec = min(niter_before, ndiis)
+        const int nb = S.niter - 1;
+        const int slot = (nb - 1) % ndiis, nvec = min(nb, ndiis);
+        double *B = Bm + (int64_t)s * kMaxDiis * kMaxDiis;
+        for (int j = 0; j < nvec; j++) B[slot * kMaxDiis + j] = B[j * kMaxDiis + slot] = brow[s * kMaxDiis + j];
+        double *c = coef + s * kMaxDiis;
+        for (int j = 0; j < kMaxDiis; j++) c[j] = 0.0;
+        if (!go || nvec < 2 || !pulay_device(B, nvec, c)) {
+            for (int j = 0; j < kMaxDiis; j++) c[j] = 0.0;
+            c[slot] = 1.0;
+        }
+    }
+    if (!go && S.status == 0) S.status = (finite && dt >= tol) ? 2 : 1;
+    active_next[s] = go ? 1 : 0;
+    st[s] = S;
+}
+
+// active <- active_next; count of active solves for the host's poll.
+__global__ void k_active_swap(int nsolves, uint8_t *__restrict__ active, const uint8_t *__restrict__ active_next,
+                              int *__restrict__ count)
+{
+    int c = 0;
+    for (int s = threadIdx.x; s < nsolves; s += blockDim.x) {
+        const uint8_t a = active_next[s];
+        active[s] = a;
+        c += a;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    __shared__ int w[32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) tot += w[k];
+        *count = tot;
+    }
+}
+
+// t <- t_new for the solves still iterating this round (replay mode)
+__global__ void k_commit(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                         const double *__restrict__ t_new, double *__restrict__ t,
+                         const uint8_t *__restrict__ active)
 {
     const ChunkDev ch = chunks[blockIdx.x];
+    if (!active[ch.solve]) return;
     const SolveDev s = solves[ch.solve];
     const int loc = ch.start + threadIdx.x;
-    const bool on = active[ch.solve] && loc < s.namp;
+    if (loc < s.namp) t[s.amp0 + loc] = t_new[s.amp0 + loc];
+}
+
+// DIIS push with per-solve slot and history length (solves need not be in step)
+__global__ void __launch_bounds__(kChunk) k_diis_push2(const ChunkDev *__restrict__ chunks,
+                                                       const SolveDev *__restrict__ solves,
+                                                       const IterState *__restrict__ st, int ndiis, int64_t namp,
+                                                       const double *__restrict__ t,
+                                                       const double *__restrict__ t_new,
+                                                       double *__restrict__ hist_t, double *__restrict__ hist_e,
+                                                       double *__restrict__ part,
+                                                       const uint8_t *__restrict__ active)
+{
+    const ChunkDev ch = chunks[blockIdx.x];
+    if (!active[ch.solve]) return;  // whole CTA: one solve
+    const SolveDev s = solves[ch.solve];
+    const int nb = st[ch.solve].niter;  // before k_control increments it
+    const int slot = (nb - 1) % ndiis, nvec = min(nb, ndiis);
+    const int loc = ch.start + threadIdx.x;
+    const bool on = loc < s.namp;
     double e = 0.0;
     int64_t p = 0;
     if (on) {
@@ -746,11 +882,13 @@ __global__ void __launch_bounds__(kChunk) k_diis_push(const ChunkDev *__restrict
     }
 }
 
-// brow[s*kMaxDiis + j] = sum over the solve's chunks of part[chunk][j]
-__global__ void k_diis_rows(const int *__restrict__ chunk_begin, const double *__restrict__ part, int nvec,
-                            double *__restrict__ brow)
+__global__ void k_diis_rows2(const int *__restrict__ chunk_begin, const IterState *__restrict__ st, int ndiis,
+                             const double *__restrict__ part, double *__restrict__ brow,
+                             const uint8_t *__restrict__ active)
 {
     const int s = blockIdx.x;
+    if (!active[s]) return;
+    const int nvec = min(st[s].niter, ndiis);
     const int c0 = chunk_begin[s], c1 = chunk_begin[s + 1];
     for (int jv = 0; jv < nvec; jv++) {
         double acc = 0.0;
@@ -761,10 +899,9 @@ __global__ void k_diis_rows(const int *__restrict__ chunk_begin, const double *_
     }
 }
 
-// t = sum_j coef[s][j] hist_t[j]  (active solves)
-__global__ void k_diis_extrap(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
-                              int64_t namp, const double *__restrict__ hist_t, const double *__restrict__ coef,
-                              int nvec, double *__restrict__ t, const uint8_t *__restrict__ active)
+__global__ void k_diis_extrap2(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                               int64_t namp, const double *__restrict__ hist_t, const double *__restrict__ coef,
+                               int ndiis, double *__restrict__ t, const uint8_t *__restrict__ active)
 {
     const ChunkDev ch = chunks[blockIdx.x];
     if (!active[ch.solve]) return;
@@ -774,21 +911,45 @@ __global__ void k_diis_extrap(const ChunkDev *__restrict__ chunks, const SolveDe
     const int64_t p = s.amp0 + loc;
     const double *c = coef + ch.solve * kMaxDiis;
     double x = 0.0;
-    for (int jv = 0; jv < nvec; jv++) x = fma(c[jv], hist_t[(int64_t)jv * namp + p], x);
+    for (int jv = 0; jv < ndiis; jv++) {
+        const double cj = c[jv];
+        if (cj != 0.0) x = fma(cj, hist_t[(int64_t)jv * namp + p], x);
+    }
     t[p] = x;
 }
 
-void launch_diis_push(const DevBatch &d, int slot, int nvec, double *hist_t, double *hist_e, double *part,
-                      double *brow, cudaStream_t st)
+void launch_control(const DevBatch &d, const CtlBuffers &c, double tol, int max_iter, int ndiis, int init,
+                    cudaStream_t st)
 {
-    k_diis_push<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, d.t, d.t_new, hist_t, hist_e, slot, nvec,
-                                              part, d.active);
-    k_diis_rows<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, part, nvec, brow);
+    k_control<<<(d.nsolves + 127) / 128, 128, 0, st>>>(d.nsolves, d.red, c.brow, c.state, c.Bm, c.coef, c.rec_e,
+                                                       c.rec_dt, c.max_rec, d.active, c.active_next, tol,
+                                                       max_iter, ndiis, init);
 }
 
-void launch_diis_extrap(const DevBatch &d, const double *hist_t, const double *coef, int nvec, cudaStream_t st)
+void launch_active_swap(const DevBatch &d, const CtlBuffers &c, cudaStream_t st)
 {
-    k_diis_extrap<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, hist_t, coef, nvec, d.t, d.active);
+    k_active_swap<<<1, 1024, 0, st>>>(d.nsolves, d.active, c.active_next, c.count);
+}
+
+// One iteration: residual + update, reduction, [DIIS], control, commit, swap.  Returns launches.
+int launch_iteration(const DevBatch &d, const CtlBuffers &c, const TermFlags &f, double tol, int max_iter,
+                     int ndiis, cudaStream_t st, KernelTimer *kt)
+{
+    int n = launch_residual(d, f, 0, nullptr, st, kt);
+    if (ndiis > 0) {
+        k_diis_push2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, c.state, ndiis, d.namp, d.t, d.t_new,
+                                                   c.hist_t, c.hist_e, c.part, d.active);
+        k_diis_rows2<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, c.state, ndiis, c.part, c.brow, d.active);
+        n += 2;
+    }
+    launch_control(d, c, tol, max_iter, ndiis, 0, st);
+    if (ndiis > 0)
+        k_diis_extrap2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, c.hist_t, c.coef, ndiis, d.t,
+                                                     d.active);
+    else
+        k_commit<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.t_new, d.t, d.active);
+    launch_active_swap(d, c, st);
+    return n + 3;
 }
 
 // ----------------------------------------------------------------------------

@@ -11,18 +11,12 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
-#include <unordered_map>
 
 namespace uegccd {
 
 namespace {
 constexpr double kPi = 3.1415926535897932384626433833;  // Constants.f90:7
 
-struct VecHash {
-    size_t operator()(const std::array<int, 3> &v) const {
-        return (size_t)((v[0] + 512) * 1048576LL + (v[1] + 512) * 1024LL + (v[2] + 512));
-    }
-};
 }  // namespace
 
 double coulomb_v(double L, double madelung, int q2)
@@ -30,6 +24,26 @@ double coulomb_v(double L, double madelung, int q2)
     if (q2 == 0) return -madelung;
     return 1.0 / (L * kPi * (double)q2);
 }
+
+namespace {
+// Dense lookup over integer lattice vectors with components in [-r, r].
+struct Lattice {
+    int r = 0, side = 0;
+    std::vector<int> idx;
+    void init(int radius)
+    {
+        r = radius;
+        side = 2 * r + 1;
+        idx.assign((size_t)side * side * side, -1);
+    }
+    bool inside(int x, int y, int z) const { return std::abs(x) <= r && std::abs(y) <= r && std::abs(z) <= r; }
+    int &at(int x, int y, int z) { return idx[((size_t)(x + r) * side + (y + r)) * side + (z + r)]; }
+    int get(int x, int y, int z) const
+    {
+        return inside(x, y, z) ? idx[((size_t)(x + r) * side + (y + r)) * side + (z + r)] : -1;
+    }
+};
+}  // namespace
 
 std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
 {
@@ -40,56 +54,75 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
     p = SolvePlan();
     p.O = O; p.V = V; p.M = M;
 
-    std::unordered_map<std::array<int, 3>, int, VecHash> orb;
-    orb.reserve((size_t)M * 2);
-    int q2max = 0;
+    int nmax = 0;
+    for (int q = 0; q < M; q++)
+        for (int d = 0; d < 3; d++) nmax = std::max(nmax, std::abs(sys.n[q][d]));
+    if (nmax > 200) return "plane-wave vectors out of range";
+    // orbital lookup: n -> orbital (the basis, as FindIndex's kPointToBasisFn, HEG.f90:306-316)
+    Lattice orb;
+    orb.init(nmax);
     for (int q = 0; q < M; q++) {
-        if (!orb.emplace(sys.n[q], q).second) return "duplicate plane-wave vector in nVec";
+        int &slot = orb.at(sys.n[q][0], sys.n[q][1], sys.n[q][2]);
+        if (slot >= 0) return "duplicate plane-wave vector in nVec";
+        slot = q;
     }
-    for (int x = 0; x < M; x++)
-        for (int y = 0; y < M; y++) {
-            int d0 = sys.n[x][0] - sys.n[y][0], d1 = sys.n[x][1] - sys.n[y][1], d2 = sys.n[x][2] - sys.n[y][2];
-            q2max = std::max(q2max, d0 * d0 + d1 * d1 + d2 * d2);
-        }
+    // |q|^2 range of orbital differences: components of n_x - n_y are within [-2 nmax, 2 nmax]
+    int q2max = 0;
+    {
+        Lattice diff;
+        diff.init(2 * nmax);
+        std::vector<char> seen(diff.idx.size(), 0);
+        for (int x = 0; x < M; x++)
+            for (int y = 0; y < M; y++) {
+                int d0 = sys.n[x][0] - sys.n[y][0], d1 = sys.n[x][1] - sys.n[y][1], d2 = sys.n[x][2] - sys.n[y][2];
+                q2max = std::max(q2max, d0 * d0 + d1 * d1 + d2 * d2);
+            }
+    }
     p.q2max = q2max;
     p.vtab.resize((size_t)q2max + 1);
     for (int q2 = 0; q2 <= q2max; q2++) p.vtab[q2] = coulomb_v(sys.L, sys.madelung, q2);
 
-    auto partner = [&](int i, int j, int a) -> int {
-        std::array<int, 3> t{sys.n[i][0] + sys.n[j][0] - sys.n[a][0], sys.n[i][1] + sys.n[j][1] - sys.n[a][1],
-                             sys.n[i][2] + sys.n[j][2] - sys.n[a][2]};
-        auto it = orb.find(t);
-        return it == orb.end() ? -1 : it->second;
-    };
-
-    // Group ordered occupied pairs by K, keeping first-appearance order (i major).
-    std::map<std::array<int, 3>, int> kindex;
+    // Group ordered occupied pairs by K = n_i + n_j, first-appearance order (i major).
+    Lattice kid;
+    kid.init(2 * nmax);
     std::vector<std::vector<std::pair<int, int>>> kpairs;
     std::vector<std::array<int, 3>> kvecs;
     for (int i = 0; i < O; i++)
         for (int j = 0; j < O; j++) {
             std::array<int, 3> K{sys.n[i][0] + sys.n[j][0], sys.n[i][1] + sys.n[j][1], sys.n[i][2] + sys.n[j][2]};
-            auto it = kindex.find(K);
-            int id;
-            if (it == kindex.end()) {
+            int &id = kid.at(K[0], K[1], K[2]);
+            if (id < 0) {
                 id = (int)kpairs.size();
-                kindex.emplace(K, id);
                 kpairs.emplace_back();
                 kvecs.push_back(K);
-            } else {
-                id = it->second;
             }
             kpairs[id].emplace_back(i, j);
         }
     p.pos.assign((size_t)O * O * V, -1);
+    {
+        size_t est = 0;  // exact count of allowed amplitudes, to size the arrays once
+        for (size_t k = 0; k < kpairs.size(); k++) {
+            const auto &K = kvecs[k];
+            size_t nc = 0;
+            for (int a = O; a < M; a++)
+                if (orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]) >= O) nc++;
+            est += nc * kpairs[k].size();
+        }
+        p.amps.reserve(est);
+    }
     int64_t t0 = 0;
+    std::vector<int> cols, partner_of_col;
     for (size_t k = 0; k < kpairs.size(); k++) {
         // virtual columns of block K: a virtual whose partner b = K - a is a virtual
-        std::vector<int> cols;
-        int i0 = kpairs[k][0].first, j0 = kpairs[k][0].second;
+        cols.clear();
+        partner_of_col.clear();
+        const auto &K = kvecs[k];
         for (int a = O; a < M; a++) {
-            int b = partner(i0, j0, a);
-            if (b >= O) cols.push_back(a);
+            int b = orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]);
+            if (b >= O) {
+                cols.push_back(a);
+                partner_of_col.push_back(b);
+            }
         }
         if (cols.empty()) continue;
         SolvePlan::Block blk;
@@ -105,12 +138,11 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
         for (int a : cols) p.vir.push_back((int16_t)a);
         for (int r = 0; r < blk.o; r++) {
             int i = kpairs[k][r].first, j = kpairs[k][r].second;
+            int32_t *prow = &p.pos[((size_t)i * O + j) * V];
             for (int c = 0; c < blk.v; c++) {
                 int a = cols[c];
-                int b = partner(i, j, a);
-                int64_t idx = t0 + (int64_t)r * blk.v + c;
-                p.pos[((size_t)i * O + j) * V + (a - O)] = (int32_t)idx;
-                p.amps.push_back(AmpInfo{(int16_t)i, (int16_t)j, (int16_t)a, (int16_t)b});
+                prow[a - O] = (int32_t)(t0 + (int64_t)r * blk.v + c);
+                p.amps.push_back(AmpInfo{(int16_t)i, (int16_t)j, (int16_t)a, (int16_t)partner_of_col[c]});
             }
         }
         t0 += (int64_t)blk.o * blk.v;
@@ -120,29 +152,51 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
     if (p.namp >= (int64_t)1 << 31) return "too many amplitudes for 32-bit packed indices";
     p.ring_entries = (int64_t)O * V * O;
 
-    // particle-hole rows (i,x) grouped by their momentum Q = n_x - n_i
-    std::map<std::array<int, 3>, std::vector<std::pair<int, int>>> qrows;
+    // particle-hole rows (i,x) grouped by their momentum Q = n_x - n_i, groups in
+    // lexicographic order of Q, rows within a group by i
+    Lattice qid;
+    qid.init(2 * nmax);
+    std::vector<std::array<int, 3>> qvecs;
+    std::vector<int> qcount;
+    std::vector<int> row_q((size_t)O * V);
     for (int i = 0; i < O; i++)
         for (int x = O; x < M; x++) {
-            std::array<int, 3> Q{sys.n[x][0] - sys.n[i][0], sys.n[x][1] - sys.n[i][1], sys.n[x][2] - sys.n[i][2]};
-            qrows[Q].emplace_back(i, x);
+            int q0 = sys.n[x][0] - sys.n[i][0], q1 = sys.n[x][1] - sys.n[i][1], q2 = sys.n[x][2] - sys.n[i][2];
+            int &id = qid.at(q0, q1, q2);
+            if (id < 0) {
+                id = (int)qvecs.size();
+                qvecs.push_back({q0, q1, q2});
+                qcount.push_back(0);
+            }
+            qcount[id]++;
+            row_q[(size_t)i * V + (x - O)] = id;
         }
-    p.phrow_of.assign((size_t)O * V, -1);
-    std::map<std::array<int, 3>, int> gidx;
-    for (auto &kv : qrows) {
-        SolvePlan::PhGroup g{(int)p.ph_i.size(), (int)kv.second.size(), -1};
-        gidx[kv.first] = (int)p.groups.size();
-        p.groups.push_back(g);
-        for (auto &r : kv.second) {
-            p.phrow_of[(size_t)r.first * V + (r.second - O)] = (int32_t)p.ph_i.size();
-            p.ph_i.push_back((int16_t)r.first);
-            p.ph_x.push_back((int16_t)r.second);
-        }
+    std::vector<int> order(qvecs.size());
+    for (size_t g = 0; g < order.size(); g++) order[g] = (int)g;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return qvecs[a] < qvecs[b]; });
+    std::vector<int> gpos(qvecs.size()), gstart(qvecs.size());
+    int r0 = 0;
+    for (size_t g = 0; g < order.size(); g++) {
+        gpos[order[g]] = (int)g;
+        gstart[order[g]] = r0;
+        p.groups.push_back(SolvePlan::PhGroup{r0, qcount[order[g]], -1});
+        r0 += qcount[order[g]];
     }
-    for (auto &kv : qrows) {
-        std::array<int, 3> mQ{-kv.first[0], -kv.first[1], -kv.first[2]};
-        auto it = gidx.find(mQ);
-        if (it != gidx.end()) p.groups[gidx[kv.first]].partner = it->second;
+    p.ph_i.assign((size_t)O * V, 0);
+    p.ph_x.assign((size_t)O * V, 0);
+    p.phrow_of.assign((size_t)O * V, -1);
+    std::vector<int> fill(qvecs.size(), 0);
+    for (int i = 0; i < O; i++)
+        for (int x = O; x < M; x++) {
+            int id = row_q[(size_t)i * V + (x - O)];
+            int r = gstart[id] + fill[id]++;
+            p.ph_i[r] = (int16_t)i;
+            p.ph_x[r] = (int16_t)x;
+            p.phrow_of[(size_t)i * V + (x - O)] = r;
+        }
+    for (size_t g = 0; g < qvecs.size(); g++) {
+        int m = qid.get(-qvecs[g][0], -qvecs[g][1], -qvecs[g][2]);
+        if (m >= 0) p.groups[gpos[g]].partner = gpos[m];
     }
     return "";
 }
