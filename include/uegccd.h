@@ -123,6 +123,10 @@ int uegccd_drpa(UegccdCtx *ctx, const UegccdOptions *opt, double *t2, UegccdResu
  * drivers, bit1 mosaics, bit2 ladders, bit3 rings, bit4 crossed rings) for
  * spin-adapted amplitudes t_abab; writes G2abab in the reference layout. */
 int uegccd_ccd_g2(UegccdCtx *ctx, const double *t_abab, int32_t term_mask, double *g_abab);
+/* The same in a chosen precision: UEGCCD_MIXED forms the particle-particle ladder on
+ * the tensor cores (FP16 operands, FP32 accumulation) from t itself. */
+int uegccd_ccd_g2_ex(UegccdCtx *ctx, const double *t_abab, int32_t term_mask, int32_t precision,
+                     double *g_abab);
 
 /* ---- many independent solves in one launch per residual term ---------------- */
 typedef struct UegccdBatch UegccdBatch;

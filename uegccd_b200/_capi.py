@@ -60,7 +60,7 @@ EXPORTS = [
     "uegccd_mp2", "uegccd_ccd", "uegccd_drpa", "uegccd_ccd_g2", "uegccd_batch_create",
     "uegccd_batch_destroy", "uegccd_batch_solve", "uegccd_batch_get_amplitudes", "uegccd_last_error",
     "uegccd_version", "uegccd_batch_set_profiling", "uegccd_batch_kernel_stats",
-    "uegccd_batch_transfer_bytes",
+    "uegccd_batch_transfer_bytes", "uegccd_ccd_g2_ex",
 ]
 
 _lib = None
@@ -82,6 +82,7 @@ def lib() -> C.CDLL:
         L.uegccd_ccd.argtypes = [vp, P(Options), dp, dp, dp, P(Result)]
         L.uegccd_drpa.argtypes = [vp, P(Options), dp, P(Result)]
         L.uegccd_ccd_g2.argtypes = [vp, dp, C.c_int32, dp]
+        L.uegccd_ccd_g2_ex.argtypes = [vp, dp, C.c_int32, C.c_int32, dp]
         L.uegccd_batch_create.argtypes = [P(System), C.c_int32, P(vp)]
         L.uegccd_batch_destroy.argtypes = [vp]
         L.uegccd_batch_solve.argtypes = [vp, P(Options), C.c_int32, dp, P(Result)]

@@ -18,7 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libuegccd.so")
 OBJDIR = os.path.join(PKG, "_build")
 
-SOURCES = ["capi.cu", "kernels_fp64.cu", "plan.cpp", "heg_host.cpp"]
+SOURCES = ["capi.cu", "kernels_fp64.cu", "kernels_tc.cu", "plan.cpp", "heg_host.cpp"]
 HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -99,13 +99,13 @@ struct UegccdBatch {
     int diis_cap = 0;
     // CUDA graphs of one iteration: plain and with kernel timers, keyed by the options
     struct GraphKey {
-        int do_ring, do_xring, do_ladder, do_mosaic, drpa, ndiis, max_iter;
+        int do_ring, do_xring, do_ladder, do_mosaic, drpa, ndiis, max_iter, mixed;
         double tol;
         bool operator==(const GraphKey &o) const
         {
             return do_ring == o.do_ring && do_xring == o.do_xring && do_ladder == o.do_ladder &&
                    do_mosaic == o.do_mosaic && drpa == o.drpa && ndiis == o.ndiis && max_iter == o.max_iter &&
-                   tol == o.tol;
+                   mixed == o.mixed && tol == o.tol;
         }
     } gkey{};
     bool have_graph = false;
@@ -196,7 +196,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
 
     std::vector<SolveDev> solves(n);
     std::vector<BlockDev> blocks;
-    std::vector<LadderTile> tiles, htiles;
+    std::vector<LadderTile> tiles, htiles, tc16, tc32, tc64;
     std::vector<ChunkDev> chunks, rchunks;
     std::vector<int> chunk_begin(n + 1, 0);
     std::vector<int2> targets;
@@ -260,6 +260,11 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
                 for (int p0 = 0; p0 < B.o; p0 += np) tiles.push_back(LadderTile{bi, a0, p0, np});
             for (int q0 = 0; q0 < B.o; q0 += 128)
                 for (int p0 = 0; p0 < B.o; p0 += np) htiles.push_back(LadderTile{bi, q0, p0, np});
+            // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows
+            const int ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
+            auto &tl = ntc == 16 ? tc16 : ntc == 32 ? tc32 : tc64;
+            for (int a0 = 0; a0 < B.v; a0 += 128)
+                for (int p0 = 0; p0 < B.o; p0 += ntc) tl.push_back(LadderTile{bi, a0, p0, ntc});
         }
         pair_i.insert(pair_i.end(), P.pair_i.begin(), P.pair_i.end());
         pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
@@ -306,6 +311,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.nblocks = (int)blocks.size();
     d.ntiles = (int)tiles.size();
     d.nhtiles = (int)htiles.size();
+    d.ntc16 = (int)tc16.size();
+    d.ntc32 = (int)tc32.size();
+    d.ntc64 = (int)tc64.size();
+    std::vector<LadderTile> tct;
+    tct.insert(tct.end(), tc16.begin(), tc16.end());
+    tct.insert(tct.end(), tc32.begin(), tc32.end());
+    tct.insert(tct.end(), tc64.begin(), tc64.end());
     d.nchunks = (int)chunks.size();
     d.nrchunks = (int)rchunks.size();
     d.ntargets = (int)targets.size();
@@ -320,6 +332,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;
     if ((rc = b->upload(d.htiles, htiles))) return rc;
+    if ((rc = b->upload(d.tctiles, tct))) return rc;
     if ((rc = b->upload(d.chunks, chunks))) return rc;
     if ((rc = b->upload(d.rchunks, rchunks))) return rc;
     if ((rc = b->upload(d.chunk_begin, chunk_begin))) return rc;
@@ -433,7 +446,7 @@ int validate_options(const UegccdOptions *o, int drpa)
     if (o->scheme != UEGCCD_REPLAY && o->scheme != UEGCCD_DIIS) return fail(UEGCCD_ERR_ARG, "unknown scheme");
     if (o->scheme == UEGCCD_DIIS && (o->ndiis < 2 || o->ndiis > kDiisMax))
         return fail(UEGCCD_ERR_ARG, "ndiis must be in [2, 16]");
-    if (o->precision != UEGCCD_FP64) return fail(UEGCCD_ERR_UNSUPPORTED, "only FP64 is built");
+    if (o->precision != UEGCCD_FP64 && o->precision != UEGCCD_MIXED) return fail(UEGCCD_ERR_ARG, "unknown precision");
     return 0;
 }
 
@@ -467,7 +480,7 @@ int ctl_alloc(UegccdBatch &b, int ndiis, int max_rec)
 // Captures one iteration as a CUDA graph.
 int capture_iteration(UegccdBatch &b, const TermFlags &f, double tol, int max_iter, int ndiis)
 {
-    UegccdBatch::GraphKey key{f.do_ring, f.do_xring, f.do_ladder, f.do_mosaic, f.drpa, ndiis, max_iter, tol};
+    UegccdBatch::GraphKey key{f.do_ring, f.do_xring, f.do_ladder, f.do_mosaic, f.drpa, ndiis, max_iter, f.mixed, tol};
     if (b.have_graph && b.gkey == key) return 0;
     if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
     cudaGraph_t g = nullptr;
@@ -511,7 +524,12 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     CU(cudaMemcpyAsync(b.ctl.state, st0.data(), n * sizeof(IterState), cudaMemcpyHostToDevice, b.stream));
     CU(cudaMemsetAsync(b.ctl.Bm, 0, (size_t)n * kDiisMax * kDiisMax * sizeof(double), b.stream));
     if ((rc = set_active_all(b, 1))) return rc;
-    if ((rc = capture_iteration(b, f, opt->tol, opt->max_iter, ndiis))) return rc;
+    if (opt->precision == UEGCCD_MIXED && !d.t_ref) {
+        if ((rc = b.alloc(d.t_ref, d.namp))) return rc;
+        if ((rc = b.alloc(d.g_ref, d.namp))) return rc;
+        if ((rc = b.alloc(d.tc_err, 1))) return rc;
+    }
+    if (d.tc_err) CU(cudaMemsetAsync(d.tc_err, 0, sizeof(int), b.stream));
     b.launches = 0;
     CU(cudaEventRecord(b.ev0, b.stream));
     // CCEnergy of the start amplitudes and dT = max|T| (CCD.f90:63-64, dRPA.f90:68-69)
@@ -522,22 +540,52 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     b.launches += 4;
     int count = n, rounds = 0;
     const int max_rounds = opt->max_iter / kPoll + 2;
-    while (count > 0 && rounds < max_rounds) {
-        for (int k = 0; k < kPoll; k++) {
-            if (b.kt.on && k == kPoll - 1) {
-                // the sampled iteration of the round: direct launches between CUDA events
-                b.launches += launch_iteration(d, b.ctl, f, opt->tol, opt->max_iter, ndiis, b.stream, &b.kt);
-            } else {
-                CU(cudaGraphLaunch(b.gexec, b.stream));
-                b.launches += b.g_launches;
-            }
+    // mixed precision: tensor-core ladder of t - t_ref, t_ref refreshed (FP64) each round,
+    // then FP64 iterations from where the mixed phase stopped (refinement)
+    const bool mixed = opt->precision == UEGCCD_MIXED && f.do_ladder && f.do_pp;
+    for (int phase = mixed ? 0 : 1; phase < 2; phase++) {
+        f.mixed = phase == 0 ? 1 : 0;
+        if (phase == 1 && mixed) {
+            // reopen every solve for the FP64 sweeps
+            std::vector<IterState> st1(n);
+            CU(cudaMemcpyAsync(st1.data(), b.ctl.state, n * sizeof(IterState), cudaMemcpyDeviceToHost, b.stream));
+            CU(cudaStreamSynchronize(b.stream));
+            for (auto &x : st1) x.status = 0;
+            CU(cudaMemcpyAsync(b.ctl.state, st1.data(), n * sizeof(IterState), cudaMemcpyHostToDevice, b.stream));
+            if ((rc = set_active_all(b, 1))) return rc;
+            count = n;
+            rounds = 0;
         }
-        CU(cudaMemcpyAsync(&count, b.ctl.count, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
-        b.d2h_bytes += sizeof(int);
+        if ((rc = capture_iteration(b, f, opt->tol, opt->max_iter, ndiis))) return rc;
+        int sweeps = 0;
+        while (count > 0 && rounds < max_rounds) {
+            if (f.mixed) {
+                launch_refresh(d, b.stream);
+                b.launches += 2;
+            }
+            for (int k = 0; k < kPoll; k++) {
+                if (b.kt.on && k == kPoll - 1) {
+                    // the sampled iteration of the round: direct launches between CUDA events
+                    b.launches += launch_iteration(d, b.ctl, f, opt->tol, opt->max_iter, ndiis, b.stream, &b.kt);
+                } else {
+                    CU(cudaGraphLaunch(b.gexec, b.stream));
+                    b.launches += b.g_launches;
+                }
+            }
+            CU(cudaMemcpyAsync(&count, b.ctl.count, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+            b.d2h_bytes += sizeof(int);
+            CU(cudaStreamSynchronize(b.stream));
+            CU(cudaGetLastError());
+            b.kt.collect();
+            rounds++;
+            if (phase == 1 && mixed && ++sweeps >= std::max(1, opt->refine_sweeps)) break;
+        }
+    }
+    if (mixed) {
+        int err = 0;
+        CU(cudaMemcpyAsync(&err, d.tc_err, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
         CU(cudaStreamSynchronize(b.stream));
-        CU(cudaGetLastError());
-        b.kt.collect();
-        rounds++;
+        if (err) return fail(UEGCCD_ERR_CUDA, "tensor-core ladder: an mbarrier wait expired");
     }
     // final residual (CCD.f90:103-107, dRPA.f90:98-101)
     if ((rc = set_active_all(b, 1))) return rc;
@@ -684,9 +732,10 @@ int uegccd_drpa(UegccdCtx *c, const UegccdOptions *opt, double *t2, UegccdResult
     return st;
 }
 
-int uegccd_ccd_g2(UegccdCtx *c, const double *t_abab, int32_t mask, double *g_abab)
+int uegccd_ccd_g2_ex(UegccdCtx *c, const double *t_abab, int32_t mask, int32_t precision, double *g_abab)
 {
     if (!c || !t_abab || !g_abab) return fail(UEGCCD_ERR_ARG, "null argument");
+    if (precision != UEGCCD_FP64 && precision != UEGCCD_MIXED) return fail(UEGCCD_ERR_ARG, "unknown precision");
     UegccdBatch &b = *c->batch;
     int rc = pack_from_host(b, 0, t_abab);
     if (rc) return rc;
@@ -697,10 +746,34 @@ int uegccd_ccd_g2(UegccdCtx *c, const double *t_abab, int32_t mask, double *g_ab
     f.do_ladder = (mask & 4) ? 1 : 0;
     f.do_ring = (mask & 8) ? 1 : 0;
     f.do_xring = (mask & 16) ? 1 : 0;
+    DevBatch &d = b.d;
+    if (precision == UEGCCD_MIXED) {
+        // the tensor-core ladder of t itself: refresh point t_ref = 0, g_ref = 0
+        if (!d.t_ref) {
+            if ((rc = b.alloc(d.t_ref, d.namp))) return rc;
+            if ((rc = b.alloc(d.g_ref, d.namp))) return rc;
+            if ((rc = b.alloc(d.tc_err, 1))) return rc;
+        }
+        CU(cudaMemsetAsync(d.t_ref, 0, d.namp * sizeof(double), b.stream));
+        CU(cudaMemsetAsync(d.g_ref, 0, d.namp * sizeof(double), b.stream));
+        CU(cudaMemsetAsync(d.tc_err, 0, sizeof(int), b.stream));
+        f.mixed = 1;
+    }
     // g_out reuses t_new (mode 1 does not write the update)
-    launch_residual(b.d, f, 1, b.d.t_new, b.stream);
+    launch_residual(d, f, 1, d.t_new, b.stream);
     CU(cudaGetLastError());
-    return unpack_to_host(b, 0, b.d.t_new, g_abab, nullptr, nullptr);
+    if (precision == UEGCCD_MIXED) {
+        int err = 0;
+        CU(cudaMemcpyAsync(&err, d.tc_err, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+        CU(cudaStreamSynchronize(b.stream));
+        if (err) return fail(UEGCCD_ERR_CUDA, "tensor-core ladder: an mbarrier wait expired");
+    }
+    return unpack_to_host(b, 0, d.t_new, g_abab, nullptr, nullptr);
+}
+
+int uegccd_ccd_g2(UegccdCtx *c, const double *t_abab, int32_t mask, double *g_abab)
+{
+    return uegccd_ccd_g2_ex(c, t_abab, mask, UEGCCD_FP64, g_abab);
 }
 
 int uegccd_batch_create(const UegccdSystem *systems, int32_t n, UegccdBatch **out)

@@ -41,6 +41,11 @@ struct DevBatch {
     int16_t *ph_i = nullptr, *ph_x = nullptr;   // row -> (i, x), rows grouped by Q
     double *g_rq = nullptr, *g_xq = nullptr;    // per amplitude: ring and crossed-ring G
     RingPairDev *rpairs = nullptr;              // {Q, -Q} group pairs
+    // mixed precision: tensor-core ladder tiles sorted by row tile (16, 32, 64)
+    LadderTile *tctiles = nullptr;
+    int ntc16 = 0, ntc32 = 0, ntc64 = 0;
+    double *t_ref = nullptr, *g_ref = nullptr;  // refresh point of the defect correction
+    int *tc_err = nullptr;
     int nrpairs = 0;
     size_t rings_smem = 0;
 };
@@ -53,7 +58,8 @@ constexpr int kDiisMax = 16;   // DIIS history capacity (k_diis_* use the same b
 
 // Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
 enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
-                KID_UPDATE, KID_REDUCE, KID_PACK, KID_PH_BUILD, KID_RING_QUAD, KID_RINGS, KID_COUNT };
+                KID_UPDATE, KID_REDUCE, KID_PACK, KID_PH_BUILD, KID_RING_QUAD, KID_RINGS, KID_LADDER_TC,
+                KID_COUNT };
 struct KernelTimer {
     bool on = false;
     cudaEvent_t ev[2 * 64];
@@ -111,6 +117,7 @@ struct CtlBuffers {
 struct TermFlags {
     int do_driver = 1, do_mosaic = 1, do_ladder = 1, do_pp = 1, do_hh = 1, do_ring = 1, do_xring = 1;
     int drpa = 0;
+    int mixed = 0;  // particle-particle ladder on the tensor cores (defect correction on t - t_ref)
 };
 
 void launch_mp2(const DevBatch &d, cudaStream_t st);
@@ -122,6 +129,10 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st);
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt = nullptr);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
+// Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)
+void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st);
+// Refresh point: t_ref <- t and g_ref <- FP64 particle-particle ladder of t_ref
+void launch_refresh(const DevBatch &d, cudaStream_t st);
 // Device-side iteration control
 void launch_control(const DevBatch &d, const CtlBuffers &c, double tol, int max_iter, int ndiis, int init,
                     cudaStream_t st);

@@ -918,6 +918,19 @@ __global__ void k_diis_extrap2(const ChunkDev *__restrict__ chunks, const SolveD
     t[p] = x;
 }
 
+__global__ void k_copy(int64_t n, const double *__restrict__ src, double *__restrict__ dst)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) dst[p] = src[p];
+}
+
+void launch_refresh(const DevBatch &d, cudaStream_t st)
+{
+    k_copy<<<(unsigned)((d.namp + 255) / 256), 256, 0, st>>>(d.namp, d.t, d.t_ref);
+    k_ladder3<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t_ref, d.hh0,
+                                        d.hh, 0, 1, 0, d.g_ref, d.active);
+}
+
 void launch_control(const DevBatch &d, const CtlBuffers &c, double tol, int max_iter, int ndiis, int init,
                     cudaStream_t st)
 {
@@ -1012,7 +1025,8 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
 
 const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh", "k_ladder",
                                       "k_mosaic_s", "k_mosaic_reduce", "k_ring_int", "k_update",
-                                      "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad", "k_rings"};
+                                      "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad", "k_rings",
+                                      "k_ladder_tc"};
 
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt)
@@ -1028,11 +1042,18 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
             kt->end(st);
             n++;
         }
+        const int pp64 = (f.do_pp && !f.mixed) ? 1 : 0;
         kt->begin(KID_LADDER, st);
         k_ladder3<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t, d.hh0,
-                                            d.hh, 0, f.do_pp, f.do_hh, d.g, d.active);
+                                            d.hh, 0, pp64, f.do_hh, d.g, d.active);
         kt->end(st);
         n++;
+        if (f.do_pp && f.mixed) {
+            kt->begin(KID_LADDER_TC, st);
+            launch_ladder_tc(d, d.t_ref, d.g_ref, d.tc_err, st);
+            kt->end(st);
+            n += (d.ntc16 > 0) + (d.ntc32 > 0) + (d.ntc64 > 0);
+        }
     }
     if (f.do_mosaic) {
         kt->begin(KID_MOSAIC_S, st);

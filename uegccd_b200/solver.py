@@ -73,10 +73,11 @@ class Context:
         rc = capi.check(capi.lib().uegccd_drpa(self._h, C.byref(o), capi.dptr(t2), C.byref(r)))
         return rc, r.as_dict(), en[: r.n_recorded].copy(), dts[: r.n_recorded].copy()
 
-    def ccd_g2(self, t_abab, mask: int = 31) -> np.ndarray:
+    def ccd_g2(self, t_abab, mask: int = 31, precision: int = 0) -> np.ndarray:
+        """One residual G2 of the selected terms (precision 1: tensor-core ladder)."""
         g = self.zeros_t()
         t = np.ascontiguousarray(t_abab, dtype=np.float64)
-        capi.check(capi.lib().uegccd_ccd_g2(self._h, capi.dptr(t), mask, capi.dptr(g)))
+        capi.check(capi.lib().uegccd_ccd_g2_ex(self._h, capi.dptr(t), mask, precision, capi.dptr(g)))
         return g
 
 
