@@ -169,6 +169,10 @@ def kernel_units(st):
     return {
         "k_ladder": ("flop", 2 * (st["ov2"] + st["o2v"])),
         "k_ladder_hh": ("flop", 2 * st["o2v"]),
+        # pp ladder on the tensor cores (FP16 operands)
+        "k_ladder_tc": ("tflop16", 2 * st["ov2"]),
+        # X W, Y W per ph row (2 O^2 each) and 7 O-long dots per pair of rows (one per amplitude)
+        "k_rings": ("flop", 2 * (2 * O * O * O * V + 7 * O * A)),
         # reads t once, writes X, Y, Ex, Ey, A1, A2, A3 rows and Sx, Sy
         "k_ph_build": ("byte", 8 * A + 7 * 8 * ph + 2 * 8 * O * V),
         # reads A1, A2, A3, X, Y rows once, writes the two products per amplitude
@@ -209,6 +213,9 @@ def run_gpu(args, rank, world):
 
     from uegccd_b200 import Batch
 
+    opts = dict(SOLVE_OPTS)
+    if args.precision == "mixed":
+        opts["precision"] = 1
     tw = twists(args.twists, rank=rank)
     systems = build_systems(tw)
     batch = Batch(systems)
@@ -216,7 +223,7 @@ def run_gpu(args, rank, world):
     rc_r, e2_r, res_r = batch.solve()
     # warm-up (untimed)
     for _ in range(args.warmup):
-        rc, e2, res = batch.solve(**SOLVE_OPTS)
+        rc, e2, res = batch.solve(**opts)
     batch.set_profiling(True)
     dist = None
     if world > 1:
@@ -226,7 +233,7 @@ def run_gpu(args, rank, world):
     step_ms = []
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         for _ in range(args.steps):
-            rc, e2, res = batch.solve(**SOLVE_OPTS)
+            rc, e2, res = batch.solve(**opts)
             step_ms.append(res[0]["gpu_ms"])
     stats = batch.kernel_stats()
     batch.set_profiling(False)
@@ -239,7 +246,7 @@ def run_gpu(args, rank, world):
     for _ in range(max(1, min(args.steps, 3))):
         t0 = time.perf_counter()
         b2 = Batch(systems)
-        rc2, e2b, res2 = b2.solve(**SOLVE_OPTS)
+        rc2, e2b, res2 = b2.solve(**opts)
         amps = [b2.amplitudes(s) for s in range(b2.n)]
         hb, db = b2.transfer_bytes()
         b2.close()
@@ -305,6 +312,8 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--iters-per-solve", type=float, default=None)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="mixed: particle-particle ladder on the tensor cores (FP16/FP32, defect correction)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -361,7 +370,12 @@ def main():
         kind = kinds[0][0]
         units = sum(u[1] for u in kinds) / len(kinds) * nsys  # one launch covers every solve
         avg_s = ms / 1e3 / max(launches, 1)
-        if kind == "flop":
+        if kind == "tflop16":
+            ach = units / avg_s / 1e12
+            kern[k] = {"bound": "tensor", "achieved": ach, "peak": BF16_PEAK, "unit": "TFLOP/s",
+                       "frac": ach / BF16_PEAK, "avg_ms": avg_s * 1e3, "launches": launches,
+                       "peak_source": "measured (dense 16-bit tensor)"}
+        elif kind == "flop":
             ach = units / avg_s / 1e12
             kern[k] = {"bound": "tensor", "achieved": ach, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
                        "frac": ach / FP64_PEAK_TFLOPS, "avg_ms": avg_s * 1e3, "launches": launches,
@@ -375,9 +389,11 @@ def main():
     roof["kernel"] = top
     roof["traffic"] = TRAFFIC_PER_LAUNCH.get(top)
     flops_pp = sum(ps["ov2"] * 2 for ps in per_solve) / len(per_solve) * nsys
+    if args.precision == "mixed":
+        config["precision"] = "particle-particle ladder FP16 tensor cores (FP32 accumulate), rest FP64"
     line = {"metric": metric, "value": g["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": g["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f16/f64", "data": "synthetic", "config": config,
             "e2e": {"value": g["e2e_value"], "unit": "solves/s", "h2d_bytes_per_step": g["h2d"],
                     "d2h_bytes_per_step": g["d2h"]},
             "gpu_launches": int(g["launches_per_step"]) * args.steps,
