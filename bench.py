@@ -56,9 +56,9 @@ def _measured_peaks():
 
 
 HBM_PEAK, BF16_PEAK = _measured_peaks()
-# DRAM bytes per launch of the top kernels from one ncu capture (4 twists, scaled to
-# 100 twists by the amplitudes processed); see profiles/.
-TRAFFIC_PER_LAUNCH = {}
+# DRAM bytes of one launch per solve, from one ncu capture of an 8-twist batch
+# (dram__bytes_read.sum + dram__bytes_write.sum / 8); scaled by the solves of a launch.
+TRAFFIC_PER_SOLVE = {"k_ladder": 15.2e6 / 8, "k_rings": 36.1e6 / 8}
 
 
 def twists(n: int, seed: int = SEED, rank: int = 0):
@@ -312,6 +312,9 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--iters-per-solve", type=float, default=None)
+    ap.add_argument("--serve-requests", type=int, default=150,
+                    help="requests of the serving stream reported under 'serve' (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=150.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="mixed: particle-particle ladder on the tensor cores (FP16/FP32, defect correction)")
     args = ap.parse_args()
@@ -387,7 +390,8 @@ def main():
     top = max(kern, key=lambda k: kern[k]["avg_ms"] * kern[k]["launches"])
     roof = dict(kern[top])
     roof["kernel"] = top
-    roof["traffic"] = TRAFFIC_PER_LAUNCH.get(top)
+    tr = TRAFFIC_PER_SOLVE.get(top)
+    roof["traffic"] = tr * nsys if tr else None
     flops_pp = sum(ps["ov2"] * 2 for ps in per_solve) / len(per_solve) * nsys
     if args.precision == "mixed":
         config["precision"] = "particle-particle ladder FP16 tensor cores (FP32 accumulate), rest FP64"
@@ -405,6 +409,18 @@ def main():
                       "pp_ladder_gflop_per_iter": flops_pp / 1e9,
                       "replay_niter_mean": g["replay_niter_mean"],
                       "replay_vs_diis_max_dE": g["replay_vs_diis_max_dE"]}}
+    if world == 1 and args.serve_requests > 0:
+        from uegccd_b200 import serve
+
+        reqs = serve.poisson_stream(args.serve_requests, rate=args.serve_rate, seed=SEED)
+        srv = serve.Server(hbm_budget=40 << 30, max_batch=64, tol=1e-8)
+        wall = srv.run(reqs, realtime=True)
+        sv = serve.summarize(reqs, wall)
+        sv.update({"arrival_rate": args.serve_rate, "stream": "Poisson; N in {14,54,66,114}; rs log-uniform "
+                   "[0.5,5]; M/(N/2) in {4,8,12,16,20}; twist U[-0.5,0.5)^3; MP2/dRPA/CCD 0.2/0.2/0.6",
+                   "batches": srv.batches_started, "max_concurrent_batches": srv.max_concurrent,
+                   "hbm_budget_gib": 40})
+        line["serve"] = sv
     if world == 1 and not args.no_cpu_baseline:
         ncores = 1
         r, per_iter, wall = oracle_rate(ncores, args.cpu_iters, g["replay_niter_mean"])

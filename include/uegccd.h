@@ -147,6 +147,11 @@ int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on);
 int32_t uegccd_batch_kernel_stats(UegccdBatch *b, int32_t max, const char **names, double *ms,
                                   int64_t *launches);
 
+/* Device bytes one system needs inside a batch (tables, amplitudes, DIIS history of
+ * ndiis vectors, mixed-precision buffers when mixed != 0) and its number of allowed
+ * amplitudes: the admission measure of a serving loop.  Host-only, no device needed. */
+int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int64_t *bytes, int64_t *namp);
+
 /* Host<->device bytes the batch has moved since its creation (its upload included). */
 int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h);
 

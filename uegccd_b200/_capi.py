@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_PKG, "libuegccd.so")
 
 UEGCCD_OK = 0
 UEGCCD_NOT_CONVERGED = 1
+UEGCCD_ERR_ALLOC = -3
 UEGCCD_FP64, UEGCCD_MIXED = 0, 1
 UEGCCD_REPLAY, UEGCCD_DIIS = 0, 1
 
@@ -60,7 +61,7 @@ EXPORTS = [
     "uegccd_mp2", "uegccd_ccd", "uegccd_drpa", "uegccd_ccd_g2", "uegccd_batch_create",
     "uegccd_batch_destroy", "uegccd_batch_solve", "uegccd_batch_get_amplitudes", "uegccd_last_error",
     "uegccd_version", "uegccd_batch_set_profiling", "uegccd_batch_kernel_stats",
-    "uegccd_batch_transfer_bytes", "uegccd_ccd_g2_ex",
+    "uegccd_batch_transfer_bytes", "uegccd_ccd_g2_ex", "uegccd_footprint",
 ]
 
 _lib = None
@@ -90,6 +91,7 @@ def lib() -> C.CDLL:
         L.uegccd_batch_set_profiling.argtypes = [vp, C.c_int32]
         L.uegccd_batch_kernel_stats.argtypes = [vp, C.c_int32, P(C.c_char_p), dp, P(C.c_int64)]
         L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
+        L.uegccd_footprint.argtypes = [P(System), C.c_int32, C.c_int32, P(C.c_int64), P(C.c_int64)]
         L.uegccd_last_error.restype = C.c_char_p
         L.uegccd_version.restype = C.c_char_p
         _lib = L
@@ -126,3 +128,11 @@ def make_system(nocc: int, L: float, madelung: float, eigen: np.ndarray, nvec: n
                nv.ctypes.data_as(C.POINTER(C.c_int32)))
     s._keep = (eigen, nv)
     return s
+
+
+def footprint(system_tuple, ndiis: int = 6, mixed: bool = False):
+    """(device bytes, allowed amplitudes) of one system; no GPU needed."""
+    s = make_system(*system_tuple)
+    b, a = C.c_int64(), C.c_int64()
+    check(lib().uegccd_footprint(C.byref(s), ndiis, 1 if mixed else 0, C.byref(b), C.byref(a)))
+    return b.value, a.value

@@ -848,6 +848,32 @@ int32_t uegccd_batch_kernel_stats(UegccdBatch *b, int32_t max, const char **name
     return n;
 }
 
+int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int64_t *bytes, int64_t *namp)
+{
+    if (!sys || !bytes) return fail(UEGCCD_ERR_ARG, "null argument");
+    SystemHost h;
+    int rc = read_system(sys, h);
+    if (rc) return rc;
+    SolvePlan P;
+    std::string msg = build_solve_plan(h, P);
+    if (!msg.empty()) return fail(UEGCCD_ERR_ARG, msg);
+    const int64_t A = P.namp, O = P.O, V = P.V, M = P.M;
+    int64_t hh = 0, nblk = (int64_t)P.blocks.size();
+    for (const auto &B : P.blocks) hh += (int64_t)B.o * B.o;
+    int64_t b = 0;
+    b += A * (8 * 6 + sizeof(AmpInfo) + 4);          // t, t_new, g, S, g_rq, g_xq; amps; partner
+    b += O * O * V * 4;                              // pos
+    b += O * V * O * 8 * 3;                          // dRPA ring intermediates
+    b += O * V * 2 * 2;                              // ph rows
+    b += hh * 8 + nblk * (sizeof(BlockDev) + 8) + M * (16 + 8) + (P.q2max + 1) * 8;
+    b += A * 8 * 2 * (int64_t)std::max(0, (int)ndiis);  // DIIS history
+    if (mixed) b += A * 8 * 2;                       // t_ref, g_ref
+    b += (int64_t)O * O * V * 8 * 3;                 // reference-layout staging (one solve)
+    *bytes = b;
+    if (namp) *namp = A;
+    return 0;
+}
+
 int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h)
 {
     if (!b) return fail(UEGCCD_ERR_ARG, "null batch");

@@ -1,0 +1,208 @@
+"""Serving loop: continuous batching of independent UEG solves on one GPU.
+
+Requests (N, rs, basis ratio M/(N/2), twist, method) arrive over time.  The
+dispatcher admits every arrived request whose device footprint (amplitudes,
+index tables and DIIS history, from uegccd_footprint) fits the free part of the
+HBM budget.  It groups the admitted requests by method into a batch and starts
+that batch at once on its own CUDA stream, in a worker thread.  Batches that
+start while others run overlap with them on the device; the ctypes calls release
+the GIL.  Inside a batch every solve is iterated, and frozen when converged,
+independently of the others (device-side convergence control).  A batch's memory
+returns to the budget when its last solve finishes, which admits the next
+requests.
+
+The result of a solve does not depend on which batch it ran in: each solve's
+arithmetic, including its reductions, touches only its own data, in a fixed
+order (tests/test_gpu_serve.py).
+"""
+from __future__ import annotations
+
+import dataclasses
+import threading
+import time
+from collections import deque
+
+import numpy as np
+
+from . import _capi, heg
+from .solver import Batch
+
+METHODS = ("MP2", "dRPA", "CCD")
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    nelectron: int
+    rs: float
+    ratio: int
+    twist: tuple
+    method: str
+    t_arrival: float = 0.0
+    # filled by the server
+    system: tuple | None = None
+    nbytes: int = 0
+    t_admit: float = 0.0
+    t_done: float = 0.0
+    e2: float = float("nan")
+    ecorr: float = float("nan")
+    ecorr_sosex: float = float("nan")
+    niter: int = 0
+    status: int = 0
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_arrival
+
+
+_SHELLS = None
+
+
+def _pool_for(nocc: int, nbasis: int) -> int:
+    """Smallest |n|^2 cutoff whose lattice holds 1.5x the basis (room for the twist sort)."""
+    global _SHELLS
+    if _SHELLS is None:
+        r = 16
+        g = np.arange(-r, r + 1)
+        n2 = (g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2).ravel()
+        _SHELLS = np.cumsum(np.bincount(n2, minlength=r * r + 1))[: r * r + 1]
+    need = int(1.5 * nbasis) + 8
+    k = int(np.searchsorted(_SHELLS, need))
+    if k >= len(_SHELLS):
+        raise ValueError("basis too large for the serving set-up")
+    return max(k, 1)
+
+
+def build_system(req: Request):
+    """Host set-up of one request: the req.ratio * N/2 lowest |n + k_s|^2 plane waves."""
+    nocc = req.nelectron // 2
+    nbasis = req.ratio * nocc
+    fcut = float(req.ratio) ** (2.0 / 3.0)
+    inp = heg.default_input(nelectron=req.nelectron, maxkpoint=_pool_for(nocc, nbasis), rsmin=req.rs,
+                            rsmax=req.rs, fcut=fcut, ntwist=req.twist)
+    return heg.Heg(inp).system()
+
+
+def poisson_stream(n: int, rate: float, seed: int = 7, nelectrons=(14, 54, 66, 114), ratios=(4, 8, 12, 16, 20),
+                   weights=(0.2, 0.2, 0.6)):
+    """Seeded request stream: Poisson arrivals, N uniform over `nelectrons`, rs log-uniform
+    in [0.5, 5], basis ratio uniform over `ratios`, twist U[-0.5,0.5)^3, method MP2/dRPA/CCD."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        out.append(Request(
+            rid=k,
+            nelectron=int(rng.choice(nelectrons)),
+            rs=float(np.exp(rng.uniform(np.log(0.5), np.log(5.0)))),
+            ratio=int(rng.choice(ratios)),
+            twist=tuple(float(x) for x in rng.random(3) - 0.5),
+            method=str(rng.choice(METHODS, p=list(weights))),
+            t_arrival=t,
+        ))
+    return out
+
+
+class Server:
+    """Continuous-batching request loop over the uegccd batch API."""
+
+    def __init__(self, hbm_budget: int = 40 << 30, max_batch: int = 64, ndiis: int = 6, tol: float = 1e-8,
+                 max_iter: int = 200):
+        self.budget = hbm_budget
+        self.max_batch = max_batch
+        self.opts = dict(scheme=1, ndiis=ndiis, denom_factor=1.0, tol=tol, max_iter=max_iter)
+        self.ndiis = ndiis
+        self.lock = threading.Lock()
+        self.in_use = 0
+        self.batches_started = 0
+        self.max_concurrent = 0
+        self._live = 0
+
+    def _run_batch(self, reqs, t0):
+        method = reqs[0].method
+        try:
+            b = Batch([r.system for r in reqs])
+            if method == "MP2":
+                rc, e2, res = b.solve(max_iter=1)
+            else:
+                rc, e2, res = b.solve(drpa=(method == "dRPA"), **self.opts)
+            b.close()
+            t_done = time.perf_counter() - t0
+            for r, e, x in zip(reqs, e2, res):
+                r.e2 = float(e)
+                r.ecorr = float(e) if method == "MP2" else x["ecorr"]
+                r.ecorr_sosex = x["ecorr_sosex"]
+                r.niter = x["niter"]
+                r.status = rc
+                r.t_done = t_done
+        except _capi.UegccdError as exc:
+            t_done = time.perf_counter() - t0
+            for r in reqs:
+                r.status = exc.code
+                r.t_done = t_done
+        finally:
+            with self.lock:
+                self.in_use -= sum(r.nbytes for r in reqs)
+                self._live -= 1
+
+    def run(self, requests, realtime: bool = True, poll: float = 0.001):
+        """Serve `requests` (sorted by t_arrival).  realtime=False admits every request at t=0."""
+        pending = deque(sorted(requests, key=lambda r: r.t_arrival))
+        waiting = []   # arrived, set up, not yet admitted
+        threads = []
+        t0 = time.perf_counter()
+        while pending or waiting or any(t.is_alive() for t in threads):
+            now = time.perf_counter() - t0
+            while pending and (not realtime or pending[0].t_arrival <= now):
+                r = pending.popleft()
+                if not realtime:
+                    r.t_arrival = now
+                r.system = build_system(r)
+                r.nbytes = _capi.footprint(r.system, self.ndiis)[0]
+                if r.nbytes > self.budget:  # can never be admitted
+                    r.status = _capi.UEGCCD_ERR_ALLOC
+                    r.t_done = time.perf_counter() - t0
+                    continue
+                waiting.append(r)
+            started = False
+            for method in METHODS:
+                group = []
+                with self.lock:
+                    free = self.budget - self.in_use
+                    for r in [w for w in waiting if w.method == method]:
+                        if len(group) >= self.max_batch:
+                            break
+                        if r.nbytes <= free:
+                            group.append(r)
+                            free -= r.nbytes
+                    if group:
+                        self.in_use += sum(r.nbytes for r in group)
+                        self._live += 1
+                        self.max_concurrent = max(self.max_concurrent, self._live)
+                if group:
+                    t_admit = time.perf_counter() - t0
+                    for r in group:
+                        r.t_admit = t_admit
+                        waiting.remove(r)
+                    th = threading.Thread(target=self._run_batch, args=(group, t0), daemon=True)
+                    th.start()
+                    threads.append(th)
+                    self.batches_started += 1
+                    started = True
+            if not started:
+                time.sleep(poll)
+        for th in threads:
+            th.join()
+        return time.perf_counter() - t0
+
+
+def summarize(reqs, wall: float) -> dict:
+    lat = np.array([r.latency for r in reqs])
+    done = [r for r in reqs if r.status >= 0]
+    return {
+        "requests": len(reqs), "completed": len(done), "wall_s": wall,
+        "solves_per_s": len(done) / wall if wall > 0 else float("nan"),
+        "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "by_method": {m: sum(1 for r in reqs if r.method == m) for m in METHODS},
+    }
