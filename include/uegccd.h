@@ -140,6 +140,11 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
                        UegccdResult *results);
 /* Copies solve s's amplitudes out in the reference layout (T2abab). */
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
+/* Solve s's per-iteration energies and biggest changes from the last batch solve (the
+ * rows of the reference's iteration table, CCD.f90:76,96 / dRPA.f90:77,92): copies at
+ * most max_rec of each (either pointer may be NULL) and sets *n_recorded. */
+int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dts, int32_t max_rec,
+                         int32_t *n_recorded);
 
 /* Live kernel timing: when on, every kernel of a batch solve is bracketed by CUDA
  * events on the batch's stream; stats return per-kernel total ms and launches. */

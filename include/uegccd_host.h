@@ -61,6 +61,30 @@ int uegccd_heg_info(const UegccdHeg *h, UegccdHegInfo *info);
 void uegccd_find_tol(double rs, double *tolmax, double *failratio, double *denomfactor);
 const char *uegccd_host_last_error(void);
 
+/* ---- The ZCode program (Main.f90:2-320) ------------------------------------ */
+
+#define UEGCCD_CONN_LIMIT 400   /* ConnectivityLimit, MP2.f90:26 */
+
+/* Connectivity histogram of one basis (MP2.f90:56-87): conn[q-1] counts the allowed
+ * excitations ij->ab outside the core (every index >= core_n) with |n_i - n_a|^2 = q,
+ * plus those with |n_i - n_b|^2 = q.  conn has UEGCCD_CONN_LIMIT entries. */
+int uegccd_connectivity(const UegccdSystem *sys, int32_t core_n, int32_t *conn);
+/* Special twist (Main.f90:176,213-231): conn holds ntwists histograms; writes the
+ * average histogram (conn_avg, UEGCCD_CONN_LIMIT, may be NULL), each twist's weighted
+ * squared distance sum_q ((conn_q - avg_q)/q^2)^2 (diff2, ntwists, may be NULL) and
+ * the index of the first twist with the smallest distance. */
+int uegccd_special_twist(int32_t ntwists, const int32_t *conn, double *conn_avg, double *diff2, int32_t *best);
+/* One REAL(8) item of gfortran list-directed output (write(u,*)), as fort.59 holds
+ * them: a blank, then 17 significant digits in a G25 field.  Returns its length. */
+int32_t uegccd_list_real(double x, char *buf, int32_t len);
+/* The whole program in the working directory: reads input_path (NULL: "Input"),
+ * writes Output, fort.58 and fort.59.  twists_path (may be NULL) lists the twist
+ * angles of the average, three numbers per line; missing ones are drawn from a
+ * seeded U[-0.5,0.5)^3 stream.  scheme is UEGCCD_REPLAY or UEGCCD_DIIS.  The
+ * solves run on the current CUDA device; every twist of the average is one batch. */
+int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme);
+const char *uegccd_zcode_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

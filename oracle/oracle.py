@@ -107,7 +107,9 @@ def _ptr(a: np.ndarray, ctype=C.c_double):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
-# Defaults for keys that older Input files (the benchmarks' key set) do not set.
+# Defaults for keys that older Input files (the benchmarks' key set) do not set.  A key
+# added after those files were written takes the behaviour of the code that predates it:
+# DoSkipTA F (the twist average always ran; Main.f90:95 added the stop).
 DEFAULTS = {
     "# Electrons": "14", "Momentum Cutoff": "2", "rSMin": "1.0", "rSMax": "1.0", "# rS Points": "1",
     "Safe ERI": "F", "Do Rings": "T", "Do XRings": "T", "Do Ladders": "T", "Do Mosaics": "T",
@@ -118,7 +120,7 @@ DEFAULTS = {
     "CoreFactor": "0.0", "TACalcN": "0", "DoCalcTACCD": "F", "DodRPASOSEX": "F",
     "DoTruncCoulombHF": "F", "DoTruncCoulombAll": "F", "DoKS": "F", "MadelungFactor": "1.0",
     "DoSingleCalc": "T", "Gap": "0.0", "fcut": "10.0", "corefcut": "1.0", "fcut2ecut": "F",
-    "GapII": "-0.01", "DoSFCalcMP2": "F", "DoSFCalcCCD": "F", "DoSkipTA": "T", "DoOnlyMP2Grid": "F",
+    "GapII": "-0.01", "DoSFCalcMP2": "F", "DoSFCalcCCD": "F", "DoSkipTA": "F", "DoOnlyMP2Grid": "F",
 }
 
 

@@ -106,6 +106,7 @@ def g5(ref):
     return dict(keys=keys, e_scf=e_scf, eigen=eig, e2=e2, iterations=it, ec_ccd=ecs[0], niter=conv[0],
                 max_res=maxres[0], ta_twists=[r[:3] for r in rows], ta_hf_mp2_ccd=[r[3:6] for r in rows],
                 special_twist=special, special_ec_ccd=ecs[-1], special_niter=conv[-1],
+                output_lines=lines, fort59_lines=f59,
                 source="source/Test/Output, source/Test/fort.59")
 
 

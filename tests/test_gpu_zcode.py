@@ -1,0 +1,99 @@
+"""The ZCode drop-in end to end on the GPU: Output and fort.59 against the
+reference's own files (G5: source/Test; G3: benchmarks/ZRun-v6-N14) and the G1
+dRPA benchmark.
+
+Output is compared line by line: the text around the numbers (every label, width
+and integer, iteration counts included) must be identical; each real number must
+agree within 2e-10 (the last printed digit of the F15.10 iteration table).
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from uegccd_b200 import zcode
+
+pytestmark = pytest.mark.gpu
+
+FLOAT = re.compile(r"-?\d+\.\d+(?:E[+-]\d+)?")
+TOL = 2e-10
+
+
+def _skeleton(line):
+    return FLOAT.sub(lambda m: "#" * len(m.group()), line)
+
+
+def _compare_output(ours, ref):
+    assert len(ours) == len(ref), (len(ours), len(ref))
+    for k, (a, b) in enumerate(zip(ours, ref)):
+        assert _skeleton(a) == _skeleton(b), (k, a, b)
+        xa = [float(x) for x in FLOAT.findall(a)]
+        xb = [float(x) for x in FLOAT.findall(b)]
+        np.testing.assert_allclose(xa, xb, rtol=0, atol=TOL, err_msg=f"line {k}: {a!r} vs {b!r}")
+
+
+def _write_twists(path, tws):
+    with open(path, "w") as f:
+        for t in tws:
+            f.write("%.17g %.17g %.17g\n" % tuple(t))
+
+
+def test_g5_output_and_fort59(goldens, tmp_path, monkeypatch):
+    g = goldens["G5"]
+    (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in g["keys"].items()))
+    _write_twists(tmp_path / "Twists", g["ta_twists"])
+    monkeypatch.chdir(tmp_path)
+    zcode.run("Input", "Twists")
+    _compare_output((tmp_path / "Output").read_text().splitlines(), g["output_lines"])
+    ours = (tmp_path / "fort.59").read_text().splitlines()
+    ref = g["fort59_lines"]
+    assert len(ours) == len(ref)
+    for a, b in zip(ours, ref):
+        assert _skeleton(a) == _skeleton(b), (a, b)
+        np.testing.assert_allclose([float(x) for x in FLOAT.findall(a)], [float(x) for x in FLOAT.findall(b)],
+                                   rtol=1e-12, atol=1e-15)
+    # the twist-independent host lines are bit-identical text
+    for a, b in zip(ours, ref):
+        if "conn" in b or "special" in b or "lowest" in b or re.fullmatch(r"\s+\d+\s+\S+\s*", b):
+            assert a == b
+
+
+def test_g3_hundred_twists_ccd(goldens, tmp_path, monkeypatch):
+    g = goldens["G3"]
+    (tmp_path / "Input").write_text(g["input_text"])
+    _write_twists(tmp_path / "Twists", g["twists"])
+    monkeypatch.chdir(tmp_path)
+    zcode.run("Input", "Twists")
+    rows = [[float(x) for x in l.split()] for l in (tmp_path / "fort.59").read_text().splitlines()[:100]]
+    rows = np.array(rows)
+    np.testing.assert_array_equal(rows[:, :3], np.array(g["twists"]))
+    np.testing.assert_allclose(rows[:, 3:6], np.array(g["hf_mp2_ccd"]), rtol=0, atol=1e-9)
+    out = (tmp_path / "Output").read_text()
+    ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
+    conv = [int(x) for x in re.findall(r"converged in\s+(\d+)", out)]
+    assert len(ecs) == 101                       # 100 twists + the special twist
+    assert conv[-1] == g["special_niter"]
+    assert abs(ecs[-1] - g["special_ec_ccd"]) < 1e-9
+    f59 = (tmp_path / "fort.59").read_text()
+    special = [float(x) for x in FLOAT.findall([l for l in f59.splitlines() if "special" in l][0])]
+    np.testing.assert_array_equal(special, g["special_twist"])
+
+
+def test_g1_drpa_executable(goldens, tmp_path):
+    """The uegccd_zcode executable on the G1 dRPA benchmark Input (no twist average)."""
+    g = goldens["G1"]
+    exe = os.path.join(os.path.dirname(zcode.__file__), "uegccd_zcode")
+    (tmp_path / "Input").write_text(g["input_text"])
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    out = (tmp_path / "Output").read_text()
+    ec = float(re.search(r"Ec\(dRPA\) is\s+(-?\d+\.\d+)", out).group(1))
+    es = float(re.search(r"Ec\(SOSEX\) is\s+(-?\d+\.\d+)", out).group(1))
+    niter = int(re.search(r"dRPA has converged in\s+(\d+)", out).group(1))
+    assert niter == g["niter"]
+    assert abs(ec - g["ec_drpa"]) < 2e-12 and abs(es - g["ec_sosex"]) < 2e-12
+    e2 = float(re.search(r"E\(2\) is\s+(-?\d+\.\d+)", out).group(1))
+    assert abs(e2 - g["e2"]) < 2e-12
+    assert not (tmp_path / "fort.59").exists()   # TACalcN 0: no twist average

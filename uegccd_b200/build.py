@@ -16,9 +16,10 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libuegccd.so")
+ZCODE = os.path.join(PKG, "uegccd_zcode")
 OBJDIR = os.path.join(PKG, "_build")
 
-SOURCES = ["capi.cu", "kernels_fp64.cu", "kernels_tc.cu", "plan.cpp", "heg_host.cpp"]
+SOURCES = ["capi.cu", "kernels_fp64.cu", "kernels_tc.cu", "plan.cpp", "heg_host.cpp", "zcode.cpp"]
 HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -57,6 +58,14 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
         subprocess.run(cmd, check=True)
     if _stale(LIB, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    main = os.path.join(CSRC, "zcode_main.cpp")
+    if _stale(ZCODE, [LIB, main] + hdrs):
+        # the drop-in executable for the reference's ZCode program, linked to the library beside it
+        cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), main, "-o", ZCODE, "-L", PKG,
+               "-luegccd", "-Xlinker", "-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -97,6 +97,7 @@ struct UegccdBatch {
     // device-side iteration control (allocated on first solve; DIIS history grows on demand)
     CtlBuffers ctl;
     int diis_cap = 0;
+    std::vector<int> last_niter;     // iterations of each solve in the last solve call
     // CUDA graphs of one iteration: plain and with kernel timers, keyed by the options
     struct GraphKey {
         int do_ring, do_xring, do_ladder, do_mosaic, drpa, ndiis, max_iter, mixed;
@@ -619,6 +620,8 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     float ms = 0.f;
     CU(cudaEventElapsedTime(&ms, b.ev0, b.ev1));
     int status = 0;
+    b.last_niter.assign(n, 0);
+    for (int s = 0; s < n; s++) b.last_niter[s] = std::min(st[s].niter, max_rec);
     for (int s = 0; s < n; s++) {
         UegccdResult &r = res[s];
         r.ecorr = st[s].e;
@@ -886,6 +889,24 @@ int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab)
 {
     if (!b || !t_abab || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
     return unpack_to_host(*b, s, b->d.t, t_abab, nullptr, nullptr);
+}
+
+int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dts, int32_t max_rec,
+                         int32_t *n_recorded)
+{
+    if (!b || s < 0 || s >= b->d.nsolves || max_rec < 0 || !n_recorded)
+        return fail(UEGCCD_ERR_ARG, "bad argument");
+    if (b->last_niter.size() != (size_t)b->d.nsolves || !b->ctl.rec_e)
+        return fail(UEGCCD_ERR_ARG, "no solve has run on this batch");
+    const int n = std::min(b->last_niter[s], max_rec);
+    const size_t off = (size_t)s * b->ctl.max_rec;
+    if (n > 0 && energies)
+        CU(cudaMemcpyAsync(energies, b->ctl.rec_e + off, n * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    if (n > 0 && dts)
+        CU(cudaMemcpyAsync(dts, b->ctl.rec_dt + off, n * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    *n_recorded = n;
+    return UEGCCD_OK;
 }
 
 }  // extern "C"

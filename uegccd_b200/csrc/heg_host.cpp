@@ -207,7 +207,9 @@ void uegccd_default_input(UegccdInput *in)
     in->corefcut = 1.0;
     in->gapii = -0.01;
     in->do_single_calc = 1;
-    in->do_skip_ta = 1;
+    // keys newer than an Input file take the behaviour of the code that predates them:
+    // without DoSkipTA the twist average always ran
+    in->do_skip_ta = 0;
 }
 
 // ReadInput (IO.f90:14-348): "Key: Value" lines, '!' comments; every key of the

@@ -1,0 +1,489 @@
+// zcode.cpp -- the reference's ZCode program (Main.f90:2-320) as a library
+// function, with its hot path on the GPU through include/uegccd.h.
+//
+// Steps of uegccd_zcode (Main.f90 line ranges):
+//   44-48    ReadInput, init_HEG (the GPU path serves the default integrals;
+//            other ERI selections are refused by the option checks)
+//   78-79    change_rs to rSMin
+//   83-93    DoSingleCalc: MP2, then CCD or dRPA from the MP2 amplitudes
+//   95-97    DoSkipTA: stop after the single calculation
+//   112-168  every twist's MP2 (and CCD/dRPA when DoCalcTACCD) -- solved here as
+//            ONE GPU batch over all twists; the Output blocks are then written
+//            in twist order, as the reference's loop writes them
+//   170-231  averages, connectivity histogram, special twist (fort.58, fort.59)
+//   233-255  MP2 + CCD/dRPA at the special twist with the twist-averaged
+//            eigenvalues, NumRSPoints times
+//
+// Twists: the reference draws them with gfortran's rand() seeded 86456
+// (Main.f90:30,81; HEG.f90:535-549), which is not reproduced here.  The caller
+// passes a twist file (three numbers per line, used in order); missing twists
+// come from a std::mt19937_64 stream seeded 86456, U[-0.5,0.5)^3.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/uegccd.h"
+#include "../../include/uegccd_host.h"
+
+namespace {
+
+thread_local std::string g_zc_error;
+
+int zfail(int code, const std::string &m)
+{
+    g_zc_error = m;
+    return code;
+}
+
+// ---- gfortran list-directed output (write(u,*)) -----------------------------
+// REAL(8): a blank, then 17 significant digits in a 25-wide G field: F form
+// (20 wide, then 5 blanks) for 0.1 <= |x| < 1e17, else E form with a
+// three-digit exponent.  INTEGER: a blank, then I11.  CHARACTER: a blank, then
+// the text.
+std::string ld_real(double x)
+{
+    char m[64], f[96], num[64];
+    if (!std::isfinite(x)) {
+        std::snprintf(f, sizeof f, " %20s     ", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
+        return f;
+    }
+    int ex = 0;
+    if (x != 0.0) {
+        std::snprintf(m, sizeof m, "%.16e", x);  // 17 significant digits, correctly rounded
+        ex = std::atoi(std::strchr(m, 'e') + 1);
+    }
+    if (x == 0.0 || (ex >= -1 && ex < 17)) {
+        const int dec = x == 0.0 ? 16 : 16 - ex;
+        std::snprintf(num, sizeof num, "%.*f", dec, x);
+        std::snprintf(f, sizeof f, " %20s     ", num);
+        return f;
+    }
+    const std::string s(m);
+    const size_t e = s.find('e');
+    std::snprintf(num, sizeof num, "%sE%c%03d", s.substr(0, e).c_str(), ex < 0 ? '-' : '+', std::abs(ex));
+    std::snprintf(f, sizeof f, " %25s", num);
+    return f;
+}
+
+std::string ld_int(long long v)
+{
+    char f[32];
+    std::snprintf(f, sizeof f, " %11lld", v);
+    return f;
+}
+
+std::string ld_str(const char *s) { return std::string(" ") + s; }
+
+// ---- Output blocks (formats of MP2.f90:143-150, CCD.f90:127-140, dRPA.f90:123-138)
+
+const char *kStars = "              **************************************************\n";
+const char *kBar = "              *------------------------------------------------*\n";
+
+void write_mp2(FILE *f, double ehf, const double *eig, int nocc, int nao, double e2)
+{
+    std::fputs(kStars, f);
+    std::fprintf(f, "              * E(SCF) is             %18.12f a.u.  *\n", ehf);
+    std::fputs(kBar, f);
+    std::fprintf(f, "              *                RHF Eigenvalues:                *\n");
+    std::fputs(kBar, f);
+    for (int i = 0; i < nocc; i++) std::fprintf(f, "              *            %24.16E            *\n", eig[i]);
+    std::fprintf(f, "              *            ------------------------            *\n");
+    for (int a = nocc; a < nao; a++) std::fprintf(f, "              *            %24.16E            *\n", eig[a]);
+    std::fputs(kStars, f);
+    std::fprintf(f, "              * E(2) is               %18.12f a.u.  *\n", e2);
+    std::fprintf(f, "              * E(SCF) + E(2) is      %18.12f a.u.  *\n", e2 + ehf);
+    std::fputs(kStars, f);
+}
+
+void write_cc(FILE *f, const UegccdInput &in, int drpa, const UegccdResult &r, const double *en,
+              const double *dt, int nrec, double ehf)
+{
+    std::fprintf(f, drpa ? "              *              dRPA summary follows              *\n"
+                         : "              *               CCD summary follows              *\n");
+    std::fputs(kBar, f);
+    if (in.do_ring) std::fprintf(f, "              * Including ring diagrams...                     *\n");
+    if (!drpa && in.do_xring) std::fprintf(f, "              * Including crossed ring diagrams...             *\n");
+    if (!drpa && in.do_ladder) std::fprintf(f, "              * Including ladder diagrams...                   *\n");
+    if (in.do_mosaic) std::fprintf(f, "              * Including mosaic diagrams...                   *\n");
+    std::fputs(kBar, f);
+    std::fprintf(f, drpa ? "              * dRPA Energy      Iteration    Biggest change   *\n"
+                         : "              *  CCD Energy      Iteration    Biggest change   *\n");
+    for (int k = 0; k < nrec; k++)
+        std::fprintf(f, "              * %15.10f  %5d       %14.10f    *\n", en[k], k + 1, dt[k]);
+    std::fputs(kBar, f);
+    if (r.fail) {
+        std::fprintf(f, drpa ? "              * Final dRPA Energy is   DID NOT CONVERGE        *\n"
+                             : "              * Final CCD Energy is   DID NOT CONVERGE         *\n");
+    } else if (!drpa) {
+        std::fprintf(f, "              * CCD has converged in %3d iterations            *\n", r.niter);
+        std::fprintf(f, "              * Ec(CCD) is           %18.12f a.u.   *\n", r.ecorr);
+        std::fprintf(f, "              * Final CCD Energy is  %18.12f a.u.   *\n", r.ecorr + ehf);
+    } else {
+        std::fprintf(f, "              * dRPA has converged in %3d iterations           *\n", r.niter);
+        std::fprintf(f, "              * Ec(dRPA) is          %18.12f a.u.   *\n", r.ecorr);
+        std::fprintf(f, "              * Final dRPA Energy is %18.12f a.u.   *\n", r.ecorr + ehf);
+        std::fprintf(f, "              * Ec(SOSEX) is         %18.12f a.u.   *\n", r.ecorr_sosex);
+        std::fprintf(f, "              * Final SOSEX Energy is%18.12f a.u.   *\n", r.ecorr_sosex + ehf);
+    }
+    char es[32];
+    std::snprintf(es, sizeof es, "%.12E", r.max_res);  // ES18.12
+    std::fprintf(f, "              * Max CCD Residual is      %18s    *\n", es);
+    std::fputs(kStars, f);
+}
+
+// DrvCCD / DrvdRPA options from the Input (FindTol sees rS = 1, HEG.f90:28; the
+// dRPA driver's FailRatio is 1e4, dRPA.f90:100)
+UegccdOptions options_for(const UegccdInput &in, int32_t scheme)
+{
+    UegccdOptions o;
+    uegccd_default_options(&o);
+    double tolmax = 1e-8, failratio = 100, denom = 2.0;
+    uegccd_find_tol(1.0, &tolmax, &failratio, &denom);
+    o.tol = tolmax;
+    o.fail_ratio = in.do_drpa_sosex ? 1.0e4 : failratio;
+    o.denom_factor = denom;
+    o.do_ring = in.do_ring;
+    o.do_xring = in.do_xring;
+    o.do_ladder = in.do_ladder;
+    o.do_mosaic = in.do_mosaic;
+    o.core_n = (int32_t)((in.nelectron / 2) * in.core_factor);
+    o.gapii = in.gapii;
+    o.range_flags = in.range_flags;
+    if (scheme == UEGCCD_DIIS) {
+        o.scheme = UEGCCD_DIIS;
+        o.ndiis = 6;
+        o.denom_factor = 1.0;
+    }
+    return o;
+}
+
+struct Amps {
+    std::vector<double> aaaa, abab, abba;
+    explicit Amps(const UegccdSystem &s)
+    {
+        const size_t n = (size_t)s.nocc * s.nocc * (s.nao - s.nocc);
+        aaaa.assign(n, 0.0);
+        abab.assign(n, 0.0);
+        abba.assign(n, 0.0);
+    }
+};
+
+// DrvMBPT into x, then DrvCCD/DrvdRPA on t (started from x when copy_start);
+// both Output blocks appended.
+int mp2_then_cc(const UegccdInput &in, const UegccdSystem &sys, double ehf, const UegccdOptions &opt, Amps &x,
+                Amps &t, bool copy_start, UegccdResult *res)
+{
+    UegccdCtx *ctx = nullptr;
+    if (uegccd_ctx_create(&sys, &ctx)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
+    double e2 = 0.0;
+    int rc = uegccd_mp2(ctx, x.aaaa.data(), x.abab.data(), x.abba.data(), &e2);
+    if (rc) {
+        zfail(rc, uegccd_last_error());
+        uegccd_ctx_destroy(ctx);
+        return rc;
+    }
+    FILE *f = std::fopen("Output", "a");
+    if (!f) {
+        uegccd_ctx_destroy(ctx);
+        return zfail(UEGCCD_ERR_ARG, "cannot append to Output");
+    }
+    write_mp2(f, ehf, sys.eigen, sys.nocc, sys.nao, e2);
+    if (copy_start) t = x;
+    UegccdOptions o = opt;
+    std::vector<double> en(1100), dt(1100);
+    o.energies = en.data();
+    o.dts = dt.data();
+    o.max_rec = 1100;
+    rc = in.do_drpa_sosex ? uegccd_drpa(ctx, &o, t.aaaa.data(), res)
+                          : uegccd_ccd(ctx, &o, t.aaaa.data(), t.abab.data(), t.abba.data(), res);
+    if (rc >= 0) {
+        write_cc(f, in, in.do_drpa_sosex, *res, en.data(), dt.data(), res->n_recorded, ehf);
+        rc = 0;
+    } else {
+        zfail(rc, uegccd_last_error());
+    }
+    std::fclose(f);
+    uegccd_ctx_destroy(ctx);
+    return rc;
+}
+
+std::vector<std::array<double, 3>> twist_list(const char *path, int count)
+{
+    std::vector<std::array<double, 3>> tw;
+    if (path && *path) {
+        std::ifstream f(path);
+        double x, y, z;
+        while ((int)tw.size() < count && (f >> x >> y >> z)) tw.push_back({x, y, z});
+    }
+    std::mt19937_64 rng(86456);
+    std::uniform_real_distribution<double> u(-0.5, 0.5);
+    while ((int)tw.size() < count) {
+        const double a = u(rng), b = u(rng), c = u(rng);
+        tw.push_back({a, b, c});
+    }
+    return tw;
+}
+
+struct HegGuard {
+    UegccdHeg *h = nullptr;
+    HegGuard() = default;
+    HegGuard(const HegGuard &) = delete;
+    HegGuard &operator=(const HegGuard &) = delete;
+    ~HegGuard() { uegccd_heg_destroy(h); }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char *uegccd_zcode_last_error(void) { return g_zc_error.c_str(); }
+
+int uegccd_connectivity(const UegccdSystem *s, int32_t core_n, int32_t *conn)
+{
+    if (!s || !conn || !s->nvec || s->nocc <= 0 || s->nao <= s->nocc)
+        return zfail(UEGCCD_ERR_ARG, "bad argument");
+    const int O = s->nocc, M = s->nao;
+    auto n = [&](int p, int d) { return s->nvec[p + (size_t)M * d]; };
+    int r = 0;
+    for (int p = 0; p < M; p++)
+        for (int d = 0; d < 3; d++) r = std::max(r, std::abs(n(p, d)));
+    const int side = 4 * r + 1;
+    std::vector<int> orb((size_t)side * side * side, -1);
+    auto key = [&](int x, int y, int z) {
+        return ((size_t)(x + 2 * r) * side + (size_t)(y + 2 * r)) * side + (size_t)(z + 2 * r);
+    };
+    for (int p = 0; p < M; p++) orb[key(n(p, 0), n(p, 1), n(p, 2))] = p;
+    std::fill(conn, conn + UEGCCD_CONN_LIMIT, 0);
+    for (int i = 0; i < O; i++)
+        for (int j = 0; j < O; j++)
+            for (int a = O; a < M; a++) {
+                // FindIndex: the virtual b with n_b = n_i + n_j - n_a
+                const int x = n(i, 0) + n(j, 0) - n(a, 0), y = n(i, 1) + n(j, 1) - n(a, 1),
+                          z = n(i, 2) + n(j, 2) - n(a, 2);
+                if (std::abs(x) > 2 * r || std::abs(y) > 2 * r || std::abs(z) > 2 * r) continue;
+                const int b = orb[key(x, y, z)];
+                if (b < O) continue;
+                // dK2(I,J,A,B) = |n_i - n_a|^2, dK2(I,J,B,A) = |n_i - n_b|^2 (HEG.f90:985-1005)
+                int qa = 0, qb = 0;
+                for (int d = 0; d < 3; d++) {
+                    qa += (n(i, d) - n(a, d)) * (n(i, d) - n(a, d));
+                    qb += (n(i, d) - n(b, d)) * (n(i, d) - n(b, d));
+                }
+                if (qa > UEGCCD_CONN_LIMIT || qb > UEGCCD_CONN_LIMIT)
+                    return zfail(UEGCCD_ERR_ARG, "Connectivity greater than current ConnectivityLimit");
+                if (i < core_n || j < core_n || a < core_n || b < core_n) continue;  // InCore
+                conn[qb - 1]++;
+                conn[qa - 1]++;
+            }
+    return UEGCCD_OK;
+}
+
+int uegccd_special_twist(int32_t ntw, const int32_t *conn, double *conn_avg, double *diff2, int32_t *best)
+{
+    if (ntw <= 0 || !conn || !best) return zfail(UEGCCD_ERR_ARG, "bad argument");
+    std::vector<long long> sum(UEGCCD_CONN_LIMIT, 0);
+    for (int t = 0; t < ntw; t++)
+        for (int k = 0; k < UEGCCD_CONN_LIMIT; k++) sum[k] += conn[(size_t)t * UEGCCD_CONN_LIMIT + k];
+    std::vector<double> avg(UEGCCD_CONN_LIMIT);
+    for (int k = 0; k < UEGCCD_CONN_LIMIT; k++) avg[k] = (double)sum[k] / ntw;
+    double best_d = 1.0 * 100000;
+    int bt = 0;
+    for (int t = 0; t < ntw; t++) {
+        double d2 = 0.0;
+        for (int k = 0; k < UEGCCD_CONN_LIMIT; k++) {
+            const double d = (conn[(size_t)t * UEGCCD_CONN_LIMIT + k] - avg[k]) / std::pow((double)(k + 1), 2.0);
+            d2 = d2 + d * d;
+        }
+        if (t == 0) best_d = d2;
+        if (d2 < best_d) {
+            best_d = d2;
+            bt = t;
+        }
+        if (diff2) diff2[t] = d2;
+    }
+    if (conn_avg) std::copy(avg.begin(), avg.end(), conn_avg);
+    *best = bt;
+    return UEGCCD_OK;
+}
+
+int32_t uegccd_list_real(double x, char *buf, int32_t len)
+{
+    const std::string s = ld_real(x);
+    if (!buf || len <= (int32_t)s.size()) return zfail(UEGCCD_ERR_ARG, "buffer too small");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return (int32_t)s.size();
+}
+
+int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme)
+{
+    UegccdInput in;
+    if (uegccd_read_input(input_path ? input_path : "Input", 0, &in))
+        return zfail(UEGCCD_ERR_ARG, std::string("ReadInput: ") + uegccd_host_last_error());
+    HegGuard h;
+    if (uegccd_heg_create(&in, &h.h)) return zfail(UEGCCD_ERR_ARG, std::string("init_HEG: ") + uegccd_host_last_error());
+    if (FILE *f = std::fopen("Output", "w")) std::fclose(f);  // Main.f90:61-62
+    else return zfail(UEGCCD_ERR_ARG, "cannot create Output");
+    const UegccdOptions opt = options_for(in, scheme);
+    UegccdHegInfo info;
+    UegccdSystem sys;
+    UegccdResult res;
+    int rc = 0;
+    if (in.do_single_calc) {
+        uegccd_heg_info(h.h, &info);
+        uegccd_heg_system(h.h, &sys);
+        Amps x(sys), t(sys);
+        if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, true, &res))) return rc;
+    }
+    if (in.do_skip_ta) return UEGCCD_OK;  // "Finishing calculation after single point calculation"
+    const int ntw = in.tacalcn;
+    if (ntw <= 0) return UEGCCD_OK;       // no twists to average
+    const auto tw = twist_list(twists_path, ntw);
+
+    // every twist's basis (ChangeTwist), eigenvalues, E_HF and connectivity
+    std::vector<HegGuard> hs(ntw);
+    std::vector<UegccdSystem> systems(ntw);
+    std::vector<double> hf(ntw), mp2(ntw), cc(ntw);
+    std::vector<int32_t> conn((size_t)ntw * UEGCCD_CONN_LIMIT);
+    for (int t = 0; t < ntw; t++) {
+        UegccdInput ti = in;
+        for (int d = 0; d < 3; d++) ti.ntwist[d] = tw[t][d];
+        if (uegccd_heg_create(&ti, &hs[t].h)) return zfail(UEGCCD_ERR_ARG, uegccd_host_last_error());
+        uegccd_heg_info(hs[t].h, &info);
+        hf[t] = info.ehf;
+        uegccd_heg_system(hs[t].h, &systems[t]);
+        if (systems[t].nao != systems[0].nao) return zfail(UEGCCD_ERR_ARG, "twists give different basis sizes");
+        if ((rc = uegccd_connectivity(&systems[t], opt.core_n, &conn[(size_t)t * UEGCCD_CONN_LIMIT]))) return rc;
+    }
+
+    // all twists in one batch: MP2, then CCD/dRPA when DoCalcTACCD (Main.f90:126-139)
+    UegccdBatch *b = nullptr;
+    if (uegccd_batch_create(systems.data(), ntw, &b)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
+    std::vector<UegccdResult> br(ntw);
+    UegccdOptions bo = opt;
+    if (!in.do_calc_ta_ccd) bo.max_iter = 1;  // the start amplitudes only: MP2
+    rc = uegccd_batch_solve(b, &bo, in.do_drpa_sosex, mp2.data(), br.data());
+    if (rc < 0) {
+        zfail(rc, uegccd_last_error());
+        uegccd_batch_destroy(b);
+        return rc;
+    }
+    FILE *out = std::fopen("Output", "a");
+    if (!out) {
+        uegccd_batch_destroy(b);
+        return zfail(UEGCCD_ERR_ARG, "cannot append to Output");
+    }
+    std::vector<double> en(1100), dt(1100);
+    for (int t = 0; t < ntw; t++) {
+        const UegccdSystem &s = systems[t];
+        write_mp2(out, hf[t], s.eigen, s.nocc, s.nao, mp2[t]);
+        cc[t] = mp2[t];
+        if (in.do_calc_ta_ccd) {
+            int32_t nrec = 0;
+            uegccd_batch_history(b, t, en.data(), dt.data(), 1100, &nrec);
+            write_cc(out, in, in.do_drpa_sosex, br[t], en.data(), dt.data(), nrec, hf[t]);
+            // HEGData%ECorr after the driver: Ec(SOSEX) for a converged dRPA, else the last energy
+            cc[t] = (in.do_drpa_sosex && !br[t].fail) ? br[t].ecorr_sosex : br[t].ecorr;
+        }
+    }
+    std::fclose(out);
+    uegccd_batch_destroy(b);
+
+    // fort.59 per-twist rows and fort.58 connectivity rows (Main.f90:144-153)
+    FILE *f59 = std::fopen("fort.59", "w");
+    FILE *f58 = std::fopen("fort.58", "w");
+    if (!f59 || !f58) {
+        if (f59) std::fclose(f59);
+        if (f58) std::fclose(f58);
+        return zfail(UEGCCD_ERR_ARG, "cannot write fort.58/fort.59");
+    }
+    int cmax = 0;
+    for (int k = UEGCCD_CONN_LIMIT; k >= 1; k--)
+        if (conn[k - 1] > 0) {
+            cmax = k;
+            break;
+        }
+    const int M = systems[0].nao;
+    std::vector<double> eig_sum(M, 0.0);
+    std::array<double, 3> tws{0, 0, 0}, tws2{0, 0, 0};
+    double s_hf = 0, s_mp2 = 0, s_cc = 0, s_hf2 = 0, s_mp22 = 0, s_cc2 = 0;
+    for (int t = 0; t < ntw; t++) {
+        std::string row;
+        for (int d = 0; d < 3; d++) row += ld_real(tw[t][d]);
+        row += ld_real(hf[t]) + ld_real(mp2[t]) + ld_real(cc[t]);
+        std::fprintf(f59, "%s\n", row.c_str());
+        row.clear();
+        for (int k = 0; k < cmax; k++) row += ld_int(conn[(size_t)t * UEGCCD_CONN_LIMIT + k]);
+        std::fprintf(f58, "%s\n", row.c_str());
+        s_cc += cc[t];
+        s_mp2 += mp2[t];
+        s_hf += hf[t];
+        for (int d = 0; d < 3; d++) {
+            tws[d] += tw[t][d];
+            tws2[d] += std::pow(tw[t][d], 2.0);
+        }
+        for (int p = 0; p < M; p++) eig_sum[p] = eig_sum[p] + systems[t].eigen[p];
+        s_cc2 += std::pow(cc[t], 2.0);
+        s_mp22 += std::pow(mp2[t], 2.0);
+        s_hf2 += std::pow(hf[t], 2.0);
+    }
+    std::fclose(f58);
+    // averages, <x^2>, errors sqrt((<x^2>-<x>^2)/(N-1)) (Main.f90:170-199)
+    const double N = ntw;
+    auto err = [&](double m2, double m) { return std::pow((m2 - std::pow(m, 2.0)) / (N - 1), 0.5); };
+    std::string l1, l2, l3;
+    for (int d = 0; d < 3; d++) {
+        l1 += ld_real(tws[d] / N);
+        l2 += ld_real(tws2[d] / N);
+        l3 += ld_real(err(tws2[d] / N, tws[d] / N));
+    }
+    l1 += ld_real(s_hf / N) + ld_real(s_mp2 / N) + ld_real(s_cc / N) + ld_str("averages");
+    l2 += ld_real(s_hf2 / N) + ld_real(s_mp22 / N) + ld_real(s_cc2 / N) + ld_str("squared averages");
+    l3 += ld_real(err(s_hf2 / N, s_hf / N)) + ld_real(err(s_mp22 / N, s_mp2 / N)) + ld_real(err(s_cc2 / N, s_cc / N)) +
+          ld_str("errors");
+    std::fprintf(f59, "%s\n%s\n%s\n", l1.c_str(), l2.c_str(), l3.c_str());
+    std::vector<double> eig_avg(M);
+    std::string le;
+    for (int p = 0; p < M; p++) {
+        eig_avg[p] = eig_sum[p] / N;
+        le += ld_real(eig_avg[p]);
+    }
+    std::fprintf(f59, "%s\n", (le + ld_str("eigenvalue averages")).c_str());
+    std::vector<double> cavg(UEGCCD_CONN_LIMIT), diff2(ntw);
+    int32_t best = 0;
+    uegccd_special_twist(ntw, conn.data(), cavg.data(), diff2.data(), &best);
+    int amax = 0;
+    for (int k = UEGCCD_CONN_LIMIT; k >= 1; k--)
+        if (cavg[k - 1] > 0) {
+            amax = k;
+            break;
+        }
+    std::string lc;
+    for (int k = 0; k < amax; k++) lc += ld_real(cavg[k]);
+    std::fprintf(f59, "%s\n", (lc + ld_str("conn")).c_str());
+    for (int t = 0; t < ntw; t++) std::fprintf(f59, "%s\n", (ld_int(t + 1) + ld_real(diff2[t])).c_str());
+    std::fprintf(f59, "%s\n",
+                 (ld_str("special twist angle found") + ld_real(tw[best][0]) + ld_real(tw[best][1]) +
+                  ld_real(tw[best][2]))
+                     .c_str());
+    std::fprintf(f59, "%s\n", (ld_str("lowest connectivity diff squared") + ld_real(diff2[best])).c_str());
+    std::fclose(f59);
+
+    // the special twist with the twist-averaged eigenvalues (Main.f90:233-255)
+    if (uegccd_heg_change_twist(h.h, tw[best].data()) || uegccd_heg_set_eigen(h.h, eig_avg.data()))
+        return zfail(UEGCCD_ERR_ARG, uegccd_host_last_error());
+    uegccd_heg_info(h.h, &info);
+    uegccd_heg_system(h.h, &sys);
+    Amps x(sys), t(sys);
+    for (int ip = 0; ip < std::max(1, in.num_rs_points); ip++)
+        if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, ip == 0, &res))) return rc;
+    return UEGCCD_OK;
+}
+
+}  // extern "C"
