@@ -140,6 +140,21 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
                        UegccdResult *results);
 /* Copies solve s's amplitudes out in the reference layout (T2abab). */
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
+/* E(2) of one system, as uegccd_mp2 computes it, with no device allocation: this
+ * entry point has no counterpart in the reference.  It is for callers that cannot
+ * allocate device memory when they call: a host whose device memory already belongs
+ * to its own pool allocator, or one running other streams that must not be stalled
+ * by the device-wide synchronisation a cudaFree brings.  All device storage is one
+ * fixed array of about 1.1 MB inside the library, so the system must have at most
+ * 2048 orbitals and plane-wave components |n_d| <= 31; larger systems return
+ * UEGCCD_ERR_ARG.  stream is a cudaStream_t (NULL: the legacy default stream); the
+ * call returns when e2 is written.  Every call on a device shares that array:
+ * calls must not overlap on one device (from several streams or threads), or
+ * their results are wrong.  The first call on a device looks up the array's
+ * address (which may load the library's device code): make that first call before
+ * any stream capture begins on the device. */
+int uegccd_mp2_energy_static(const UegccdSystem *sys, void *stream, double *e2);
+
 /* Solve s's per-iteration energies and biggest changes from the last batch solve (the
  * rows of the reference's iteration table, CCD.f90:76,96 / dRPA.f90:77,92): copies at
  * most max_rec of each (either pointer may be NULL) and sets *n_recorded. */

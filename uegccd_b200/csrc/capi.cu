@@ -642,6 +642,11 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
 
 }  // namespace
 
+namespace uegccd {
+// The message uegccd_last_error returns, for entry points defined in other files.
+int set_last_error(int code, const char *msg) { return fail(code, msg); }
+}  // namespace uegccd
+
 extern "C" {
 
 const char *uegccd_last_error(void) { return g_last_error.c_str(); }
