@@ -209,9 +209,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int64_t> hh0;
     std::vector<RingPairDev> rpairs;
     std::vector<int16_t> ph_i, ph_x;
-    size_t rings_smem = 0;
     int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0;
-    int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_occ = 0;
+    int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_v = 0, max_occ = 0;
     // offsets of each solve in the large concatenated arrays (filled in parallel below)
     std::vector<int64_t> s_amp0(n), s_pos0(n), s_phr0(n);
     for (int s = 0; s < n; s++) {
@@ -242,7 +241,6 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             if (G.partner < 0 || G.partner < (int)gi) continue;  // each {Q, -Q} once
             const auto &H2 = P.groups[G.partner];
             rpairs.push_back(RingPairDev{s, G.r0, G.n, H2.r0, H2.n});
-            rings_smem = std::max(rings_smem, rings_smem_bytes(P.O, G.n + H2.n));
         }
         for (const auto &B : P.blocks) {
             BlockDev bd;
@@ -255,6 +253,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             hh0.push_back(hhoff);
             hhoff += (int64_t)B.o * B.o;
             max_o = std::max(max_o, B.o);
+            max_v = std::max(max_v, B.v);
             // row tile NP follows o_K (8, 16, 32); columns in tiles of 128 (4 warps x 32)
             const int np = B.o <= 8 ? 8 : B.o <= 16 ? 16 : 32;
             for (int a0 = 0; a0 < B.v; a0 += 128)
@@ -323,12 +322,32 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.nrchunks = (int)rchunks.size();
     d.ntargets = (int)targets.size();
     d.max_o = max_o;
+    d.max_v = max_v;
+    d.ladder_smem = ladder_smem_bytes(max_v);
+    if (d.ladder_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder block exceeds shared memory");
+    set_ladder_smem_limit(d.ladder_smem);
     d.max_occ = max_occ;
     d.namp = amp0;
+    // ring pairs by kernel class: k_rings (two shared-memory sizes), then k_rings_wide
+    {
+        auto cls = [&](const RingPairDev &r) {
+            const size_t b = rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max);
+            return b <= kRingSmemSmall ? 0 : b <= kRingSmemMax ? 1 : 2;
+        };
+        std::stable_sort(rpairs.begin(), rpairs.end(),
+                         [&](const RingPairDev &x, const RingPairDev &y) { return cls(x) < cls(y); });
+        for (const auto &r : rpairs) {
+            const int c = cls(r);
+            d.nring[c]++;
+            const size_t b = c < 2 ? rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max)
+                                   : rings_smem_bytes(solves[r.solve].O, r.n1 + r.n2);
+            d.ring_smem[c] = std::max(d.ring_smem[c], b);
+        }
+    }
     d.nrpairs = (int)rpairs.size();
-    d.rings_smem = rings_smem;
-    if (rings_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ring group pair exceeds shared memory");
-    set_rings_smem_limit(rings_smem);
+    if (d.ring_smem[2] > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ring group pair exceeds shared memory");
+    set_rings_smem_limit(0, std::max(d.ring_smem[0], d.ring_smem[1]));
+    set_rings_smem_limit(1, d.ring_smem[2]);
     if ((rc = b->upload(d.solves, solves))) return rc;
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;

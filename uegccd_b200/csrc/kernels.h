@@ -12,6 +12,8 @@ namespace uegccd {
 struct DevBatch {
     int nsolves = 0, nblocks = 0, ntiles = 0, nchunks = 0, nrchunks = 0, ntargets = 0;
     int max_o = 0;      // largest o_K
+    int max_v = 0;      // largest v_K
+    size_t ladder_smem = 0;  // dynamic shared memory of k_ladder3
     int max_occ = 0;    // largest NOcc
     int64_t namp = 0;
     SolveDev *solves = nullptr;
@@ -47,11 +49,21 @@ struct DevBatch {
     double *t_ref = nullptr, *g_ref = nullptr;  // refresh point of the defect correction
     int *tc_err = nullptr;
     int nrpairs = 0;
-    size_t rings_smem = 0;
+    // ring pair classes, rpairs sorted in this order: k_rings with the smaller and the
+    // larger shared-memory size, then k_rings_wide
+    int nring[3] = {0, 0, 0};
+    size_t ring_smem[3] = {0, 0, 0};
 };
-// dynamic shared memory of k_rings for NOcc = O and R rows of a group pair
+// dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
-void set_rings_smem_limit(size_t bytes);
+// dynamic shared memory of k_ladder3 for blocks of at most max_v virtuals
+size_t ladder_smem_bytes(int max_v);
+void set_ladder_smem_limit(size_t bytes);
+// dynamic shared memory of k_rings for NOcc = O and groups of n1 and n2 rows
+size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max);
+constexpr size_t kRingSmemSmall = 72 * 1024;   // k_rings pairs up to this size: 3 CTAs per SM
+constexpr size_t kRingSmemMax = 200 * 1024;    // above this the pair goes to k_rings_wide
+void set_rings_smem_limit(int wide, size_t bytes);
 
 constexpr int kPhRows = 8;
 constexpr int kDiisMax = 16;   // DIIS history capacity (k_diis_* use the same bound)   // ph rows per CTA of k_ph_build (one warp each)

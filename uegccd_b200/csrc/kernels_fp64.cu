@@ -192,13 +192,33 @@ __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, doubl
                  : "d"(a), "d"(b));
 }
 
+// The t rows of the tile pass through shared memory in chunks of kLadKC columns,
+// double-buffered with cp.async (8-byte copies: rows of odd length are not 16-byte
+// aligned); the block's virtual n-vectors and the |q|^2 table are staged once.
+constexpr int kLadKC = 32;            // c columns per chunk
+constexpr int kLadLd = kLadKC + 4;    // chunk row stride: = 4 mod 16 doubles, conflict-free fragments
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+size_t ladder_smem_bytes(int max_v)
+{
+    return sizeof(double) * (2 * 32 * kLadLd + kVtabSmem) + sizeof(int4) * (size_t)max_v;
+}
+
 template <int NP>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
                                              const int4 *__restrict__ nv4, const double *__restrict__ vtab,
                                              const double *__restrict__ t, const double *__restrict__ H, int mode,
                                              int do_pp, int do_hh, double *__restrict__ out, const double *sv,
-                                             bool vsm)
+                                             bool vsm, double *ts, const int4 *nvc)
 {
     constexpr int NN = NP / 8;  // n fragments
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -206,7 +226,7 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     const int v = B.v, o = B.o;
     const int ncol = mode == 0 ? v : o;
     const int colbase = T.a0 + warp * 32;
-    if (colbase >= ncol) return;  // no barriers below
+    const bool wact = colbase < ncol;  // warps past the last column only help with the copies
     // n-vectors of this lane's A-fragment rows (one per m fragment)
     int4 na[4];
 #pragma unroll
@@ -220,31 +240,53 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     for (int m = 0; m < 4; m++)
 #pragma unroll
         for (int n = 0; n < NN; n++) acc[m][n][0] = acc[m][n][1] = 0.0;
-    const double *trow[NN];
-    bool prow[NN];
-#pragma unroll
-    for (int n = 0; n < NN; n++) {
-        int p = T.p0 + n * 8 + gid;
-        prow[n] = p < o;
-        trow[n] = t + B.t0 + (int64_t)(prow[n] ? p : 0) * v;
-    }
     if (do_pp || mode == 1) {
-        for (int c0 = 0; c0 < v; c0 += 4) {
-            const int c = c0 + tig;
-            const bool cok = c < v;
-            const int4 nc = cok ? nv4[s.orb0 + vir[B.vir0 + c]] : make_int4(0, 0, 0, 0);
-            double bf[NN];
-#pragma unroll
-            for (int n = 0; n < NN; n++) bf[n] = (cok && prow[n]) ? __ldg(trow[n] + c) : 0.0;
-#pragma unroll
-            for (int m = 0; m < 4; m++) {
-                int q2 = q2_of(na[m], nc);
-                double af = cok ? (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2])) : 0.0;
-#pragma unroll
-                for (int n = 0; n < NN; n++) dmma_884(acc[m][n][0], acc[m][n][1], af, bf[n]);
+        const int nchunk = (v + kLadKC - 1) / kLadKC;
+        const double *trow0 = t + B.t0;
+        // chunk j of the tile's t rows -> buffer b
+        auto issue = [&](int j, int b) {
+            double *dst = ts + b * (NP * kLadLd);
+            const int c0 = j * kLadKC;
+            for (int e = threadIdx.x; e < NP * kLadKC; e += blockDim.x) {
+                const int r = e / kLadKC, c = e - r * kLadKC;
+                const int p = T.p0 + r, cc = c0 + c;
+                if (p < o && cc < v) cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + cc);
+                else dst[r * kLadLd + c] = 0.0;
             }
+            cp_async_commit();
+        };
+        issue(0, 0);
+        for (int j = 0; j < nchunk; j++) {
+            if (j + 1 < nchunk) {
+                issue(j + 1, (j + 1) & 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (wact) {
+                const double *tb = ts + (j & 1) * (NP * kLadLd);
+                const int c0 = j * kLadKC;
+#pragma unroll 2
+                for (int kk = 0; kk < kLadKC; kk += 4) {
+                    const int c = min(c0 + kk + tig, v - 1);  // beyond v the t column is zero
+                    const int4 nc = nvc[c];
+                    double bf[NN];
+#pragma unroll
+                    for (int n = 0; n < NN; n++) bf[n] = tb[(n * 8 + gid) * kLadLd + kk + tig];
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        const int q2 = q2_of(na[m], nc);
+                        const double af = vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]);
+#pragma unroll
+                        for (int n = 0; n < NN; n++) dmma_884(acc[m][n][0], acc[m][n][1], af, bf[n]);
+                    }
+                }
+            }
+            __syncthreads();
         }
     }
+    if (!wact) return;  // no barriers below
     if (mode == 0 && do_hh) {
         // acc[a][p] += sum_q t[q][a] H[p][q]
         for (int q0 = 0; q0 < o; q0 += 4) {
@@ -299,17 +341,30 @@ __global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ 
     const BlockDev B = blocks[T.blk];
     if (!active[B.solve]) return;
     const SolveDev s = solves[B.solve];
-    __shared__ double sv[kVtabSmem];
+    extern __shared__ double lsm[];
+    double *ts = lsm;                              // 2 x 32 x kLadLd
+    double *sv = ts + 2 * 32 * kLadLd;             // kVtabSmem
+    int4 *nvc = (int4 *)(sv + kVtabSmem);          // v_K n-vectors of the block's virtuals
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
         for (int q = threadIdx.x; q <= s.q2max; q += blockDim.x) sv[q] = vtab[s.vtab0 + q];
+    for (int c = threadIdx.x; c < B.v; c += blockDim.x) nvc[c] = nv4[s.orb0 + vir[B.vir0 + c]];
     __syncthreads();
     double *H = hh + hh0[T.blk];
     double *out = mode == 0 ? g : H;
     switch (T.pad) {
-    case 8: ladder3_tile<8>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm); break;
-    case 16: ladder3_tile<16>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm); break;
-    default: ladder3_tile<32>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm); break;
+    case 8: ladder3_tile<8>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    case 16: ladder3_tile<16>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    default: ladder3_tile<32>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    }
+}
+
+void set_ladder_smem_limit(size_t bytes)
+{
+    static size_t current = 48 * 1024;
+    if (bytes > current) {
+        cudaFuncSetAttribute(k_ladder3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        current = bytes;
     }
 }
 
@@ -461,7 +516,9 @@ __global__ void k_ring_int(const ChunkDev *__restrict__ rchunks, const SolveDev 
 // ----------------------------------------------------------------------------
 constexpr int kRingCh = 16;  // A rows per chunk
 
-__global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ pairs,
+// The FMA form below serves group pairs too large for k_rings' shared-memory tiles
+// (NOcc around 57 and above).
+__global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restrict__ pairs,
                                                const SolveDev *__restrict__ solves,
                                                const int16_t *__restrict__ ph_i, const int16_t *__restrict__ ph_x,
                                                const int32_t *__restrict__ pos, const int32_t *__restrict__ partner,
@@ -598,13 +655,254 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     }
 }
 
-void set_rings_smem_limit(size_t bytes)
+
+// ----------------------------------------------------------------------------
+// Rings on the FP64 tensor cores (mma.sync m8n8k4 f64), one CTA per {Q, -Q}
+// group pair.  With W[k][l] = v(n_k - n_l - Q) (the -Q group uses W^T),
+// Vs_r[l] = v(n_l - n_i(r)) and, per row r:
+//   XW_r = X_r W_r,   U_r = Y_r W_r - Vs_r
+// the products of the fused form above regroup into small GEMMs over l:
+//   ring (i1,i2,x1) = lin + base_1 (2 Sx_2 - Sy_2) + sum_l [XW_1 (Y_2 - 2 X_2) + U_1 X_2 - X_1 Vs_2]
+//   xring(i1,i2,x2) =                                sum_l [U_1 Y_2 - Y_1 Vs_2]
+// lin = 2 vd_1 (Sx_1 + Sx_2) - vd_1 (Sy_1 + Sy_2), base_1 = vd_1 (2 Sx_1 - Sy_1); the
+// -Ex/-Ey terms of the fused form are the Vs products.  Rows are padded to
+// multiples of 8 and k to Op = NOcc rounded up to 8, with zeros; row stride
+// ld = Op + 4 (= 4 or 12 mod 16 doubles) keeps the fragment loads free of bank
+// conflicts.
+// ----------------------------------------------------------------------------
+constexpr int kRingThreads = 256;
+constexpr int kRingGather = 4;   // gather elements in flight per thread
+
+__host__ __device__ __forceinline__ int round8(int x) { return (x + 7) & ~7; }
+
+size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
 {
-    // keep the largest limit ever requested: batches of different sizes coexist
-    static size_t current = 0;
-    if (bytes > current) {
-        cudaFuncSetAttribute(k_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        current = bytes;
+    const int Op = round8(O), ld = Op + 4, Rp = round8(n1) + round8(n2);
+    const int nsv = q2max < kVtabSmem ? round8(q2max + 1) : 0;
+    return sizeof(double) * ((size_t)Op * ld + 5 * (size_t)Rp * ld + 3 * (size_t)Rp + nsv) + sizeof(int) * 2 * Rp +
+           sizeof(int4) * ((size_t)O + Rp);
+}
+
+__global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__restrict__ pairs,
+                                                        const SolveDev *__restrict__ solves,
+                                                        const int16_t *__restrict__ ph_i,
+                                                        const int16_t *__restrict__ ph_x,
+                                                        const int32_t *__restrict__ pos,
+                                                        const int4 *__restrict__ nv4,
+                                                        const double *__restrict__ vtab,
+                                                        const double *__restrict__ t, int do_ring, int do_xring,
+                                                        double *__restrict__ g_rq, double *__restrict__ g_xq,
+                                                        const uint8_t *__restrict__ active)
+{
+    const RingPairDev P = pairs[blockIdx.x];
+    if (!active[P.solve]) return;
+    const SolveDev s = solves[P.solve];
+    const int O = s.O, Op = round8(O), ld = Op + 4;
+    const int n1 = P.n1, n2 = P.n2, n1p = round8(n1), n2p = round8(n2), Rp = n1p + n2p;
+    const bool vsm = s.q2max < kVtabSmem;
+    const int nsv = vsm ? round8(s.q2max + 1) : 0;
+    extern __shared__ double smem[];
+    double *W = smem;                 // Op x ld
+    double *X = W + Op * ld;          // Rp x ld: X[r][k] = t(i_r k, x_r)
+    double *Y = X + Rp * ld;          // Rp x ld: Y[r][k] = t(k i_r, x_r) = t(i_r k, c)
+    double *Vs = Y + Rp * ld;         // Rp x ld
+    double *XW = Vs + Rp * ld;        // Rp x ld
+    double *U = XW + Rp * ld;         // Rp x ld
+    double *Sx = U + Rp * ld;         // Rp
+    double *Sy = Sx + Rp;             // Rp
+    double *Vd = Sy + Rp;             // Rp
+    double *sv = Vd + Rp;             // nsv: the |q|^2 table
+    int *ri = (int *)(sv + nsv);      // Rp, -1 on padding rows
+    int *rx = ri + Rp;                // Rp
+    int4 *no = (int4 *)(rx + Rp);     // O occupied n-vectors (16-byte aligned: Rp, nsv multiples of 8)
+    int4 *nx = no + O;                // Rp: n-vector of each row's virtual
+    const int tid = threadIdx.x;
+    auto V = [&](int q2) -> double {
+        return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]));
+    };
+    for (int q = tid; q < nsv; q += kRingThreads) sv[q] = q <= s.q2max ? vtab[s.vtab0 + q] : 0.0;
+    for (int r = tid; r < Rp; r += kRingThreads) {
+        int row = -1;
+        if (r < n1) row = P.r1 + r;
+        else if (r >= n1p && r - n1p < n2) row = P.r2 + (r - n1p);
+        const int i = row >= 0 ? ph_i[s.phr0 + row] : -1, x = row >= 0 ? ph_x[s.phr0 + row] : -1;
+        ri[r] = i;
+        rx[r] = x;
+        nx[r] = x >= 0 ? nv4[s.orb0 + x] : make_int4(0, 0, 0, 0);
+    }
+    for (int k = tid; k < O; k += kRingThreads) no[k] = nv4[s.orb0 + k];
+    __syncthreads();
+    // Q = n_x - n_i of group 1 (the negative of group 2's)
+    int Qx, Qy, Qz;
+    {
+        const int r = n1 > 0 ? 0 : n1p;
+        const int4 qa = nx[r], qb = no[ri[r]];
+        const int sg = n1 > 0 ? 1 : -1;
+        Qx = sg * (qa.x - qb.x);
+        Qy = sg * (qa.y - qb.y);
+        Qz = sg * (qa.z - qb.z);
+    }
+    // X, Y gathers: all position loads of a batch first, then all amplitude loads
+    for (int e0 = tid; e0 < Rp * Op; e0 += kRingThreads * kRingGather) {
+        int p1[kRingGather], p2[kRingGather];
+#pragma unroll
+        for (int u = 0; u < kRingGather; u++) {
+            const int e = e0 + u * kRingThreads;
+            p1[u] = p2[u] = -1;
+            if (e < Rp * Op) {
+                const int r = e / Op, k = e - r * Op;
+                const int i = ri[r];
+                if (i >= 0 && k < O) {
+                    p1[u] = posmap(s, pos, i, k, rx[r]);
+                    p2[u] = posmap(s, pos, k, i, rx[r]);
+                }
+            }
+        }
+        double xv[kRingGather], yv[kRingGather];
+#pragma unroll
+        for (int u = 0; u < kRingGather; u++) {
+            xv[u] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
+            yv[u] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kRingGather; u++) {
+            const int e = e0 + u * kRingThreads;
+            if (e < Rp * Op) {
+                const int r = e / Op, k = e - r * Op;
+                X[r * ld + k] = xv[u];
+                Y[r * ld + k] = yv[u];
+            }
+        }
+    }
+    // exchange kernel W and the direct rows Vs (shared-memory table lookups)
+    for (int e = tid; e < Op * Op; e += kRingThreads) {
+        const int k = e / Op, l = e - k * Op;
+        double w = 0.0;
+        if (k < O && l < O) {
+            const int dx = no[k].x - no[l].x - Qx, dy = no[k].y - no[l].y - Qy, dz = no[k].z - no[l].z - Qz;
+            w = V(dx * dx + dy * dy + dz * dz);
+        }
+        W[k * ld + l] = w;
+    }
+    for (int e = tid; e < Rp * Op; e += kRingThreads) {
+        const int r = e / Op, k = e - r * Op;
+        const int i = ri[r];
+        Vs[r * ld + k] = (i >= 0 && k < O) ? V(q2_of(no[k], no[i])) : 0.0;
+    }
+    __syncthreads();
+    for (int r = tid; r < Rp; r += kRingThreads) {
+        double sx = 0.0, sy = 0.0;
+        for (int k = 0; k < O; k++) {
+            sx += X[r * ld + k];
+            sy += Y[r * ld + k];
+        }
+        Sx[r] = sx;
+        Sy[r] = sy;
+        Vd[r] = ri[r] >= 0 ? V(q2_of(no[ri[r]], nx[r])) : 0.0;
+    }
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, tg = lane & 3;
+    constexpr int kWarps = kRingThreads / 32;
+    // phase 1: XW = X W_r and U = Y W_r - Vs, tasks of 8 rows x 32 columns
+    {
+        const int mfr = Rp / 8, nng = (Op + 31) / 32;
+        const int ntask = 2 * mfr * nng;
+        for (int task = warp; task < ntask; task += kWarps) {
+            const int mat = task / (mfr * nng), rem = task - mat * (mfr * nng);
+            const int mf = rem / nng, ng = rem - mf * nng;
+            const int r0 = mf * 8, nbase = ng * 32;
+            const bool grp2 = r0 >= n1p;
+            const double *A = (mat == 0 ? X : Y) + (r0 + g) * ld + tg;
+            double acc[4][2];
+#pragma unroll
+            for (int f = 0; f < 4; f++) acc[f][0] = acc[f][1] = 0.0;
+            for (int k0 = 0; k0 < Op; k0 += 4) {
+                const double a = A[k0];
+#pragma unroll
+                for (int f = 0; f < 4; f++) {
+                    if (nbase + f * 8 >= Op) break;
+                    const int n = nbase + f * 8 + g;
+                    const double b = grp2 ? W[n * ld + k0 + tg] : W[(k0 + tg) * ld + n];
+                    dmma_884(acc[f][0], acc[f][1], a, b);
+                }
+            }
+            double *Out = mat == 0 ? XW : U;
+            const int r = r0 + g;
+#pragma unroll
+            for (int f = 0; f < 4; f++) {
+                if (nbase + f * 8 >= Op) break;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int n = nbase + f * 8 + 2 * tg + h;
+                    double v = acc[f][h];
+                    if (mat == 1) v -= Vs[r * ld + n];
+                    Out[r * ld + n] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // phase 2: both directions, tasks of 8 (r1) x 16 (r2)
+    const int t1 = (n1p / 8) * ((n2p + 15) / 16), t2 = (n2p / 8) * ((n1p + 15) / 16);
+    for (int task = warp; task < t1 + t2; task += kWarps) {
+        const int dir = task < t1 ? 0 : 1, tt = dir ? task - t1 : task;
+        const int a0 = dir ? n1p : 0, na = dir ? n2 : n1;
+        const int b0 = dir ? 0 : n1p, nb = dir ? n1 : n2, nbp = dir ? n1p : n2p;
+        const int nng = (nbp + 15) / 16;
+        const int mf = tt / nng, ng = tt - mf * nng;
+        const int ra = a0 + mf * 8 + g;
+        double ring[2][2], xr[2][2];
+#pragma unroll
+        for (int f = 0; f < 2; f++) ring[f][0] = ring[f][1] = xr[f][0] = xr[f][1] = 0.0;
+        for (int k0 = 0; k0 < Op; k0 += 4) {
+            const int k = k0 + tg;
+            const double axw = XW[ra * ld + k], au = U[ra * ld + k], ax = X[ra * ld + k], ay = Y[ra * ld + k];
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                const int nloc = ng * 16 + f * 8;
+                if (nloc >= nbp) break;
+                const int rb = b0 + nloc + g;
+                const double bx = X[rb * ld + k], by = Y[rb * ld + k], bv = -Vs[rb * ld + k];
+                const double bz = by - 2.0 * bx;
+                dmma_884(ring[f][0], ring[f][1], axw, bz);
+                dmma_884(ring[f][0], ring[f][1], au, bx);
+                dmma_884(ring[f][0], ring[f][1], ax, bv);
+                dmma_884(xr[f][0], xr[f][1], au, by);
+                dmma_884(xr[f][0], xr[f][1], ay, bv);
+            }
+        }
+        const int m = mf * 8 + g;
+        if (m >= na) continue;
+        const int r1 = a0 + m, i1 = ri[r1];
+        const double vd = Vd[r1], sx1 = Sx[r1], sy1 = Sy[r1];
+        const double base = vd * (2.0 * sx1 - sy1);
+#pragma unroll
+        for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int nloc = ng * 16 + f * 8 + 2 * tg + h;
+                if (nloc >= nb) continue;
+                const int r2 = b0 + nloc, i2 = ri[r2];
+                if (do_ring) {
+                    const double lin = 2.0 * vd * (sx1 + Sx[r2]) - vd * (sy1 + Sy[r2]);
+                    const int p = posmap(s, pos, i1, i2, rx[r1]);
+                    if (p >= 0) g_rq[p] = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ring[f][h];
+                }
+                if (do_xring) {
+                    const int p = posmap(s, pos, i1, i2, rx[r2]);
+                    if (p >= 0) g_xq[p] = xr[f][h];
+                }
+            }
+    }
+}
+
+void set_rings_smem_limit(int wide, size_t bytes)
+{
+    // keep the largest limit ever requested per kernel: batches of different sizes coexist
+    static size_t current[2] = {0, 0};
+    if (bytes > current[wide ? 1 : 0]) {
+        if (wide) cudaFuncSetAttribute(k_rings_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        else cudaFuncSetAttribute(k_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        current[wide ? 1 : 0] = bytes;
     }
 }
 
@@ -927,7 +1225,7 @@ __global__ void k_copy(int64_t n, const double *__restrict__ src, double *__rest
 void launch_refresh(const DevBatch &d, cudaStream_t st)
 {
     k_copy<<<(unsigned)((d.namp + 255) / 256), 256, 0, st>>>(d.namp, d.t, d.t_ref);
-    k_ladder3<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t_ref, d.hh0,
+    k_ladder3<<<d.ntiles, 128, d.ladder_smem, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t_ref, d.hh0,
                                         d.hh, 0, 1, 0, d.g_ref, d.active);
 }
 
@@ -1037,14 +1335,14 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     if (f.do_ladder && d.nblocks > 0) {
         if (f.do_hh) {
             kt->begin(KID_HH_W, st);
-            k_ladder3<<<d.nhtiles, 128, 0, st>>>(d.htiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t,
+            k_ladder3<<<d.nhtiles, 128, d.ladder_smem, st>>>(d.htiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t,
                                                  d.hh0, d.hh, 1, f.do_pp, f.do_hh, d.g, d.active);
             kt->end(st);
             n++;
         }
         const int pp64 = (f.do_pp && !f.mixed) ? 1 : 0;
         kt->begin(KID_LADDER, st);
-        k_ladder3<<<d.ntiles, 128, 0, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t, d.hh0,
+        k_ladder3<<<d.ntiles, 128, d.ladder_smem, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t, d.hh0,
                                             d.hh, 0, pp64, f.do_hh, d.g, d.active);
         kt->end(st);
         n++;
@@ -1074,9 +1372,19 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     }
     if ((f.do_ring || f.do_xring) && !f.drpa) {
         kt->begin(KID_RINGS, st);
-        k_rings<<<d.nrpairs, 256, d.rings_smem, st>>>(d.rpairs, d.solves, d.ph_i, d.ph_x, d.pos, d.partner, d.nv4,
-                                                       d.vtab, d.t, f.do_ring, f.do_xring, d.g_rq, d.g_xq,
-                                                       d.active);
+        // pair classes (sorted in this order): DMMA tiles in two shared-memory sizes, then the FMA form
+        int off = 0;
+        for (int c = 0; c < 2; c++) {
+            if (d.nring[c] > 0)
+                k_rings<<<d.nring[c], kRingThreads, d.ring_smem[c], st>>>(
+                    d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.pos, d.nv4, d.vtab, d.t, f.do_ring, f.do_xring,
+                    d.g_rq, d.g_xq, d.active);
+            off += d.nring[c];
+        }
+        if (d.nring[2] > 0)
+            k_rings_wide<<<d.nring[2], 256, d.ring_smem[2], st>>>(d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.pos,
+                                                                 d.partner, d.nv4, d.vtab, d.t, f.do_ring,
+                                                                 f.do_xring, d.g_rq, d.g_xq, d.active);
         kt->end(st);
         n++;
     }
