@@ -292,6 +292,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     partner.resize(amp0);
     ph_i.resize(phr0);
     ph_x.resize(phr0);
+    // per ph row (i, x) and occupied k: packed index of t(ik, x) and of t(ki, x)
+    std::vector<int32_t> ridx_x(ph0), ridx_y(ph0);
     parallel_for(n, nthreads, [&](int s) {
         const SolvePlan &P = b->plans[s];
         const int64_t a0 = s_amp0[s];
@@ -304,6 +306,14 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         }
         std::copy(P.ph_i.begin(), P.ph_i.end(), ph_i.begin() + s_phr0[s]);
         std::copy(P.ph_x.begin(), P.ph_x.end(), ph_x.begin() + s_phr0[s]);
+        const int64_t h0 = solves[s].ph0;
+        for (int64_t r = 0; r < (int64_t)P.ph_i.size(); r++) {
+            const int i = P.ph_i[r], x = P.ph_x[r];
+            for (int k = 0; k < P.O; k++) {
+                ridx_x[h0 + r * P.O + k] = pdst[((size_t)i * P.O + k) * P.V + (x - P.O)];
+                ridx_y[h0 + r * P.O + k] = pdst[((size_t)k * P.O + i) * P.V + (x - P.O)];
+            }
+        }
     });
 
     DevBatch &d = b->d;
@@ -370,6 +380,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.rpairs, rpairs))) return rc;
     if ((rc = b->upload(d.ph_i, ph_i))) return rc;
     if ((rc = b->upload(d.ph_x, ph_x))) return rc;
+    if ((rc = b->upload(d.ridx_x, ridx_x))) return rc;
+    if ((rc = b->upload(d.ridx_y, ridx_y))) return rc;
     if ((rc = b->alloc(d.g_rq, amp0))) return rc;
     if ((rc = b->alloc(d.g_xq, amp0))) return rc;
     if ((rc = b->alloc(d.t, amp0))) return rc;
@@ -892,6 +904,7 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     b += O * O * V * 4;                              // pos
     b += O * V * O * 8 * 3;                          // dRPA ring intermediates
     b += O * V * 2 * 2;                              // ph rows
+    b += O * V * O * 4 * 2;                          // ring gather indices
     b += hh * 8 + nblk * (sizeof(BlockDev) + 8) + M * (16 + 8) + (P.q2max + 1) * 8;
     b += A * 8 * 2 * (int64_t)std::max(0, (int)ndiis);  // DIIS history
     if (mixed) b += A * 8 * 2;                       // t_ref, g_ref

@@ -41,6 +41,7 @@ struct DevBatch {
     uint8_t *active = nullptr;       // per solve
     // particle-hole form of the ring terms
     int16_t *ph_i = nullptr, *ph_x = nullptr;   // row -> (i, x), rows grouped by Q
+    int32_t *ridx_x = nullptr, *ridx_y = nullptr;  // at ph0 + row*O + k: index of t(ik, x), t(ki, x)
     double *g_rq = nullptr, *g_xq = nullptr;    // per amplitude: ring and crossed-ring G
     RingPairDev *rpairs = nullptr;              // {Q, -Q} group pairs
     // mixed precision: tensor-core ladder tiles sorted by row tile (16, 32, 64)

@@ -687,7 +687,8 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
                                                         const SolveDev *__restrict__ solves,
                                                         const int16_t *__restrict__ ph_i,
                                                         const int16_t *__restrict__ ph_x,
-                                                        const int32_t *__restrict__ pos,
+                                                        const int32_t *__restrict__ ridx_x,
+                                                        const int32_t *__restrict__ ridx_y,
                                                         const int4 *__restrict__ nv4,
                                                         const double *__restrict__ vtab,
                                                         const double *__restrict__ t, int do_ring, int do_xring,
@@ -713,10 +714,11 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
     double *Vd = Sy + Rp;             // Rp
     double *sv = Vd + Rp;             // nsv: the |q|^2 table
     int *ri = (int *)(sv + nsv);      // Rp, -1 on padding rows
-    int *rx = ri + Rp;                // Rp
-    int4 *no = (int4 *)(rx + Rp);     // O occupied n-vectors (16-byte aligned: Rp, nsv multiples of 8)
+    int *rw = ri + Rp;                // Rp: the row's offset in the gather-index tables, -1 on padding rows
+    int4 *no = (int4 *)(rw + Rp);     // O occupied n-vectors (16-byte aligned: Rp, nsv multiples of 8)
     int4 *nx = no + O;                // Rp: n-vector of each row's virtual
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int kWarps = kRingThreads / 32;
     auto V = [&](int q2) -> double {
         return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]));
     };
@@ -727,7 +729,7 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
         else if (r >= n1p && r - n1p < n2) row = P.r2 + (r - n1p);
         const int i = row >= 0 ? ph_i[s.phr0 + row] : -1, x = row >= 0 ? ph_x[s.phr0 + row] : -1;
         ri[r] = i;
-        rx[r] = x;
+        rw[r] = row >= 0 ? row * O : -1;
         nx[r] = x >= 0 ? nv4[s.orb0 + x] : make_int4(0, 0, 0, 0);
     }
     for (int k = tid; k < O; k += kRingThreads) no[k] = nv4[s.orb0 + k];
@@ -742,52 +744,42 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
         Qy = sg * (qa.y - qb.y);
         Qz = sg * (qa.z - qb.z);
     }
-    // X, Y gathers: all position loads of a batch first, then all amplitude loads
-    for (int e0 = tid; e0 < Rp * Op; e0 += kRingThreads * kRingGather) {
-        int p1[kRingGather], p2[kRingGather];
+    // X, Y gathers: a warp per row, lanes over k; the index loads of kRingGather rows
+    // are issued before their amplitude loads
+    const int32_t *gx = ridx_x + s.ph0, *gy = ridx_y + s.ph0;
+    for (int r0 = warp; r0 < Rp; r0 += kWarps * kRingGather) {
+        for (int k = lane; k < Op; k += 32) {
+            int p1[kRingGather], p2[kRingGather];
 #pragma unroll
-        for (int u = 0; u < kRingGather; u++) {
-            const int e = e0 + u * kRingThreads;
-            p1[u] = p2[u] = -1;
-            if (e < Rp * Op) {
-                const int r = e / Op, k = e - r * Op;
-                const int i = ri[r];
-                if (i >= 0 && k < O) {
-                    p1[u] = posmap(s, pos, i, k, rx[r]);
-                    p2[u] = posmap(s, pos, k, i, rx[r]);
-                }
+            for (int u = 0; u < kRingGather; u++) {
+                const int r = r0 + u * kWarps;
+                const int w = (r < Rp && k < O) ? rw[r] : -1;
+                p1[u] = w >= 0 ? __ldg(&gx[w + k]) : -1;
+                p2[u] = w >= 0 ? __ldg(&gy[w + k]) : -1;
             }
-        }
-        double xv[kRingGather], yv[kRingGather];
 #pragma unroll
-        for (int u = 0; u < kRingGather; u++) {
-            xv[u] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
-            yv[u] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kRingGather; u++) {
-            const int e = e0 + u * kRingThreads;
-            if (e < Rp * Op) {
-                const int r = e / Op, k = e - r * Op;
-                X[r * ld + k] = xv[u];
-                Y[r * ld + k] = yv[u];
+            for (int u = 0; u < kRingGather; u++) {
+                const int r = r0 + u * kWarps;
+                if (r < Rp) {
+                    X[r * ld + k] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
+                    Y[r * ld + k] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
+                }
             }
         }
     }
     // exchange kernel W and the direct rows Vs (shared-memory table lookups)
-    for (int e = tid; e < Op * Op; e += kRingThreads) {
-        const int k = e / Op, l = e - k * Op;
-        double w = 0.0;
-        if (k < O && l < O) {
-            const int dx = no[k].x - no[l].x - Qx, dy = no[k].y - no[l].y - Qy, dz = no[k].z - no[l].z - Qz;
-            w = V(dx * dx + dy * dy + dz * dz);
+    for (int k = warp; k < Op; k += kWarps)
+        for (int l = lane; l < Op; l += 32) {
+            double w = 0.0;
+            if (k < O && l < O) {
+                const int dx = no[k].x - no[l].x - Qx, dy = no[k].y - no[l].y - Qy, dz = no[k].z - no[l].z - Qz;
+                w = V(dx * dx + dy * dy + dz * dz);
+            }
+            W[k * ld + l] = w;
         }
-        W[k * ld + l] = w;
-    }
-    for (int e = tid; e < Rp * Op; e += kRingThreads) {
-        const int r = e / Op, k = e - r * Op;
+    for (int r = warp; r < Rp; r += kWarps) {
         const int i = ri[r];
-        Vs[r * ld + k] = (i >= 0 && k < O) ? V(q2_of(no[k], no[i])) : 0.0;
+        for (int k = lane; k < Op; k += 32) Vs[r * ld + k] = (i >= 0 && k < O) ? V(q2_of(no[k], no[i])) : 0.0;
     }
     __syncthreads();
     for (int r = tid; r < Rp; r += kRingThreads) {
@@ -800,8 +792,7 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
         Sy[r] = sy;
         Vd[r] = ri[r] >= 0 ? V(q2_of(no[ri[r]], nx[r])) : 0.0;
     }
-    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, tg = lane & 3;
-    constexpr int kWarps = kRingThreads / 32;
+    const int g = lane >> 2, tg = lane & 3;
     // phase 1: XW = X W_r and U = Y W_r - Vs, tasks of 8 rows x 32 columns
     {
         const int mfr = Rp / 8, nng = (Op + 31) / 32;
@@ -882,13 +873,14 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
                 const int nloc = ng * 16 + f * 8 + 2 * tg + h;
                 if (nloc >= nb) continue;
                 const int r2 = b0 + nloc, i2 = ri[r2];
+                // ring amplitude (i1, i2, x1) is X_r1[i2]; crossed ring (i1, i2, x2) is Y_r2[i1]
                 if (do_ring) {
                     const double lin = 2.0 * vd * (sx1 + Sx[r2]) - vd * (sy1 + Sy[r2]);
-                    const int p = posmap(s, pos, i1, i2, rx[r1]);
+                    const int p = __ldg(&gx[rw[r1] + i2]);
                     if (p >= 0) g_rq[p] = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ring[f][h];
                 }
                 if (do_xring) {
-                    const int p = posmap(s, pos, i1, i2, rx[r2]);
+                    const int p = __ldg(&gy[rw[r2] + i1]);
                     if (p >= 0) g_xq[p] = xr[f][h];
                 }
             }
@@ -1377,8 +1369,8 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         for (int c = 0; c < 2; c++) {
             if (d.nring[c] > 0)
                 k_rings<<<d.nring[c], kRingThreads, d.ring_smem[c], st>>>(
-                    d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.pos, d.nv4, d.vtab, d.t, f.do_ring, f.do_xring,
-                    d.g_rq, d.g_xq, d.active);
+                    d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, f.do_ring,
+                    f.do_xring, d.g_rq, d.g_xq, d.active);
             off += d.nring[c];
         }
         if (d.nring[2] > 0)
