@@ -212,7 +212,7 @@ size_t ladder_smem_bytes(int max_v)
     return sizeof(double) * (2 * 32 * kLadLd + kVtabSmem) + sizeof(int4) * (size_t)max_v;
 }
 
-template <int NP>
+template <int NP, bool KS>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
                                              const int4 *__restrict__ nv4, const double *__restrict__ vtab,
@@ -225,7 +225,10 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     const int gid = lane >> 2, tig = lane & 3;
     const int v = B.v, o = B.o;
     const int ncol = mode == 0 ? v : o;
-    const int colbase = T.a0 + warp * 32;
+    // hole-hole intermediate with at most 32 columns left: the 4 warps share the columns
+    // and split the c sum instead (each takes every 4th k step), then reduce
+    const bool ksplit = KS && ncol - T.a0 <= 32;
+    const int colbase = ksplit ? T.a0 : T.a0 + warp * 32;
     const bool wact = colbase < ncol;  // warps past the last column only help with the copies
     // n-vectors of this lane's A-fragment rows (one per m fragment)
     int4 na[4];
@@ -267,8 +270,9 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
             if (wact) {
                 const double *tb = ts + (j & 1) * (NP * kLadLd);
                 const int c0 = j * kLadKC;
+                const int kstart = KS && ksplit ? 4 * warp : 0, kstep = KS && ksplit ? 16 : 4;
 #pragma unroll 2
-                for (int kk = 0; kk < kLadKC; kk += 4) {
+                for (int kk = kstart; kk < kLadKC; kk += kstep) {
                     const int c = min(c0 + kk + tig, v - 1);  // beyond v the t column is zero
                     const int4 nc = nvc[c];
                     double bf[NN];
@@ -285,6 +289,34 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
             }
             __syncthreads();
         }
+    }
+    if (KS && ksplit) {
+        // acc of warps 2, 3 into warps 0, 1, then warp 1 into warp 0 (through the idle chunk buffer)
+        constexpr int kPart = 4 * NN * 2 * 32;
+        for (int round = 0; round < 2; round++) {
+            const int lo = round == 0 ? 2 : 1, nw = round == 0 ? 2 : 1;
+            if (warp >= lo && warp < lo + nw) {
+                double *dst = ts + (warp - lo) * kPart;
+#pragma unroll
+                for (int m = 0; m < 4; m++)
+#pragma unroll
+                    for (int n = 0; n < NN; n++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) dst[((m * NN + n) * 2 + h) * 32 + lane] = acc[m][n][h];
+            }
+            __syncthreads();
+            if (warp < nw) {
+                const double *src = ts + warp * kPart;
+#pragma unroll
+                for (int m = 0; m < 4; m++)
+#pragma unroll
+                    for (int n = 0; n < NN; n++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) acc[m][n][h] += src[((m * NN + n) * 2 + h) * 32 + lane];
+            }
+            __syncthreads();
+        }
+        if (warp != 0) return;
     }
     if (!wact) return;  // no barriers below
     if (mode == 0 && do_hh) {
@@ -352,10 +384,19 @@ __global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ 
     __syncthreads();
     double *H = hh + hh0[T.blk];
     double *out = mode == 0 ? g : H;
+    // the hole-hole intermediate (mode 1) may split its c sum across the warps
+    if (mode == 1) {
+        switch (T.pad) {
+        case 8: ladder3_tile<8, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+        case 16: ladder3_tile<16, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+        default: ladder3_tile<32, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+        }
+        return;
+    }
     switch (T.pad) {
-    case 8: ladder3_tile<8>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-    case 16: ladder3_tile<16>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-    default: ladder3_tile<32>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    case 8: ladder3_tile<8, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    case 16: ladder3_tile<16, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    default: ladder3_tile<32, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
     }
 }
 
