@@ -66,8 +66,7 @@ constexpr size_t kRingSmemSmall = 72 * 1024;   // k_rings pairs up to this size:
 constexpr size_t kRingSmemMax = 200 * 1024;    // above this the pair goes to k_rings_wide
 void set_rings_smem_limit(int wide, size_t bytes);
 
-constexpr int kPhRows = 8;
-constexpr int kDiisMax = 16;   // DIIS history capacity (k_diis_* use the same bound)   // ph rows per CTA of k_ph_build (one warp each)
+constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* use the same bound)
 
 // Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
 enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
@@ -139,8 +138,10 @@ void launch_energy(const DevBatch &d, int kind, double csosex, cudaStream_t st);
 // d.t_new = T2aaaa of d.t (t(ij,a) - t(ij,b))
 void launch_to_aaaa(const DevBatch &d, cudaStream_t st);
 // Residual of the selected terms for d.t; mode 0 also updates into d.t_new.  Returns launches.
+struct CtlBuffers;
+// diis/ndiis (mode 0 only): fuse the Pulay DIIS push into the update kernel
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
-                    KernelTimer *kt = nullptr);
+                    KernelTimer *kt = nullptr, const CtlBuffers *diis = nullptr, int ndiis = 0);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)
 void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st);

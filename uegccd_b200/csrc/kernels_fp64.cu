@@ -974,6 +974,12 @@ struct UpdateArgs {
     const double *g_rq, *g_xq;
     const uint8_t *active;
     int do_ladder, do_mosaic, do_ring, do_xring, do_driver, drpa, mode;
+    // Pulay DIIS push fused into the update (mode 0, ndiis > 0): the new (t', e) pair
+    // goes to the solve's history slot and the chunk partials of e . e_j to dpart
+    const IterState *st;
+    int ndiis;
+    int64_t namp;
+    double *hist_t, *hist_e, *dpart;
 };
 
 __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
@@ -1031,6 +1037,32 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
             if (A.drpa) esum = via * tn * 2.0;  // SOSEX part added by k_drpa_energy at the end
             else esum = tn * (2.0 * via - vpq(s, A.nv4, A.vtab, a, j));
             if (!(fabs(tn) < 1e300)) dtmax = __longlong_as_double(0x7ff0000000000000LL);  // +Inf marks NaN/Inf
+            if (A.ndiis > 0) {
+                const int slot = (A.st[ch.solve].niter - 1) % A.ndiis;
+                A.hist_t[(int64_t)slot * A.namp + p] = tn;
+                A.hist_e[(int64_t)slot * A.namp + p] = tn - told;
+            }
+        }
+    }
+    if (A.mode == 0 && A.ndiis > 0 && on) {
+        // e . e_j of every stored j (the chunk belongs to one solve: the loop is uniform)
+        const int nb = A.st[ch.solve].niter;
+        const int slot = (nb - 1) % A.ndiis, nvec = min(nb, A.ndiis);
+        const bool mine = loc < s.namp;
+        const int64_t p = s.amp0 + loc;
+        const double e = mine ? A.hist_e[(int64_t)slot * A.namp + p] : 0.0;
+        __shared__ double sd[kChunk / 32][kDiisMax];
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        for (int jv = 0; jv < nvec; jv++) {
+            double d = mine ? e * (jv == slot ? e : A.hist_e[(int64_t)jv * A.namp + p]) : 0.0;
+            for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+            if (l == 0) sd[w][jv] = d;
+        }
+        __syncthreads();
+        if (threadIdx.x < nvec) {
+            double d = 0.0;
+            for (int k = 0; k < kChunk / 32; k++) d += sd[k][threadIdx.x];
+            A.dpart[(int64_t)blockIdx.x * kDiisMax + threadIdx.x] = d;
         }
     }
     block_reduce3<kChunk>(esum, dtmax, rmax);
@@ -1045,8 +1077,8 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
 // Pulay DIIS (new in this library; the reference's GetTFromDIIS, DIISCC.f90:52-131,
 // builds a singular matrix and never extrapolates).  Error vector e = t' - t of
 // the (damped) Jacobi step; history of ndiis (t', e) pairs per solve.
-// k_diis_push2 stores the solve's current slot and forms the dot products e . e_j
-// of every stored j (per-chunk partials, reduced per solve in chunk order).
+// k_update stores the solve's current slot and forms the dot products e . e_j of
+// every stored j (per-chunk partials); k_diis_rows2 reduces them per solve in chunk order.
 // ----------------------------------------------------------------------------
 constexpr int kMaxDiis = 16;
 // ----------------------------------------------------------------------------
@@ -1179,40 +1211,6 @@ __global__ void k_commit(const ChunkDev *__restrict__ chunks, const SolveDev *__
     if (loc < s.namp) t[s.amp0 + loc] = t_new[s.amp0 + loc];
 }
 
-// DIIS push with per-solve slot and history length (solves need not be in step)
-__global__ void __launch_bounds__(kChunk) k_diis_push2(const ChunkDev *__restrict__ chunks,
-                                                       const SolveDev *__restrict__ solves,
-                                                       const IterState *__restrict__ st, int ndiis, int64_t namp,
-                                                       const double *__restrict__ t,
-                                                       const double *__restrict__ t_new,
-                                                       double *__restrict__ hist_t, double *__restrict__ hist_e,
-                                                       double *__restrict__ part,
-                                                       const uint8_t *__restrict__ active)
-{
-    const ChunkDev ch = chunks[blockIdx.x];
-    if (!active[ch.solve]) return;  // whole CTA: one solve
-    const SolveDev s = solves[ch.solve];
-    const int nb = st[ch.solve].niter;  // before k_control increments it
-    const int slot = (nb - 1) % ndiis, nvec = min(nb, ndiis);
-    const int loc = ch.start + threadIdx.x;
-    const bool on = loc < s.namp;
-    double e = 0.0;
-    int64_t p = 0;
-    if (on) {
-        p = s.amp0 + loc;
-        const double tn = t_new[p];
-        e = tn - t[p];
-        hist_t[(int64_t)slot * namp + p] = tn;
-        hist_e[(int64_t)slot * namp + p] = e;
-    }
-    for (int jv = 0; jv < nvec; jv++) {
-        double d = on ? e * hist_e[(int64_t)jv * namp + p] : 0.0;
-        d = block_sum<kChunk>(d);
-        if (threadIdx.x == 0) part[(int64_t)blockIdx.x * kMaxDiis + jv] = d;
-        __syncthreads();
-    }
-}
-
 __global__ void k_diis_rows2(const int *__restrict__ chunk_begin, const IterState *__restrict__ st, int ndiis,
                              const double *__restrict__ part, double *__restrict__ brow,
                              const uint8_t *__restrict__ active)
@@ -1279,12 +1277,11 @@ void launch_active_swap(const DevBatch &d, const CtlBuffers &c, cudaStream_t st)
 int launch_iteration(const DevBatch &d, const CtlBuffers &c, const TermFlags &f, double tol, int max_iter,
                      int ndiis, cudaStream_t st, KernelTimer *kt)
 {
-    int n = launch_residual(d, f, 0, nullptr, st, kt);
+    // the DIIS push (history slot and e . e_j partials) happens inside k_update
+    int n = launch_residual(d, f, 0, nullptr, st, kt, &c, ndiis);
     if (ndiis > 0) {
-        k_diis_push2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, c.state, ndiis, d.namp, d.t, d.t_new,
-                                                   c.hist_t, c.hist_e, c.part, d.active);
         k_diis_rows2<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, c.state, ndiis, c.part, c.brow, d.active);
-        n += 2;
+        n += 1;
     }
     launch_control(d, c, tol, max_iter, ndiis, 0, st);
     if (ndiis > 0)
@@ -1360,7 +1357,7 @@ const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh"
                                       "k_ladder_tc"};
 
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
-                    KernelTimer *kt)
+                    KernelTimer *kt, const CtlBuffers *diis, int ndiis)
 {
     KernelTimer dummy;
     if (!kt) kt = &dummy;
@@ -1429,6 +1426,9 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
     A.g_rq = d.g_rq; A.g_xq = d.g_xq;
+    A.st = diis ? diis->state : nullptr; A.ndiis = (diis && mode == 0) ? ndiis : 0; A.namp = d.namp;
+    A.hist_t = diis ? diis->hist_t : nullptr; A.hist_e = diis ? diis->hist_e : nullptr;
+    A.dpart = diis ? diis->part : nullptr;
     kt->begin(KID_UPDATE, st);
     k_update<<<d.nchunks, kChunk, 0, st>>>(A);
     kt->end(st);
