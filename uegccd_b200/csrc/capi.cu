@@ -209,7 +209,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int64_t> hh0;
     std::vector<RingPairDev> rpairs;
     std::vector<int16_t> ph_i, ph_x;
-    int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0;
+    int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0, mrows = 0, mcols = 0;
+    std::vector<int> s_t0(n);   // first mosaic target of each solve
     int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_v = 0, max_occ = 0;
     // offsets of each solve in the large concatenated arrays (filled in parallel below)
     std::vector<int64_t> s_amp0(n), s_pos0(n), s_phr0(n);
@@ -248,6 +249,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             bd.pair0 = (int)pair_i.size() + B.pair0;
             bd.vir0 = (int)vir.size() + B.vir0;
             bd.t0 = amp0 + B.t0;
+            bd.row0 = mrows;
+            bd.col0 = mcols;   // shifted past all rows below
+            mrows += B.o;
+            mcols += B.v;
             int bi = (int)blocks.size();
             blocks.push_back(bd);
             hh0.push_back(hhoff);
@@ -275,6 +280,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         chunk_begin[s] = (int)chunks.size();
         for (int64_t st = 0; st < P.namp; st += kChunk) chunks.push_back(ChunkDev{s, (int32_t)st});
         for (int64_t st = 0; st < P.ring_entries; st += kChunk) rchunks.push_back(ChunkDev{s, (int32_t)st});
+        s_t0[s] = (int)targets.size();
         for (int x = 0; x < P.V + P.O; x++) targets.push_back(make_int2(s, x));
         amp0 += P.namp;
         pos0 += (int64_t)P.O * P.O * P.V;
@@ -316,6 +322,40 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         }
     });
 
+    // mosaic targets: Jvv(c) adds the column sums of c over the blocks holding it, Joo(k)
+    // the row sums of the pairs (k, l); both in block order
+    for (auto &bd : blocks) bd.col0 += mrows;
+    std::vector<int32_t> mt_start(targets.size() + 1, 0);
+    parallel_for(n, nthreads, [&](int s) {
+        const SolvePlan &P = b->plans[s];
+        for (const auto &B : P.blocks) {
+            for (int c = 0; c < B.v; c++) mt_start[s_t0[s] + (P.vir[B.vir0 + c] - P.O) + 1]++;
+            for (int r = 0; r < B.o; r++) mt_start[s_t0[s] + P.V + P.pair_i[B.pair0 + r] + 1]++;
+        }
+    });
+    for (size_t k = 0; k + 1 < mt_start.size(); k++) mt_start[k + 1] += mt_start[k];
+    std::vector<int32_t> mt_list(mt_start.back());
+    std::vector<int16_t> pcol(vir.size());
+    parallel_for(n, nthreads, [&](int s) {
+        const SolvePlan &P = b->plans[s];
+        std::vector<int> fill(P.V + P.O, 0);
+        for (size_t bi = 0; bi < P.blocks.size(); bi++) {
+            const auto &B = P.blocks[bi];
+            const BlockDev &bd = blocks[solves[s].blk0 + bi];
+            // partner column from row 0: the same for every row of the block
+            for (int c = 0; c < B.v; c++) pcol[bd.vir0 + c] = (int16_t)(partner[bd.t0 + c] - bd.t0);
+            for (int c = 0; c < B.v; c++) {
+                const int y = P.vir[B.vir0 + c] - P.O;
+                mt_list[mt_start[s_t0[s] + y] + fill[y]++] = (int32_t)(bd.col0 + c);
+            }
+            for (int r = 0; r < B.o; r++) {
+                const int y = P.V + P.pair_i[B.pair0 + r];
+                mt_list[mt_start[s_t0[s] + y] + fill[y]++] = (int32_t)(bd.row0 + r);
+            }
+        }
+    });
+    if (mrows + mcols >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit mosaic indices");
+
     DevBatch &d = b->d;
     d.nsolves = n;
     d.nblocks = (int)blocks.size();
@@ -336,6 +376,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.ladder_smem = ladder_smem_bytes(max_v);
     if (d.ladder_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder block exceeds shared memory");
     set_ladder_smem_limit(d.ladder_smem);
+    d.mosaic_smem = mosaic_smem_bytes(max_v);
+    if (d.mosaic_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "mosaic block exceeds shared memory");
+    set_mosaic_smem_limit(d.mosaic_smem);
     d.max_occ = max_occ;
     d.namp = amp0;
     // ring pairs by kernel class: k_rings (two shared-memory sizes), then k_rings_wide
@@ -367,6 +410,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.rchunks, rchunks))) return rc;
     if ((rc = b->upload(d.chunk_begin, chunk_begin))) return rc;
     if ((rc = b->upload(d.targets, targets))) return rc;
+    if ((rc = b->upload(d.pcol, pcol))) return rc;
+    if ((rc = b->upload(d.mt_start, mt_start))) return rc;
+    if ((rc = b->upload(d.mt_list, mt_list))) return rc;
+    if ((rc = b->alloc(d.mpart, mrows + mcols))) return rc;
     if ((rc = b->upload(d.pair_i, pair_i))) return rc;
     if ((rc = b->upload(d.pair_j, pair_j))) return rc;
     if ((rc = b->upload(d.vir, vir))) return rc;
@@ -387,7 +434,6 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->alloc(d.t, amp0))) return rc;
     if ((rc = b->alloc(d.t_new, amp0))) return rc;
     if ((rc = b->alloc(d.g, amp0))) return rc;
-    if ((rc = b->alloc(d.S, amp0))) return rc;
     if ((rc = b->alloc(d.jvv, jvv0))) return rc;
     if ((rc = b->alloc(d.joo, joo0))) return rc;
     if ((rc = b->alloc(d.J1, ph0))) return rc;
@@ -900,7 +946,10 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     int64_t hh = 0, nblk = (int64_t)P.blocks.size();
     for (const auto &B : P.blocks) hh += (int64_t)B.o * B.o;
     int64_t b = 0;
-    b += A * (8 * 6 + sizeof(AmpInfo) + 4);          // t, t_new, g, S, g_rq, g_xq; amps; partner
+    int64_t sum_ov = 0;
+    for (const auto &B : P.blocks) sum_ov += B.o + B.v;
+    b += A * (8 * 5 + sizeof(AmpInfo) + 4);          // t, t_new, g, g_rq, g_xq; amps; partner
+    b += sum_ov * (8 + 4) + (V + O + 1) * (4 + 8);   // mosaic partials and target lists
     b += O * O * V * 4;                              // pos
     b += O * V * O * 8 * 3;                          // dRPA ring intermediates
     b += O * V * 2 * 2;                              // ph rows

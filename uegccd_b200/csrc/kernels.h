@@ -13,6 +13,10 @@ struct DevBatch {
     int nsolves = 0, nblocks = 0, ntiles = 0, nchunks = 0, nrchunks = 0, ntargets = 0;
     int max_o = 0;      // largest o_K
     int max_v = 0;      // largest v_K
+    // mosaics: block row and column sums, and per target the list of partials to add
+    double *mpart = nullptr;
+    int32_t *mt_start = nullptr, *mt_list = nullptr;
+    size_t mosaic_smem = 0;
     size_t ladder_smem = 0;  // dynamic shared memory of k_ladder3
     int max_occ = 0;    // largest NOcc
     int64_t namp = 0;
@@ -26,12 +30,13 @@ struct DevBatch {
     int *chunk_begin = nullptr;      // nsolves+1: first chunk of each solve
     int2 *targets = nullptr;         // mosaic targets (solve, id)
     int16_t *pair_i = nullptr, *pair_j = nullptr, *vir = nullptr;
+    int16_t *pcol = nullptr;          // beside vir: column of the partner d = K - c in the same block
     int32_t *pos = nullptr;          // dense (i,j,a) -> global packed index or -1
     int32_t *partner = nullptr;      // packed -> packed index of (i,j,b)
     AmpInfo *amps = nullptr;
     int4 *nv4 = nullptr;
     double *eigen = nullptr, *vtab = nullptr;
-    double *t = nullptr, *t_new = nullptr, *g = nullptr, *S = nullptr;
+    double *t = nullptr, *t_new = nullptr, *g = nullptr;
     double *jvv = nullptr, *joo = nullptr;
     double *J1 = nullptr, *J2 = nullptr, *J3 = nullptr;
     int64_t *hh0 = nullptr;          // per block: offset of H_K in hh
@@ -57,6 +62,9 @@ struct DevBatch {
 };
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
+// dynamic shared memory of k_mosaic_blk for blocks of at most max_v virtuals
+size_t mosaic_smem_bytes(int max_v);
+void set_mosaic_smem_limit(size_t bytes);
 // dynamic shared memory of k_ladder3 for blocks of at most max_v virtuals
 size_t ladder_smem_bytes(int max_v);
 void set_ladder_smem_limit(size_t bytes);

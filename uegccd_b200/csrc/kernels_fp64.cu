@@ -415,60 +415,110 @@ void set_ladder_smem_limit(size_t bytes)
 //            = v(c-k) (2t(kl,c) - t(kl,d)) - v(c-l) (t(kl,c) - 2t(kl,d))
 //   Jvv(c) = sum_{k,l} s(k,l,c),  Joo(k) = sum_{l,c} s(k,l,c)
 // dRPA (dRPA.f90:415-431): s(k,l,c) = 2 v(c-k) t(kl,c).
+// s lives only in registers: one CTA per K block forms it row by row (d = K - c is
+// in the same row) and writes the block's row sums (-> Joo of the row's k) and
+// column sums (-> Jvv of the column's c); k_mosaic_sum adds the partials of each
+// target in a fixed order.
 // ----------------------------------------------------------------------------
-__global__ void k_mosaic_s(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
-                           const AmpInfo *__restrict__ amps, const int32_t *__restrict__ partner,
-                           const int4 *__restrict__ nv4, const double *__restrict__ vtab,
-                           const double *__restrict__ t, int drpa, double *__restrict__ S,
-                           const uint8_t *__restrict__ active)
+constexpr int kMosThreads = 128;
+
+size_t mosaic_smem_bytes(int max_v)
 {
-    const ChunkDev ch = chunks[blockIdx.x];
-    if (!active[ch.solve]) return;
-    const SolveDev s = solves[ch.solve];
-    const int loc = ch.start + threadIdx.x;
-    if (loc >= s.namp) return;
-    const int64_t p = s.amp0 + loc;
-    const AmpInfo q = amps[p];
-    double x = t[p];
-    double vck = vpq(s, nv4, vtab, q.a, q.i);
-    if (drpa) {
-        S[p] = 2.0 * vck * x;
-    } else {
-        double y = t[partner[p]];
-        double vcl = vpq(s, nv4, vtab, q.a, q.j);
-        S[p] = vck * (2.0 * x - y) - vcl * (x - 2.0 * y);
+    return sizeof(double) * ((size_t)kVtabSmem + (size_t)(kMosThreads / 32) * max_v) + sizeof(int4) * (size_t)max_v +
+           sizeof(int) * (size_t)max_v;
+}
+
+__global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__restrict__ blocks,
+                                                           const SolveDev *__restrict__ solves,
+                                                           const int16_t *__restrict__ pair_i,
+                                                           const int16_t *__restrict__ pair_j,
+                                                           const int16_t *__restrict__ vir,
+                                                           const int4 *__restrict__ nv4,
+                                                           const double *__restrict__ vtab,
+                                                           const double *__restrict__ t,
+                                                           const int16_t *__restrict__ pcol, int drpa,
+                                                           double *__restrict__ mpart,
+                                                           const uint8_t *__restrict__ active)
+{
+    const BlockDev B = blocks[blockIdx.x];
+    if (!active[B.solve]) return;
+    const SolveDev s = solves[B.solve];
+    const int v = B.v, o = B.o;
+    constexpr int kW = kMosThreads / 32;
+    extern __shared__ double msm[];
+    double *sv = msm;                          // kVtabSmem
+    int4 *nvc = (int4 *)(sv + kVtabSmem);      // v: n-vectors of the block's virtuals
+    double *cacc = (double *)(nvc + v);        // kW x v: per-warp column sums
+    int *pc = (int *)(cacc + kW * v);          // v: column of the partner d = K - c
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool vsm = s.q2max < kVtabSmem;
+    if (vsm)
+        for (int q = tid; q <= s.q2max; q += kMosThreads) sv[q] = vtab[s.vtab0 + q];
+    for (int c = tid; c < v; c += kMosThreads) {
+        nvc[c] = nv4[s.orb0 + vir[B.vir0 + c]];
+        pc[c] = pcol[B.vir0 + c];
+    }
+    for (int e = tid; e < kW * v; e += kMosThreads) cacc[e] = 0.0;
+    __syncthreads();
+    auto V = [&](int q2) -> double { return vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]); };
+    for (int r = warp; r < o; r += kW) {
+        const int4 nk = nv4[s.orb0 + pair_i[B.pair0 + r]], nl = nv4[s.orb0 + pair_j[B.pair0 + r]];
+        const int64_t row = B.t0 + (int64_t)r * v;
+        double rs = 0.0;
+        for (int c = lane; c < v; c += 32) {
+            const double x = t[row + c];
+            const double vck = V(q2_of(nvc[c], nk));
+            double sval;
+            if (drpa) {
+                sval = 2.0 * vck * x;
+            } else {
+                const double y = t[row + pc[c]];  // t(kl, d), same row
+                const double vcl = V(q2_of(nvc[c], nl));
+                sval = vck * (2.0 * x - y) - vcl * (x - 2.0 * y);
+            }
+            rs += sval;
+            cacc[warp * v + c] += sval;
+        }
+        for (int off = 16; off > 0; off >>= 1) rs += __shfl_down_sync(0xffffffffu, rs, off);
+        if (lane == 0) mpart[B.row0 + r] = rs;
+    }
+    __syncthreads();
+    for (int c = tid; c < v; c += kMosThreads) {
+        double a = 0.0;
+        for (int w = 0; w < kW; w++) a += cacc[w * v + c];
+        mpart[B.col0 + c] = a;
     }
 }
 
-// One CTA per mosaic target: targets [0, V) are Jvv(c = O + x), [V, V+O) are Joo(k).
-__global__ void k_mosaic_reduce(const int2 *__restrict__ targets, const SolveDev *__restrict__ solves,
-                                const int32_t *__restrict__ pos, const double *__restrict__ S,
-                                double *__restrict__ jvv, double *__restrict__ joo,
-                                const uint8_t *__restrict__ active)
+// One warp per target: targets (s, y < V) are Jvv(c = O + y), (s, y >= V) are Joo(k = y - V).
+__global__ void __launch_bounds__(256) k_mosaic_sum(const int2 *__restrict__ targets, int ntargets,
+                                                   const SolveDev *__restrict__ solves,
+                                                   const int32_t *__restrict__ mt_start,
+                                                   const int32_t *__restrict__ mt_list,
+                                                   const double *__restrict__ mpart, double *__restrict__ jvv,
+                                                   double *__restrict__ joo, const uint8_t *__restrict__ active)
 {
-    const int2 tg = targets[blockIdx.x];
+    const int lane = threadIdx.x & 31;
+    const int tix = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (tix >= ntargets) return;
+    const int2 tg = targets[tix];
     if (!active[tg.x]) return;
-    const SolveDev s = solves[tg.x];
-    const int O = s.O, V = s.V;
-    double acc = 0.0;
-    if (tg.y < V) {
-        const int cx = tg.y;
-        for (int kl = threadIdx.x; kl < O * O; kl += blockDim.x) {
-            int p = pos[s.pos0 + (int64_t)kl * V + cx];
-            if (p >= 0) acc += S[p];
-        }
-    } else {
-        const int k = tg.y - V;
-        const int64_t base = s.pos0 + (int64_t)k * O * V;
-        for (int lc = threadIdx.x; lc < O * V; lc += blockDim.x) {
-            int p = pos[base + lc];
-            if (p >= 0) acc += S[p];
-        }
+    double a = 0.0;
+    for (int e = mt_start[tix] + lane; e < mt_start[tix + 1]; e += 32) a += mpart[mt_list[e]];
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+    if (lane == 0) {
+        const SolveDev s = solves[tg.x];
+        if (tg.y < s.V) jvv[s.jvv0 + tg.y] = a;
+        else joo[s.joo0 + tg.y - s.V] = a;
     }
-    acc = block_sum<256>(acc);
-    if (threadIdx.x == 0) {
-        if (tg.y < V) jvv[s.jvv0 + tg.y] = acc;
-        else joo[s.joo0 + tg.y - V] = acc;
+}
+
+void set_mosaic_smem_limit(size_t bytes)
+{
+    static size_t current = 48 * 1024;
+    if (bytes > current) {
+        cudaFuncSetAttribute(k_mosaic_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        current = bytes;
     }
 }
 
@@ -1352,7 +1402,7 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
 }
 
 const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh", "k_ladder",
-                                      "k_mosaic_s", "k_mosaic_reduce", "k_ring_int", "k_update",
+                                      "k_mosaic_blk", "k_mosaic_sum", "k_ring_int", "k_update",
                                       "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad", "k_rings",
                                       "k_ladder_tc"};
 
@@ -1385,11 +1435,13 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     }
     if (f.do_mosaic) {
         kt->begin(KID_MOSAIC_S, st);
-        k_mosaic_s<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.amps, d.partner, d.nv4, d.vtab, d.t, f.drpa,
-                                                 d.S, d.active);
+        k_mosaic_blk<<<d.nblocks, kMosThreads, d.mosaic_smem, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir,
+                                                                   d.nv4, d.vtab, d.t, d.pcol, f.drpa, d.mpart,
+                                                                   d.active);
         kt->end(st);
         kt->begin(KID_MOSAIC_RED, st);
-        k_mosaic_reduce<<<d.ntargets, 256, 0, st>>>(d.targets, d.solves, d.pos, d.S, d.jvv, d.joo, d.active);
+        k_mosaic_sum<<<(d.ntargets + 7) / 8, 256, 0, st>>>(d.targets, d.ntargets, d.solves, d.mt_start, d.mt_list,
+                                                           d.mpart, d.jvv, d.joo, d.active);
         kt->end(st);
         n += 2;
     }

@@ -41,6 +41,7 @@ struct BlockDev {
     int pair0;              // offset into pair_i/pair_j
     int vir0;               // offset into vir (absolute orbital indices, local to the solve)
     int64_t t0;             // global packed index of element (row 0, col 0)
+    int64_t row0, col0;     // offsets of the block's row and column sums in the mosaic partials
 };
 
 // One tile of the particle-particle ladder: rows [p0, p0+P) x columns [a0, a0+A) of block blk.
