@@ -429,6 +429,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.ph_x, ph_x))) return rc;
     if ((rc = b->upload(d.ridx_x, ridx_x))) return rc;
     if ((rc = b->upload(d.ridx_y, ridx_y))) return rc;
+    if ((rc = b->alloc(d.vcoef, amp0))) return rc;
     if ((rc = b->alloc(d.g_rq, amp0))) return rc;
     if ((rc = b->alloc(d.g_xq, amp0))) return rc;
     if ((rc = b->alloc(d.t, amp0))) return rc;
@@ -450,6 +451,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     b->red.assign(3 * (size_t)n, 0.0);
     b->active.assign(n, 1);
     CU(cudaMemcpyAsync(d.active, b->active.data(), n, cudaMemcpyHostToDevice, b->stream));
+    launch_vcoef(d, b->stream);
     size_t dn = 0;
     for (int s = 0; s < n; s++) dn = std::max(dn, (size_t)b->plans[s].O * b->plans[s].O * b->plans[s].V);
     b->dense_n = dn;
@@ -948,7 +950,7 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     int64_t b = 0;
     int64_t sum_ov = 0;
     for (const auto &B : P.blocks) sum_ov += B.o + B.v;
-    b += A * (8 * 5 + sizeof(AmpInfo) + 4);          // t, t_new, g, g_rq, g_xq; amps; partner
+    b += A * (8 * 5 + 16 + sizeof(AmpInfo) + 4);     // t, t_new, g, g_rq, g_xq; Coulomb factors; amps; partner
     b += sum_ov * (8 + 4) + (V + O + 1) * (4 + 8);   // mosaic partials and target lists
     b += O * O * V * 4;                              // pos
     b += O * V * O * 8 * 3;                          // dRPA ring intermediates

@@ -37,6 +37,7 @@ struct DevBatch {
     int4 *nv4 = nullptr;
     double *eigen = nullptr, *vtab = nullptr;
     double *t = nullptr, *t_new = nullptr, *g = nullptr;
+    double2 *vcoef = nullptr;         // per amplitude {v(i-a), v(a-j)} (k_vcoef, once per batch)
     double *jvv = nullptr, *joo = nullptr;
     double *J1 = nullptr, *J2 = nullptr, *J3 = nullptr;
     int64_t *hh0 = nullptr;          // per block: offset of H_K in hh
@@ -151,6 +152,7 @@ struct CtlBuffers;
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt = nullptr, const CtlBuffers *diis = nullptr, int ndiis = 0);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
+void launch_vcoef(const DevBatch &d, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)
 void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st);
 // Refresh point: t_ref <- t and g_ref <- FP64 particle-particle ladder of t_ref

@@ -1030,7 +1030,27 @@ struct UpdateArgs {
     int ndiis;
     int64_t namp;
     double *hist_t, *hist_e, *dpart;
+    const double2 *vcoef;     // per amplitude {v(i-a), v(a-j)}
 };
+
+// Static per-amplitude Coulomb factors of the update: {v(i-a), v(a-j)}.
+__global__ void k_vcoef(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                        const AmpInfo *__restrict__ amps, const int4 *__restrict__ nv4,
+                        const double *__restrict__ vtab, double2 *__restrict__ vcoef)
+{
+    const ChunkDev ch = chunks[blockIdx.x];
+    const SolveDev s = solves[ch.solve];
+    const int loc = ch.start + threadIdx.x;
+    if (loc >= s.namp) return;
+    const int64_t p = s.amp0 + loc;
+    const AmpInfo q = amps[p];
+    vcoef[p] = make_double2(vpq(s, nv4, vtab, q.i, q.a), vpq(s, nv4, vtab, q.a, q.j));
+}
+
+void launch_vcoef(const DevBatch &d, cudaStream_t st)
+{
+    k_vcoef<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.amps, d.nv4, d.vtab, d.vcoef);
+}
 
 __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
 {
@@ -1046,7 +1066,8 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
         const int i = q.i, j = q.j, a = q.a, b = q.b;
         const int O = s.O;
         const double told = A.t[p];
-        const double via = vpq(s, A.nv4, A.vtab, i, a);
+        const double2 vc = A.vcoef[p];
+        const double via = vc.x;
         double g = A.do_ladder ? A.g_ladder[p] : 0.0;
         if (A.do_driver) g += via;  // GetG2Drivers: G2abab = V(n_i - n_a)
         if (A.do_mosaic)
@@ -1085,7 +1106,7 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
             A.t_new[p] = tn;
             dtmax = fabs(tn - told);
             if (A.drpa) esum = via * tn * 2.0;  // SOSEX part added by k_drpa_energy at the end
-            else esum = tn * (2.0 * via - vpq(s, A.nv4, A.vtab, a, j));
+            else esum = tn * (2.0 * via - vc.y);
             if (!(fabs(tn) < 1e300)) dtmax = __longlong_as_double(0x7ff0000000000000LL);  // +Inf marks NaN/Inf
             if (A.ndiis > 0) {
                 const int slot = (A.st[ch.solve].niter - 1) % A.ndiis;
@@ -1481,6 +1502,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     A.st = diis ? diis->state : nullptr; A.ndiis = (diis && mode == 0) ? ndiis : 0; A.namp = d.namp;
     A.hist_t = diis ? diis->hist_t : nullptr; A.hist_e = diis ? diis->hist_e : nullptr;
     A.dpart = diis ? diis->part : nullptr;
+    A.vcoef = d.vcoef;
     kt->begin(KID_UPDATE, st);
     k_update<<<d.nchunks, kChunk, 0, st>>>(A);
     kt->end(st);
