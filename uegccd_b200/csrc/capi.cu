@@ -385,22 +385,26 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     {
         auto cls = [&](const RingPairDev &r) {
             const size_t b = rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max);
-            return b <= kRingSmemSmall ? 0 : b <= kRingSmemMax ? 1 : 2;
+            for (int c = 0; c < kRingClasses; c++)
+                if (b <= kRingSmemClass[c]) return c;
+            return kRingClasses;
         };
         std::stable_sort(rpairs.begin(), rpairs.end(),
                          [&](const RingPairDev &x, const RingPairDev &y) { return cls(x) < cls(y); });
         for (const auto &r : rpairs) {
             const int c = cls(r);
             d.nring[c]++;
-            const size_t b = c < 2 ? rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max)
-                                   : rings_smem_bytes(solves[r.solve].O, r.n1 + r.n2);
+            const size_t b = c < kRingClasses
+                                 ? rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max)
+                                 : rings_smem_bytes(solves[r.solve].O, r.n1 + r.n2);
             d.ring_smem[c] = std::max(d.ring_smem[c], b);
         }
     }
     d.nrpairs = (int)rpairs.size();
-    if (d.ring_smem[2] > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ring group pair exceeds shared memory");
-    set_rings_smem_limit(0, std::max(d.ring_smem[0], d.ring_smem[1]));
-    set_rings_smem_limit(1, d.ring_smem[2]);
+    if (d.ring_smem[kRingClasses] > 227 * 1024)
+        return fail(UEGCCD_ERR_UNSUPPORTED, "ring group pair exceeds shared memory");
+    set_rings_smem_limit(0, *std::max_element(d.ring_smem, d.ring_smem + kRingClasses));
+    set_rings_smem_limit(1, d.ring_smem[kRingClasses]);
     if ((rc = b->upload(d.solves, solves))) return rc;
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;

@@ -56,10 +56,10 @@ struct DevBatch {
     double *t_ref = nullptr, *g_ref = nullptr;  // refresh point of the defect correction
     int *tc_err = nullptr;
     int nrpairs = 0;
-    // ring pair classes, rpairs sorted in this order: k_rings with the smaller and the
-    // larger shared-memory size, then k_rings_wide
-    int nring[3] = {0, 0, 0};
-    size_t ring_smem[3] = {0, 0, 0};
+    // ring pair classes, rpairs sorted in this order: k_rings in kRingClasses shared-memory
+    // sizes (kRingSmemClass), then k_rings_wide
+    int nring[4] = {0, 0, 0, 0};
+    size_t ring_smem[4] = {0, 0, 0, 0};
 };
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
@@ -71,8 +71,9 @@ size_t ladder_smem_bytes(int max_v);
 void set_ladder_smem_limit(size_t bytes);
 // dynamic shared memory of k_rings for NOcc = O and groups of n1 and n2 rows
 size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max);
-constexpr size_t kRingSmemSmall = 72 * 1024;   // k_rings pairs up to this size: 3 CTAs per SM
-constexpr size_t kRingSmemMax = 200 * 1024;    // above this the pair goes to k_rings_wide
+constexpr int kRingClasses = 3;
+// k_rings pairs up to these sizes (5, 3 and 1 CTAs per SM); above the last: k_rings_wide
+constexpr size_t kRingSmemClass[kRingClasses] = {40 * 1024, 72 * 1024, 200 * 1024};
 void set_rings_smem_limit(int wide, size_t bytes);
 
 constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* use the same bound)

@@ -749,29 +749,36 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
 
 // ----------------------------------------------------------------------------
 // Rings on the FP64 tensor cores (mma.sync m8n8k4 f64), one CTA per {Q, -Q}
-// group pair.  With W[k][l] = v(n_k - n_l - Q) (the -Q group uses W^T),
-// Vs_r[l] = v(n_l - n_i(r)) and, per row r:
-//   XW_r = X_r W_r,   U_r = Y_r W_r - Vs_r
-// the products of the fused form above regroup into small GEMMs over l:
-//   ring (i1,i2,x1) = lin + base_1 (2 Sx_2 - Sy_2) + sum_l [XW_1 (Y_2 - 2 X_2) + U_1 X_2 - X_1 Vs_2]
-//   xring(i1,i2,x2) =                                sum_l [U_1 Y_2 - Y_1 Vs_2]
-// lin = 2 vd_1 (Sx_1 + Sx_2) - vd_1 (Sy_1 + Sy_2), base_1 = vd_1 (2 Sx_1 - Sy_1); the
-// -Ex/-Ey terms of the fused form are the Vs products.  Rows are padded to
-// multiples of 8 and k to Op = NOcc rounded up to 8, with zeros; row stride
-// ld = Op + 4 (= 4 or 12 mod 16 doubles) keeps the fragment loads free of bank
+// group pair, on compressed matrices.  Rows a of group 1 are (i_a, x_a) with
+// n_x - n_i = Q; rows b of group 2 are (i_b, x_b) with -Q.  The amplitude
+// t(i_a k, x_a) exists exactly for k in occ2 = {i_b}: its partner is x_b.  So every
+// ph row of one group is dense over the occupied indices of the other group:
+//   X1[a][b] = t(i_a i_b, x_a)   Y1[a][b] = t(i_b i_a, x_a)   (n1 x n2)
+//   X2[b][a] = t(i_b i_a, x_b)   Y2[b][a] = t(i_a i_b, x_b)   (n2 x n1)
+//   W[b][a]  = v(n_{i_b} - n_{i_a} - Q)      (the -Q group uses W^T)
+//   Vs1[a][a'] = v(n_{i_a'} - n_{i_a}),  Vs2[b][b'] = v(n_{i_b'} - n_{i_b})
+//   XW1 = X1 W,  U1 = Y1 W - Vs1,   XW2 = X2 W^T,  U2 = Y2 W^T - Vs2
+// and the fused ring form above becomes, for the amplitude pair (a, b):
+//   ring (i_a, i_b, x_a) = lin + base_a (2 Sx_b - Sy_b)
+//                          + sum_a' [XW1[a][a'] (Y2 - 2 X2)[b][a'] + U1[a][a'] X2[b][a']]
+//                          - sum_b' X1[a][b'] Vs2[b][b']
+//   xring(i_a, i_b, x_b) = sum_a' U1[a][a'] Y2[b][a'] - sum_b' Y1[a][b'] Vs2[b][b']
+// (lin, base as above), and the same with 1 <-> 2 for the amplitudes (i_b, i_a, .).
+// The matrix sides are the group sizes (padded to 8), not NOcc.  Row strides are
+// the padded width + 4 (= 4 or 12 mod 16 doubles): fragment loads without bank
 // conflicts.
 // ----------------------------------------------------------------------------
-constexpr int kRingThreads = 256;
+constexpr int kRingThreads = 128;
 constexpr int kRingGather = 4;   // gather elements in flight per thread
 
 __host__ __device__ __forceinline__ int round8(int x) { return (x + 7) & ~7; }
 
 size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
 {
-    const int Op = round8(O), ld = Op + 4, Rp = round8(n1) + round8(n2);
-    const int nsv = q2max < kVtabSmem ? round8(q2max + 1) : 0;
-    return sizeof(double) * ((size_t)Op * ld + 5 * (size_t)Rp * ld + 3 * (size_t)Rp + nsv) + sizeof(int) * 2 * Rp +
-           sizeof(int4) * ((size_t)O + Rp);
+    const size_t N1 = round8(n1), N2 = round8(n2), l1 = N1 + 4, l2 = N2 + 4;
+    const size_t nsv = q2max < kVtabSmem ? round8(q2max + 1) : 0;
+    const size_t dbl = 2 * N1 * l2 + 3 * N2 * l1 + 3 * N1 * l1 + 3 * N2 * l2 + 3 * (N1 + N2) + nsv;
+    return sizeof(double) * dbl + sizeof(int) * 2 * (N1 + N2) + sizeof(int4) * ((size_t)O + N1 + N2);
 }
 
 __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__restrict__ pairs,
@@ -789,35 +796,42 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
     const RingPairDev P = pairs[blockIdx.x];
     if (!active[P.solve]) return;
     const SolveDev s = solves[P.solve];
-    const int O = s.O, Op = round8(O), ld = Op + 4;
-    const int n1 = P.n1, n2 = P.n2, n1p = round8(n1), n2p = round8(n2), Rp = n1p + n2p;
+    const int O = s.O;
+    const int n1 = P.n1, n2 = P.n2;
+    if (n1 <= 0 || n2 <= 0) return;  // a ring pair always has both groups; whole CTA
+    const int N1 = round8(n1), N2 = round8(n2), l1 = N1 + 4, l2 = N2 + 4, R = N1 + N2;
     const bool vsm = s.q2max < kVtabSmem;
     const int nsv = vsm ? round8(s.q2max + 1) : 0;
     extern __shared__ double smem[];
-    double *W = smem;                 // Op x ld
-    double *X = W + Op * ld;          // Rp x ld: X[r][k] = t(i_r k, x_r)
-    double *Y = X + Rp * ld;          // Rp x ld: Y[r][k] = t(k i_r, x_r) = t(i_r k, c)
-    double *Vs = Y + Rp * ld;         // Rp x ld
-    double *XW = Vs + Rp * ld;        // Rp x ld
-    double *U = XW + Rp * ld;         // Rp x ld
-    double *Sx = U + Rp * ld;         // Rp
-    double *Sy = Sx + Rp;             // Rp
-    double *Vd = Sy + Rp;             // Rp
-    double *sv = Vd + Rp;             // nsv: the |q|^2 table
-    int *ri = (int *)(sv + nsv);      // Rp, -1 on padding rows
-    int *rw = ri + Rp;                // Rp: the row's offset in the gather-index tables, -1 on padding rows
-    int4 *no = (int4 *)(rw + Rp);     // O occupied n-vectors (16-byte aligned: Rp, nsv multiples of 8)
-    int4 *nx = no + O;                // Rp: n-vector of each row's virtual
+    double *X1 = smem;              // N1 x l2
+    double *Y1 = X1 + N1 * l2;      // N1 x l2
+    double *X2 = Y1 + N1 * l2;      // N2 x l1
+    double *Y2 = X2 + N2 * l1;      // N2 x l1
+    double *W = Y2 + N2 * l1;       // N2 x l1
+    double *Vs1 = W + N2 * l1;      // N1 x l1
+    double *XW1 = Vs1 + N1 * l1;    // N1 x l1
+    double *U1 = XW1 + N1 * l1;     // N1 x l1
+    double *Vs2 = U1 + N1 * l1;     // N2 x l2
+    double *XW2 = Vs2 + N2 * l2;    // N2 x l2
+    double *U2 = XW2 + N2 * l2;     // N2 x l2
+    double *Sx = U2 + N2 * l2;      // R: group 1 rows at [0, N1), group 2 rows at [N1, R)
+    double *Sy = Sx + R;
+    double *Vd = Sy + R;
+    double *sv = Vd + R;            // nsv
+    int *ri = (int *)(sv + nsv);    // R: occupied index of the row (-1 on padding)
+    int *rw = ri + R;               // R: row * O, the row's offset in the gather-index tables
+    int4 *no = (int4 *)(rw + R);    // O
+    int4 *nx = no + O;              // R: n-vector of the row's virtual
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int kWarps = kRingThreads / 32;
     auto V = [&](int q2) -> double {
         return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]));
     };
     for (int q = tid; q < nsv; q += kRingThreads) sv[q] = q <= s.q2max ? vtab[s.vtab0 + q] : 0.0;
-    for (int r = tid; r < Rp; r += kRingThreads) {
+    for (int r = tid; r < R; r += kRingThreads) {
         int row = -1;
         if (r < n1) row = P.r1 + r;
-        else if (r >= n1p && r - n1p < n2) row = P.r2 + (r - n1p);
+        else if (r >= N1 && r - N1 < n2) row = P.r2 + (r - N1);
         const int i = row >= 0 ? ph_i[s.phr0 + row] : -1, x = row >= 0 ? ph_x[s.phr0 + row] : -1;
         ri[r] = i;
         rw[r] = row >= 0 ? row * O : -1;
@@ -825,156 +839,195 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
     }
     for (int k = tid; k < O; k += kRingThreads) no[k] = nv4[s.orb0 + k];
     __syncthreads();
-    // Q = n_x - n_i of group 1 (the negative of group 2's)
-    int Qx, Qy, Qz;
-    {
-        const int r = n1 > 0 ? 0 : n1p;
-        const int4 qa = nx[r], qb = no[ri[r]];
-        const int sg = n1 > 0 ? 1 : -1;
-        Qx = sg * (qa.x - qb.x);
-        Qy = sg * (qa.y - qb.y);
-        Qz = sg * (qa.z - qb.z);
-    }
-    // X, Y gathers: a warp per row, lanes over k; the index loads of kRingGather rows
-    // are issued before their amplitude loads
+    const int4 q1x = nx[0], q1i = no[ri[0]];
+    const int Qx = q1x.x - q1i.x, Qy = q1x.y - q1i.y, Qz = q1x.z - q1i.z;
     const int32_t *gx = ridx_x + s.ph0, *gy = ridx_y + s.ph0;
-    for (int r0 = warp; r0 < Rp; r0 += kWarps * kRingGather) {
-        for (int k = lane; k < Op; k += 32) {
+    // gathers: (X1, Y1) over (a, b) and (X2, Y2) over (b, a); index loads of a batch first
+    for (int side = 0; side < 2; side++) {
+        const int nr = side == 0 ? N1 : N2, nc = side == 0 ? N2 : N1;
+        const int vr = side == 0 ? n1 : n2, vc = side == 0 ? n2 : n1;
+        const int rbase = side == 0 ? 0 : N1, cbase = side == 0 ? N1 : 0;
+        const int ldc = side == 0 ? l2 : l1;
+        double *Xs = side == 0 ? X1 : X2, *Ys = side == 0 ? Y1 : Y2;
+        const int ne = nr * nc;
+        for (int e0 = tid; e0 < ne; e0 += kRingThreads * kRingGather) {
             int p1[kRingGather], p2[kRingGather];
 #pragma unroll
             for (int u = 0; u < kRingGather; u++) {
-                const int r = r0 + u * kWarps;
-                const int w = (r < Rp && k < O) ? rw[r] : -1;
-                p1[u] = w >= 0 ? __ldg(&gx[w + k]) : -1;
-                p2[u] = w >= 0 ? __ldg(&gy[w + k]) : -1;
+                const int e = e0 + u * kRingThreads;
+                p1[u] = p2[u] = -1;
+                if (e < ne) {
+                    const int r = e / nc, c = e - r * nc;
+                    if (r < vr && c < vc) {
+                        const int w = rw[rbase + r] + ri[cbase + c];
+                        p1[u] = __ldg(&gx[w]);
+                        p2[u] = __ldg(&gy[w]);
+                    }
+                }
             }
 #pragma unroll
             for (int u = 0; u < kRingGather; u++) {
-                const int r = r0 + u * kWarps;
-                if (r < Rp) {
-                    X[r * ld + k] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
-                    Y[r * ld + k] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
+                const int e = e0 + u * kRingThreads;
+                if (e < ne) {
+                    const int r = e / nc, c = e - r * nc;
+                    Xs[r * ldc + c] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
+                    Ys[r * ldc + c] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
                 }
             }
         }
     }
-    // exchange kernel W and the direct rows Vs (shared-memory table lookups)
-    for (int k = warp; k < Op; k += kWarps)
-        for (int l = lane; l < Op; l += 32) {
-            double w = 0.0;
-            if (k < O && l < O) {
-                const int dx = no[k].x - no[l].x - Qx, dy = no[k].y - no[l].y - Qy, dz = no[k].z - no[l].z - Qz;
-                w = V(dx * dx + dy * dy + dz * dz);
-            }
-            W[k * ld + l] = w;
+    // W[b][a] and the direct kernels Vs1, Vs2 (shared-memory table lookups)
+    for (int e = tid; e < N2 * N1; e += kRingThreads) {
+        const int b = e / N1, a = e - b * N1;
+        double w = 0.0;
+        if (b < n2 && a < n1) {
+            const int4 nb = no[ri[N1 + b]], na = no[ri[a]];
+            const int dx = nb.x - na.x - Qx, dy = nb.y - na.y - Qy, dz = nb.z - na.z - Qz;
+            w = V(dx * dx + dy * dy + dz * dz);
         }
-    for (int r = warp; r < Rp; r += kWarps) {
-        const int i = ri[r];
-        for (int k = lane; k < Op; k += 32) Vs[r * ld + k] = (i >= 0 && k < O) ? V(q2_of(no[k], no[i])) : 0.0;
+        W[b * l1 + a] = w;
+    }
+    for (int e = tid; e < N1 * N1; e += kRingThreads) {
+        const int a = e / N1, c = e - a * N1;
+        Vs1[a * l1 + c] = (a < n1 && c < n1) ? V(q2_of(no[ri[c]], no[ri[a]])) : 0.0;
+    }
+    for (int e = tid; e < N2 * N2; e += kRingThreads) {
+        const int b = e / N2, c = e - b * N2;
+        Vs2[b * l2 + c] = (b < n2 && c < n2) ? V(q2_of(no[ri[N1 + c]], no[ri[N1 + b]])) : 0.0;
     }
     __syncthreads();
-    for (int r = tid; r < Rp; r += kRingThreads) {
+    for (int r = tid; r < R; r += kRingThreads) {
+        const bool g1 = r < N1;
+        const double *xr = g1 ? X1 + r * l2 : X2 + (r - N1) * l1;
+        const double *yr = g1 ? Y1 + r * l2 : Y2 + (r - N1) * l1;
+        const int nc = g1 ? n2 : n1;
         double sx = 0.0, sy = 0.0;
-        for (int k = 0; k < O; k++) {
-            sx += X[r * ld + k];
-            sy += Y[r * ld + k];
+        for (int c = 0; c < nc; c++) {
+            sx += xr[c];
+            sy += yr[c];
         }
         Sx[r] = sx;
         Sy[r] = sy;
         Vd[r] = ri[r] >= 0 ? V(q2_of(no[ri[r]], nx[r])) : 0.0;
     }
     const int g = lane >> 2, tg = lane & 3;
-    // phase 1: XW = X W_r and U = Y W_r - Vs, tasks of 8 rows x 32 columns
+    // phase 1: XW1 = X1 W, U1 = Y1 W - Vs1 (K = N2); XW2 = X2 W^T, U2 = Y2 W^T - Vs2 (K = N1).
+    // Tasks: one 8-row fragment row x up to 4 column fragments.
     {
-        const int mfr = Rp / 8, nng = (Op + 31) / 32;
-        const int ntask = 2 * mfr * nng;
+        const int ng1 = (N1 + 31) / 32, ng2 = (N2 + 31) / 32;
+        const int t1 = (N1 / 8) * ng1, t2 = (N2 / 8) * ng2;   // per matrix of each group
+        const int ntask = 2 * t1 + 2 * t2;
         for (int task = warp; task < ntask; task += kWarps) {
-            const int mat = task / (mfr * nng), rem = task - mat * (mfr * nng);
-            const int mf = rem / nng, ng = rem - mf * nng;
-            const int r0 = mf * 8, nbase = ng * 32;
-            const bool grp2 = r0 >= n1p;
-            const double *A = (mat == 0 ? X : Y) + (r0 + g) * ld + tg;
+            const bool grp2 = task >= 2 * t1;
+            const int tt = grp2 ? task - 2 * t1 : task, tg1 = grp2 ? t2 : t1, ngr = grp2 ? ng2 : ng1;
+            const int mat = tt / tg1, rem = tt - mat * tg1;
+            const int mf = rem / ngr, ng = rem - mf * ngr;
+            const int Ncol = grp2 ? N2 : N1, K = grp2 ? N1 : N2, lda = grp2 ? l1 : l2, ldo = grp2 ? l2 : l1;
+            const double *A = (grp2 ? (mat == 0 ? X2 : Y2) : (mat == 0 ? X1 : Y1)) + (mf * 8 + g) * lda + tg;
+            const int nbase = ng * 32;
             double acc[4][2];
 #pragma unroll
             for (int f = 0; f < 4; f++) acc[f][0] = acc[f][1] = 0.0;
-            for (int k0 = 0; k0 < Op; k0 += 4) {
-                const double a = A[k0];
+            for (int k0 = 0; k0 < K; k0 += 4) {
+                const double av = A[k0];
 #pragma unroll
                 for (int f = 0; f < 4; f++) {
-                    if (nbase + f * 8 >= Op) break;
+                    if (nbase + f * 8 >= Ncol) break;
                     const int n = nbase + f * 8 + g;
-                    const double b = grp2 ? W[n * ld + k0 + tg] : W[(k0 + tg) * ld + n];
-                    dmma_884(acc[f][0], acc[f][1], a, b);
+                    // group 1: B(k=b, n=a') = W[b][a'];  group 2: B(k=a, n=b') = W[b'][a]
+                    const double bv = grp2 ? W[n * l1 + k0 + tg] : W[(k0 + tg) * l1 + n];
+                    dmma_884(acc[f][0], acc[f][1], av, bv);
                 }
             }
-            double *Out = mat == 0 ? XW : U;
-            const int r = r0 + g;
+            double *Out = grp2 ? (mat == 0 ? XW2 : U2) : (mat == 0 ? XW1 : U1);
+            const double *Vsg = grp2 ? Vs2 : Vs1;
+            const int r = mf * 8 + g;
 #pragma unroll
             for (int f = 0; f < 4; f++) {
-                if (nbase + f * 8 >= Op) break;
+                if (nbase + f * 8 >= Ncol) break;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int n = nbase + f * 8 + 2 * tg + h;
                     double v = acc[f][h];
-                    if (mat == 1) v -= Vs[r * ld + n];
-                    Out[r * ld + n] = v;
+                    if (mat == 1) v -= Vsg[r * ldo + n];
+                    Out[r * ldo + n] = v;
                 }
             }
         }
     }
     __syncthreads();
-    // phase 2: both directions, tasks of 8 (r1) x 16 (r2)
-    const int t1 = (n1p / 8) * ((n2p + 15) / 16), t2 = (n2p / 8) * ((n1p + 15) / 16);
+    // phase 2: dir 0 rows a x columns b, dir 1 rows b x columns a; tasks of 8 x 16
+    const int t1 = (N1 / 8) * ((N2 + 15) / 16), t2 = (N2 / 8) * ((N1 + 15) / 16);
     for (int task = warp; task < t1 + t2; task += kWarps) {
         const int dir = task < t1 ? 0 : 1, tt = dir ? task - t1 : task;
-        const int a0 = dir ? n1p : 0, na = dir ? n2 : n1;
-        const int b0 = dir ? 0 : n1p, nb = dir ? n1 : n2, nbp = dir ? n1p : n2p;
-        const int nng = (nbp + 15) / 16;
+        // dir 0: A side group 1 (XW1, U1 with K1 = N1 over a'; X1, Y1 with K2 = N2 over b'),
+        //        B side group 2 (X2, Y2 rows b over a'; Vs2 rows b over b')
+        const int Mv = dir ? n2 : n1, Nv = dir ? n1 : n2, Np = dir ? N1 : N2;
+        const int K1 = dir ? N2 : N1, K2 = dir ? N1 : N2;
+        const double *AXW = dir ? XW2 : XW1, *AU = dir ? U2 : U1;   // stride K1 + 4
+        const double *AX = dir ? X2 : X1, *AY = dir ? Y2 : Y1;      // stride K2 + 4
+        const double *BX = dir ? X1 : X2, *BY = dir ? Y1 : Y2;      // stride K1 + 4
+        const double *BV = dir ? Vs1 : Vs2;                         // stride K2 + 4
+        const int lk1 = K1 + 4, lk2 = K2 + 4;
+        const int nng = (Np + 15) / 16;
         const int mf = tt / nng, ng = tt - mf * nng;
-        const int ra = a0 + mf * 8 + g;
-        double ring[2][2], xr[2][2];
-#pragma unroll
-        for (int f = 0; f < 2; f++) ring[f][0] = ring[f][1] = xr[f][0] = xr[f][1] = 0.0;
-        for (int k0 = 0; k0 < Op; k0 += 4) {
-            const int k = k0 + tg;
-            const double axw = XW[ra * ld + k], au = U[ra * ld + k], ax = X[ra * ld + k], ay = Y[ra * ld + k];
-#pragma unroll
-            for (int f = 0; f < 2; f++) {
-                const int nloc = ng * 16 + f * 8;
-                if (nloc >= nbp) break;
-                const int rb = b0 + nloc + g;
-                const double bx = X[rb * ld + k], by = Y[rb * ld + k], bv = -Vs[rb * ld + k];
-                const double bz = by - 2.0 * bx;
-                dmma_884(ring[f][0], ring[f][1], axw, bz);
-                dmma_884(ring[f][0], ring[f][1], au, bx);
-                dmma_884(ring[f][0], ring[f][1], ax, bv);
-                dmma_884(xr[f][0], xr[f][1], au, by);
-                dmma_884(xr[f][0], xr[f][1], ay, bv);
-            }
-        }
-        const int m = mf * 8 + g;
-        if (m >= na) continue;
-        const int r1 = a0 + m, i1 = ri[r1];
-        const double vd = Vd[r1], sx1 = Sx[r1], sy1 = Sy[r1];
-        const double base = vd * (2.0 * sx1 - sy1);
+        const int m0 = mf * 8;
+        double ra[2][2], rb[2][2], xa[2][2], xb[2][2];
 #pragma unroll
         for (int f = 0; f < 2; f++)
 #pragma unroll
+            for (int h = 0; h < 2; h++) ra[f][h] = rb[f][h] = xa[f][h] = xb[f][h] = 0.0;
+        for (int k0 = 0; k0 < K1; k0 += 4) {
+            const int k = k0 + tg;
+            const double axw = AXW[(m0 + g) * lk1 + k], au = AU[(m0 + g) * lk1 + k];
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                const int n0 = ng * 16 + f * 8;
+                if (n0 >= Np) break;
+                const double bx = BX[(n0 + g) * lk1 + k], by = BY[(n0 + g) * lk1 + k];
+                dmma_884(ra[f][0], ra[f][1], axw, by - 2.0 * bx);
+                dmma_884(rb[f][0], rb[f][1], au, bx);
+                dmma_884(xa[f][0], xa[f][1], au, by);
+            }
+        }
+        for (int k0 = 0; k0 < K2; k0 += 4) {
+            const int k = k0 + tg;
+            const double ax = AX[(m0 + g) * lk2 + k], ay = AY[(m0 + g) * lk2 + k];
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                const int n0 = ng * 16 + f * 8;
+                if (n0 >= Np) break;
+                const double bv = -BV[(n0 + g) * lk2 + k];
+                dmma_884(rb[f][0], rb[f][1], ax, bv);
+                dmma_884(xb[f][0], xb[f][1], ay, bv);
+            }
+        }
+        const int m = m0 + g;
+        if (m >= Mv) continue;
+        const int r1 = dir ? N1 + m : m;                 // this lane's row (slot index)
+        const double vd = Vd[r1], sx1 = Sx[r1], sy1 = Sy[r1];
+        const double base = vd * (2.0 * sx1 - sy1);
+#pragma unroll
+        for (int f = 0; f < 2; f++) {
+            const int n0 = ng * 16 + f * 8;
+            if (n0 >= Np) break;
+#pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int nloc = ng * 16 + f * 8 + 2 * tg + h;
-                if (nloc >= nb) continue;
-                const int r2 = b0 + nloc, i2 = ri[r2];
-                // ring amplitude (i1, i2, x1) is X_r1[i2]; crossed ring (i1, i2, x2) is Y_r2[i1]
+                const int n = n0 + 2 * tg + h;
+                if (n >= Nv) continue;
+                const int r2 = dir ? n : N1 + n;
+                // ring amplitude (i_r1, i_r2, x_r1) and crossed ring (i_r1, i_r2, x_r2)
                 if (do_ring) {
                     const double lin = 2.0 * vd * (sx1 + Sx[r2]) - vd * (sy1 + Sy[r2]);
-                    const int p = __ldg(&gx[rw[r1] + i2]);
-                    if (p >= 0) g_rq[p] = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ring[f][h];
+                    const int p = __ldg(&gx[rw[r1] + ri[r2]]);
+                    if (p >= 0) g_rq[p] = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ra[f][h] + rb[f][h];
                 }
                 if (do_xring) {
-                    const int p = __ldg(&gy[rw[r2] + i1]);
-                    if (p >= 0) g_xq[p] = xr[f][h];
+                    const int p = __ldg(&gy[rw[r2] + ri[r1]]);
+                    if (p >= 0) g_xq[p] = xa[f][h] + xb[f][h];
                 }
             }
+        }
     }
 }
 
@@ -1477,15 +1530,15 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         kt->begin(KID_RINGS, st);
         // pair classes (sorted in this order): DMMA tiles in two shared-memory sizes, then the FMA form
         int off = 0;
-        for (int c = 0; c < 2; c++) {
+        for (int c = 0; c < kRingClasses; c++) {
             if (d.nring[c] > 0)
                 k_rings<<<d.nring[c], kRingThreads, d.ring_smem[c], st>>>(
                     d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, f.do_ring,
                     f.do_xring, d.g_rq, d.g_xq, d.active);
             off += d.nring[c];
         }
-        if (d.nring[2] > 0)
-            k_rings_wide<<<d.nring[2], 256, d.ring_smem[2], st>>>(d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.pos,
+        if (d.nring[kRingClasses] > 0)
+            k_rings_wide<<<d.nring[kRingClasses], 256, d.ring_smem[kRingClasses], st>>>(d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.pos,
                                                                  d.partner, d.nv4, d.vtab, d.t, f.do_ring,
                                                                  f.do_xring, d.g_rq, d.g_xq, d.active);
         kt->end(st);
