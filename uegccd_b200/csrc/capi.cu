@@ -385,8 +385,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     {
         auto cls = [&](const RingPairDev &r) {
             const size_t b = rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max);
+            if (b > kRingSmemMax) return kRingClasses;
+            const int rows = ((r.n1 + 7) & ~7) + ((r.n2 + 7) & ~7);
             for (int c = 0; c < kRingClasses; c++)
-                if (b <= kRingSmemClass[c]) return c;
+                if (rows <= kRingClassRows[c]) return c;
             return kRingClasses;
         };
         std::stable_sort(rpairs.begin(), rpairs.end(),

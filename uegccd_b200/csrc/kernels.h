@@ -58,8 +58,8 @@ struct DevBatch {
     int nrpairs = 0;
     // ring pair classes, rpairs sorted in this order: k_rings in kRingClasses shared-memory
     // sizes (kRingSmemClass), then k_rings_wide
-    int nring[4] = {0, 0, 0, 0};
-    size_t ring_smem[4] = {0, 0, 0, 0};
+    int nring[5] = {0, 0, 0, 0, 0};
+    size_t ring_smem[5] = {0, 0, 0, 0, 0};
 };
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
@@ -71,9 +71,12 @@ size_t ladder_smem_bytes(int max_v);
 void set_ladder_smem_limit(size_t bytes);
 // dynamic shared memory of k_rings for NOcc = O and groups of n1 and n2 rows
 size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max);
-constexpr int kRingClasses = 3;
-// k_rings pairs up to these sizes (5, 3 and 1 CTAs per SM); above the last: k_rings_wide
-constexpr size_t kRingSmemClass[kRingClasses] = {40 * 1024, 72 * 1024, 200 * 1024};
+// k_rings classes by padded pair size N1 + N2 (up to kRingClassRows), each with its
+// CTA size; pairs above the last class, or above kRingSmemMax, go to k_rings_wide
+constexpr int kRingClasses = 4;
+constexpr int kRingClassRows[kRingClasses] = {16, 32, 48, 1 << 30};
+constexpr int kRingClassThreads[kRingClasses] = {32, 64, 128, 256};
+constexpr size_t kRingSmemMax = 200 * 1024;
 void set_rings_smem_limit(int wide, size_t bytes);
 
 constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* use the same bound)

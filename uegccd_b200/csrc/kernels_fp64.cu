@@ -768,8 +768,7 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
 // the padded width + 4 (= 4 or 12 mod 16 doubles): fragment loads without bank
 // conflicts.
 // ----------------------------------------------------------------------------
-constexpr int kRingThreads = 128;
-constexpr int kRingGather = 4;   // gather elements in flight per thread
+constexpr int kRingGather = 8;   // gather elements in flight per thread
 
 __host__ __device__ __forceinline__ int round8(int x) { return (x + 7) & ~7; }
 
@@ -781,7 +780,7 @@ size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
     return sizeof(double) * dbl + sizeof(int) * 2 * (N1 + N2) + sizeof(int4) * ((size_t)O + N1 + N2);
 }
 
-__global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__restrict__ pairs,
+__global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ pairs,
                                                         const SolveDev *__restrict__ solves,
                                                         const int16_t *__restrict__ ph_i,
                                                         const int16_t *__restrict__ ph_x,
@@ -822,13 +821,13 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
     int *rw = ri + R;               // R: row * O, the row's offset in the gather-index tables
     int4 *no = (int4 *)(rw + R);    // O
     int4 *nx = no + O;              // R: n-vector of the row's virtual
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    constexpr int kWarps = kRingThreads / 32;
+    // the CTA is 1, 2 or 4 warps, by pair size
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, kWarps = nt >> 5;
     auto V = [&](int q2) -> double {
         return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]));
     };
-    for (int q = tid; q < nsv; q += kRingThreads) sv[q] = q <= s.q2max ? vtab[s.vtab0 + q] : 0.0;
-    for (int r = tid; r < R; r += kRingThreads) {
+    for (int q = tid; q < nsv; q += nt) sv[q] = q <= s.q2max ? vtab[s.vtab0 + q] : 0.0;
+    for (int r = tid; r < R; r += nt) {
         int row = -1;
         if (r < n1) row = P.r1 + r;
         else if (r >= N1 && r - N1 < n2) row = P.r2 + (r - N1);
@@ -837,47 +836,46 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
         rw[r] = row >= 0 ? row * O : -1;
         nx[r] = x >= 0 ? nv4[s.orb0 + x] : make_int4(0, 0, 0, 0);
     }
-    for (int k = tid; k < O; k += kRingThreads) no[k] = nv4[s.orb0 + k];
+    for (int k = tid; k < O; k += nt) no[k] = nv4[s.orb0 + k];
     __syncthreads();
     const int4 q1x = nx[0], q1i = no[ri[0]];
     const int Qx = q1x.x - q1i.x, Qy = q1x.y - q1i.y, Qz = q1x.z - q1i.z;
     const int32_t *gx = ridx_x + s.ph0, *gy = ridx_y + s.ph0;
-    // gathers: (X1, Y1) over (a, b) and (X2, Y2) over (b, a); index loads of a batch first
-    for (int side = 0; side < 2; side++) {
-        const int nr = side == 0 ? N1 : N2, nc = side == 0 ? N2 : N1;
-        const int vr = side == 0 ? n1 : n2, vc = side == 0 ? n2 : n1;
-        const int rbase = side == 0 ? 0 : N1, cbase = side == 0 ? N1 : 0;
-        const int ldc = side == 0 ? l2 : l1;
-        double *Xs = side == 0 ? X1 : X2, *Ys = side == 0 ? Y1 : Y2;
-        const int ne = nr * nc;
-        for (int e0 = tid; e0 < ne; e0 += kRingThreads * kRingGather) {
-            int p1[kRingGather], p2[kRingGather];
+    // gathers: (X1, Y1) over (a, b), then (X2, Y2) over (b, a), as one flat range; the
+    // index loads of a batch are issued before its amplitude loads
+    const int ne1 = N1 * N2, ne = 2 * ne1;
+    for (int e0 = tid; e0 < ne; e0 += nt * kRingGather) {
+        int p1[kRingGather], p2[kRingGather];
 #pragma unroll
-            for (int u = 0; u < kRingGather; u++) {
-                const int e = e0 + u * kRingThreads;
-                p1[u] = p2[u] = -1;
-                if (e < ne) {
-                    const int r = e / nc, c = e - r * nc;
-                    if (r < vr && c < vc) {
-                        const int w = rw[rbase + r] + ri[cbase + c];
-                        p1[u] = __ldg(&gx[w]);
-                        p2[u] = __ldg(&gy[w]);
-                    }
+        for (int u = 0; u < kRingGather; u++) {
+            const int e = e0 + u * nt;
+            p1[u] = p2[u] = -1;
+            if (e < ne) {
+                const bool s2 = e >= ne1;
+                const int el = s2 ? e - ne1 : e, nc = s2 ? N1 : N2;
+                const int r = el / nc, c = el - r * nc;
+                if (r < (s2 ? n2 : n1) && c < (s2 ? n1 : n2)) {
+                    const int w = s2 ? rw[N1 + r] + ri[c] : rw[r] + ri[N1 + c];
+                    p1[u] = __ldg(&gx[w]);
+                    p2[u] = __ldg(&gy[w]);
                 }
             }
+        }
 #pragma unroll
-            for (int u = 0; u < kRingGather; u++) {
-                const int e = e0 + u * kRingThreads;
-                if (e < ne) {
-                    const int r = e / nc, c = e - r * nc;
-                    Xs[r * ldc + c] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
-                    Ys[r * ldc + c] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
-                }
+        for (int u = 0; u < kRingGather; u++) {
+            const int e = e0 + u * nt;
+            if (e < ne) {
+                const bool s2 = e >= ne1;
+                const int el = s2 ? e - ne1 : e, nc = s2 ? N1 : N2;
+                const int r = el / nc, c = el - r * nc;
+                const int o = r * (nc + 4) + c;
+                (s2 ? X2 : X1)[o] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
+                (s2 ? Y2 : Y1)[o] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
             }
         }
     }
     // W[b][a] and the direct kernels Vs1, Vs2 (shared-memory table lookups)
-    for (int e = tid; e < N2 * N1; e += kRingThreads) {
+    for (int e = tid; e < N2 * N1; e += nt) {
         const int b = e / N1, a = e - b * N1;
         double w = 0.0;
         if (b < n2 && a < n1) {
@@ -887,16 +885,16 @@ __global__ void __launch_bounds__(kRingThreads) k_rings(const RingPairDev *__res
         }
         W[b * l1 + a] = w;
     }
-    for (int e = tid; e < N1 * N1; e += kRingThreads) {
+    for (int e = tid; e < N1 * N1; e += nt) {
         const int a = e / N1, c = e - a * N1;
         Vs1[a * l1 + c] = (a < n1 && c < n1) ? V(q2_of(no[ri[c]], no[ri[a]])) : 0.0;
     }
-    for (int e = tid; e < N2 * N2; e += kRingThreads) {
+    for (int e = tid; e < N2 * N2; e += nt) {
         const int b = e / N2, c = e - b * N2;
         Vs2[b * l2 + c] = (b < n2 && c < n2) ? V(q2_of(no[ri[N1 + c]], no[ri[N1 + b]])) : 0.0;
     }
     __syncthreads();
-    for (int r = tid; r < R; r += kRingThreads) {
+    for (int r = tid; r < R; r += nt) {
         const bool g1 = r < N1;
         const double *xr = g1 ? X1 + r * l2 : X2 + (r - N1) * l1;
         const double *yr = g1 ? Y1 + r * l2 : Y2 + (r - N1) * l1;
@@ -1532,7 +1530,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         int off = 0;
         for (int c = 0; c < kRingClasses; c++) {
             if (d.nring[c] > 0)
-                k_rings<<<d.nring[c], kRingThreads, d.ring_smem[c], st>>>(
+                k_rings<<<d.nring[c], kRingClassThreads[c], d.ring_smem[c], st>>>(
                     d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, f.do_ring,
                     f.do_xring, d.g_rq, d.g_xq, d.active);
             off += d.nring[c];
