@@ -58,7 +58,8 @@ def _measured_peaks():
 HBM_PEAK, BF16_PEAK = _measured_peaks()
 # DRAM bytes of one launch per solve, from one ncu capture of an 8-twist batch
 # (dram__bytes_read.sum + dram__bytes_write.sum / 8); scaled by the solves of a launch.
-TRAFFIC_PER_SOLVE = {"k_ladder": 15.2e6 / 8, "k_rings": 36.1e6 / 8}
+TRAFFIC_PER_SOLVE = {"k_ladder": 15.3e6 / 8, "k_rings": (96.0e6 + 28.8e6) / 8, "k_update": (98.0e6 + 6.3e6) / 8,
+                     "k_mosaic_blk": 15.3e6 / 8}
 
 
 def twists(n: int, seed: int = SEED, rank: int = 0):
@@ -141,7 +142,8 @@ class ClockSampler:
 
 # ------------------------------------------------------------------- GPU arm
 def plan_stats(sysl):
-    """Per-solve sizes of the momentum-block plan: O, V, A, sum o v^2, sum o^2 v."""
+    """Per-solve sizes of the momentum-block plan: O, V, A, sum o v^2, sum o^2 v, and the
+    ring flops over the {Q, -Q} particle-hole group pairs."""
     from collections import defaultdict
 
     import numpy as np
@@ -158,27 +160,37 @@ def plan_stats(sysl):
             if blocks[K][1] is None:
                 blocks[K][1] = sum(1 for a in range(O, M) if idx.get(tuple(np.array(K) - nv[a]), -1) >= O)
     ov = [(o, v) for o, v in blocks.values() if v > 0]
+    groups = defaultdict(int)
+    for i in range(O):
+        for x in range(O, M):
+            groups[tuple(nv[x] - nv[i])] += 1
+    ring = 0
+    for Q, n1 in groups.items():
+        mq = tuple(-q for q in Q)
+        if Q < mq and mq in groups:
+            n2 = groups[mq]
+            ring += 14 * n1 * n2 * (n1 + n2)
     return {"O": O, "V": M - O, "A": sum(o * v for o, v in ov), "ov2": sum(o * v * v for o, v in ov),
-            "o2v": sum(o * o * v for o, v in ov)}
+            "o2v": sum(o * o * v for o, v in ov), "ring_flop": ring}
 
 
 def kernel_units(st):
     """Algorithmic work of one launch per solve: ('flop', F) or ('byte', B)."""
-    O, V, A = st["O"], st["V"], st["A"]
-    ph = O * V * O
+    A = st["A"]
+    ndiis = SOLVE_OPTS["ndiis"]
     return {
         "k_ladder": ("flop", 2 * (st["ov2"] + st["o2v"])),
         "k_ladder_hh": ("flop", 2 * st["o2v"]),
         # pp ladder on the tensor cores (FP16 operands)
         "k_ladder_tc": ("tflop16", 2 * st["ov2"]),
-        # X W, Y W per ph row (2 O^2 each) and 7 O-long dots per pair of rows (one per amplitude)
-        "k_rings": ("flop", 2 * (2 * O * O * O * V + 7 * O * A)),
-        # reads t once, writes X, Y, Ex, Ey, A1, A2, A3 rows and Sx, Sy
-        "k_ph_build": ("byte", 8 * A + 7 * 8 * ph + 2 * 8 * O * V),
-        # reads A1, A2, A3, X, Y rows once, writes the two products per amplitude
-        "k_ring_quad": ("byte", 5 * 8 * ph + 2 * 8 * A),
-        # reads t, ladder G, the two ring products, writes t'
-        "k_update": ("byte", 5 * 8 * A),
+        # per {Q, -Q} group pair (n1, n2 rows): X W, Y W of both groups, 4 n1 n2 (n1 + n2), and
+        # the ring and crossed-ring products of both directions, 10 n1 n2 (n1 + n2)
+        "k_rings": ("flop", st["ring_flop"]),
+        # reads t once (s is formed in registers; the partial sums are small)
+        "k_mosaic_blk": ("byte", 8 * A),
+        # reads t, the ladder G and the two ring G, writes t'; Pulay push: writes t', e to the
+        # history and reads the other ndiis - 1 error vectors
+        "k_update": ("byte", (5 + 2 + (ndiis - 1)) * 8 * A),
     }
 
 
