@@ -202,8 +202,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int> chunk_begin(n + 1, 0);
     std::vector<int2> targets;
     std::vector<int16_t> pair_i, pair_j, vir;
-    std::vector<int32_t> pos, partner;
-    std::vector<AmpInfo> amps;
+    std::vector<int16_t> pcol;   // beside vir: the partner's column in the same block
     std::vector<int4> nv4;
     std::vector<double> eigen, vtab;
     std::vector<int64_t> hh0;
@@ -213,7 +212,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int> s_t0(n);   // first mosaic target of each solve
     int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_v = 0, max_occ = 0;
     // offsets of each solve in the large concatenated arrays (filled in parallel below)
-    std::vector<int64_t> s_amp0(n), s_pos0(n), s_phr0(n);
+    std::vector<int64_t> s_phr0(n);
     for (int s = 0; s < n; s++) {
         const SolvePlan &P = b->plans[s];
         const SystemHost &H = b->sys[s];
@@ -234,8 +233,6 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         S.denom_factor = 2.0;
         S.phr0 = phr0;
         max_occ = std::max(max_occ, P.O);
-        s_amp0[s] = amp0;
-        s_pos0[s] = pos0;
         s_phr0[s] = phr0;
         for (size_t gi = 0; gi < P.groups.size(); gi++) {
             const auto &G = P.groups[gi];
@@ -274,6 +271,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         pair_i.insert(pair_i.end(), P.pair_i.begin(), P.pair_i.end());
         pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
         vir.insert(vir.end(), P.vir.begin(), P.vir.end());
+        pcol.insert(pcol.end(), P.pcol.begin(), P.pcol.end());
         for (int p = 0; p < P.M; p++) nv4.push_back(make_int4(H.n[p][0], H.n[p][1], H.n[p][2], 0));
         eigen.insert(eigen.end(), H.eigen.begin(), H.eigen.end());
         vtab.insert(vtab.end(), P.vtab.begin(), P.vtab.end());
@@ -293,33 +291,12 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         if (amp0 >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit packed indices");
     }
     chunk_begin[n] = (int)chunks.size();
-    pos.resize(pos0);
-    amps.resize(amp0);
-    partner.resize(amp0);
     ph_i.resize(phr0);
     ph_x.resize(phr0);
-    // per ph row (i, x) and occupied k: packed index of t(ik, x) and of t(ki, x)
-    std::vector<int32_t> ridx_x(ph0), ridx_y(ph0);
     parallel_for(n, nthreads, [&](int s) {
         const SolvePlan &P = b->plans[s];
-        const int64_t a0 = s_amp0[s];
-        int32_t *pdst = pos.data() + s_pos0[s];
-        for (size_t k = 0; k < P.pos.size(); k++) pdst[k] = P.pos[k] >= 0 ? (int32_t)(P.pos[k] + a0) : -1;
-        for (size_t k = 0; k < P.amps.size(); k++) {
-            const AmpInfo &q = P.amps[k];
-            amps[a0 + k] = q;
-            partner[a0 + k] = (int32_t)(P.pos[((size_t)q.i * P.O + q.j) * P.V + (q.b - P.O)] + a0);
-        }
         std::copy(P.ph_i.begin(), P.ph_i.end(), ph_i.begin() + s_phr0[s]);
         std::copy(P.ph_x.begin(), P.ph_x.end(), ph_x.begin() + s_phr0[s]);
-        const int64_t h0 = solves[s].ph0;
-        for (int64_t r = 0; r < (int64_t)P.ph_i.size(); r++) {
-            const int i = P.ph_i[r], x = P.ph_x[r];
-            for (int k = 0; k < P.O; k++) {
-                ridx_x[h0 + r * P.O + k] = pdst[((size_t)i * P.O + k) * P.V + (x - P.O)];
-                ridx_y[h0 + r * P.O + k] = pdst[((size_t)k * P.O + i) * P.V + (x - P.O)];
-            }
-        }
     });
 
     // mosaic targets: Jvv(c) adds the column sums of c over the blocks holding it, Joo(k)
@@ -335,15 +312,12 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     });
     for (size_t k = 0; k + 1 < mt_start.size(); k++) mt_start[k + 1] += mt_start[k];
     std::vector<int32_t> mt_list(mt_start.back());
-    std::vector<int16_t> pcol(vir.size());
     parallel_for(n, nthreads, [&](int s) {
         const SolvePlan &P = b->plans[s];
         std::vector<int> fill(P.V + P.O, 0);
         for (size_t bi = 0; bi < P.blocks.size(); bi++) {
             const auto &B = P.blocks[bi];
             const BlockDev &bd = blocks[solves[s].blk0 + bi];
-            // partner column from row 0: the same for every row of the block
-            for (int c = 0; c < B.v; c++) pcol[bd.vir0 + c] = (int16_t)(partner[bd.t0 + c] - bd.t0);
             for (int c = 0; c < B.v; c++) {
                 const int y = P.vir[B.vir0 + c] - P.O;
                 mt_list[mt_start[s_t0[s] + y] + fill[y]++] = (int32_t)(bd.col0 + c);
@@ -423,9 +397,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.pair_i, pair_i))) return rc;
     if ((rc = b->upload(d.pair_j, pair_j))) return rc;
     if ((rc = b->upload(d.vir, vir))) return rc;
-    if ((rc = b->upload(d.pos, pos))) return rc;
-    if ((rc = b->upload(d.partner, partner))) return rc;
-    if ((rc = b->upload(d.amps, amps))) return rc;
+    if ((rc = b->alloc(d.pos, pos0))) return rc;
+    if ((rc = b->alloc(d.partner, amp0))) return rc;
+    if ((rc = b->alloc(d.amps, amp0))) return rc;
     if ((rc = b->upload(d.nv4, nv4))) return rc;
     if ((rc = b->upload(d.eigen, eigen))) return rc;
     if ((rc = b->upload(d.vtab, vtab))) return rc;
@@ -433,8 +407,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.rpairs, rpairs))) return rc;
     if ((rc = b->upload(d.ph_i, ph_i))) return rc;
     if ((rc = b->upload(d.ph_x, ph_x))) return rc;
-    if ((rc = b->upload(d.ridx_x, ridx_x))) return rc;
-    if ((rc = b->upload(d.ridx_y, ridx_y))) return rc;
+    if ((rc = b->alloc(d.ridx_x, ph0))) return rc;
+    if ((rc = b->alloc(d.ridx_y, ph0))) return rc;
     if ((rc = b->alloc(d.vcoef, amp0))) return rc;
     if ((rc = b->alloc(d.g_rq, amp0))) return rc;
     if ((rc = b->alloc(d.g_xq, amp0))) return rc;
@@ -457,6 +431,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     b->red.assign(3 * (size_t)n, 0.0);
     b->active.assign(n, 1);
     CU(cudaMemcpyAsync(d.active, b->active.data(), n, cudaMemcpyHostToDevice, b->stream));
+    // position map, amplitude list, partners and ring gather indices, from the blocks
+    CU(cudaMemsetAsync(d.pos, 0xff, (size_t)pos0 * sizeof(int32_t), b->stream));   // -1: not allowed
+    launch_block_tables(d, b->stream);
     launch_vcoef(d, b->stream);
     size_t dn = 0;
     for (int s = 0; s < n; s++) dn = std::max(dn, (size_t)b->plans[s].O * b->plans[s].O * b->plans[s].V);

@@ -157,6 +157,8 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
                     KernelTimer *kt = nullptr, const CtlBuffers *diis = nullptr, int ndiis = 0);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
 void launch_vcoef(const DevBatch &d, cudaStream_t st);
+// pos (pre-set to -1), amps, partner, then the ring gather indices, from the block structure
+void launch_block_tables(const DevBatch &d, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)
 void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st);
 // Refresh point: t_ref <- t and g_ref <- FP64 particle-particle ladder of t_ref

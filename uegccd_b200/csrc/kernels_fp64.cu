@@ -1084,6 +1084,54 @@ struct UpdateArgs {
     const double2 *vcoef;     // per amplitude {v(i-a), v(a-j)}
 };
 
+// One CTA per momentum block: for every element (pair r = (i, j), column c = a) the
+// amplitude record (i, j, a, b), the position map entry (i, j, a) -> packed index and
+// the packed index of the partner (i, j, b), b in column pcol[c] of the same block.
+__global__ void k_block_tables(const BlockDev *__restrict__ blocks, const SolveDev *__restrict__ solves,
+                               const int16_t *__restrict__ pair_i, const int16_t *__restrict__ pair_j,
+                               const int16_t *__restrict__ vir, const int16_t *__restrict__ pcol,
+                               AmpInfo *__restrict__ amps, int32_t *__restrict__ pos, int32_t *__restrict__ partner)
+{
+    const BlockDev B = blocks[blockIdx.x];
+    const SolveDev s = solves[B.solve];
+    const int n = B.o * B.v;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int r = e / B.v, c = e - r * B.v;
+        const int i = pair_i[B.pair0 + r], j = pair_j[B.pair0 + r];
+        const int a = vir[B.vir0 + c], pc = pcol[B.vir0 + c];
+        const int64_t p = B.t0 + e;
+        amps[p] = AmpInfo{(int16_t)i, (int16_t)j, (int16_t)a, vir[B.vir0 + pc]};
+        pos[s.pos0 + ((int64_t)i * s.O + j) * s.V + (a - s.O)] = (int32_t)p;
+        partner[p] = (int32_t)(B.t0 + (int64_t)r * B.v + pc);
+    }
+}
+
+// Ring gather indices per ph row (i, x) and occupied k: t(ik, x) and t(ki, x).
+__global__ void k_ring_index(const ChunkDev *__restrict__ rchunks, const SolveDev *__restrict__ solves,
+                             const int16_t *__restrict__ ph_i, const int16_t *__restrict__ ph_x,
+                             const int32_t *__restrict__ pos, int32_t *__restrict__ ridx_x,
+                             int32_t *__restrict__ ridx_y)
+{
+    const ChunkDev ch = rchunks[blockIdx.x];
+    const SolveDev s = solves[ch.solve];
+    const int e = ch.start + threadIdx.x;
+    if (e >= s.O * s.V * s.O) return;
+    const int r = e / s.O, k = e - r * s.O;
+    const int i = ph_i[s.phr0 + r], x = ph_x[s.phr0 + r];
+    ridx_x[s.ph0 + e] = posmap(s, pos, i, k, x);
+    ridx_y[s.ph0 + e] = posmap(s, pos, k, i, x);
+}
+
+void launch_block_tables(const DevBatch &d, cudaStream_t st)
+{
+    if (d.nblocks > 0)
+        k_block_tables<<<d.nblocks, 256, 0, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir, d.pcol, d.amps,
+                                                  d.pos, d.partner);
+    if (d.nrchunks > 0)
+        k_ring_index<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.ph_i, d.ph_x, d.pos, d.ridx_x,
+                                                    d.ridx_y);
+}
+
 // Static per-amplitude Coulomb factors of the update: {v(i-a), v(a-j)}.
 __global__ void k_vcoef(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
                         const AmpInfo *__restrict__ amps, const int4 *__restrict__ nv4,

@@ -98,20 +98,10 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
             }
             kpairs[id].emplace_back(i, j);
         }
-    p.pos.assign((size_t)O * O * V, -1);
-    {
-        size_t est = 0;  // exact count of allowed amplitudes, to size the arrays once
-        for (size_t k = 0; k < kpairs.size(); k++) {
-            const auto &K = kvecs[k];
-            size_t nc = 0;
-            for (int a = O; a < M; a++)
-                if (orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]) >= O) nc++;
-            est += nc * kpairs[k].size();
-        }
-        p.amps.reserve(est);
-    }
+    // the position map, amplitude list and partner indices are built on the device from
+    // the blocks (k_block_tables); the host keeps only the block structure
     int64_t t0 = 0;
-    std::vector<int> cols, partner_of_col;
+    std::vector<int> cols, partner_of_col, col_of(M, -1);
     for (size_t k = 0; k < kpairs.size(); k++) {
         // virtual columns of block K: a virtual whose partner b = K - a is a virtual
         cols.clear();
@@ -136,15 +126,9 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
             p.pair_j.push_back((int16_t)pr.second);
         }
         for (int a : cols) p.vir.push_back((int16_t)a);
-        for (int r = 0; r < blk.o; r++) {
-            int i = kpairs[k][r].first, j = kpairs[k][r].second;
-            int32_t *prow = &p.pos[((size_t)i * O + j) * V];
-            for (int c = 0; c < blk.v; c++) {
-                int a = cols[c];
-                prow[a - O] = (int32_t)(t0 + (int64_t)r * blk.v + c);
-                p.amps.push_back(AmpInfo{(int16_t)i, (int16_t)j, (int16_t)a, (int16_t)partner_of_col[c]});
-            }
-        }
+        for (int c = 0; c < blk.v; c++) col_of[cols[c]] = c;
+        for (int c = 0; c < blk.v; c++) p.pcol.push_back((int16_t)col_of[partner_of_col[c]]);
+        for (int c = 0; c < blk.v; c++) col_of[cols[c]] = -1;
         t0 += (int64_t)blk.o * blk.v;
         p.blocks.push_back(blk);
     }
@@ -184,7 +168,6 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
     }
     p.ph_i.assign((size_t)O * V, 0);
     p.ph_x.assign((size_t)O * V, 0);
-    p.phrow_of.assign((size_t)O * V, -1);
     std::vector<int> fill(qvecs.size(), 0);
     for (int i = 0; i < O; i++)
         for (int x = O; x < M; x++) {
@@ -192,7 +175,6 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
             int r = gstart[id] + fill[id]++;
             p.ph_i[r] = (int16_t)i;
             p.ph_x[r] = (int16_t)x;
-            p.phrow_of[(size_t)i * V + (x - O)] = r;
         }
     for (size_t g = 0; g < qvecs.size(); g++) {
         int m = qid.get(-qvecs[g][0], -qvecs[g][1], -qvecs[g][2]);

@@ -26,13 +26,11 @@ struct SolvePlan {
     std::vector<Block> blocks;
     std::vector<int16_t> pair_i, pair_j;    // concatenated pair lists
     std::vector<int16_t> vir;               // concatenated virtual lists (absolute orbital index)
-    std::vector<int32_t> pos;               // (i*O + j)*V + (a-O) -> packed index or -1
-    std::vector<AmpInfo> amps;              // packed index -> (i,j,a,b)
+    std::vector<int16_t> pcol;              // beside vir: column of the partner b = K - a in the same block
     int64_t namp = 0;
     int64_t ring_entries = 0;               // O*V*O
     // particle-hole rows (i,x), x virtual, sorted by Q = n_x - n_i
     std::vector<int16_t> ph_i, ph_x;        // row -> (i, x)
-    std::vector<int32_t> phrow_of;          // i*V + (x-O) -> row
     struct PhGroup { int r0, n, partner; }; // partner: index of the -Q group or -1
     std::vector<PhGroup> groups;
 };
