@@ -263,7 +263,7 @@ def run_gpu(args, rank, world):
         t0 = time.perf_counter()
         b2 = Batch(systems)
         rc2, e2b, res2 = b2.solve(**opts)
-        amps = [b2.amplitudes(s) for s in range(b2.n)]
+        amps = b2.all_amplitudes()
         hb, db = b2.transfer_bytes()
         b2.close()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)

@@ -155,6 +155,15 @@ int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
  * any stream capture begins on the device. */
 int uegccd_mp2_energy_static(const UegccdSystem *sys, void *stream, double *e2);
 
+/* T2abab of every solve of the batch in the reference layout, solve after solve: solve s
+ * fills NOcc_s * NOcc_s * (NAO_s - NOcc_s) doubles (the batched form of
+ * uegccd_batch_get_amplitudes: one device-to-host copy for the whole batch). */
+int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab);
+/* A destroyed batch leaves its device memory in a small per-process cache (at most
+ * 8 GiB) that the next batch reuses, and large amplitude downloads keep a pinned host
+ * staging buffer; this returns both to the driver. */
+int uegccd_trim_cache(void);
+
 /* Solve s's per-iteration energies and biggest changes from the last batch solve (the
  * rows of the reference's iteration table, CCD.f90:76,96 / dRPA.f90:77,92): copies at
  * most max_rec of each (either pointer may be NULL) and sets *n_recorded. */

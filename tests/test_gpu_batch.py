@@ -78,3 +78,26 @@ def test_batch_drpa_equals_alone(goldens):
         e2a, ta, tb, tc = ctx.mp2()
         rca, ra, en, _ = ctx.drpa(ta.copy(), do_mosaic=0)
         assert abs(res[s]["ecorr"] - ra["ecorr"]) < 1e-12
+
+
+def test_all_amplitudes_and_reused_memory(goldens):
+    """The batch-wide download equals the per-solve one, and a batch built on device
+    memory that a destroyed batch left in the cache gives bitwise the same solves."""
+    from uegccd_b200 import Batch, _capi
+
+    systems = [_tuple(o) for o in _systems(goldens)]
+    runs = []
+    for rep in range(3):
+        b = Batch(systems)
+        rc, e2, res = b.solve(max_iter=6)
+        allt = b.all_amplitudes()
+        for s in range(b.n):
+            np.testing.assert_array_equal(allt[s], b.amplitudes(s))
+        runs.append(([r["ecorr"] for r in res], [a.copy() for a in allt]))
+        b.close()
+        if rep == 1:
+            _capi.lib().uegccd_trim_cache()
+    for e, amps in runs[1:]:
+        assert e == runs[0][0]
+        for a, c in zip(amps, runs[0][1]):
+            np.testing.assert_array_equal(a, c)

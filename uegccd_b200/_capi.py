@@ -88,6 +88,7 @@ def lib() -> C.CDLL:
         L.uegccd_batch_destroy.argtypes = [vp]
         L.uegccd_batch_solve.argtypes = [vp, P(Options), C.c_int32, dp, P(Result)]
         L.uegccd_batch_get_amplitudes.argtypes = [vp, C.c_int32, dp]
+        L.uegccd_batch_get_all_amplitudes.argtypes = [vp, dp]
         L.uegccd_batch_set_profiling.argtypes = [vp, C.c_int32]
         L.uegccd_batch_kernel_stats.argtypes = [vp, C.c_int32, P(C.c_char_p), dp, P(C.c_int64)]
         L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]

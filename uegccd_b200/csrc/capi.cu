@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -65,10 +66,14 @@ int check_device()
         return fail(UEGCCD_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
     int dev = 0;
     CU(cudaGetDevice(&dev));
-    cudaDeviceProp p;
-    CU(cudaGetDeviceProperties(&p, dev));
-    if (p.major != 10)
+    // one attribute query (cudaGetDeviceProperties reads every property: tens of ms per call)
+    int major = 0;
+    CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) {
+        cudaDeviceProp p;
+        CU(cudaGetDeviceProperties(&p, dev));
         return fail(UEGCCD_ERR_CUDA, std::string("the library is built for sm_100a (B200); device is ") + p.name);
+    }
     return 0;
 }
 
@@ -77,19 +82,97 @@ int check_device()
 // ----------------------------------------------------------------------------
 // Batch: plans + device buffers of n systems
 // ----------------------------------------------------------------------------
+// Device memory of a batch: carved from chunks of at least kArenaChunk bytes. Chunks
+// freed by a destroyed batch are kept in a small per-process cache (up to kPoolCap
+// bytes) for the next batch; uegccd_trim_cache returns them to the driver.
+namespace {
+constexpr size_t kArenaChunk = 64ull << 20;
+constexpr size_t kPoolCap = 8ull << 30;
+struct DevChunk {
+    char *p;
+    size_t size;
+    int dev;
+};
+// pinned staging buffer of the batch-wide amplitude download (grown on demand, kept)
+constexpr size_t kStageMin = 8ull << 20;
+std::mutex g_stage_mu;
+char *g_stage = nullptr;
+size_t g_stage_bytes = 0;
+std::mutex g_pool_mu;
+std::vector<DevChunk> g_pool;
+size_t g_pool_bytes = 0;
+
+cudaError_t chunk_get(size_t need, int dev, DevChunk &out)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        int best = -1;
+        for (size_t k = 0; k < g_pool.size(); k++)
+            if (g_pool[k].dev == dev && g_pool[k].size >= need && g_pool[k].size <= 2 * need + kArenaChunk &&
+                (best < 0 || g_pool[k].size < g_pool[best].size))
+                best = (int)k;
+        if (best >= 0) {
+            out = g_pool[best];
+            g_pool_bytes -= out.size;
+            g_pool.erase(g_pool.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+        // give the cache of this device back to the driver and try once more
+        cudaGetLastError();
+        std::vector<DevChunk> drop;
+        {
+            std::lock_guard<std::mutex> lock(g_pool_mu);
+            for (size_t k = 0; k < g_pool.size();)
+                if (g_pool[k].dev == dev) {
+                    drop.push_back(g_pool[k]);
+                    g_pool_bytes -= g_pool[k].size;
+                    g_pool.erase(g_pool.begin() + k);
+                } else {
+                    k++;
+                }
+        }
+        for (auto &c : drop) cudaFree(c.p);
+        e = cudaMalloc(&p, need);
+    }
+    if (e == cudaSuccess) out = DevChunk{(char *)p, need, dev};
+    return e;
+}
+
+void chunk_put(const DevChunk &c)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (g_pool_bytes + c.size <= kPoolCap) {
+            g_pool.push_back(c);
+            g_pool_bytes += c.size;
+            return;
+        }
+    }
+    cudaFree(c.p);
+}
+}  // namespace
+
 struct UegccdBatch {
     std::vector<SystemHost> sys;
     std::vector<SolvePlan> plans;
     std::vector<SolveDev> hsolves;
     std::vector<int> chunk_begin;
     DevBatch d;
-    std::vector<void *> allocs;
+    std::vector<DevChunk> chunks;    // device memory of the batch (see chunk_get)
+    size_t chunk_used = 0;           // bytes used in the last chunk
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_solve0 = nullptr, ev_solve1 = nullptr;
     std::vector<double> red;         // host copy: 3 per solve
     std::vector<uint8_t> active;     // host copy
     double *dense[3] = {nullptr, nullptr, nullptr};  // reference-layout scratch of the largest solve
     size_t dense_n = 0;
+    double *dense_all = nullptr;     // reference layout of every solve, back to back (on first use)
+    int64_t *dense_off = nullptr;
+    size_t dense_all_n = 0;
     int launches = 0;
     int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the calls so far
     KernelTimer kt;
@@ -118,7 +201,8 @@ struct UegccdBatch {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (kt_events)
             for (auto &e : kt.ev) cudaEventDestroy(e);
-        for (void *p : allocs) cudaFree(p);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto &c : chunks) chunk_put(c);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev_solve0) cudaEventDestroy(ev_solve0);
@@ -131,9 +215,18 @@ struct UegccdBatch {
     {
         p = nullptr;
         if (n == 0) n = 1;
-        cudaError_t e = cudaMalloc((void **)&p, n * sizeof(T));
-        if (e != cudaSuccess) return fail(UEGCCD_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        allocs.push_back(p);
+        const size_t bytes = (n * sizeof(T) + 255) & ~(size_t)255;
+        if (chunks.empty() || chunk_used + bytes > chunks.back().size) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            DevChunk c;
+            cudaError_t e = chunk_get(std::max(bytes, kArenaChunk), dev, c);
+            if (e != cudaSuccess) return fail(UEGCCD_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            chunks.push_back(c);
+            chunk_used = 0;
+        }
+        p = reinterpret_cast<T *>(chunks.back().p + chunk_used);
+        chunk_used += bytes;
         return 0;
     }
     template <class T>
@@ -357,7 +450,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.namp = amp0;
     // ring pairs by kernel class: k_rings (two shared-memory sizes), then k_rings_wide
     {
-        auto cls = [&](const RingPairDev &r) {
+        auto cls_of = [&](const RingPairDev &r) {
             const size_t b = rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max);
             if (b > kRingSmemMax) return kRingClasses;
             const int rows = ((r.n1 + 7) & ~7) + ((r.n2 + 7) & ~7);
@@ -365,10 +458,16 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
                 if (rows <= kRingClassRows[c]) return c;
             return kRingClasses;
         };
-        std::stable_sort(rpairs.begin(), rpairs.end(),
-                         [&](const RingPairDev &x, const RingPairDev &y) { return cls(x) < cls(y); });
+        // stable counting sort by class
+        std::vector<int> cls(rpairs.size());
+        std::vector<size_t> start(kRingClasses + 2, 0);
+        for (size_t k = 0; k < rpairs.size(); k++) start[(cls[k] = cls_of(rpairs[k])) + 1]++;
+        for (int c = 0; c <= kRingClasses; c++) start[c + 1] += start[c];
+        std::vector<RingPairDev> sorted(rpairs.size());
+        for (size_t k = 0; k < rpairs.size(); k++) sorted[start[cls[k]]++] = rpairs[k];
+        rpairs.swap(sorted);
         for (const auto &r : rpairs) {
-            const int c = cls(r);
+            const int c = cls_of(r);
             d.nring[c]++;
             const size_t b = c < kRingClasses
                                  ? rings_dmma_smem_bytes(solves[r.solve].O, r.n1, r.n2, solves[r.solve].q2max)
@@ -960,6 +1059,68 @@ int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab)
 {
     if (!b || !t_abab || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
     return unpack_to_host(*b, s, b->d.t, t_abab, nullptr, nullptr);
+}
+
+int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab)
+{
+    if (!b || !t_abab) return fail(UEGCCD_ERR_ARG, "bad argument");
+    const int n = b->d.nsolves;
+    if (!b->dense_all) {
+        std::vector<int64_t> off(n + 1, 0);
+        for (int s = 0; s < n; s++) off[s + 1] = off[s] + (int64_t)b->plans[s].O * b->plans[s].O * b->plans[s].V;
+        int rc = b->upload(b->dense_off, off);
+        if (rc) return rc;
+        if ((rc = b->alloc(b->dense_all, (size_t)off[n]))) return rc;
+        b->dense_all_n = (size_t)off[n];
+    }
+    CU(cudaMemsetAsync(b->dense_all, 0, b->dense_all_n * sizeof(double), b->stream));
+    launch_unpack_all(b->d, b->dense_off, b->d.t, b->dense_all, b->stream);
+    b->launches++;
+    CU(cudaGetLastError());
+    const size_t bytes = b->dense_all_n * sizeof(double);
+    b->d2h_bytes += (int64_t)bytes;
+    if (bytes < kStageMin) {
+        CU(cudaMemcpyAsync(t_abab, b->dense_all, bytes, cudaMemcpyDeviceToHost, b->stream));
+        CU(cudaStreamSynchronize(b->stream));
+        return UEGCCD_OK;
+    }
+    // large downloads: through a cached pinned buffer, copied out on all host cores
+    // (a pageable copy is staged by the driver on one thread)
+    std::lock_guard<std::mutex> lock(g_stage_mu);
+    if (g_stage_bytes < bytes) {
+        if (g_stage) cudaFreeHost(g_stage);
+        g_stage = nullptr;
+        g_stage_bytes = 0;
+        CU(cudaHostAlloc((void **)&g_stage, bytes, cudaHostAllocDefault));
+        g_stage_bytes = bytes;
+    }
+    CU(cudaMemcpyAsync(g_stage, b->dense_all, bytes, cudaMemcpyDeviceToHost, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    const size_t piece = (bytes + nth - 1) / nth;
+    parallel_for(nth, nth, [&](int k) {
+        const size_t a = (size_t)k * piece, e = std::min(bytes, a + piece);
+        if (a < e) std::memcpy((char *)t_abab + a, g_stage + a, e - a);
+    });
+    return UEGCCD_OK;
+}
+
+int uegccd_trim_cache(void)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_stage_mu);
+        if (g_stage) cudaFreeHost(g_stage);
+        g_stage = nullptr;
+        g_stage_bytes = 0;
+    }
+    std::vector<DevChunk> drop;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        drop.swap(g_pool);
+        g_pool_bytes = 0;
+    }
+    for (auto &c : drop) cudaFree(c.p);
+    return UEGCCD_OK;
 }
 
 int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dts, int32_t max_rec,

@@ -157,6 +157,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
                     KernelTimer *kt = nullptr, const CtlBuffers *diis = nullptr, int ndiis = 0);
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
 void launch_vcoef(const DevBatch &d, cudaStream_t st);
+void launch_unpack_all(const DevBatch &d, const int64_t *dense_off, const double *t, double *out, cudaStream_t st);
 // pos (pre-set to -1), amps, partner, then the ring gather indices, from the block structure
 void launch_block_tables(const DevBatch &d, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)

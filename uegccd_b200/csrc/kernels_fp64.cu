@@ -1496,6 +1496,25 @@ __global__ void k_unpack(const SolveDev *__restrict__ solves, int sidx, const Am
     if (d_aaaa) d_aaaa[x] = ta + (-tb);
 }
 
+// T2abab of every solve in the reference layout, solve after solve (dense_off[s]).
+__global__ void k_unpack_all(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                             const int64_t *__restrict__ dense_off, const AmpInfo *__restrict__ amps,
+                             const double *__restrict__ t, double *__restrict__ out)
+{
+    const ChunkDev ch = chunks[blockIdx.x];
+    const SolveDev s = solves[ch.solve];
+    const int loc = ch.start + threadIdx.x;
+    if (loc >= s.namp) return;
+    const int64_t p = s.amp0 + loc;
+    const AmpInfo q = amps[p];
+    out[dense_off[ch.solve] + q.i + (int64_t)s.O * q.j + (int64_t)s.O * s.O * (q.a - s.O)] = t[p];
+}
+
+void launch_unpack_all(const DevBatch &d, const int64_t *dense_off, const double *t, double *out, cudaStream_t st)
+{
+    k_unpack_all<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, dense_off, d.amps, t, out);
+}
+
 // ----------------------------------------------------------------------------
 // Launch wrappers
 // ----------------------------------------------------------------------------

@@ -136,3 +136,14 @@ class Batch:
         t = np.zeros(self._shapes[s])
         capi.check(capi.lib().uegccd_batch_get_amplitudes(self._h, s, capi.dptr(t)))
         return t
+
+    def all_amplitudes(self) -> list:
+        """T2abab of every solve (views into one host buffer, one device-to-host copy)."""
+        sizes = [int(np.prod(sh)) for sh in self._shapes]
+        buf = np.empty(sum(sizes))
+        capi.check(capi.lib().uegccd_batch_get_all_amplitudes(self._h, capi.dptr(buf)))
+        out, off = [], 0
+        for sh, n in zip(self._shapes, sizes):
+            out.append(buf[off:off + n].reshape(sh))
+            off += n
+        return out
