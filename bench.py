@@ -188,9 +188,9 @@ def kernel_units(st):
         "k_rings": ("flop", st["ring_flop"]),
         # reads t once (s is formed in registers; the partial sums are small)
         "k_mosaic_blk": ("byte", 8 * A),
-        # reads t, the ladder G and the two ring G, writes t'; Pulay push: writes t', e to the
-        # history and reads the other ndiis - 1 error vectors
-        "k_update": ("byte", (5 + 2 + (ndiis - 1)) * 8 * A),
+        # reads t, the ladder G and the two ring G; Pulay push: writes t' (FP64) and e (FP32)
+        # to the history and reads the other ndiis - 1 error vectors (FP32)
+        "k_update": ("byte", (4 * 8 + 8 + 4 + (ndiis - 1) * 4) * A),
     }
 
 

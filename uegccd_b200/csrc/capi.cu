@@ -1039,7 +1039,7 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     b += O * V * 2 * 2;                              // ph rows
     b += O * V * O * 4 * 2;                          // ring gather indices
     b += hh * 8 + nblk * (sizeof(BlockDev) + 8) + M * (16 + 8) + (P.q2max + 1) * 8;
-    b += A * 8 * 2 * (int64_t)std::max(0, (int)ndiis);  // DIIS history
+    b += A * (8 + 4) * (int64_t)std::max(0, (int)ndiis);  // DIIS history (t' FP64, e FP32)
     if (mixed) b += A * 8 * 2;                       // t_ref, g_ref
     b += (int64_t)O * O * V * 8 * 3;                 // reference-layout staging (one solve)
     *bytes = b;

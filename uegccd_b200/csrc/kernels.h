@@ -134,7 +134,8 @@ struct CtlBuffers {
     uint8_t *active_next = nullptr;
     int *count = nullptr;
     double *Bm = nullptr, *coef = nullptr, *brow = nullptr, *part = nullptr;
-    double *hist_t = nullptr, *hist_e = nullptr;
+    double *hist_t = nullptr;   // DIIS history: updated amplitudes t' (FP64)
+    float *hist_e = nullptr;    // and error vectors e = t' - t (FP32: they only enter the B-matrix dots)
     double *rec_e = nullptr, *rec_dt = nullptr;
     int max_rec = 0;
 };

@@ -1080,7 +1080,8 @@ struct UpdateArgs {
     const IterState *st;
     int ndiis;
     int64_t namp;
-    double *hist_t, *hist_e, *dpart;
+    double *hist_t, *dpart;
+    float *hist_e;
     const double2 *vcoef;     // per amplitude {v(i-a), v(a-j)}
 };
 
@@ -1202,7 +1203,7 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
         if (A.mode == 0) {
             const double f = s.denom_factor;
             const double tn = (g / denom - (1.0 - f) * told) / f;
-            A.t_new[p] = tn;
+            if (A.ndiis == 0) A.t_new[p] = tn;  // with DIIS the history slot holds t'
             dtmax = fabs(tn - told);
             if (A.drpa) esum = via * tn * 2.0;  // SOSEX part added by k_drpa_energy at the end
             else esum = tn * (2.0 * via - vc.y);
@@ -1210,7 +1211,7 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
             if (A.ndiis > 0) {
                 const int slot = (A.st[ch.solve].niter - 1) % A.ndiis;
                 A.hist_t[(int64_t)slot * A.namp + p] = tn;
-                A.hist_e[(int64_t)slot * A.namp + p] = tn - told;
+                A.hist_e[(int64_t)slot * A.namp + p] = (float)(tn - told);
             }
         }
     }
@@ -1220,11 +1221,11 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
         const int slot = (nb - 1) % A.ndiis, nvec = min(nb, A.ndiis);
         const bool mine = loc < s.namp;
         const int64_t p = s.amp0 + loc;
-        const double e = mine ? A.hist_e[(int64_t)slot * A.namp + p] : 0.0;
+        const double e = mine ? (double)A.hist_e[(int64_t)slot * A.namp + p] : 0.0;
         __shared__ double sd[kChunk / 32][kDiisMax];
         const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
         for (int jv = 0; jv < nvec; jv++) {
-            double d = mine ? e * (jv == slot ? e : A.hist_e[(int64_t)jv * A.namp + p]) : 0.0;
+            double d = mine ? e * (jv == slot ? e : (double)A.hist_e[(int64_t)jv * A.namp + p]) : 0.0;
             for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
             if (l == 0) sd[w][jv] = d;
         }
