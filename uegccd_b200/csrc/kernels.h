@@ -83,7 +83,7 @@ constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* u
 
 // Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
 enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
-                KID_UPDATE, KID_REDUCE, KID_PACK, KID_PH_BUILD, KID_RING_QUAD, KID_RINGS, KID_LADDER_TC,
+                KID_UPDATE, KID_REDUCE, KID_RINGS, KID_LADDER_TC,
                 KID_COUNT };
 struct KernelTimer {
     bool on = false;

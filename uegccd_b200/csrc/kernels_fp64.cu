@@ -589,9 +589,9 @@ __global__ void k_ring_int(const ChunkDev *__restrict__ rchunks, const SolveDev 
 //   linear xrings  (CCD.f90:845-892): -Ey_ib[j] - Ey_ja[i]
 //   quadratic rings  (CCD.f90:801-808): A1_ia . X_jb - A2_ia . Y_jb
 //   quadratic xrings (CCD.f90:927-934): A3_ib . Y_ja
-// The quadratic products pair the rows of momentum Q with those of -Q, which is
-// what k_ring_quad does, group by group; every amplitude receives exactly one
-// ring and one crossed-ring product, so no atomics are needed.
+// The quadratic products pair the rows of momentum Q with those of -Q, group by
+// group; every amplitude receives exactly one ring and one crossed-ring product, so
+// no atomics are needed.
 // Row layout: row r (local) of solve s: scalars at s.phr0 + r, vectors at s.ph0 + r * O (O entries).
 // ----------------------------------------------------------------------------
 // ----------------------------------------------------------------------------
@@ -1543,7 +1543,7 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
 
 const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh", "k_ladder",
                                       "k_mosaic_blk", "k_mosaic_sum", "k_ring_int", "k_update",
-                                      "k_reduce_solves", "k_pack", "k_ph_build", "k_ring_quad", "k_rings",
+                                      "k_reduce_solves", "k_rings",
                                       "k_ladder_tc"};
 
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
