@@ -78,11 +78,15 @@ int uegccd_special_twist(int32_t ntwists, const int32_t *conn, double *conn_avg,
  * them: a blank, then 17 significant digits in a G25 field.  Returns its length. */
 int32_t uegccd_list_real(double x, char *buf, int32_t len);
 /* The whole program in the working directory: reads input_path (NULL: "Input"),
- * writes Output, fort.58 and fort.59.  twists_path (may be NULL) lists the twist
+ * writes Output, fort.58, fort.59 and fort.60.  twists_path (may be NULL) lists the twist
  * angles of the average, three numbers per line; missing ones are drawn from a
  * seeded U[-0.5,0.5)^3 stream.  scheme is UEGCCD_REPLAY or UEGCCD_DIIS.  The
  * solves run on the current CUDA device; every twist of the average is one batch. */
 int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme);
+/* The set-up part of the program alone, on the host (no GPU): the fort.60 log that
+ * uegccd_zcode writes (the reference's write(60,*) lines of HEG.f90 and Main.f90),
+ * into out_path (NULL: "fort.60"). */
+int uegccd_zcode_fort60(const char *input_path, const char *twists_path, const char *out_path);
 const char *uegccd_zcode_last_error(void);
 
 #ifdef __cplusplus

@@ -5,7 +5,7 @@ Run in a container that has the reference checkout (default path below, or
 relative to the reference checkout:
 
   G1  benchmarks/ZRun-dRPA/{Input,Output}       N=14, 57 plane waves, rs=1, dRPA+SOSEX
-  G5  source/Test/{Output,fort.59}              N=24, 34 orbitals, rs=5, twist (0.1,0.2,0.45), CCD;
+  G5  source/Test/{Output,fort.59,fort.60}      N=24, 34 orbitals, rs=5, twist (0.1,0.2,0.45), CCD;
                                                 10-twist MP2 average and the special-twist CCD
   G3  benchmarks/ZRun-v6-N14/{Input,fort.59,Output}  N=14, 19 plane waves, rs=1, 100 twists x CCD
 
@@ -107,6 +107,7 @@ def g5(ref):
                 max_res=maxres[0], ta_twists=[r[:3] for r in rows], ta_hf_mp2_ccd=[r[3:6] for r in rows],
                 special_twist=special, special_ec_ccd=ecs[-1], special_niter=conv[-1],
                 output_lines=lines, fort59_lines=f59,
+                fort60_lines=open(os.path.join(d, "fort.60")).read().splitlines(),
                 source="source/Test/Output, source/Test/fort.59")
 
 

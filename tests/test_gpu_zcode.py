@@ -58,6 +58,11 @@ def test_g5_output_and_fort59(goldens, tmp_path, monkeypatch):
     for a, b in zip(ours, ref):
         if "conn" in b or "special" in b or "lowest" in b or re.fullmatch(r"\s+\d+\s+\S+\s*", b):
             assert a == b
+    # fort.60: the set-up log, identical to the reference's up to its older 'om:' label
+    # and its trailing change_rs block (tests/test_zcode_host.py)
+    f60 = (tmp_path / "fort.60").read_text().splitlines()
+    ref60 = [l.replace(" om:", " Omega:", 1) if l.startswith(" om:") else l for l in g["fort60_lines"]]
+    assert len(f60) > 800 and f60 == ref60[: len(f60)]
 
 
 def test_g3_hundred_twists_ccd(goldens, tmp_path, monkeypatch):

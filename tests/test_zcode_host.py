@@ -123,3 +123,28 @@ def test_zcode_without_gpu_reports_error(goldens, tmp_path, monkeypatch):
     with pytest.raises(_capi.UegccdError):
         zcode.run("Input")
     assert not (tmp_path / "fort.59").exists()
+
+
+def test_fort60_log_matches_reference(goldens, tmp_path, monkeypatch):
+    """The set-up log (fort.60) of the G5 program against the reference's own file.
+
+    Every line is identical, with two differences. The reference's stored file is
+    from a build that labelled Omega as 'om:'; the current source (HEG.f90:606)
+    writes 'Omega:'. It also ends with one more change_rs block, which the current
+    Main.f90 has commented out (Main.f90:236-242)."""
+    import ctypes as C
+
+    g = goldens["G5"]
+    (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in g["keys"].items()))
+    (tmp_path / "Twists").write_text("".join("%.17g %.17g %.17g\n" % tuple(t) for t in g["ta_twists"]))
+    monkeypatch.chdir(tmp_path)
+    L = heg._lib()
+    L.uegccd_zcode_fort60.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p]
+    assert L.uegccd_zcode_fort60(b"Input", b"Twists", b"fort.60") == 0
+    ours = (tmp_path / "fort.60").read_text().splitlines()
+    ref = [l.replace(" om:", " Omega:", 1) if l.startswith(" om:") else l for l in g["fort60_lines"]]
+    assert len(ours) > 800
+    assert ours == ref[: len(ours)]
+    tail = ref[len(ours):]
+    assert tail[2].strip() == "Calculating Madelung Constant - Fraser et al. PRB 53 4 1814"
+    assert sum(1 for l in tail if l.startswith(" Omega:")) == 1

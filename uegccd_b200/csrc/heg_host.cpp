@@ -17,11 +17,22 @@
 
 #include "../../include/uegccd.h"
 #include "../../include/uegccd_host.h"
+#include "listdir.h"
 
 namespace {
 
 constexpr double kPi = 3.1415926535897932384626433833;  // Constants.f90:7
 thread_local std::string g_host_error;
+thread_local std::string *g_log = nullptr;   // fort.60 lines (set by the ZCode program)
+
+using uegccd::ld_int;
+using uegccd::ld_real;
+using uegccd::ld_str;
+
+void log_line(const std::string &l)
+{
+    if (g_log) *g_log += l + "\n";
+}
 
 int herr(int code, const std::string &m)
 {
@@ -60,30 +71,74 @@ int fcut_to_basis_fn(double fcut, int nel)
     return m;
 }
 
+// PrintShells (HEG.f90:44-87): cumulative plane-wave counts per |n|^2 < kc^2 (fort.60 only).
+void log_shells(int kc)
+{
+    if (!g_log) return;
+    std::vector<int> hist(kc * kc + 1, 0);
+    for (int l1 = -kc; l1 <= kc; l1++)
+        for (int l2 = -kc; l2 <= kc; l2++)
+            for (int l3 = -kc; l3 <= kc; l3++) {
+                const int e = l1 * l1 + l2 * l2 + l3 * l3;
+                if (e < kc * kc) hist[e]++;
+            }
+    log_line(ld_str(""));
+    log_line(ld_str("--------------------"));
+    log_line(ld_str("Basis sets available"));
+    log_line(ld_str("--------------------"));
+    log_line(ld_str("# ecut k-points M"));
+    int culm = 0;
+    for (int e = 0; e <= kc * kc; e++)
+        if (hist[e] != 0) {
+            culm += hist[e];
+            log_line(ld_int(e) + ld_int(culm) + ld_int(culm * 2));
+        }
+}
+
+// CalcMadelung (HEG.f90:89-148).  Each pass of the l4 loop restarts its sum, so the
+// result is the l4 = 10 pass; the earlier passes only feed the fort.60 log.
 double calc_madelung(double omega, double L)
 {
     double kappa = 2.8 / std::pow(omega, 1.0 / 3.0);
     double term2 = -kPi / (std::pow(kappa, 2.0) * std::pow(L, 3.0));
     double term4 = -2.0 * kappa / std::sqrt(kPi);
-    const int l4 = 10;  // only the last pass of the l4 loop survives its reset
+    if (g_log) {
+        log_line(ld_str(""));
+        log_line(ld_str("-----------------------------------------------------------"));
+        log_line(ld_str("Calculating Madelung Constant - Fraser et al. PRB 53 4 1814"));
+        log_line(ld_str("-----------------------------------------------------------"));
+        log_line(ld_str("kappa taken from CASINO manual to be") + ld_real(kappa));
+        log_line(ld_real(term2) + ld_str("term2"));
+        log_line(ld_real(term4) + ld_str("term4"));
+    }
     double recip = 0.0;
-    for (int l1 = -l4; l1 <= l4; l1++)
-        for (int l2 = -l4; l2 <= l4; l2++)
-            for (int l3 = -l4; l3 <= l4; l3++) {
-                int n2 = l1 * l1 + l2 * l2 + l3 * l3;
-                if (n2 == 0) continue;
-                double k2 = (1.0 / std::pow(L, 2.0)) * (double)n2;
-                double ek2 = (1.0 / std::pow(L, 3.0)) * (1.0 / (kPi * k2)) *
-                             std::exp(-(std::pow(kPi, 2.0) * k2) / std::pow(kappa, 2.0));
-                recip = recip + ek2;
-            }
+    for (int l4 = g_log ? 1 : 10; l4 <= 10; l4++) {
+        recip = 0.0;
+        for (int l1 = -l4; l1 <= l4; l1++)
+            for (int l2 = -l4; l2 <= l4; l2++)
+                for (int l3 = -l4; l3 <= l4; l3++) {
+                    int n2 = l1 * l1 + l2 * l2 + l3 * l3;
+                    if (n2 == 0) continue;
+                    double k2 = (1.0 / std::pow(L, 2.0)) * (double)n2;
+                    double ek2 = (1.0 / std::pow(L, 3.0)) * (1.0 / (kPi * k2)) *
+                                 std::exp(-(std::pow(kPi, 2.0) * k2) / std::pow(kappa, 2.0));
+                    recip = recip + ek2;
+                }
+        log_line(ld_int(l4) + ld_real(recip));
+    }
+    log_line(ld_str("reciprocal space") + ld_real(recip));
     double real = 0.0;
-    for (int l1 = -l4; l1 <= l4; l1++)
-        for (int l2 = -l4; l2 <= l4; l2++)
-            for (int l3 = -l4; l3 <= l4; l3++) {
-                double modr = L * std::sqrt((double)(l1 * l1 + l2 * l2 + l3 * l3));
-                if (modr != 0.0) real = real + std::erfc(kappa * modr) / modr;
-            }
+    for (int l4 = g_log ? 1 : 10; l4 <= 10; l4++) {
+        real = 0.0;
+        for (int l1 = -l4; l1 <= l4; l1++)
+            for (int l2 = -l4; l2 <= l4; l2++)
+                for (int l3 = -l4; l3 <= l4; l3++) {
+                    double modr = L * std::sqrt((double)(l1 * l1 + l2 * l2 + l3 * l3));
+                    if (modr != 0.0) real = real + std::erfc(kappa * modr) / modr;
+                }
+        log_line(ld_int(l4) + ld_real(real));
+    }
+    log_line(ld_str("real space") + ld_real(real));
     return real + recip + term2 + term4;
 }
 
@@ -102,6 +157,8 @@ void form_eigen(UegccdHeg &h)
             }
         }
         h.eigen[p] = e;
+        log_line(ld_int(p + 1) + ld_int(h.nvec[p]) + ld_int(h.nvec[p + (size_t)h.nao]) +
+                 ld_int(h.nvec[p + 2 * (size_t)h.nao]) + ld_real(e));
     }
 }
 
@@ -122,12 +179,27 @@ void hf_energy(UegccdHeg &h)
     }
     ehf = ehf * 2.0;
     h.xhf = xhf * 2.0;
+    // print_HF (HEG.f90:605-610)
+    if (g_log) {
+        log_line(ld_str("L:") + ld_real(h.L));
+        log_line(ld_str("Omega:") + ld_real(h.omega));
+        log_line(ld_str("cell:") + ld_int(h.cell));
+        log_line(ld_str("HF energy:") + ld_real(ehf / h.nel + h.madelung / 2.0));
+        log_line(ld_str("Exchange energy:") + ld_real(h.xhf / h.nel + h.madelung / 2.0));
+        log_line(ld_str("Madelung:") + ld_real(h.madelung));
+    }
     h.ehf = ehf + h.madelung * 0.5 * h.nel;
 }
 
 int setup_basis(UegccdHeg &h)
 {
     const int cell = h.cell;
+    log_line(ld_str(""));
+    log_line(ld_str("-----------------------------------------------------------"));
+    log_line(ld_str("Setting up HEG basis set"));
+    log_line(ld_str("-----------------------------------------------------------"));
+    log_line(ld_str("G1 memory allocated for") + ld_int((2 * cell + 1) * (2 * cell + 1) * (2 * cell + 1)) +
+             ld_str("basis functions"));
     std::vector<G1Entry> g1;
     g1.reserve((size_t)(2 * cell + 1) * (2 * cell + 1) * (2 * cell + 1));
     for (int l1 = -cell; l1 <= cell; l1++)
@@ -143,6 +215,7 @@ int setup_basis(UegccdHeg &h)
                 if (g.n2 <= h.maxkpoint) g1.push_back(g);
             }
     int nbasis = (int)g1.size();
+    log_line(ld_str("Actual basis set size") + ld_int(nbasis));
     // stable ascending sort by twisted |n+k|^2 (the reference's bubble sort)
     for (;;) {
         bool swapped = false;
@@ -157,10 +230,12 @@ int setup_basis(UegccdHeg &h)
     double mtarget = std::pow(h.in.fcut, 3.0 / 2.0) * h.nel / 2;
     if (std::fabs(mfcut - mtarget) > std::fabs(mfcut + 1 - mtarget)) mfcut = mfcut + 1;
     if (mfcut < nbasis) nbasis = mfcut;
+    log_line(ld_str("Basis set size after fcut") + ld_int(nbasis));
     int mcore = fcut_to_basis_fn(h.in.corefcut, h.nel);
     if ((h.in.corefcut - 1.0) < 1e-6 && mcore != h.nel / 2)
         return herr(UEGCCD_ERR_ARG, "ERROR in setup_basis: corefcut is less than 1 rather than equal to 1");
     nbasis = nbasis - mcore + h.nel / 2;
+    log_line(ld_str("Basis set size after corefcut") + ld_int(nbasis));
     if (nbasis <= h.nel / 2) return herr(UEGCCD_ERR_ARG, "basis has no virtual orbitals");
     h.nao = nbasis;
     h.kvec.assign((size_t)nbasis * 3, 0.0);
@@ -189,6 +264,10 @@ bool parse_bool(const std::string &v)
 }
 
 }  // namespace
+
+namespace uegccd {
+void heg_log_to(std::string *sink) { g_log = sink; }
+}  // namespace uegccd
 
 extern "C" {
 
@@ -321,11 +400,13 @@ int uegccd_heg_create(const UegccdInput *in, UegccdHeg **out)
     }
     for (int d = 0; d < 3; d++) h->ntwist[d] = in->ntwist[d];
     // init_HEG at rS = 1
+    log_shells(10);
     h->rS = 1.0;
     h->L = h->rS * std::pow(4.0 / 3.0 * kPi * h->nel, 1.0 / 3.0);
     h->omega = h->L * h->L * h->L;
     h->madelung = calc_madelung(h->omega, h->L) * in->madelung_factor;
     h->cell = (int)std::sqrt((double)h->maxkpoint) + 3;
+    log_line(ld_str("Madelung constant calculated as") + ld_real(h->madelung));
     int rc = setup_basis(*h);
     if (rc) { delete h; return rc; }
     // change_rs to rSMin (Main.f90:78-79)
@@ -346,6 +427,13 @@ int uegccd_heg_change_twist(UegccdHeg *h, const double twist[3])
 {
     if (!h || !twist) return herr(UEGCCD_ERR_ARG, "null argument");
     int nao = h->nao;
+    if (g_log) {  // ChangeTwist (HEG.f90:565)
+        std::string l = ld_str("changing twist angle from");
+        for (int d = 0; d < 3; d++) l += ld_real(h->ntwist[d]);
+        l += ld_str("to");
+        for (int d = 0; d < 3; d++) l += ld_real(twist[d]);
+        log_line(l);
+    }
     for (int d = 0; d < 3; d++) h->ntwist[d] = twist[d];
     int rc = setup_basis(*h);
     if (rc) return rc;

@@ -31,8 +31,13 @@
 
 #include "../../include/uegccd.h"
 #include "../../include/uegccd_host.h"
+#include "listdir.h"
 
 namespace {
+
+using uegccd::ld_int;
+using uegccd::ld_real;
+using uegccd::ld_str;
 
 thread_local std::string g_zc_error;
 
@@ -41,45 +46,6 @@ int zfail(int code, const std::string &m)
     g_zc_error = m;
     return code;
 }
-
-// ---- gfortran list-directed output (write(u,*)) -----------------------------
-// REAL(8): a blank, then 17 significant digits in a 25-wide G field: F form
-// (20 wide, then 5 blanks) for 0.1 <= |x| < 1e17, else E form with a
-// three-digit exponent.  INTEGER: a blank, then I11.  CHARACTER: a blank, then
-// the text.
-std::string ld_real(double x)
-{
-    char m[64], f[96], num[64];
-    if (!std::isfinite(x)) {
-        std::snprintf(f, sizeof f, " %20s     ", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
-        return f;
-    }
-    int ex = 0;
-    if (x != 0.0) {
-        std::snprintf(m, sizeof m, "%.16e", x);  // 17 significant digits, correctly rounded
-        ex = std::atoi(std::strchr(m, 'e') + 1);
-    }
-    if (x == 0.0 || (ex >= -1 && ex < 17)) {
-        const int dec = x == 0.0 ? 16 : 16 - ex;
-        std::snprintf(num, sizeof num, "%.*f", dec, x);
-        std::snprintf(f, sizeof f, " %20s     ", num);
-        return f;
-    }
-    const std::string s(m);
-    const size_t e = s.find('e');
-    std::snprintf(num, sizeof num, "%sE%c%03d", s.substr(0, e).c_str(), ex < 0 ? '-' : '+', std::abs(ex));
-    std::snprintf(f, sizeof f, " %25s", num);
-    return f;
-}
-
-std::string ld_int(long long v)
-{
-    char f[32];
-    std::snprintf(f, sizeof f, " %11lld", v);
-    return f;
-}
-
-std::string ld_str(const char *s) { return std::string(" ") + s; }
 
 // ---- Output blocks (formats of MP2.f90:143-150, CCD.f90:127-140, dRPA.f90:123-138)
 
@@ -321,21 +287,39 @@ int32_t uegccd_list_real(double x, char *buf, int32_t len)
     return (int32_t)s.size();
 }
 
-int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme)
+// The program; gpu = false runs only the host set-up (it writes fort.60 and nothing else).
+static int run_zcode(const char *input_path, const char *twists_path, int32_t scheme, bool gpu, const char *log_path)
 {
     UegccdInput in;
     if (uegccd_read_input(input_path ? input_path : "Input", 0, &in))
         return zfail(UEGCCD_ERR_ARG, std::string("ReadInput: ") + uegccd_host_last_error());
+    // fort.60: the set-up log, collected while the program runs and written at the end
+    struct LogFile {
+        std::string text;
+        std::string path;
+        explicit LogFile(const char *p) : path(p) { uegccd::heg_log_to(&text); }
+        ~LogFile()
+        {
+            uegccd::heg_log_to(nullptr);
+            if (FILE *f = std::fopen(path.c_str(), "w")) {
+                std::fputs(text.c_str(), f);
+                std::fclose(f);
+            }
+        }
+    } log(log_path);
+    auto logl = [&](const std::string &l) { log.text += l + "\n"; };
     HegGuard h;
     if (uegccd_heg_create(&in, &h.h)) return zfail(UEGCCD_ERR_ARG, std::string("init_HEG: ") + uegccd_host_last_error());
-    if (FILE *f = std::fopen("Output", "w")) std::fclose(f);  // Main.f90:61-62
-    else return zfail(UEGCCD_ERR_ARG, "cannot create Output");
+    if (gpu) {
+        if (FILE *f = std::fopen("Output", "w")) std::fclose(f);  // Main.f90:61-62
+        else return zfail(UEGCCD_ERR_ARG, "cannot create Output");
+    }
     const UegccdOptions opt = options_for(in, scheme);
     UegccdHegInfo info;
     UegccdSystem sys;
     UegccdResult res;
     int rc = 0;
-    if (in.do_single_calc) {
+    if (in.do_single_calc && gpu) {
         uegccd_heg_info(h.h, &info);
         uegccd_heg_system(h.h, &sys);
         Amps x(sys), t(sys);
@@ -346,21 +330,36 @@ int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme
     if (ntw <= 0) return UEGCCD_OK;       // no twists to average
     const auto tw = twist_list(twists_path, ntw);
 
-    // every twist's basis (ChangeTwist), eigenvalues, E_HF and connectivity
-    std::vector<HegGuard> hs(ntw);
+    // every twist's basis, eigenvalues, E_HF and connectivity: ChangeTwist on the one
+    // set-up, as the reference's loop does (Main.f90:112-118), the arrays copied out
     std::vector<UegccdSystem> systems(ntw);
+    std::vector<std::vector<double>> eigs(ntw);
+    std::vector<std::vector<int32_t>> nvecs(ntw);
     std::vector<double> hf(ntw), mp2(ntw), cc(ntw);
     std::vector<int32_t> conn((size_t)ntw * UEGCCD_CONN_LIMIT);
     for (int t = 0; t < ntw; t++) {
-        UegccdInput ti = in;
-        for (int d = 0; d < 3; d++) ti.ntwist[d] = tw[t][d];
-        if (uegccd_heg_create(&ti, &hs[t].h)) return zfail(UEGCCD_ERR_ARG, uegccd_host_last_error());
-        uegccd_heg_info(hs[t].h, &info);
+        logl(ld_int(t + 1) + ld_str("of") + ld_int(ntw));
+        logl(ld_str("randomizing twist angle"));  // GenerateTwist (HEG.f90:541-547): here, the listed twist
+        logl(ld_str("generated") + ld_real(tw[t][0]) + ld_real(tw[t][1]) + ld_real(tw[t][2]));
+        if (uegccd_heg_change_twist(h.h, tw[t].data())) return zfail(UEGCCD_ERR_ARG, uegccd_host_last_error());
+        uegccd_heg_info(h.h, &info);
         hf[t] = info.ehf;
-        uegccd_heg_system(hs[t].h, &systems[t]);
+        uegccd_heg_system(h.h, &systems[t]);
+        if (t == 0) logl(ld_str("EIGEN") + ld_int(systems[t].nao));
+        eigs[t].assign(systems[t].eigen, systems[t].eigen + systems[t].nao);
+        nvecs[t].assign(systems[t].nvec, systems[t].nvec + 3 * (size_t)systems[t].nao);
+        systems[t].eigen = eigs[t].data();
+        systems[t].nvec = nvecs[t].data();
         if (systems[t].nao != systems[0].nao) return zfail(UEGCCD_ERR_ARG, "twists give different basis sizes");
         if ((rc = uegccd_connectivity(&systems[t], opt.core_n, &conn[(size_t)t * UEGCCD_CONN_LIMIT]))) return rc;
     }
+    const int M = systems[0].nao;
+    std::vector<double> cavg(UEGCCD_CONN_LIMIT), diff2(ntw);
+    int32_t best = 0;
+    uegccd_special_twist(ntw, conn.data(), cavg.data(), diff2.data(), &best);
+    if (!gpu)  // the special twist's ChangeTwist ends the set-up log
+        return uegccd_heg_change_twist(h.h, tw[best].data()) ? zfail(UEGCCD_ERR_ARG, uegccd_host_last_error())
+                                                             : UEGCCD_OK;
 
     // all twists in one batch: MP2, then CCD/dRPA when DoCalcTACCD (Main.f90:126-139)
     UegccdBatch *b = nullptr;
@@ -409,7 +408,6 @@ int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme
             cmax = k;
             break;
         }
-    const int M = systems[0].nao;
     std::vector<double> eig_sum(M, 0.0);
     std::array<double, 3> tws{0, 0, 0}, tws2{0, 0, 0};
     double s_hf = 0, s_mp2 = 0, s_cc = 0, s_hf2 = 0, s_mp22 = 0, s_cc2 = 0;
@@ -455,9 +453,6 @@ int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme
         le += ld_real(eig_avg[p]);
     }
     std::fprintf(f59, "%s\n", (le + ld_str("eigenvalue averages")).c_str());
-    std::vector<double> cavg(UEGCCD_CONN_LIMIT), diff2(ntw);
-    int32_t best = 0;
-    uegccd_special_twist(ntw, conn.data(), cavg.data(), diff2.data(), &best);
     int amax = 0;
     for (int k = UEGCCD_CONN_LIMIT; k >= 1; k--)
         if (cavg[k - 1] > 0) {
@@ -484,6 +479,16 @@ int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme
     for (int ip = 0; ip < std::max(1, in.num_rs_points); ip++)
         if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, ip == 0, &res))) return rc;
     return UEGCCD_OK;
+}
+
+int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme)
+{
+    return run_zcode(input_path, twists_path, scheme, true, "fort.60");
+}
+
+int uegccd_zcode_fort60(const char *input_path, const char *twists_path, const char *out_path)
+{
+    return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, out_path ? out_path : "fort.60");
 }
 
 }  // extern "C"
