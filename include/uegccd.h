@@ -4,7 +4,7 @@
  * The entry points replace the Fortran module procedures of the reference
  * (shepherd-group/uegccd) on the MP2 / CCD / dRPA hot path.  They take plain
  * pointers in the reference's own layout so that a Fortran host can bind them
- * with iso_c_binding (the binding is shown in INTEGRATION.md):
+ * with iso_c_binding:
  *
  *   amplitude arrays  T(NOcc, NOcc, NOcc+1:NAO), FP64, column-major, i.e. element
  *                     (i,j,a) (1-based, a > NOcc) at (i-1) + O*(j-1) + O*O*(a-O-1);
@@ -105,13 +105,15 @@ int uegccd_ctx_destroy(UegccdCtx *ctx);
 /* Replaces the eigenvalues (the twist-averaged-eigenvalue solve, Main.f90:243). */
 int uegccd_ctx_set_eigen(UegccdCtx *ctx, const double *eigen);
 
-/* DrvMBPT (MP2.f90:11-157) without the structure-factor dump: writes the MP2
- * amplitudes T2aaaa/T2abab/T2abba (each may be NULL) and E(2). */
+/* DrvMBPT (MP2.f90:11-157): writes the MP2 amplitudes T2aaaa/T2abab/T2abba (each
+ * may be NULL) and E(2).  Its structure factor is uegccd_structure_factor of T2abab. */
 int uegccd_mp2(UegccdCtx *ctx, double *t_aaaa, double *t_abab, double *t_abba, double *e2);
 
 /* DrvCCD (CCD.f90:18-183): iterates from the amplitudes given (the MP2 guess in
  * Main.f90:85-89) and writes the converged amplitudes back in place.  Requires
- * do_ring == do_xring (the spin-adapted form). */
+ * do_ring == do_xring: the library stores the spin-adapted amplitude T2abab alone,
+ * with T2abba(i,j,a) = -T2abab(i,j,b) and T2aaaa = T2abab + T2abba, which the
+ * reference's equations keep only when rings and crossed rings are both on or both off. */
 int uegccd_ccd(UegccdCtx *ctx, const UegccdOptions *opt, double *t_aaaa, double *t_abab,
                double *t_abba, UegccdResult *res);
 
@@ -128,6 +130,28 @@ int uegccd_ccd_g2(UegccdCtx *ctx, const double *t_abab, int32_t term_mask, doubl
 int uegccd_ccd_g2_ex(UegccdCtx *ctx, const double *t_abab, int32_t term_mask, int32_t precision,
                      double *g_abab);
 
+/* ---- structure factors ----------------------------------------------------------
+ * The amplitude sums that CCEnergyAndSF (CCD.f90:240-351; fort.80) and DrvMBPT
+ * (MP2.f90:86-117; fort.81) accumulate over the momentum transfers q = n_a - n_i,
+ * on the reference's grid Sf(-S:S,-S:S,-S:S) with S = uegccd_sf_length(sys)
+ * (SfLength of SendForAllocation, HEG.f90:1051-1065).  Column-major like the
+ * Fortran array: q = (x,y,z) at (x+S) + W*(y+S) + W*W*(z+S), W = 2S+1.  Each pointer
+ * may be NULL; the others receive W^3 doubles:
+ *   sum   SfSum:  T2aaaa+T2abab added at q = n_a-n_i, T2aaaa+T2abba subtracted at n_a-n_j
+ *   dsum  SfDSum: 2*T2abab added, 2*T2abba subtracted
+ *   xsum  SfXSum: T2aaaa-T2abab added, T2aaaa-T2abba subtracted
+ *   g     SfG:    |q|*2*pi/L at every q that an allowed amplitude reaches, else 0
+ *   v     SfV:    V(q) of BaseERI (HEG.f90:969-976) at the same points, else 0
+ * (MP2.f90 fills sum, g and v only.)  sum.v/2 is the correlation energy of the
+ * amplitudes.  A transfer outside the grid returns UEGCCD_ERR_ARG. */
+typedef struct {
+    double *sum, *dsum, *xsum, *g, *v;
+} UegccdSfGrid;
+/* S = 2*maxval(nVec)+1 (host-only), or < 0 on a bad argument. */
+int32_t uegccd_sf_length(const UegccdSystem *sys);
+/* The structure factor of spin-adapted amplitudes t_abab (reference layout). */
+int uegccd_structure_factor(UegccdCtx *ctx, const double *t_abab, const UegccdSfGrid *out);
+
 /* ---- many independent solves in one launch per residual term ---------------- */
 typedef struct UegccdBatch UegccdBatch;
 
@@ -138,6 +162,14 @@ int uegccd_batch_destroy(UegccdBatch *b);
 /* MP2 start + CCD (or dRPA when drpa != 0) of every system; results[n]. */
 int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2,
                        UegccdResult *results);
+/* DrvMBPT for every system: the MP2 amplitudes stay in the batch (what
+ * uegccd_batch_structure_factor and uegccd_batch_get_amplitudes then read); e2[n]
+ * may be NULL. */
+int uegccd_batch_mp2(UegccdBatch *b, double *e2);
+/* The structure factor of solve s from the amplitudes the batch holds: the MP2 ones
+ * after uegccd_batch_mp2, the converged ones after a CCD uegccd_batch_solve (not
+ * after a dRPA solve, whose amplitude is T2aaaa). */
+int uegccd_batch_structure_factor(UegccdBatch *b, int32_t s, const UegccdSfGrid *out);
 /* Copies solve s's amplitudes out in the reference layout (T2abab). */
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
 /* E(2) of one system, as uegccd_mp2 computes it, with no device allocation: this

@@ -35,7 +35,9 @@ typedef struct {
     int32_t fcut2ecut;
     double gapii;
     int32_t do_skip_ta;
-    int32_t diagnostics_requested;   /* DoSFCalcMP2/CCD or DoOnlyMP2Grid set (not on the GPU path) */
+    int32_t do_sf_calc_mp2;          /* DoSFCalcMP2: fort.80 block of the start amplitudes in DrvCCD */
+    int32_t do_sf_calc_ccd;          /* DoSFCalcCCD: fort.80 block of the converged amplitudes        */
+    int32_t do_only_mp2_grid;        /* DoOnlyMP2Grid: stop after the first DrvMBPT (MP2.f90:152-154) */
 } UegccdInput;
 
 typedef struct {
@@ -59,6 +61,11 @@ int uegccd_heg_set_eigen(UegccdHeg *h, const double *eigen);
 int uegccd_heg_system(const UegccdHeg *h, UegccdSystem *sys);
 int uegccd_heg_info(const UegccdHeg *h, UegccdHegInfo *info);
 void uegccd_find_tol(double rs, double *tolmax, double *failratio, double *denomfactor);
+/* print_ex_SF (HEG.f90:617-674): pair counts ExSf and ExV = (1/Omega) 4 pi/|k_l1-k_l2|^2
+ * over ordered pairs l1 != l2 of occupied orbitals, on the grid of q = n_l1 - n_l2 with
+ * |q_d| <= maxq, column-major from -maxq (side 2*maxq+1).  Sets *maxq; either grid may be
+ * NULL (both NULL: only *maxq). */
+int uegccd_heg_exchange_sf(const UegccdHeg *h, int32_t *maxq, int32_t *ex_sf, double *ex_v);
 const char *uegccd_host_last_error(void);
 
 /* ---- The ZCode program (Main.f90:2-320) ------------------------------------ */
@@ -78,7 +85,9 @@ int uegccd_special_twist(int32_t ntwists, const int32_t *conn, double *conn_avg,
  * them: a blank, then 17 significant digits in a G25 field.  Returns its length. */
 int32_t uegccd_list_real(double x, char *buf, int32_t len);
 /* The whole program in the working directory: reads input_path (NULL: "Input"),
- * writes Output, fort.58, fort.59 and fort.60.  twists_path (may be NULL) lists the twist
+ * writes Output, fort.58, fort.59, fort.60, the structure factors fort.81 (every
+ * DrvMBPT) and fort.82 (every print_HF), and fort.80 when DoSFCalcMP2/DoSFCalcCCD
+ * are set.  twists_path (may be NULL) lists the twist
  * angles of the average, three numbers per line; missing ones are drawn from a
  * seeded U[-0.5,0.5)^3 stream.  scheme is UEGCCD_REPLAY or UEGCCD_DIIS.  The
  * solves run on the current CUDA device; every twist of the average is one batch. */
@@ -87,6 +96,10 @@ int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme
  * uegccd_zcode writes (the reference's write(60,*) lines of HEG.f90 and Main.f90),
  * into out_path (NULL: "fort.60"). */
 int uegccd_zcode_fort60(const char *input_path, const char *twists_path, const char *out_path);
+/* The same with the exchange structure factors (fort.82) of the set-up into
+ * fort82_path as well (NULL: not written). */
+int uegccd_zcode_host_logs(const char *input_path, const char *twists_path, const char *fort60_path,
+                           const char *fort82_path);
 const char *uegccd_zcode_last_error(void);
 
 #ifdef __cplusplus

@@ -96,6 +96,12 @@ def lib():
         L.uo_ccd_energy.argtypes = [C.c_void_p, dp, dp, dp]
         L.uo_drpa_energy.restype = C.c_double
         L.uo_drpa_energy.argtypes = [C.c_void_p, dp, C.c_double]
+        L.uo_sf_length.restype = C.c_int
+        L.uo_sf_length.argtypes = [C.c_void_p]
+        L.uo_structure_factor.restype = C.c_double
+        L.uo_structure_factor.argtypes = [C.c_void_p, dp, dp, dp, dp, dp, dp, dp, dp, P(C.c_int)]
+        L.uo_exchange_sf.restype = C.c_int
+        L.uo_exchange_sf.argtypes = [C.c_void_p, P(C.c_int), dp]
         L.uo_twist_average.restype = C.c_int
         L.uo_twist_average.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, P(UoSolveStats), dp]
         _lib = L
@@ -285,6 +291,30 @@ class Oracle:
 
     def drpa_energy(self, t2, csosex: float) -> float:
         return self.L.uo_drpa_energy(self.h, _ptr(t2), csosex)
+
+    def sf_length(self) -> int:
+        return self.L.uo_sf_length(self.h)
+
+    def structure_factor(self, t_aaaa, t_abab, t_abba) -> dict:
+        """CCEnergyAndSF grids (W,W,W) indexed [z+S, y+S, x+S] (Fortran order), and ECorr."""
+        S = self.sf_length()
+        W = 2 * S + 1
+        g = {k: np.zeros((W, W, W)) for k in ("sum", "g", "v", "dsum", "xsum")}
+        oob = C.c_int()
+        e = self.L.uo_structure_factor(self.h, _ptr(np.ascontiguousarray(t_aaaa)), _ptr(np.ascontiguousarray(t_abab)),
+                                       _ptr(np.ascontiguousarray(t_abba)), _ptr(g["sum"]), _ptr(g["g"]), _ptr(g["v"]),
+                                       _ptr(g["dsum"]), _ptr(g["xsum"]), C.byref(oob))
+        g.update(S=S, ecorr=e, oob=oob.value)
+        return g
+
+    def exchange_sf(self) -> dict:
+        """print_ex_SF grids (W,W,W) indexed [z+maxq, y+maxq, x+maxq]."""
+        maxq = self.L.uo_exchange_sf(self.h, None, None)
+        W = 2 * maxq + 1
+        n = np.zeros((W, W, W), dtype=np.int32)
+        v = np.zeros((W, W, W))
+        self.L.uo_exchange_sf(self.h, _ptr(n, C.c_int), _ptr(v))
+        return dict(maxq=maxq, n=n, v=v)
 
     def twist_average(self, twists: np.ndarray):
         tw = np.ascontiguousarray(twists, dtype=np.float64).reshape(-1, 3)

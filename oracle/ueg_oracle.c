@@ -598,6 +598,108 @@ double uo_ccd_energy(UoCtx *c, const double *t_aaaa, const double *t_abab, const
     return ecorr;
 }
 
+/* --------------------------------------------------- structure factors */
+
+/* SendForAllocation (HEG.f90:1051-1065): SfLength = maxval(nvec)*2+1 */
+int uo_sf_length(const UoCtx *c)
+{
+    const Heg *h = &c->heg;
+    int m = h->nvec[0];
+    for (int k = 0; k < 3 * c->info.nao; k++)
+        if (h->nvec[k] > m) m = h->nvec[k];
+    return m * 2 + 1;
+}
+
+/* The structure-factor loop of CCEnergyAndSF (CCD.f90:240-351), whose SfSum/SfG/SfV
+ * part is also the loop of DrvMBPT (MP2.f90:86-95).  Grids (2S+1)^3, S = uo_sf_length,
+ * column-major from -S; every pointer may be NULL.  Contributions are added in the
+ * reference's loop order (I, J, A, A innermost; direct before exchange).  Returns
+ * the ECorr the routine computes.  Out-of-grid transfers (the reference writes
+ * outside its arrays there) are skipped and counted in *oob. */
+double uo_structure_factor(UoCtx *c, const double *t_aaaa, const double *t_abab, const double *t_abba,
+                           double *sf_sum, double *sf_g, double *sf_v, double *sf_dsum, double *sf_xsum, int *oob)
+{
+    const Info *u = &c->info;
+    const Heg *h = &c->heg;
+    const int O = u->nocc, M = u->nao, S = uo_sf_length(c), W = 2 * S + 1;
+    const size_t W3 = (size_t)W * W * W;
+    double *grids[5] = {sf_sum, sf_g, sf_v, sf_dsum, sf_xsum};
+    for (int k = 0; k < 5; k++)
+        if (grids[k]) memset(grids[k], 0, W3 * sizeof(double));
+    int bad = 0;
+    double ecorr = 0.0;
+    const double scale = pow(2.0 * PI / h->L, 2.0);
+    for (int i = 1; i <= O; i++)
+        for (int j = 1; j <= O; j++)
+            for (int a = O + 1; a <= M; a++) {
+                int b = FIND(c, i, j, a);
+                if (b <= O) continue;
+                double v_ijab = ERI(c, a, b, i, j, u->irange_energy);
+                double v_ijba = ERI(c, a, b, j, i, u->irange_energy);
+                if (fmin(v_ijab, v_ijba) < -80.0) continue;
+                int x = tix(O, i, j, a);
+                double de = v_ijab * (t_aaaa[x] + t_abab[x]) - v_ijba * (t_aaaa[x] + t_abba[x]);
+                ecorr = ecorr + F12 * de;
+                for (int pass = 0; pass < 2; pass++) {
+                    /* dK(a,b,i,j) = -nvec(i)+nvec(a), then dK(a,b,j,i) */
+                    const int o = pass == 0 ? i : j;
+                    int q[3];
+                    for (int d = 1; d <= 3; d++) q[d - 1] = -NV(h, o, d) + NV(h, a, d);
+                    if (abs(q[0]) > S || abs(q[1]) > S || abs(q[2]) > S) { bad++; continue; }
+                    size_t g = (size_t)(q[0] + S) + (size_t)W * ((size_t)(q[1] + S) + (size_t)W * (size_t)(q[2] + S));
+                    double q2 = (double)(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                    if (pass == 0) {
+                        if (sf_sum) sf_sum[g] = sf_sum[g] + (t_aaaa[x] + t_abab[x]);
+                        if (sf_g) sf_g[g] = pow(q2 * scale, 0.5);
+                        if (sf_v) sf_v[g] = v_ijab;
+                        if (sf_dsum) sf_dsum[g] = sf_dsum[g] + (2.0 * t_abab[x]);
+                        if (sf_xsum) sf_xsum[g] = sf_xsum[g] + (t_aaaa[x] - t_abab[x]);
+                    } else {
+                        if (sf_sum) sf_sum[g] = sf_sum[g] - (t_aaaa[x] + t_abba[x]);
+                        if (sf_g) sf_g[g] = pow(q2 * scale, 0.5);
+                        if (sf_v) sf_v[g] = v_ijba;
+                        if (sf_dsum) sf_dsum[g] = sf_dsum[g] - (2.0 * t_abba[x]);
+                        if (sf_xsum) sf_xsum[g] = sf_xsum[g] - (t_aaaa[x] - t_abba[x]);
+                    }
+                }
+            }
+    if (oob) *oob = bad;
+    return ecorr;
+}
+
+/* print_ex_SF (HEG.f90:617-674): the exchange structure factor of the occupied
+ * orbitals.  Returns maxq; with ex_sf/ex_v non-NULL fills the (2*maxq+1)^3 grids
+ * (column-major from -maxq). */
+int uo_exchange_sf(const UoCtx *c, int *ex_sf, double *ex_v)
+{
+    const Heg *h = &c->heg;
+    const int no = h->nel / 2;
+    int qmax[3] = {0, 0, 0};
+    for (int l1 = 1; l1 <= no; l1++)
+        for (int l2 = 1; l2 <= no; l2++)
+            if (l2 != l1)
+                for (int d = 1; d <= 3; d++) {
+                    int q = abs(NV(h, l1, d) - NV(h, l2, d));
+                    if (q > qmax[d - 1]) qmax[d - 1] = q;
+                }
+    const int maxq = imax3(qmax[0], qmax[1], qmax[2]) + 1, W = 2 * maxq + 1;
+    if (!ex_sf && !ex_v) return maxq;
+    const size_t W3 = (size_t)W * W * W;
+    if (ex_sf) memset(ex_sf, 0, W3 * sizeof(int));
+    if (ex_v) memset(ex_v, 0, W3 * sizeof(double));
+    for (int l1 = 1; l1 <= no; l1++)
+        for (int l2 = 1; l2 <= no; l2++) {
+            if (l2 == l1) continue;
+            int q[3];
+            for (int d = 1; d <= 3; d++) q[d - 1] = NV(h, l1, d) - NV(h, l2, d);
+            size_t g = (size_t)(q[0] + maxq) + (size_t)W * ((size_t)(q[1] + maxq) + (size_t)W * (size_t)(q[2] + maxq));
+            if (ex_sf) ex_sf[g] += 1;
+            double k1 = KV(h, l1, 1) - KV(h, l2, 1), k2 = KV(h, l1, 2) - KV(h, l2, 2), k3 = KV(h, l1, 3) - KV(h, l2, 3);
+            if (ex_v) ex_v[g] = (1.0 / h->omega) * (4.0 * PI / (k1 * k1 + k2 * k2 + k3 * k3));
+        }
+    return maxq;
+}
+
 /* SolveCC (CCD.f90:354-386; dRPA.f90:223-255) */
 static void solve_cc(UoCtx *c, double *t2, const double *g2, double df)
 {

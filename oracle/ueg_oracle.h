@@ -105,6 +105,17 @@ void   uo_drpa_g2(UoCtx *c, const double *t2, int term_mask, double *g2);
 double uo_ccd_energy(UoCtx *c, const double *t_aaaa, const double *t_abab, const double *t_abba);
 double uo_drpa_energy(UoCtx *c, const double *t2, double csosex);
 
+/* Structure factors.  uo_sf_length: SfLength of SendForAllocation (HEG.f90:1051-1065).
+ * uo_structure_factor: the grids of CCEnergyAndSF (CCD.f90:240-351) -- SfSum, SfG, SfV,
+ * SfDSum, SfXSum, each (2S+1)^3 column-major from -S, NULL to skip -- whose first
+ * three are also DrvMBPT's (MP2.f90:86-117); returns ECorr.  uo_exchange_sf:
+ * print_ex_SF (HEG.f90:617-674); returns maxq, grids (2*maxq+1)^3 when non-NULL. */
+int    uo_sf_length(const UoCtx *c);
+double uo_structure_factor(UoCtx *c, const double *t_aaaa, const double *t_abab, const double *t_abba,
+                           double *sf_sum, double *sf_g, double *sf_v, double *sf_dsum, double *sf_xsum,
+                           int *oob);
+int    uo_exchange_sf(const UoCtx *c, int *ex_sf, double *ex_v);
+
 /* Twist-average driver (Main.f90:99-255) over an explicit twist list.
  * per_twist: ntw x 3 (hf, mp2, ccd).  special: the chosen twist (3).
  * final_st: the special-twist solve (CCD or dRPA by Input). */

@@ -67,6 +67,10 @@ EXPORTS = [
 _lib = None
 
 
+class SfGrid(C.Structure):
+    _fields_ = [(k, C.POINTER(C.c_double)) for k in ("sum", "dsum", "xsum", "g", "v")]
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
@@ -89,6 +93,11 @@ def lib() -> C.CDLL:
         L.uegccd_batch_solve.argtypes = [vp, P(Options), C.c_int32, dp, P(Result)]
         L.uegccd_batch_get_amplitudes.argtypes = [vp, C.c_int32, dp]
         L.uegccd_batch_get_all_amplitudes.argtypes = [vp, dp]
+        L.uegccd_batch_mp2.argtypes = [vp, dp]
+        L.uegccd_sf_length.argtypes = [P(System)]
+        L.uegccd_sf_length.restype = C.c_int32
+        L.uegccd_structure_factor.argtypes = [vp, dp, P(SfGrid)]
+        L.uegccd_batch_structure_factor.argtypes = [vp, C.c_int32, P(SfGrid)]
         L.uegccd_batch_set_profiling.argtypes = [vp, C.c_int32]
         L.uegccd_batch_kernel_stats.argtypes = [vp, C.c_int32, P(C.c_char_p), dp, P(C.c_int64)]
         L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]

@@ -195,6 +195,12 @@ struct UegccdBatch {
     bool have_graph = false;
     cudaGraphExec_t gexec = nullptr;
     int g_launches = 0;          // kernels per iteration
+    // structure factors (on first use): every solve's particle-hole groups {first row, rows},
+    // solve s at [sf_g0[s], sf_g0[s+1]); one grid of the largest solve
+    int2 *sf_groups = nullptr;
+    std::vector<int> sf_g0;
+    double *sf_grid = nullptr;
+    int *sf_err = nullptr;
 
     ~UegccdBatch()
     {
@@ -808,6 +814,72 @@ namespace uegccd {
 int set_last_error(int code, const char *msg) { return fail(code, msg); }
 }  // namespace uegccd
 
+// SendForAllocation (HEG.f90:1051-1065): SfLength = maxval(nVec)*2+1
+int sf_length(const SystemHost &h)
+{
+    int m = h.n.empty() ? 0 : h.n[0][0];
+    for (const auto &v : h.n) m = std::max(m, std::max(v[0], std::max(v[1], v[2])));
+    return m * 2 + 1;
+}
+
+// Structure factors of solve s from the batch's amplitudes: the sums on the device
+// (k_sf), then SfG and SfV -- functions of q alone -- at the points the sums reached,
+// with the reference's expressions: SfG = (|q|^2 (2 pi/L)^2)**0.5 (dK2scaled,
+// HEG.f90:1011-1031), SfV = BaseERI (HEG.f90:969-976).
+int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
+{
+    DevBatch &d = b.d;
+    const int n = d.nsolves;
+    int rc = 0;
+    if (!b.sf_groups) {
+        std::vector<int2> g;
+        b.sf_g0.assign(n + 1, 0);
+        int64_t w3max = 1;
+        for (int k = 0; k < n; k++) {
+            for (const auto &G : b.plans[k].groups) g.push_back(make_int2(G.r0, G.n));
+            b.sf_g0[k + 1] = (int)g.size();
+            const int64_t w = 2 * sf_length(b.sys[k]) + 1;
+            w3max = std::max(w3max, w * w * w);
+        }
+        if ((rc = b.upload(b.sf_groups, g))) return rc;
+        if ((rc = b.alloc(b.sf_grid, 4 * (size_t)w3max))) return rc;
+        if ((rc = b.alloc(b.sf_err, 1))) return rc;
+    }
+    const SystemHost &H = b.sys[s];
+    const int S = sf_length(H);
+    const int64_t W = 2 * S + 1, W3 = W * W * W;
+    CU(cudaMemsetAsync(b.sf_grid, 0, 4 * (size_t)W3 * sizeof(double), b.stream));
+    CU(cudaMemsetAsync(b.sf_err, 0, sizeof(int), b.stream));
+    launch_sf(d, b.sf_groups + b.sf_g0[s], b.sf_g0[s + 1] - b.sf_g0[s], s, S, b.sf_grid, b.sf_err, b.stream);
+    b.launches++;
+    CU(cudaGetLastError());
+    double *dst[3] = {out.sum, out.dsum, out.xsum};
+    for (int k = 0; k < 3; k++)
+        if (dst[k]) CU(cudaMemcpyAsync(dst[k], b.sf_grid + k * W3, W3 * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+    std::vector<double> cnt(W3);
+    CU(cudaMemcpyAsync(cnt.data(), b.sf_grid + 3 * W3, W3 * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+    int err = 0;
+    CU(cudaMemcpyAsync(&err, b.sf_err, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+    b.d2h_bytes += (int64_t)((3 + 1) * W3 * sizeof(double));
+    if (err) return fail(UEGCCD_ERR_ARG, "a momentum transfer falls outside the structure-factor grid");
+    const double c = 2.0 * kPi / H.L, scale = c * c;
+    for (int64_t z = 0; z < W; z++)
+        for (int64_t y = 0; y < W; y++)
+            for (int64_t x = 0; x < W; x++) {
+                const int64_t k = x + W * (y + W * z);
+                double g = 0.0, v = 0.0;
+                if (cnt[k] > 0.0) {
+                    const int q2 = (int)((x - S) * (x - S) + (y - S) * (y - S) + (z - S) * (z - S));
+                    g = std::pow((double)q2 * scale, 0.5);
+                    v = coulomb_v(H.L, H.madelung, q2);
+                }
+                if (out.g) out.g[k] = g;
+                if (out.v) out.v[k] = v;
+            }
+    return UEGCCD_OK;
+}
+
 extern "C" {
 
 const char *uegccd_last_error(void) { return g_last_error.c_str(); }
@@ -938,6 +1010,23 @@ int uegccd_ccd_g2_ex(UegccdCtx *c, const double *t_abab, int32_t mask, int32_t p
         if (err) return fail(UEGCCD_ERR_CUDA, "tensor-core ladder: an mbarrier wait expired");
     }
     return unpack_to_host(b, 0, d.t_new, g_abab, nullptr, nullptr);
+}
+
+int32_t uegccd_sf_length(const UegccdSystem *sys)
+{
+    if (!sys || !sys->nvec || sys->nao <= 0) return fail(UEGCCD_ERR_ARG, "bad system");
+    int m = sys->nvec[0];
+    for (int64_t k = 0; k < 3 * (int64_t)sys->nao; k++) m = std::max(m, (int)sys->nvec[k]);
+    return m * 2 + 1;
+}
+
+int uegccd_structure_factor(UegccdCtx *c, const double *t_abab, const UegccdSfGrid *out)
+{
+    if (!c || !t_abab || !out) return fail(UEGCCD_ERR_ARG, "null argument");
+    UegccdBatch &b = *c->batch;
+    int rc = pack_from_host(b, 0, t_abab);
+    if (rc) return rc;
+    return structure_factor(b, 0, *out);
 }
 
 int uegccd_ccd_g2(UegccdCtx *c, const double *t_abab, int32_t mask, double *g_abab)
@@ -1103,6 +1192,30 @@ int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab)
         if (a < e) std::memcpy((char *)t_abab + a, g_stage + a, e - a);
     });
     return UEGCCD_OK;
+}
+
+int uegccd_batch_mp2(UegccdBatch *b, double *e2)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    b->kt.begin(KID_MP2, b->stream);
+    launch_mp2(b->d, b->stream);
+    b->kt.end(b->stream);
+    launch_reduce(b->d, b->stream);
+    b->launches += 2;
+    int rc = read_red(*b);
+    if (rc) return rc;
+    int status = UEGCCD_OK;
+    for (int s = 0; s < b->d.nsolves; s++) {
+        if (e2) e2[s] = b->red[3 * s];
+        if (!std::isfinite(b->red[3 * s])) status = fail(UEGCCD_ERR_NUMERIC, "non-finite MP2 energy");
+    }
+    return status;
+}
+
+int uegccd_batch_structure_factor(UegccdBatch *b, int32_t s, const UegccdSfGrid *out)
+{
+    if (!b || !out || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
+    return structure_factor(*b, s, *out);
 }
 
 int uegccd_trim_cache(void)

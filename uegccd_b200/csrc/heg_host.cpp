@@ -3,8 +3,9 @@
 // hot path.  Restates IO.f90 ReadInput/ParseLine (IO.f90:14-391) and, from
 // HEG.f90, init_HEG (16-43), CalcMadelung (89-148), SetupBasis (150-324),
 // FcutToBasisFn (326-342), change_rs (494-533), ChangeTwist (551-578), print_HF
-// (581-615) and FindTol (1073-1086).  Floating-point expressions keep the
+// (581-615), print_ex_SF (617-674) and FindTol (1073-1086).  Floating-point expressions keep the
 // Fortran evaluation order, so the eigenvalues equal the reference's printout.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +25,7 @@ namespace {
 constexpr double kPi = 3.1415926535897932384626433833;  // Constants.f90:7
 thread_local std::string g_host_error;
 thread_local std::string *g_log = nullptr;   // fort.60 lines (set by the ZCode program)
+thread_local std::string *g_log82 = nullptr; // fort.82 lines (the exchange structure factors)
 
 using uegccd::ld_int;
 using uegccd::ld_real;
@@ -162,6 +164,55 @@ void form_eigen(UegccdHeg &h)
     }
 }
 
+// print_ex_SF (HEG.f90:617-674): ordered pairs of occupied orbitals l1 != l2 counted on
+// the grid of q = n_l1 - n_l2 (side 2*maxq+1, column-major from -maxq), with the last
+// pair's (1/Omega) 4 pi/|k_l1 - k_l2|^2 at each q.
+int exchange_sf(const UegccdHeg &h, std::vector<int32_t> *ex_sf, std::vector<double> *ex_v)
+{
+    const int no = h.nel / 2;
+    auto n = [&](int p, int d) { return h.nvec[p + (size_t)h.nao * d]; };
+    int qmax[3] = {0, 0, 0};
+    for (int l1 = 0; l1 < no; l1++)
+        for (int l2 = 0; l2 < no; l2++)
+            if (l2 != l1)
+                for (int d = 0; d < 3; d++) qmax[d] = std::max(qmax[d], std::abs(n(l1, d) - n(l2, d)));
+    const int maxq = std::max(qmax[0], std::max(qmax[1], qmax[2])) + 1;
+    if (!ex_sf && !ex_v) return maxq;
+    const size_t W = 2 * maxq + 1;
+    if (ex_sf) ex_sf->assign(W * W * W, 0);
+    if (ex_v) ex_v->assign(W * W * W, 0.0);
+    for (int l1 = 0; l1 < no; l1++)
+        for (int l2 = 0; l2 < no; l2++) {
+            if (l2 == l1) continue;
+            const size_t g = (size_t)(n(l1, 0) - n(l2, 0) + maxq) +
+                             W * ((size_t)(n(l1, 1) - n(l2, 1) + maxq) + W * (size_t)(n(l1, 2) - n(l2, 2) + maxq));
+            if (ex_sf) (*ex_sf)[g] += 1;
+            const double *k = &h.kvec[3 * l1], *kq = &h.kvec[3 * l2];
+            const double q1 = k[0] - kq[0], q2 = k[1] - kq[1], q3 = k[2] - kq[2];
+            if (ex_v) (*ex_v)[g] = (1.0 / h.omega) * (4.0 * kPi / (q1 * q1 + q2 * q2 + q3 * q3));
+        }
+    return maxq;
+}
+
+// the fort.82 block of one print_ex_SF call
+void log_exchange_sf(const UegccdHeg &h)
+{
+    if (!g_log82) return;
+    std::vector<int32_t> cnt;
+    std::vector<double> v;
+    const int m = exchange_sf(h, &cnt, &v);
+    const int W = 2 * m + 1;
+    std::string &o = *g_log82;
+    o += ld_str("--------") + "\n" + ld_str("Starting a new structure factor") + "\n" + ld_str("--------") + "\n";
+    for (int x = -m; x <= m; x++)
+        for (int y = -m; y <= m; y++)
+            for (int z = -m; z <= m; z++) {
+                const size_t g = (size_t)(x + m) + (size_t)W * ((size_t)(y + m) + (size_t)W * (size_t)(z + m));
+                if (cnt[g] > 0)  // ExSf > 1e-10
+                    o += ld_int(x) + ld_int(y) + ld_int(z) + ld_int(cnt[g]) + ld_real(v[g]) + "\n";
+            }
+}
+
 void hf_energy(UegccdHeg &h)
 {
     double ehf = 0.0, xhf = 0.0;
@@ -189,6 +240,7 @@ void hf_energy(UegccdHeg &h)
         log_line(ld_str("Madelung:") + ld_real(h.madelung));
     }
     h.ehf = ehf + h.madelung * 0.5 * h.nel;
+    log_exchange_sf(h);
 }
 
 int setup_basis(UegccdHeg &h)
@@ -267,6 +319,7 @@ bool parse_bool(const std::string &v)
 
 namespace uegccd {
 void heg_log_to(std::string *sink) { g_log = sink; }
+void heg_sf_log_to(std::string *sink) { g_log82 = sink; }
 }  // namespace uegccd
 
 extern "C" {
@@ -357,9 +410,10 @@ int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
         } else if (key == "DoKS") in->do_ks = parse_bool(val);
         else if (key == "MadelungFactor") vs >> in->madelung_factor;
         else if (key == "DoSingleCalc") in->do_single_calc = parse_bool(val);
-        else if (key == "DoSFCalcMP2" || key == "DoSFCalcCCD" || key == "DoOnlyMP2Grid") {
-            if (parse_bool(val)) in->diagnostics_requested = 1;
-        } else if (key == "DoSkipTA") in->do_skip_ta = parse_bool(val);
+        else if (key == "DoSFCalcMP2") in->do_sf_calc_mp2 = parse_bool(val);
+        else if (key == "DoSFCalcCCD") in->do_sf_calc_ccd = parse_bool(val);
+        else if (key == "DoOnlyMP2Grid") in->do_only_mp2_grid = parse_bool(val);
+        else if (key == "DoSkipTA") in->do_skip_ta = parse_bool(val);
         else if (key == "Gap") vs >> in->gap;
         else if (key == "fcut") vs >> in->fcut;
         else if (key == "corefcut") vs >> in->corefcut;
@@ -477,6 +531,17 @@ int uegccd_heg_info(const UegccdHeg *h, UegccdHegInfo *info)
 }
 
 // FindTol (HEG.f90:1073-1086), fed HEGData%rS as the reference does (always 1).
+int uegccd_heg_exchange_sf(const UegccdHeg *h, int32_t *maxq, int32_t *ex_sf, double *ex_v)
+{
+    if (!h || !maxq) return herr(UEGCCD_ERR_ARG, "null argument");
+    std::vector<int32_t> c;
+    std::vector<double> v;
+    *maxq = exchange_sf(*h, ex_sf ? &c : nullptr, ex_v ? &v : nullptr);
+    if (ex_sf) std::copy(c.begin(), c.end(), ex_sf);
+    if (ex_v) std::copy(v.begin(), v.end(), ex_v);
+    return UEGCCD_OK;
+}
+
 void uegccd_find_tol(double rs, double *tolmax, double *failratio, double *denomfactor)
 {
     *tolmax = 1.0e-8;

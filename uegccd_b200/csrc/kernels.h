@@ -159,6 +159,11 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
 void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaStream_t st);
 void launch_vcoef(const DevBatch &d, cudaStream_t st);
 void launch_unpack_all(const DevBatch &d, const int64_t *dense_off, const double *t, double *out, cudaStream_t st);
+// Structure-factor sums of solve `solve` from d.t: groups = its particle-hole groups
+// {first row, rows}; grid = 4 arrays of (2S+1)^3 (SfSum, SfDSum, SfXSum, contributions),
+// column-major from -S, zeroed by the caller; *err = 1 if a transfer falls outside.
+void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, int S, double *grid, int *err,
+               cudaStream_t st);
 // pos (pre-set to -1), amps, partner, then the ring gather indices, from the block structure
 void launch_block_tables(const DevBatch &d, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)

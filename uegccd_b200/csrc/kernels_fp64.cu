@@ -1517,6 +1517,94 @@ void launch_unpack_all(const DevBatch &d, const int64_t *dense_off, const double
 }
 
 // ----------------------------------------------------------------------------
+// Structure factors on the momentum-transfer grid (CCEnergyAndSF, CCD.f90:290-331;
+// DrvMBPT, MP2.f90:86-95).  For every stored (i,j,a) the reference adds
+//   at q = n_a - n_i:  SfSum += T2aaaa + T2abab,  SfDSum += 2 T2abab,  SfXSum += T2aaaa - T2abab
+//   at q = n_a - n_j:  SfSum -= T2aaaa + T2abba,  SfDSum -= 2 T2abba,  SfXSum -= T2aaaa - T2abba
+// with T2abba(i,j,a) = -t(ij,b) and T2aaaa = T2abab + T2abba (CCD.f90:90).
+// Particle-hole row (i,x) of group Q = n_x - n_i, with occupied k, holds the direct
+// transfer of t(ik,x) and the exchange transfer of t(ki,x): every contribution to grid
+// point Q comes from the rows of group Q.  One CTA per group therefore owns its grid
+// point and writes it without atomics, summing in a fixed order.
+// ----------------------------------------------------------------------------
+constexpr int kSfThreads = 128;
+
+__global__ void __launch_bounds__(kSfThreads)
+    k_sf(const int2 *__restrict__ groups, const SolveDev *__restrict__ solves, int solve,
+         const int16_t *__restrict__ ph_i, const int16_t *__restrict__ ph_x, const int4 *__restrict__ nv4,
+         const int32_t *__restrict__ ridx_x, const int32_t *__restrict__ ridx_y,
+         const int32_t *__restrict__ partner, const double *__restrict__ t, int S, double *__restrict__ grid,
+         int *__restrict__ err)
+{
+    const int2 G = groups[blockIdx.x];   // rows [G.x, G.x + G.y) of the solve
+    const SolveDev s = solves[solve];
+    const int O = s.O;
+    double sum = 0.0, dsum = 0.0, xsum = 0.0, cnt = 0.0;
+    const int n = G.y * O;
+    for (int e = threadIdx.x; e < n; e += kSfThreads) {
+        const int r = G.x + e / O, k = e - (e / O) * O;
+        const int64_t ri = s.ph0 + (int64_t)r * O + k;
+        const int pd = __ldg(&ridx_x[ri]);
+        if (pd >= 0) {  // direct: (I,J,A) = (i,k,x)
+            const double tab = __ldg(&t[pd]), tba = -__ldg(&t[__ldg(&partner[pd])]);
+            const double taa = tab + tba;
+            sum += taa + tab;
+            dsum += 2.0 * tab;
+            xsum += taa - tab;
+            cnt += 1.0;
+        }
+        const int px = __ldg(&ridx_y[ri]);
+        if (px >= 0) {  // exchange: (I,J,A) = (k,i,x)
+            const double tab = __ldg(&t[px]), tba = -__ldg(&t[__ldg(&partner[px])]);
+            const double taa = tab + tba;
+            sum -= taa + tba;
+            dsum -= 2.0 * tba;
+            xsum -= taa - tba;
+            cnt += 1.0;
+        }
+    }
+    __shared__ double red[4][kSfThreads / 32];
+    double v[4] = {sum, dsum, xsum, cnt};
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+#pragma unroll
+        for (int q = 0; q < 4; q++) red[q][w] = v[q];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double tot[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        tot[q] = red[q][0];
+        for (int k = 1; k < kSfThreads / 32; k++) tot[q] += red[q][k];
+    }
+    if (tot[3] == 0.0) return;   // no stored amplitude reaches this transfer
+    const int i = ph_i[s.phr0 + G.x], x = ph_x[s.phr0 + G.x];
+    const int4 a = nv4[s.orb0 + x], b = nv4[s.orb0 + i];
+    const int q0 = a.x - b.x, q1 = a.y - b.y, q2 = a.z - b.z;
+    if (q0 < -S || q0 > S || q1 < -S || q1 > S || q2 < -S || q2 > S) {
+        atomicExch(err, 1);
+        return;
+    }
+    const int64_t W = 2 * S + 1, W3 = W * W * W;
+    const int64_t c = (q0 + S) + W * ((q1 + S) + W * (int64_t)(q2 + S));
+    grid[c] = tot[0];
+    grid[W3 + c] = tot[1];
+    grid[2 * W3 + c] = tot[2];
+    grid[3 * W3 + c] = tot[3];
+}
+
+void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, int S, double *grid, int *err,
+               cudaStream_t st)
+{
+    if (ngroups > 0)
+        k_sf<<<ngroups, kSfThreads, 0, st>>>(groups, d.solves, solve, d.ph_i, d.ph_x, d.nv4, d.ridx_x, d.ridx_y,
+                                            d.partner, d.t, S, grid, err);
+}
+
+// ----------------------------------------------------------------------------
 // Launch wrappers
 // ----------------------------------------------------------------------------
 void launch_mp2(const DevBatch &d, cudaStream_t st)

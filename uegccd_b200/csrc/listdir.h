@@ -1,5 +1,5 @@
 // listdir.h -- gfortran list-directed output (write(u,*)) of the items that the
-// reference's fort.58, fort.59 and fort.60 hold.
+// reference's fort.58, fort.59, fort.60 and fort.80-82 hold.
 //   REAL(8):   a blank, then 17 significant digits in a 25-wide G field: F form
 //              (20 wide, then 5 blanks) for 0.1 <= |x| < 1e17, else E form with a
 //              three-digit exponent.
@@ -51,5 +51,7 @@ inline std::string ld_str(const char *s) { return std::string(" ") + s; }
 // The fort.60 log of the host set-up: lines are appended here while a sink is set
 // (per host thread; the ZCode program sets it, nothing else does).
 void heg_log_to(std::string *sink);
+// The fort.82 lines (exchange structure factor of every print_HF), the same way.
+void heg_sf_log_to(std::string *sink);
 
 }  // namespace uegccd

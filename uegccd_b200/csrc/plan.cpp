@@ -14,11 +14,6 @@
 
 namespace uegccd {
 
-namespace {
-constexpr double kPi = 3.1415926535897932384626433833;  // Constants.f90:7
-
-}  // namespace
-
 double coulomb_v(double L, double madelung, int q2)
 {
     if (q2 == 0) return -madelung;

@@ -9,6 +9,8 @@
 
 namespace uegccd {
 
+constexpr double kPi = 3.1415926535897932384626433833;  // Constants.f90:7
+
 // One system as the hot path sees it (HEGData/UEGInfo fields, Types.f90:7-82).
 struct SystemHost {
     int O = 0, M = 0;

@@ -13,6 +13,10 @@
 //   170-231  averages, connectivity histogram, special twist (fort.58, fort.59)
 //   233-255  MP2 + CCD/dRPA at the special twist with the twist-averaged
 //            eigenvalues, NumRSPoints times
+// Structure factors: fort.81 after every DrvMBPT (MP2.f90:98-113), fort.80 in
+// DrvCCD when DoSFCalcMP2 / DoSFCalcCCD (CCD.f90:65,109), fort.82 after every
+// print_HF (HEG.f90:612); DoOnlyMP2Grid stops after the first DrvMBPT
+// (MP2.f90:152-154).
 //
 // Twists: the reference draws them with gfortran's rand() seeded 86456
 // (Main.f90:30,81; HEG.f90:535-549), which is not reproduced here.  The caller
@@ -130,6 +134,71 @@ UegccdOptions options_for(const UegccdInput &in, int32_t scheme)
     return o;
 }
 
+// ---- structure-factor files (fort.80, fort.81), opened on their first block
+
+struct SfGrids {
+    int S = 0;
+    std::vector<double> sum, dsum, xsum, g, v;
+    UegccdSfGrid view(int32_t S_)
+    {
+        S = S_;
+        const size_t W = 2 * (size_t)S + 1, n = W * W * W;
+        for (auto *a : {&sum, &dsum, &xsum, &g, &v}) a->assign(n, 0.0);
+        return UegccdSfGrid{sum.data(), dsum.data(), xsum.data(), g.data(), v.data()};
+    }
+};
+
+// One block: fort.81 (DrvMBPT, MP2.f90:98-113: the points with SfG > 0; q, SfG, SfSum,
+// SfV) or fort.80 (CCEnergyAndSF, CCD.f90:263-266,334-342: SfG > 1e-10; also SfDSum,
+// SfXSum).  x outermost, z innermost, as the reference's loops run.
+std::string sf_block(const SfGrids &f, bool ccd)
+{
+    std::string o = ld_str("--------") + "\n" + ld_str("Starting a new structure factor") + "\n" +
+                    ld_str("--------") + "\n";
+    const int S = f.S;
+    const size_t W = 2 * (size_t)S + 1;
+    for (int x = -S; x <= S; x++)
+        for (int y = -S; y <= S; y++)
+            for (int z = -S; z <= S; z++) {
+                const size_t k = (size_t)(x + S) + W * ((size_t)(y + S) + W * (size_t)(z + S));
+                if (!(ccd ? f.g[k] > 1.0e-10 : f.g[k] > 0.0)) continue;
+                o += ld_int(x) + ld_int(y) + ld_int(z) + ld_real(f.g[k]) + ld_real(f.sum[k]) + ld_real(f.v[k]);
+                if (ccd) o += ld_real(f.dsum[k]) + ld_real(f.xsum[k]);
+                o += "\n";
+            }
+    return o;
+}
+
+struct SfFiles {
+    FILE *f80 = nullptr, *f81 = nullptr;
+    bool mp2_in_cc = false, ccd = false;   // DoSFCalcMP2, DoSFCalcCCD
+    SfFiles() = default;
+    SfFiles(const SfFiles &) = delete;
+    SfFiles &operator=(const SfFiles &) = delete;
+    ~SfFiles()
+    {
+        if (f80) std::fclose(f80);
+        if (f81) std::fclose(f81);
+    }
+    int put(int unit, const std::string &text)
+    {
+        FILE *&f = unit == 80 ? f80 : f81;
+        if (!f) f = std::fopen(unit == 80 ? "fort.80" : "fort.81", "w");
+        if (!f) return zfail(UEGCCD_ERR_ARG, unit == 80 ? "cannot write fort.80" : "cannot write fort.81");
+        std::fputs(text.c_str(), f);
+        return UEGCCD_OK;
+    }
+};
+
+// fort.81 or fort.80 block of spin-adapted amplitudes on a context
+int sf_ctx(UegccdCtx *ctx, const UegccdSystem &sys, const double *t_abab, SfFiles &sf, int unit)
+{
+    SfGrids g;
+    const UegccdSfGrid v = g.view(uegccd_sf_length(&sys));
+    if (int rc = uegccd_structure_factor(ctx, t_abab, &v)) return zfail(rc, uegccd_last_error());
+    return sf.put(unit, sf_block(g, unit == 80));
+}
+
 struct Amps {
     std::vector<double> aaaa, abab, abba;
     explicit Amps(const UegccdSystem &s)
@@ -142,9 +211,10 @@ struct Amps {
 };
 
 // DrvMBPT into x, then DrvCCD/DrvdRPA on t (started from x when copy_start);
-// both Output blocks appended.
+// both Output blocks appended, and the structure-factor blocks.  Under DoOnlyMP2Grid
+// it returns after the MP2 step (the program ends there).
 int mp2_then_cc(const UegccdInput &in, const UegccdSystem &sys, double ehf, const UegccdOptions &opt, Amps &x,
-                Amps &t, bool copy_start, UegccdResult *res)
+                Amps &t, bool copy_start, UegccdResult *res, SfFiles &sf)
 {
     UegccdCtx *ctx = nullptr;
     if (uegccd_ctx_create(&sys, &ctx)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
@@ -155,23 +225,38 @@ int mp2_then_cc(const UegccdInput &in, const UegccdSystem &sys, double ehf, cons
         uegccd_ctx_destroy(ctx);
         return rc;
     }
+    if ((rc = sf_ctx(ctx, sys, x.abab.data(), sf, 81))) {
+        uegccd_ctx_destroy(ctx);
+        return rc;
+    }
     FILE *f = std::fopen("Output", "a");
     if (!f) {
         uegccd_ctx_destroy(ctx);
         return zfail(UEGCCD_ERR_ARG, "cannot append to Output");
     }
     write_mp2(f, ehf, sys.eigen, sys.nocc, sys.nao, e2);
+    if (in.do_only_mp2_grid) {  // "DoOnlyMP2Grid flag is true, so calculation stopping here"
+        std::fclose(f);
+        uegccd_ctx_destroy(ctx);
+        return UEGCCD_OK;
+    }
     if (copy_start) t = x;
     UegccdOptions o = opt;
     std::vector<double> en(1100), dt(1100);
     o.energies = en.data();
     o.dts = dt.data();
     o.max_rec = 1100;
+    if (!in.do_drpa_sosex && sf.mp2_in_cc && (rc = sf_ctx(ctx, sys, t.abab.data(), sf, 80))) {
+        std::fclose(f);
+        uegccd_ctx_destroy(ctx);
+        return rc;
+    }
     rc = in.do_drpa_sosex ? uegccd_drpa(ctx, &o, t.aaaa.data(), res)
                           : uegccd_ccd(ctx, &o, t.aaaa.data(), t.abab.data(), t.abba.data(), res);
     if (rc >= 0) {
-        write_cc(f, in, in.do_drpa_sosex, *res, en.data(), dt.data(), res->n_recorded, ehf);
         rc = 0;
+        if (!in.do_drpa_sosex && sf.ccd) rc = sf_ctx(ctx, sys, t.abab.data(), sf, 80);
+        write_cc(f, in, in.do_drpa_sosex, *res, en.data(), dt.data(), res->n_recorded, ehf);
     } else {
         zfail(rc, uegccd_last_error());
     }
@@ -287,26 +372,34 @@ int32_t uegccd_list_real(double x, char *buf, int32_t len)
     return (int32_t)s.size();
 }
 
-// The program; gpu = false runs only the host set-up (it writes fort.60 and nothing else).
-static int run_zcode(const char *input_path, const char *twists_path, int32_t scheme, bool gpu, const char *log_path)
+// The program; gpu = false runs only the host set-up (it writes the fort.60 log, and
+// fort.82 when f82_path is given).
+static int run_zcode(const char *input_path, const char *twists_path, int32_t scheme, bool gpu, const char *log_path,
+                     const char *f82_path)
 {
     UegccdInput in;
     if (uegccd_read_input(input_path ? input_path : "Input", 0, &in))
         return zfail(UEGCCD_ERR_ARG, std::string("ReadInput: ") + uegccd_host_last_error());
-    // fort.60: the set-up log, collected while the program runs and written at the end
+    // fort.60 (set-up log) and fort.82 (exchange structure factors): collected while the
+    // program runs and written at the end
     struct LogFile {
         std::string text;
         std::string path;
-        explicit LogFile(const char *p) : path(p) { uegccd::heg_log_to(&text); }
+        void (*sink)(std::string *);
+        LogFile(const char *p, void (*set)(std::string *)) : path(p ? p : ""), sink(set)
+        {
+            if (!path.empty()) sink(&text);
+        }
         ~LogFile()
         {
-            uegccd::heg_log_to(nullptr);
+            if (path.empty()) return;
+            sink(nullptr);
             if (FILE *f = std::fopen(path.c_str(), "w")) {
                 std::fputs(text.c_str(), f);
                 std::fclose(f);
             }
         }
-    } log(log_path);
+    } log(log_path, uegccd::heg_log_to), log82(f82_path, uegccd::heg_sf_log_to);
     auto logl = [&](const std::string &l) { log.text += l + "\n"; };
     HegGuard h;
     if (uegccd_heg_create(&in, &h.h)) return zfail(UEGCCD_ERR_ARG, std::string("init_HEG: ") + uegccd_host_last_error());
@@ -314,16 +407,22 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
         if (FILE *f = std::fopen("Output", "w")) std::fclose(f);  // Main.f90:61-62
         else return zfail(UEGCCD_ERR_ARG, "cannot create Output");
     }
+    SfFiles sf;
+    sf.mp2_in_cc = in.do_sf_calc_mp2 != 0;
+    sf.ccd = in.do_sf_calc_ccd != 0;
     const UegccdOptions opt = options_for(in, scheme);
     UegccdHegInfo info;
     UegccdSystem sys;
     UegccdResult res;
     int rc = 0;
-    if (in.do_single_calc && gpu) {
-        uegccd_heg_info(h.h, &info);
-        uegccd_heg_system(h.h, &sys);
-        Amps x(sys), t(sys);
-        if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, true, &res))) return rc;
+    if (in.do_single_calc) {
+        if (gpu) {
+            uegccd_heg_info(h.h, &info);
+            uegccd_heg_system(h.h, &sys);
+            Amps x(sys), t(sys);
+            if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, true, &res, sf))) return rc;
+        }
+        if (in.do_only_mp2_grid) return UEGCCD_OK;  // stopped in the first DrvMBPT
     }
     if (in.do_skip_ta) return UEGCCD_OK;  // "Finishing calculation after single point calculation"
     const int ntw = in.tacalcn;
@@ -331,13 +430,15 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
     const auto tw = twist_list(twists_path, ntw);
 
     // every twist's basis, eigenvalues, E_HF and connectivity: ChangeTwist on the one
-    // set-up, as the reference's loop does (Main.f90:112-118), the arrays copied out
-    std::vector<UegccdSystem> systems(ntw);
-    std::vector<std::vector<double>> eigs(ntw);
-    std::vector<std::vector<int32_t>> nvecs(ntw);
-    std::vector<double> hf(ntw), mp2(ntw), cc(ntw);
-    std::vector<int32_t> conn((size_t)ntw * UEGCCD_CONN_LIMIT);
-    for (int t = 0; t < ntw; t++) {
+    // set-up, as the reference's loop does (Main.f90:112-118), the arrays copied out.
+    // DoOnlyMP2Grid stops in the first twist's DrvMBPT.
+    const int nset = in.do_only_mp2_grid ? 1 : ntw;
+    std::vector<UegccdSystem> systems(nset);
+    std::vector<std::vector<double>> eigs(nset);
+    std::vector<std::vector<int32_t>> nvecs(nset);
+    std::vector<double> hf(nset), mp2(nset), cc(nset);
+    std::vector<int32_t> conn((size_t)nset * UEGCCD_CONN_LIMIT);
+    for (int t = 0; t < nset; t++) {
         logl(ld_int(t + 1) + ld_str("of") + ld_int(ntw));
         logl(ld_str("randomizing twist angle"));  // GenerateTwist (HEG.f90:541-547): here, the listed twist
         logl(ld_str("generated") + ld_real(tw[t][0]) + ld_real(tw[t][1]) + ld_real(tw[t][2]));
@@ -354,36 +455,59 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
         if ((rc = uegccd_connectivity(&systems[t], opt.core_n, &conn[(size_t)t * UEGCCD_CONN_LIMIT]))) return rc;
     }
     const int M = systems[0].nao;
-    std::vector<double> cavg(UEGCCD_CONN_LIMIT), diff2(ntw);
+    std::vector<double> cavg(UEGCCD_CONN_LIMIT), diff2(nset);
     int32_t best = 0;
-    uegccd_special_twist(ntw, conn.data(), cavg.data(), diff2.data(), &best);
-    if (!gpu)  // the special twist's ChangeTwist ends the set-up log
+    if (!in.do_only_mp2_grid) uegccd_special_twist(ntw, conn.data(), cavg.data(), diff2.data(), &best);
+    if (!gpu) {
+        if (in.do_only_mp2_grid) return UEGCCD_OK;
+        // the special twist's ChangeTwist ends the set-up log
         return uegccd_heg_change_twist(h.h, tw[best].data()) ? zfail(UEGCCD_ERR_ARG, uegccd_host_last_error())
                                                              : UEGCCD_OK;
+    }
 
-    // all twists in one batch: MP2, then CCD/dRPA when DoCalcTACCD (Main.f90:126-139)
-    UegccdBatch *b = nullptr;
-    if (uegccd_batch_create(systems.data(), ntw, &b)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
-    std::vector<UegccdResult> br(ntw);
-    UegccdOptions bo = opt;
-    if (!in.do_calc_ta_ccd) bo.max_iter = 1;  // the start amplitudes only: MP2
-    rc = uegccd_batch_solve(b, &bo, in.do_drpa_sosex, mp2.data(), br.data());
-    if (rc < 0) {
-        zfail(rc, uegccd_last_error());
-        uegccd_batch_destroy(b);
-        return rc;
+    // all twists in one batch: MP2 and its structure factor (fort.81), then CCD/dRPA
+    // when DoCalcTACCD (Main.f90:126-139)
+    struct BatchGuard {
+        UegccdBatch *b = nullptr;
+        ~BatchGuard() { uegccd_batch_destroy(b); }
+    } bg;
+    if (uegccd_batch_create(systems.data(), nset, &bg.b)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
+    UegccdBatch *b = bg.b;
+    if ((rc = uegccd_batch_mp2(b, mp2.data()))) return zfail(rc, uegccd_last_error());
+    const bool cc_sf = in.do_calc_ta_ccd && !in.do_drpa_sosex;
+    std::vector<std::string> mp2_80(nset);   // DrvCCD's DoSFCalcMP2 blocks, written beside the CCD ones
+    for (int t = 0; t < nset; t++) {
+        SfGrids g;
+        const UegccdSfGrid v = g.view(uegccd_sf_length(&systems[t]));
+        if ((rc = uegccd_batch_structure_factor(b, t, &v))) return zfail(rc, uegccd_last_error());
+        if ((rc = sf.put(81, sf_block(g, false)))) return rc;
+        if (cc_sf && sf.mp2_in_cc) mp2_80[t] = sf_block(g, true);
+    }
+    std::vector<UegccdResult> br(nset);
+    if (in.do_calc_ta_ccd && !in.do_only_mp2_grid) {
+        rc = uegccd_batch_solve(b, &opt, in.do_drpa_sosex, mp2.data(), br.data());
+        if (rc < 0) return zfail(rc, uegccd_last_error());
     }
     FILE *out = std::fopen("Output", "a");
-    if (!out) {
-        uegccd_batch_destroy(b);
-        return zfail(UEGCCD_ERR_ARG, "cannot append to Output");
-    }
+    if (!out) return zfail(UEGCCD_ERR_ARG, "cannot append to Output");
     std::vector<double> en(1100), dt(1100);
-    for (int t = 0; t < ntw; t++) {
+    for (int t = 0; t < nset; t++) {
         const UegccdSystem &s = systems[t];
         write_mp2(out, hf[t], s.eigen, s.nocc, s.nao, mp2[t]);
+        if (in.do_only_mp2_grid) break;  // "DoOnlyMP2Grid flag is true, so calculation stopping here"
         cc[t] = mp2[t];
         if (in.do_calc_ta_ccd) {
+            if (cc_sf && sf.mp2_in_cc) rc = sf.put(80, mp2_80[t]);
+            if (!rc && cc_sf && sf.ccd) {
+                SfGrids g;
+                const UegccdSfGrid v = g.view(uegccd_sf_length(&s));
+                rc = uegccd_batch_structure_factor(b, t, &v) ? zfail(UEGCCD_ERR_CUDA, uegccd_last_error())
+                                                              : sf.put(80, sf_block(g, true));
+            }
+            if (rc) {
+                std::fclose(out);
+                return rc;
+            }
             int32_t nrec = 0;
             uegccd_batch_history(b, t, en.data(), dt.data(), 1100, &nrec);
             write_cc(out, in, in.do_drpa_sosex, br[t], en.data(), dt.data(), nrec, hf[t]);
@@ -392,7 +516,9 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
         }
     }
     std::fclose(out);
-    uegccd_batch_destroy(b);
+    if (in.do_only_mp2_grid) return UEGCCD_OK;
+    uegccd_batch_destroy(bg.b);   // before the special-twist solve allocates its own
+    bg.b = nullptr;
 
     // fort.59 per-twist rows and fort.58 connectivity rows (Main.f90:144-153)
     FILE *f59 = std::fopen("fort.59", "w");
@@ -477,18 +603,25 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
     uegccd_heg_system(h.h, &sys);
     Amps x(sys), t(sys);
     for (int ip = 0; ip < std::max(1, in.num_rs_points); ip++)
-        if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, ip == 0, &res))) return rc;
+        if ((rc = mp2_then_cc(in, sys, info.ehf, opt, x, t, ip == 0, &res, sf))) return rc;
     return UEGCCD_OK;
 }
 
 int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme)
 {
-    return run_zcode(input_path, twists_path, scheme, true, "fort.60");
+    return run_zcode(input_path, twists_path, scheme, true, "fort.60", "fort.82");
 }
 
 int uegccd_zcode_fort60(const char *input_path, const char *twists_path, const char *out_path)
 {
-    return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, out_path ? out_path : "fort.60");
+    return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, out_path ? out_path : "fort.60", nullptr);
+}
+
+int uegccd_zcode_host_logs(const char *input_path, const char *twists_path, const char *fort60_path,
+                           const char *fort82_path)
+{
+    return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, fort60_path ? fort60_path : "fort.60",
+                     fort82_path);
 }
 
 }  // extern "C"

@@ -22,7 +22,8 @@ class Input(C.Structure):
         ("do_calc_ta_ccd", C.c_int32), ("do_drpa_sosex", C.c_int32), ("do_ks", C.c_int32),
         ("madelung_factor", C.c_double), ("do_single_calc", C.c_int32), ("gap", C.c_double),
         ("fcut", C.c_double), ("corefcut", C.c_double), ("fcut2ecut", C.c_int32), ("gapii", C.c_double),
-        ("do_skip_ta", C.c_int32), ("diagnostics_requested", C.c_int32),
+        ("do_skip_ta", C.c_int32), ("do_sf_calc_mp2", C.c_int32),
+        ("do_sf_calc_ccd", C.c_int32), ("do_only_mp2_grid", C.c_int32),
     ]
 
 
@@ -55,6 +56,7 @@ def _lib():
         L.uegccd_find_tol.argtypes = [C.c_double, P(C.c_double), P(C.c_double), P(C.c_double)]
         L.uegccd_find_tol.restype = None
         L.uegccd_host_last_error.restype = C.c_char_p
+        L.uegccd_heg_exchange_sf.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_double)]
         _bound = True
     return L
 
@@ -117,6 +119,18 @@ class Heg:
     def set_eigen(self, e) -> None:
         e = np.ascontiguousarray(e, dtype=np.float64)
         _check(_lib().uegccd_heg_set_eigen(self._h, e.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def exchange_sf(self) -> dict:
+        """print_ex_SF (HEG.f90:617-674): pair counts n and ExV v on (W,W,W) grids indexed
+        [z+maxq, y+maxq, x+maxq]."""
+        m = C.c_int32()
+        _check(_lib().uegccd_heg_exchange_sf(self._h, C.byref(m), None, None))
+        W = 2 * m.value + 1
+        n = np.zeros((W, W, W), dtype=np.int32)
+        v = np.zeros((W, W, W))
+        _check(_lib().uegccd_heg_exchange_sf(self._h, C.byref(m), n.ctypes.data_as(C.POINTER(C.c_int32)),
+                                             v.ctypes.data_as(C.POINTER(C.c_double))))
+        return dict(maxq=m.value, n=n, v=v)
 
     def system(self):
         """(nocc, L, madelung, eigen copy, nvec (NAO,3) copy)"""

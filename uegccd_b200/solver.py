@@ -4,6 +4,7 @@ Mirrors the reference's driver entry points on the hot path:
     DrvMBPT  (MP2.f90:11)   -> Context.mp2
     DrvCCD   (CCD.f90:18)   -> Context.ccd
     DrvdRPA  (dRPA.f90:23)  -> Context.drpa
+    CCEnergyAndSF (CCD.f90:240), the SF of DrvMBPT (MP2.f90:86) -> Context.structure_factor
 Amplitude arrays use the reference layout T(NOcc,NOcc,NOcc+1:NAO) column-major,
 which is a C-ordered numpy array of shape (V, O, O) indexed [a-O-1, j-1, i-1].
 """
@@ -14,6 +15,19 @@ import ctypes as C
 import numpy as np
 
 from . import _capi as capi
+
+
+def _sf_call(system, call) -> dict:
+    """Runs one structure-factor call into fresh (W,W,W) grids indexed [z+S, y+S, x+S]."""
+    S = capi.lib().uegccd_sf_length(C.byref(system))
+    if S < 0:
+        capi.check(S)
+    W = 2 * S + 1
+    out = {k: np.zeros((W, W, W)) for k in ("sum", "dsum", "xsum", "g", "v")}
+    grid = capi.SfGrid(*(capi.dptr(out[k]) for k in ("sum", "dsum", "xsum", "g", "v")))
+    capi.check(call(C.byref(grid)))
+    out["S"] = S
+    return out
 
 
 class Context:
@@ -80,6 +94,11 @@ class Context:
         capi.check(capi.lib().uegccd_ccd_g2_ex(self._h, capi.dptr(t), mask, precision, capi.dptr(g)))
         return g
 
+    def structure_factor(self, t_abab) -> dict:
+        """CCEnergyAndSF grids of spin-adapted amplitudes: sum, dsum, xsum, g, v and S."""
+        t = np.ascontiguousarray(t_abab, dtype=np.float64)
+        return _sf_call(self._sys, lambda g: capi.lib().uegccd_structure_factor(self._h, capi.dptr(t), g))
+
 
 class Batch:
     """uegccd_batch_*: many independent systems solved together."""
@@ -114,6 +133,16 @@ class Batch:
         res = (capi.Result * self.n)()
         rc = capi.check(capi.lib().uegccd_batch_solve(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2), res))
         return rc, e2, [r.as_dict() for r in res]
+
+    def mp2(self) -> np.ndarray:
+        """DrvMBPT of every system; the MP2 amplitudes stay in the batch.  Returns E(2)."""
+        e2 = np.zeros(self.n)
+        capi.check(capi.lib().uegccd_batch_mp2(self._h, capi.dptr(e2)))
+        return e2
+
+    def structure_factor(self, s: int) -> dict:
+        """Structure-factor grids of solve s from the amplitudes the batch holds."""
+        return _sf_call(self._systems[s], lambda g: capi.lib().uegccd_batch_structure_factor(self._h, s, g))
 
     def set_profiling(self, on: bool) -> None:
         capi.check(capi.lib().uegccd_batch_set_profiling(self._h, 1 if on else 0))

@@ -27,6 +27,8 @@ def _lib():
         L.uegccd_list_real.argtypes = [C.c_double, C.c_char_p, C.c_int32]
         L.uegccd_list_real.restype = C.c_int32
         L.uegccd_zcode.argtypes = [C.c_char_p, C.c_char_p, C.c_int32]
+        L.uegccd_zcode_fort60.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p]
+        L.uegccd_zcode_host_logs.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]
         L.uegccd_zcode_last_error.restype = C.c_char_p
         _bound = True
     return L
@@ -66,8 +68,16 @@ def list_real(x: float) -> str:
     return buf.value.decode()
 
 
+def host_logs(input_path: str = "Input", twists_path: str | None = None, fort60: str = "fort.60",
+              fort82: str | None = "fort.82") -> None:
+    """The program's host set-up alone (no GPU): its fort.60 log and fort.82 exchange
+    structure factors."""
+    enc = lambda x: x.encode() if x else None
+    _check(_lib().uegccd_zcode_host_logs(enc(input_path), enc(twists_path), enc(fort60), enc(fort82)))
+
+
 def run(input_path: str = "Input", twists_path: str | None = None, diis: bool = False) -> None:
-    """The ZCode program in the working directory (writes Output, fort.58, fort.59)."""
+    """The ZCode program in the working directory (writes Output, fort.58-60, fort.80-82)."""
     _check(_lib().uegccd_zcode(input_path.encode(), twists_path.encode() if twists_path else None,
                                _capi.UEGCCD_DIIS if diis else _capi.UEGCCD_REPLAY))
 
