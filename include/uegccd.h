@@ -62,8 +62,8 @@ typedef struct {
 /* Run options; uegccd_default_options() fills the reference's values. */
 typedef struct {
     int32_t do_ring, do_xring, do_ladder, do_mosaic;   /* Input "Do Rings" ... (IO.f90:170-180)   */
-    int32_t core_n;          /* UEGInfo%CoreN; must be 0 (CAS integrals are outside the GPU path) */
-    double gapii;            /* UEGInfo%GapII; must be <= 0                                     */
+    int32_t core_n;          /* UEGInfo%CoreN: integrals with an orbital <= CoreN are zero (CAS) */
+    double gapii;            /* UEGInfo%GapII: integrals above GapII are zero when GapII > 0     */
     int32_t range_flags;     /* sum of |"... Range"| Input values; must be 0                    */
     int32_t max_iter;        /* MaxIter, 1000 (CCD.f90:36)                                      */
     double tol;              /* TolMax on max|dT|, 1e-8 (HEG.f90:1078)                          */
@@ -105,6 +105,16 @@ int uegccd_ctx_destroy(UegccdCtx *ctx);
 /* Replaces the eigenvalues (the twist-averaged-eigenvalue solve, Main.f90:243). */
 int uegccd_ctx_set_eigen(UegccdCtx *ctx, const double *eigen);
 
+/* Integral options of the non-range-separated ERI routines that SetPointers selects
+ * (Main.f90:274-318): core_n = UEGInfo%CoreN zeroes every integral with an orbital
+ * <= CoreN (CoreERI, HEG.f90:835-888); gapii = UEGInfo%GapII > 0 zeroes every integral
+ * above GapII (GapERI, HEG.f90:890-942); both together are NoCaseERI.  They hold for
+ * every later call on the context (MP2, structure factors, G2 terms); uegccd_ccd and
+ * uegccd_drpa set them from their options first.  Defaults 0 and 0: the plain integrals.
+ * Amplitudes of core pairs (i or j <= CoreN) stay zero, as in the reference; amplitudes
+ * passed in are read with their core pairs set to zero. */
+int uegccd_ctx_set_integrals(UegccdCtx *ctx, int32_t core_n, double gapii);
+
 /* DrvMBPT (MP2.f90:11-157): writes the MP2 amplitudes T2aaaa/T2abab/T2abba (each
  * may be NULL) and E(2).  Its structure factor is uegccd_structure_factor of T2abab. */
 int uegccd_mp2(UegccdCtx *ctx, double *t_aaaa, double *t_abab, double *t_abba, double *e2);
@@ -141,7 +151,9 @@ int uegccd_ccd_g2_ex(UegccdCtx *ctx, const double *t_abab, int32_t term_mask, in
  *   dsum  SfDSum: 2*T2abab added, 2*T2abba subtracted
  *   xsum  SfXSum: T2aaaa-T2abab added, T2aaaa-T2abba subtracted
  *   g     SfG:    |q|*2*pi/L at every q that an allowed amplitude reaches, else 0
- *   v     SfV:    V(q) of BaseERI (HEG.f90:969-976) at the same points, else 0
+ *   v     SfV:    at the same points, the integral of the last amplitude reaching q in
+ *                 the reference's loop order: V(q) of BaseERI (HEG.f90:969-976) with the
+ *                 GapII filter, or 0 when that amplitude is a core pair; else 0
  * (MP2.f90 fills sum, g and v only.)  sum.v/2 is the correlation energy of the
  * amplitudes.  A transfer outside the grid returns UEGCCD_ERR_ARG. */
 typedef struct {
@@ -162,6 +174,9 @@ int uegccd_batch_destroy(UegccdBatch *b);
 /* MP2 start + CCD (or dRPA when drpa != 0) of every system; results[n]. */
 int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2,
                        UegccdResult *results);
+/* uegccd_ctx_set_integrals for every system of the batch (uegccd_batch_solve sets
+ * them from its options first). */
+int uegccd_batch_set_integrals(UegccdBatch *b, int32_t core_n, double gapii);
 /* DrvMBPT for every system: the MP2 amplitudes stay in the batch (what
  * uegccd_batch_structure_factor and uegccd_batch_get_amplitudes then read); e2[n]
  * may be NULL. */
@@ -172,7 +187,7 @@ int uegccd_batch_mp2(UegccdBatch *b, double *e2);
 int uegccd_batch_structure_factor(UegccdBatch *b, int32_t s, const UegccdSfGrid *out);
 /* Copies solve s's amplitudes out in the reference layout (T2abab). */
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
-/* E(2) of one system, as uegccd_mp2 computes it, with no device allocation: this
+/* E(2) of one system with the plain integrals, as uegccd_mp2 computes it, with no device allocation: this
  * entry point has no counterpart in the reference.  It is for callers that cannot
  * allocate device memory when they call: a host whose device memory already belongs
  * to its own pool allocator, or one running other streams that must not be stalled

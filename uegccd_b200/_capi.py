@@ -94,6 +94,8 @@ def lib() -> C.CDLL:
         L.uegccd_batch_get_amplitudes.argtypes = [vp, C.c_int32, dp]
         L.uegccd_batch_get_all_amplitudes.argtypes = [vp, dp]
         L.uegccd_batch_mp2.argtypes = [vp, dp]
+        L.uegccd_ctx_set_integrals.argtypes = [vp, C.c_int32, C.c_double]
+        L.uegccd_batch_set_integrals.argtypes = [vp, C.c_int32, C.c_double]
         L.uegccd_sf_length.argtypes = [P(System)]
         L.uegccd_sf_length.restype = C.c_int32
         L.uegccd_structure_factor.argtypes = [vp, dp, P(SfGrid)]

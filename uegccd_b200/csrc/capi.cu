@@ -199,6 +199,10 @@ struct UegccdBatch {
     // solve s at [sf_g0[s], sf_g0[s+1]); one grid of the largest solve
     int2 *sf_groups = nullptr;
     std::vector<int> sf_g0;
+    // integral options (CoreN, GapII) in force, and the unfiltered |q|^2 tables of all solves
+    int core_n = 0;
+    double gapii = 0.0;
+    std::vector<double> vtab_base;
     double *sf_grid = nullptr;
     int *sf_err = nullptr;
 
@@ -324,7 +328,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         S.q2max = P.q2max;
         S.amp0 = amp0;
         S.namp = (int32_t)P.namp;
-        S.pad0 = 0;
+        S.core_n = 0;
         S.pos0 = pos0;
         S.ph0 = ph0;
         S.jvv0 = jvv0;
@@ -508,6 +512,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.nv4, nv4))) return rc;
     if ((rc = b->upload(d.eigen, eigen))) return rc;
     if ((rc = b->upload(d.vtab, vtab))) return rc;
+    b->vtab_base = vtab;
     if ((rc = b->upload(d.hh0, hh0))) return rc;
     if ((rc = b->upload(d.rpairs, rpairs))) return rc;
     if ((rc = b->upload(d.ph_i, ph_i))) return rc;
@@ -601,11 +606,38 @@ int unpack_to_host(UegccdBatch &b, int s, const double *t_dev, double *ab, doubl
     return 0;
 }
 
+// Integral options for every later call on the batch (SetPointers, Main.f90:274-318, with
+// no range flags): GapII > 0 zeroes the integrals above GapII (GapERI, HEG.f90:938-940) --
+// the |q|^2 tables are filtered; CoreN > 0 zeroes those with an index p <= CoreN
+// (CoreERI, HEG.f90:882-885) -- the kernels hold core pairs at zero.  The per-amplitude
+// Coulomb factors are rebuilt from the filtered tables.
+int set_integrals(UegccdBatch &b, int core_n, double gapii)
+{
+    if (core_n < 0) return fail(UEGCCD_ERR_ARG, "CoreN must be >= 0");
+    for (const auto &P : b.plans)
+        if (core_n > P.O) return fail(UEGCCD_ERR_ARG, "CoreN exceeds NOcc");
+    const double g = gapii > 0.0 ? gapii : 0.0;
+    if (core_n == b.core_n && g == b.gapii) return 0;
+    std::vector<double> vt(b.vtab_base);
+    if (g > 0.0)
+        for (auto &v : vt)
+            if (v > g) v = 0.0;
+    CU(cudaMemcpyAsync(b.d.vtab, vt.data(), vt.size() * sizeof(double), cudaMemcpyHostToDevice, b.stream));
+    for (auto &S : b.hsolves) S.core_n = core_n;
+    CU(cudaMemcpyAsync(b.d.solves, b.hsolves.data(), b.hsolves.size() * sizeof(SolveDev), cudaMemcpyHostToDevice,
+                       b.stream));
+    launch_vcoef(b.d, b.stream);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(b.stream));
+    b.h2d_bytes += (int64_t)(vt.size() * sizeof(double) + b.hsolves.size() * sizeof(SolveDev));
+    b.core_n = core_n;
+    b.gapii = g;
+    return 0;
+}
+
 int validate_options(const UegccdOptions *o, int drpa)
 {
     if (!o) return fail(UEGCCD_ERR_ARG, "null options");
-    if (o->core_n != 0) return fail(UEGCCD_ERR_UNSUPPORTED, "CoreN > 0 (CAS integrals) is outside the GPU path");
-    if (o->gapii > 0.0) return fail(UEGCCD_ERR_UNSUPPORTED, "GapII > 0 is outside the GPU path");
     if (o->range_flags != 0) return fail(UEGCCD_ERR_UNSUPPORTED, "range-separated integrals are outside the GPU path");
     if (!drpa && (o->do_ring != 0) != (o->do_xring != 0))
         return fail(UEGCCD_ERR_UNSUPPORTED,
@@ -825,7 +857,8 @@ int sf_length(const SystemHost &h)
 // Structure factors of solve s from the batch's amplitudes: the sums on the device
 // (k_sf), then SfG and SfV -- functions of q alone -- at the points the sums reached,
 // with the reference's expressions: SfG = (|q|^2 (2 pi/L)^2)**0.5 (dK2scaled,
-// HEG.f90:1011-1031), SfV = BaseERI (HEG.f90:969-976).
+// HEG.f90:1011-1031), SfV = the integral of the last contribution in the reference's
+// loop order: BaseERI (HEG.f90:969-976) with the GapII filter, 0 for a core pair.
 int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
 {
     DevBatch &d = b.d;
@@ -842,13 +875,13 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
             w3max = std::max(w3max, w * w * w);
         }
         if ((rc = b.upload(b.sf_groups, g))) return rc;
-        if ((rc = b.alloc(b.sf_grid, 4 * (size_t)w3max))) return rc;
+        if ((rc = b.alloc(b.sf_grid, 5 * (size_t)w3max))) return rc;
         if ((rc = b.alloc(b.sf_err, 1))) return rc;
     }
     const SystemHost &H = b.sys[s];
     const int S = sf_length(H);
     const int64_t W = 2 * S + 1, W3 = W * W * W;
-    CU(cudaMemsetAsync(b.sf_grid, 0, 4 * (size_t)W3 * sizeof(double), b.stream));
+    CU(cudaMemsetAsync(b.sf_grid, 0, 5 * (size_t)W3 * sizeof(double), b.stream));
     CU(cudaMemsetAsync(b.sf_err, 0, sizeof(int), b.stream));
     launch_sf(d, b.sf_groups + b.sf_g0[s], b.sf_g0[s + 1] - b.sf_g0[s], s, S, b.sf_grid, b.sf_err, b.stream);
     b.launches++;
@@ -856,12 +889,15 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
     double *dst[3] = {out.sum, out.dsum, out.xsum};
     for (int k = 0; k < 3; k++)
         if (dst[k]) CU(cudaMemcpyAsync(dst[k], b.sf_grid + k * W3, W3 * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
-    std::vector<double> cnt(W3);
-    CU(cudaMemcpyAsync(cnt.data(), b.sf_grid + 3 * W3, W3 * sizeof(double), cudaMemcpyDeviceToHost, b.stream));
+    // contributions, and where the last one is a core pair (read under CoreN only)
+    const int ntail = b.core_n > 0 ? 2 : 1;
+    std::vector<double> cnt((size_t)ntail * W3);
+    CU(cudaMemcpyAsync(cnt.data(), b.sf_grid + 3 * W3, ntail * W3 * sizeof(double), cudaMemcpyDeviceToHost,
+                       b.stream));
     int err = 0;
     CU(cudaMemcpyAsync(&err, b.sf_err, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
     CU(cudaStreamSynchronize(b.stream));
-    b.d2h_bytes += (int64_t)((3 + 1) * W3 * sizeof(double));
+    b.d2h_bytes += (int64_t)((3 + ntail) * W3 * sizeof(double));
     if (err) return fail(UEGCCD_ERR_ARG, "a momentum transfer falls outside the structure-factor grid");
     const double c = 2.0 * kPi / H.L, scale = c * c;
     for (int64_t z = 0; z < W; z++)
@@ -873,6 +909,8 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
                     const int q2 = (int)((x - S) * (x - S) + (y - S) * (y - S) + (z - S) * (z - S));
                     g = std::pow((double)q2 * scale, 0.5);
                     v = coulomb_v(H.L, H.madelung, q2);
+                    if (b.gapii > 0.0 && v > b.gapii) v = 0.0;        // GapERI
+                    if (ntail == 2 && cnt[W3 + k] != 0.0) v = 0.0;    // CoreERI of the last pair
                 }
                 if (out.g) out.g[k] = g;
                 if (out.v) out.v[k] = v;
@@ -929,6 +967,18 @@ int uegccd_ctx_set_eigen(UegccdCtx *c, const double *eigen)
     return 0;
 }
 
+int uegccd_ctx_set_integrals(UegccdCtx *c, int32_t core_n, double gapii)
+{
+    if (!c) return fail(UEGCCD_ERR_ARG, "null context");
+    return set_integrals(*c->batch, core_n, gapii);
+}
+
+int uegccd_batch_set_integrals(UegccdBatch *b, int32_t core_n, double gapii)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    return set_integrals(*b, core_n, gapii);
+}
+
 int uegccd_mp2(UegccdCtx *c, double *t_aaaa, double *t_abab, double *t_abba, double *e2)
 {
     if (!c) return fail(UEGCCD_ERR_ARG, "null context");
@@ -953,6 +1003,7 @@ int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t
     int rc = validate_options(opt, 0);
     if (rc) return rc;
     UegccdBatch &b = *c->batch;
+    if ((rc = set_integrals(b, opt->core_n, opt->gapii))) return rc;
     if ((rc = pack_from_host(b, 0, t_abab))) return rc;
     int st = run_solves(b, opt, 0, res);
     if (st < 0) return st;
@@ -966,6 +1017,7 @@ int uegccd_drpa(UegccdCtx *c, const UegccdOptions *opt, double *t2, UegccdResult
     int rc = validate_options(opt, 1);
     if (rc) return rc;
     UegccdBatch &b = *c->batch;
+    if ((rc = set_integrals(b, opt->core_n, opt->gapii))) return rc;
     if ((rc = pack_from_host(b, 0, t2))) return rc;
     int st = run_solves(b, opt, 1, res);
     if (st < 0) return st;
@@ -1056,6 +1108,7 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
     if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
     int rc = validate_options(opt, drpa);
     if (rc) return rc;
+    if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
     CU(cudaEventRecord(b->ev_solve0, b->stream));
     b->kt.begin(KID_MP2, b->stream);
     launch_mp2(b->d, b->stream);

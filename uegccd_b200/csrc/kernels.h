@@ -160,8 +160,9 @@ void launch_pack(const DevBatch &d, int s, int namp, const double *dense, cudaSt
 void launch_vcoef(const DevBatch &d, cudaStream_t st);
 void launch_unpack_all(const DevBatch &d, const int64_t *dense_off, const double *t, double *out, cudaStream_t st);
 // Structure-factor sums of solve `solve` from d.t: groups = its particle-hole groups
-// {first row, rows}; grid = 4 arrays of (2S+1)^3 (SfSum, SfDSum, SfXSum, contributions),
-// column-major from -S, zeroed by the caller; *err = 1 if a transfer falls outside.
+// {first row, rows}; grid = 5 arrays of (2S+1)^3 (SfSum, SfDSum, SfXSum, contributions,
+// 1 where the reference's last contribution is a core pair), column-major from -S,
+// zeroed by the caller; *err = 1 if a transfer falls outside.
 void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, int S, double *grid, int *err,
                cudaStream_t st);
 // pos (pre-set to -1), amps, partner, then the ring gather indices, from the block structure

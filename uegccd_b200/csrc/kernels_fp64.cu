@@ -104,7 +104,8 @@ __global__ void k_mp2(const ChunkDev *__restrict__ chunks, const SolveDev *__res
         double denom = ev[q.i] + ev[q.j] - ev[q.a] - ev[q.b];
         double via = vpq(s, nv4, vtab, q.i, q.a);
         double vib = vpq(s, nv4, vtab, q.i, q.b);
-        double x = via / denom;
+        // a core pair's integrals are zero (CoreERI), so is its amplitude
+        double x = (q.i < s.core_n || q.j < s.core_n) ? 0.0 : via / denom;
         t[p] = x;
         e = x * (2.0 * via - vib);
         mx = fabs(x);
@@ -1195,6 +1196,7 @@ __global__ void __launch_bounds__(kChunk) k_update(UpdateArgs A)
             if (A.do_ring) g += A.g_rq[p];   // rings, linear + quadratic (CCD.f90:716-811)
             if (A.do_xring) g += A.g_xq[p];  // crossed rings (CCD.f90:845-937)
         }
+        if (i < s.core_n || j < s.core_n) g = 0.0;  // core pair: every term has a zero factor
         if (A.g_out) A.g_out[p] = g;
         const double *ev = A.eigen + s.orb0;
         const double denom = ev[i] + ev[j] - ev[a] - ev[b];
@@ -1476,7 +1478,8 @@ __global__ void k_pack(const SolveDev *__restrict__ solves, int sidx, const AmpI
     if (loc >= s.namp) return;
     int64_t p = s.amp0 + loc;
     AmpInfo q = amps[p];
-    t[p] = dense[q.i + (int64_t)s.O * q.j + (int64_t)s.O * s.O * (q.a - s.O)];
+    // core pairs are held at zero (their integrals are zero; see uegccd_internal.h)
+    t[p] = (q.i < s.core_n || q.j < s.core_n) ? 0.0 : dense[q.i + (int64_t)s.O * q.j + (int64_t)s.O * s.O * (q.a - s.O)];
 }
 
 // writes T2abab, T2abba = -t(ij,b), T2aaaa = t(ij,a) - t(ij,b) (any may be null);
@@ -1538,12 +1541,16 @@ __global__ void __launch_bounds__(kSfThreads)
 {
     const int2 G = groups[blockIdx.x];   // rows [G.x, G.x + G.y) of the solve
     const SolveDev s = solves[solve];
-    const int O = s.O;
+    const int O = s.O, V = s.V;
     double sum = 0.0, dsum = 0.0, xsum = 0.0, cnt = 0.0;
+    // position of the last contribution in the reference's loop order (I, J, A, then
+    // direct before exchange): its SfV assignment is the one that stays
+    long long last = -1;
     const int n = G.y * O;
     for (int e = threadIdx.x; e < n; e += kSfThreads) {
         const int r = G.x + e / O, k = e - (e / O) * O;
         const int64_t ri = s.ph0 + (int64_t)r * O + k;
+        const int ir = ph_i[s.phr0 + r], xr = ph_x[s.phr0 + r] - O;
         const int pd = __ldg(&ridx_x[ri]);
         if (pd >= 0) {  // direct: (I,J,A) = (i,k,x)
             const double tab = __ldg(&t[pd]), tba = -__ldg(&t[__ldg(&partner[pd])]);
@@ -1552,6 +1559,7 @@ __global__ void __launch_bounds__(kSfThreads)
             dsum += 2.0 * tab;
             xsum += taa - tab;
             cnt += 1.0;
+            last = max(last, (((long long)ir * O + k) * V + xr) * 2);
         }
         const int px = __ldg(&ridx_y[ri]);
         if (px >= 0) {  // exchange: (I,J,A) = (k,i,x)
@@ -1561,17 +1569,22 @@ __global__ void __launch_bounds__(kSfThreads)
             dsum -= 2.0 * tba;
             xsum -= taa - tba;
             cnt += 1.0;
+            last = max(last, (((long long)k * O + ir) * V + xr) * 2 + 1);
         }
     }
     __shared__ double red[4][kSfThreads / 32];
+    __shared__ long long red_last[kSfThreads / 32];
     double v[4] = {sum, dsum, xsum, cnt};
 #pragma unroll
     for (int q = 0; q < 4; q++)
         for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    for (int o = 16; o > 0; o >>= 1) last = max(last, __shfl_down_sync(0xffffffffu, last, o));
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0)
+    if (l == 0) {
 #pragma unroll
         for (int q = 0; q < 4; q++) red[q][w] = v[q];
+        red_last[w] = last;
+    }
     __syncthreads();
     if (threadIdx.x != 0) return;
     double tot[4];
@@ -1580,7 +1593,12 @@ __global__ void __launch_bounds__(kSfThreads)
         tot[q] = red[q][0];
         for (int k = 1; k < kSfThreads / 32; k++) tot[q] += red[q][k];
     }
+    for (int k = 1; k < kSfThreads / 32; k++) last = max(last, red_last[k]);
+    last = max(last, red_last[0]);
     if (tot[3] == 0.0) return;   // no stored amplitude reaches this transfer
+    // the last tuple (I,J): a core pair leaves SfV = 0 (its integral is zero under CoreN)
+    const long long ij = (last >> 1) / V;
+    const bool last_core = (int)(ij / O) < s.core_n || (int)(ij % O) < s.core_n;
     const int i = ph_i[s.phr0 + G.x], x = ph_x[s.phr0 + G.x];
     const int4 a = nv4[s.orb0 + x], b = nv4[s.orb0 + i];
     const int q0 = a.x - b.x, q1 = a.y - b.y, q2 = a.z - b.z;
@@ -1594,6 +1612,7 @@ __global__ void __launch_bounds__(kSfThreads)
     grid[W3 + c] = tot[1];
     grid[2 * W3 + c] = tot[2];
     grid[3 * W3 + c] = tot[3];
+    grid[4 * W3 + c] = last_core ? 1.0 : 0.0;
 }
 
 void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, int S, double *grid, int *err,

@@ -11,6 +11,14 @@
 // reference's other channels follow from it: T2abba(i,j,a) = -t(ij,b) and
 // T2aaaa(i,j,a) = t(ij,a) - t(ij,b).
 //
+// Integral options.  GapII (GapERI, HEG.f90:890-942) zeroes every integral above
+// GapII: it is a filter on the |q|^2 table.  CoreN (CoreERI) zeroes every integral
+// with a core index.  In every CCD, MP2 and dRPA term each internal occupied index
+// appears in the integral and in an amplitude, so for a non-core (i,j) the core
+// integrals only ever multiply core amplitudes; and every term of a core (i,j) has
+// a core integral or a core amplitude.  With the core amplitudes held at zero the
+// unmasked sums are therefore exact: the kernels zero t and G of core pairs only.
+//
 // Many independent solves (twists, rs values, basis sizes) live in one batch:
 // every per-solve array is concatenated and addressed through SolveDev offsets.
 #pragma once
@@ -27,7 +35,7 @@ struct SolveDev {
     int vtab0, q2max;       // Coulomb table: vtab[vtab0 + |q|^2], |q|^2 <= q2max
     int64_t amp0;           // first packed amplitude (global index)
     int32_t namp;           // number of stored amplitudes
-    int32_t pad0;
+    int32_t core_n;         // UEGInfo%CoreN: orbitals p < core_n are core (CoreERI, HEG.f90:835-888)
     int64_t pos0;           // offset of the dense (i,j,a) -> packed map (O*O*V entries)
     int64_t ph0;            // offset of the ring intermediates (O*V*O entries each)
     int32_t jvv0, joo0;     // offsets of the mosaic intermediates (V and O entries)

@@ -2,8 +2,8 @@
 // function, with its hot path on the GPU through include/uegccd.h.
 //
 // Steps of uegccd_zcode (Main.f90 line ranges):
-//   44-48    ReadInput, init_HEG (the GPU path serves the default integrals;
-//            other ERI selections are refused by the option checks)
+//   44-48    ReadInput, init_HEG; SetPointers' integrals: CoreN and GapII are
+//            served (CoreERI, GapERI, NoCaseERI), range flags are refused
 //   78-79    change_rs to rSMin
 //   83-93    DoSingleCalc: MP2, then CCD or dRPA from the MP2 amplitudes
 //   95-97    DoSkipTA: stop after the single calculation
@@ -219,7 +219,8 @@ int mp2_then_cc(const UegccdInput &in, const UegccdSystem &sys, double ehf, cons
     UegccdCtx *ctx = nullptr;
     if (uegccd_ctx_create(&sys, &ctx)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
     double e2 = 0.0;
-    int rc = uegccd_mp2(ctx, x.aaaa.data(), x.abab.data(), x.abba.data(), &e2);
+    int rc = uegccd_ctx_set_integrals(ctx, opt.core_n, opt.gapii);  // the ERI that SetPointers chose
+    if (!rc) rc = uegccd_mp2(ctx, x.aaaa.data(), x.abab.data(), x.abba.data(), &e2);
     if (rc) {
         zfail(rc, uegccd_last_error());
         uegccd_ctx_destroy(ctx);
@@ -473,7 +474,8 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
     } bg;
     if (uegccd_batch_create(systems.data(), nset, &bg.b)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
     UegccdBatch *b = bg.b;
-    if ((rc = uegccd_batch_mp2(b, mp2.data()))) return zfail(rc, uegccd_last_error());
+    if ((rc = uegccd_batch_set_integrals(b, opt.core_n, opt.gapii)) || (rc = uegccd_batch_mp2(b, mp2.data())))
+        return zfail(rc, uegccd_last_error());
     const bool cc_sf = in.do_calc_ta_ccd && !in.do_drpa_sosex;
     std::vector<std::string> mp2_80(nset);   // DrvCCD's DoSFCalcMP2 blocks, written beside the CCD ones
     for (int t = 0; t < nset; t++) {

@@ -60,6 +60,10 @@ class Context:
         e = np.ascontiguousarray(eigen, dtype=np.float64)
         capi.check(capi.lib().uegccd_ctx_set_eigen(self._h, capi.dptr(e)))
 
+    def set_integrals(self, core_n: int = 0, gapii: float = 0.0) -> None:
+        """CoreN and GapII of the integrals for the calls that follow (CoreERI/GapERI)."""
+        capi.check(capi.lib().uegccd_ctx_set_integrals(self._h, int(core_n), float(gapii)))
+
     def mp2(self):
         """DrvMBPT: returns (E2, T2aaaa, T2abab, T2abba)."""
         ta, tb, tc = self.zeros_t(), self.zeros_t(), self.zeros_t()
@@ -133,6 +137,10 @@ class Batch:
         res = (capi.Result * self.n)()
         rc = capi.check(capi.lib().uegccd_batch_solve(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2), res))
         return rc, e2, [r.as_dict() for r in res]
+
+    def set_integrals(self, core_n: int = 0, gapii: float = 0.0) -> None:
+        """CoreN and GapII of the integrals for the calls that follow (CoreERI/GapERI)."""
+        capi.check(capi.lib().uegccd_batch_set_integrals(self._h, int(core_n), float(gapii)))
 
     def mp2(self) -> np.ndarray:
         """DrvMBPT of every system; the MP2 amplitudes stay in the batch.  Returns E(2)."""
