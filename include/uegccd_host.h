@@ -38,6 +38,7 @@ typedef struct {
     int32_t do_sf_calc_mp2;          /* DoSFCalcMP2: fort.80 block of the start amplitudes in DrvCCD */
     int32_t do_sf_calc_ccd;          /* DoSFCalcCCD: fort.80 block of the converged amplitudes        */
     int32_t do_only_mp2_grid;        /* DoOnlyMP2Grid: stop after the first DrvMBPT (MP2.f90:152-154) */
+    int32_t core_factor_set;         /* the Input sets CoreFactor (ReadInput then writes fort.61)    */
 } UegccdInput;
 
 typedef struct {
@@ -85,7 +86,7 @@ int uegccd_special_twist(int32_t ntwists, const int32_t *conn, double *conn_avg,
  * them: a blank, then 17 significant digits in a G25 field.  Returns its length. */
 int32_t uegccd_list_real(double x, char *buf, int32_t len);
 /* The whole program in the working directory: reads input_path (NULL: "Input"),
- * writes Output, fort.58, fort.59, fort.60, the structure factors fort.81 (every
+ * writes Output, fort.58, fort.59, fort.60, fort.61, the structure factors fort.81 (every
  * DrvMBPT) and fort.82 (every print_HF), and fort.80 when DoSFCalcMP2/DoSFCalcCCD
  * are set.  twists_path (may be NULL) lists the twist
  * angles of the average, three numbers per line; missing ones are drawn from a
@@ -97,9 +98,10 @@ int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme
  * into out_path (NULL: "fort.60"). */
 int uegccd_zcode_fort60(const char *input_path, const char *twists_path, const char *out_path);
 /* The same with the exchange structure factors (fort.82) of the set-up into
- * fort82_path as well (NULL: not written). */
+ * fort82_path and ReadInput's core/active electron counts (fort.61, IO.f90:233-234,
+ * written when the Input sets CoreFactor) into fort61_path as well (NULL: not written). */
 int uegccd_zcode_host_logs(const char *input_path, const char *twists_path, const char *fort60_path,
-                           const char *fort82_path);
+                           const char *fort82_path, const char *fort61_path);
 const char *uegccd_zcode_last_error(void);
 
 #ifdef __cplusplus

@@ -108,6 +108,7 @@ def g5(ref):
                 special_twist=special, special_ec_ccd=ecs[-1], special_niter=conv[-1],
                 output_lines=lines, fort59_lines=f59,
                 fort60_lines=open(os.path.join(d, "fort.60")).read().splitlines(),
+                fort61_lines=open(os.path.join(d, "fort.61")).read().splitlines(),
                 source="source/Test/Output, source/Test/fort.59")
 
 
@@ -122,6 +123,7 @@ def g3(ref):
     conv = [int(re.search(r"in\s+(\d+)", l).group(1)) for l in lines if "converged in" in l]
     return dict(input_text=text, twists=[r[:3] for r in rows], hf_mp2_ccd=[r[3:6] for r in rows],
                 special_twist=special, special_ec_ccd=ecs[-1], special_niter=conv[-1],
+                fort61_lines=open(os.path.join(d, "fort.61")).read().splitlines(),
                 source="benchmarks/ZRun-v6-N14/fort.59, Output")
 
 

@@ -63,6 +63,7 @@ def test_g5_output_and_fort59(goldens, tmp_path, monkeypatch):
     f60 = (tmp_path / "fort.60").read_text().splitlines()
     ref60 = [l.replace(" om:", " Omega:", 1) if l.startswith(" om:") else l for l in g["fort60_lines"]]
     assert len(f60) > 800 and f60 == ref60[: len(f60)]
+    assert (tmp_path / "fort.61").read_text().splitlines() == g["fort61_lines"]
 
 
 def test_g3_hundred_twists_ccd(goldens, tmp_path, monkeypatch):
@@ -102,3 +103,27 @@ def test_g1_drpa_executable(goldens, tmp_path):
     e2 = float(re.search(r"E\(2\) is\s+(-?\d+\.\d+)", out).group(1))
     assert abs(e2 - g["e2"]) < 2e-12
     assert not (tmp_path / "fort.59").exists()   # TACalcN 0: no twist average
+
+
+def test_ta_program_with_core_and_gap(goldens, tmp_path, monkeypatch):
+    """The G5 program (source/Test) on 4 twists with CoreFactor 0.25 (CoreN = 3) and
+    GapII 0.01 (NoCaseERI; the |q|^2 = 1 integrals are cut): every twist's E_HF and
+    E_MP2 in fort.59 and the special-twist Ec(CCD) against the oracle's twist average."""
+    from oracle.oracle import Oracle, parse_input_text
+
+    g = goldens["G5"]
+    keys = dict(g["keys"])
+    keys.update({"CoreFactor": "0.25", "GapII": "0.01", "TACalcN": "4"})
+    (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))
+    _write_twists(tmp_path / "Twists", g["ta_twists"][:4])
+    monkeypatch.chdir(tmp_path)
+    zcode.run("Input", "Twists")
+    rows = np.array([[float(x) for x in l.split()] for l in (tmp_path / "fort.59").read_text().splitlines()[:4]])
+    vals = parse_input_text("")
+    vals.update(keys)
+    per, special, st, _ = Oracle(vals).twist_average(np.array(g["ta_twists"][:4]))
+    np.testing.assert_allclose(rows[:, 3:6], per, rtol=0, atol=1e-12)
+    out = (tmp_path / "Output").read_text()
+    ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
+    assert abs(ecs[-1] - st.ecorr) < 1e-9
+    assert (tmp_path / "fort.61").read_text().split() == ["6", "core", "electrons", "18", "active", "electrons"]

@@ -148,3 +148,20 @@ def test_fort60_log_matches_reference(goldens, tmp_path, monkeypatch):
     tail = ref[len(ours):]
     assert tail[2].strip() == "Calculating Madelung Constant - Fraser et al. PRB 53 4 1814"
     assert sum(1 for l in tail if l.startswith(" Omega:")) == 1
+
+
+def test_fort61_matches_reference(goldens, tmp_path, monkeypatch):
+    """fort.61, ReadInput's core and active electron counts (IO.f90:232-234), against the
+    reference's source/Test/fort.61 (G5) and benchmarks/ZRun-v6-N14/fort.61 (G3), and for
+    CoreFactor 0.3 at N=14 (CoreN = int(7*0.3) = 2)."""
+    monkeypatch.chdir(tmp_path)
+    g5 = goldens["G5"]
+    cases = [("".join(f"{k}: {v}\n" for k, v in g5["keys"].items()), g5["fort61_lines"]),
+             (goldens["G3"]["input_text"], goldens["G3"]["fort61_lines"]),
+             (goldens["G3"]["input_text"].replace("CoreFactor:       0.0", "CoreFactor:       0.3")
+              .replace("TACalcN:          100", "TACalcN:          2"),
+              ["           4 core electrons", "          10 active electrons"])]
+    for text, want in cases:
+        (tmp_path / "Input").write_text(text)
+        zcode.host_logs("Input", None, "fort.60", None, "fort.61")
+        assert (tmp_path / "fort.61").read_text().splitlines() == want

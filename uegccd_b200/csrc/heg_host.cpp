@@ -399,7 +399,10 @@ int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
             vs >> r;
             in->range_flags += std::abs(r);
         } else if (key == "NTwist") vs >> in->ntwist[0] >> in->ntwist[1] >> in->ntwist[2];
-        else if (key == "CoreFactor") vs >> in->core_factor;
+        else if (key == "CoreFactor") {
+            vs >> in->core_factor;
+            in->core_factor_set = 1;
+        }
         else if (key == "TACalcN") vs >> in->tacalcn;
         else if (key == "DoCalcTACCD") in->do_calc_ta_ccd = parse_bool(val);
         else if (key == "DodRPASOSEX") in->do_drpa_sosex = parse_bool(val);

@@ -376,11 +376,20 @@ int32_t uegccd_list_real(double x, char *buf, int32_t len)
 // The program; gpu = false runs only the host set-up (it writes the fort.60 log, and
 // fort.82 when f82_path is given).
 static int run_zcode(const char *input_path, const char *twists_path, int32_t scheme, bool gpu, const char *log_path,
-                     const char *f82_path)
+                     const char *f82_path, const char *f61_path)
 {
     UegccdInput in;
     if (uegccd_read_input(input_path ? input_path : "Input", 0, &in))
         return zfail(UEGCCD_ERR_ARG, std::string("ReadInput: ") + uegccd_host_last_error());
+    if (f61_path && in.core_factor_set) {
+        // ReadInput's CAS counts (IO.f90:232-234)
+        const int core_n = (int)((in.nelectron / 2) * in.core_factor);
+        FILE *f = std::fopen(f61_path, "w");
+        if (!f) return zfail(UEGCCD_ERR_ARG, "cannot write fort.61");
+        std::fprintf(f, "%s\n%s\n", (ld_int(core_n * 2) + ld_str("core electrons")).c_str(),
+                     (ld_int(in.nelectron - core_n * 2) + ld_str("active electrons")).c_str());
+        std::fclose(f);
+    }
     // fort.60 (set-up log) and fort.82 (exchange structure factors): collected while the
     // program runs and written at the end
     struct LogFile {
@@ -611,19 +620,19 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
 
 int uegccd_zcode(const char *input_path, const char *twists_path, int32_t scheme)
 {
-    return run_zcode(input_path, twists_path, scheme, true, "fort.60", "fort.82");
+    return run_zcode(input_path, twists_path, scheme, true, "fort.60", "fort.82", "fort.61");
 }
 
 int uegccd_zcode_fort60(const char *input_path, const char *twists_path, const char *out_path)
 {
-    return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, out_path ? out_path : "fort.60", nullptr);
+    return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, out_path ? out_path : "fort.60", nullptr, nullptr);
 }
 
 int uegccd_zcode_host_logs(const char *input_path, const char *twists_path, const char *fort60_path,
-                           const char *fort82_path)
+                           const char *fort82_path, const char *fort61_path)
 {
     return run_zcode(input_path, twists_path, UEGCCD_REPLAY, false, fort60_path ? fort60_path : "fort.60",
-                     fort82_path);
+                     fort82_path, fort61_path);
 }
 
 }  // extern "C"

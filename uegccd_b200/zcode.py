@@ -28,7 +28,7 @@ def _lib():
         L.uegccd_list_real.restype = C.c_int32
         L.uegccd_zcode.argtypes = [C.c_char_p, C.c_char_p, C.c_int32]
         L.uegccd_zcode_fort60.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p]
-        L.uegccd_zcode_host_logs.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]
+        L.uegccd_zcode_host_logs.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]
         L.uegccd_zcode_last_error.restype = C.c_char_p
         _bound = True
     return L
@@ -69,15 +69,16 @@ def list_real(x: float) -> str:
 
 
 def host_logs(input_path: str = "Input", twists_path: str | None = None, fort60: str = "fort.60",
-              fort82: str | None = "fort.82") -> None:
-    """The program's host set-up alone (no GPU): its fort.60 log and fort.82 exchange
-    structure factors."""
+              fort82: str | None = "fort.82", fort61: str | None = "fort.61") -> None:
+    """The program's host set-up alone (no GPU): its fort.60 log, fort.82 exchange
+    structure factors and fort.61 core/active electron counts."""
     enc = lambda x: x.encode() if x else None
-    _check(_lib().uegccd_zcode_host_logs(enc(input_path), enc(twists_path), enc(fort60), enc(fort82)))
+    _check(_lib().uegccd_zcode_host_logs(enc(input_path), enc(twists_path), enc(fort60), enc(fort82),
+                                         enc(fort61)))
 
 
 def run(input_path: str = "Input", twists_path: str | None = None, diis: bool = False) -> None:
-    """The ZCode program in the working directory (writes Output, fort.58-60, fort.80-82)."""
+    """The ZCode program in the working directory (writes Output, fort.58-61, fort.80-82)."""
     _check(_lib().uegccd_zcode(input_path.encode(), twists_path.encode() if twists_path else None,
                                _capi.UEGCCD_DIIS if diis else _capi.UEGCCD_REPLAY))
 
