@@ -164,6 +164,26 @@ int32_t uegccd_sf_length(const UegccdSystem *sys);
 /* The structure factor of spin-adapted amplitudes t_abab (reference layout). */
 int uegccd_structure_factor(UegccdCtx *ctx, const double *t_abab, const UegccdSfGrid *out);
 
+/* ---- DIIS for a host-side iteration loop (DIISCC.f90:10-155) -------------------
+ * A history of ndiis (T, R) pairs of n amplitudes on the device, one object per
+ * amplitude channel (the reference keeps one for T2abab and one for T2abba).
+ *   uegccd_diis_create  SetUpDIISCC: t0 (may be NULL) is the newest T until the first push.
+ *   uegccd_diis_push    the pair of this iteration: T after the update, R = -G + D.T
+ *                       (what CnvrgCC and GetRes store); the oldest pair is dropped.
+ *   uegccd_diis_get_t   GetTFromDIIS: the next T into t2.  UEGCCD_REPLAY gives the
+ *                       newest T, as the reference's singular solve does
+ *                       (DIISCC.f90:110-125); UEGCCD_DIIS extrapolates over the
+ *                       pairs held once niter >= ndiis + 5 (the reference's IWait):
+ *                       B(i,j) = R(i).R(j), [B 1; 1 0][c; y] = [0; 1], T = sum c(i) T(i);
+ *                       a singular B gives the newest T.
+ *   uegccd_diis_destroy ShutDownDIISCC.
+ * Arrays are host arrays of n doubles (any layout, the same in every call). */
+typedef struct UegccdDiis UegccdDiis;
+int uegccd_diis_create(int64_t n, int32_t ndiis, int32_t scheme, const double *t0, UegccdDiis **out);
+int uegccd_diis_push(UegccdDiis *d, const double *t, const double *r);
+int uegccd_diis_get_t(UegccdDiis *d, int32_t niter, double *t2);
+int uegccd_diis_destroy(UegccdDiis *d);
+
 /* ---- many independent solves in one launch per residual term ---------------- */
 typedef struct UegccdBatch UegccdBatch;
 

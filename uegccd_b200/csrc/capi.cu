@@ -844,6 +844,8 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
 namespace uegccd {
 // The message uegccd_last_error returns, for entry points defined in other files.
 int set_last_error(int code, const char *msg) { return fail(code, msg); }
+// 0 when a compute-capability-10 device is current, else an error status (message set).
+int device_ok() { return check_device(); }
 }  // namespace uegccd
 
 // SendForAllocation (HEG.f90:1051-1065): SfLength = maxval(nVec)*2+1
