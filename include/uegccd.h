@@ -224,7 +224,9 @@ int uegccd_mp2_energy_static(const UegccdSystem *sys, void *stream, double *e2);
 
 /* T2abab of every solve of the batch in the reference layout, solve after solve: solve s
  * fills NOcc_s * NOcc_s * (NAO_s - NOcc_s) doubles (the batched form of
- * uegccd_batch_get_amplitudes: one device-to-host copy for the whole batch). */
+ * uegccd_batch_get_amplitudes: one device-to-host copy for the whole batch).  A
+ * page-locked t_abab (cudaHostAlloc / cudaHostRegister) receives the copy directly;
+ * pageable memory goes through a cached pinned buffer. */
 int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab);
 /* A destroyed batch leaves its device memory in a small per-process cache (at most
  * 8 GiB) that the next batch reuses, and large amplitude downloads keep a pinned host

@@ -1223,7 +1223,11 @@ int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab)
     CU(cudaGetLastError());
     const size_t bytes = b->dense_all_n * sizeof(double);
     b->d2h_bytes += (int64_t)bytes;
-    if (bytes < kStageMin) {
+    // a page-locked destination takes the copy directly
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, t_abab) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    if (!pinned) cudaGetLastError();   // clear the query's status on older drivers
+    if (bytes < kStageMin || pinned) {
         CU(cudaMemcpyAsync(t_abab, b->dense_all, bytes, cudaMemcpyDeviceToHost, b->stream));
         CU(cudaStreamSynchronize(b->stream));
         return UEGCCD_OK;

@@ -174,13 +174,20 @@ class Batch:
         capi.check(capi.lib().uegccd_batch_get_amplitudes(self._h, s, capi.dptr(t)))
         return t
 
-    def all_amplitudes(self) -> list:
-        """T2abab of every solve (views into one host buffer, one device-to-host copy)."""
+    def amplitude_count(self) -> int:
+        """Doubles that all_amplitudes fills (every solve's NOcc^2 (NAO - NOcc))."""
+        return sum(int(np.prod(sh)) for sh in self._shapes)
+
+    def all_amplitudes(self, out: np.ndarray | None = None) -> list:
+        """T2abab of every solve (views into one host buffer, one device-to-host copy);
+        out: a float64 buffer of amplitude_count() entries to fill (page-locked memory
+        takes the copy directly)."""
         sizes = [int(np.prod(sh)) for sh in self._shapes]
-        buf = np.empty(sum(sizes))
+        buf = np.empty(sum(sizes)) if out is None else out
+        assert buf.dtype == np.float64 and buf.flags["C_CONTIGUOUS"] and buf.size == sum(sizes)
         capi.check(capi.lib().uegccd_batch_get_all_amplitudes(self._h, capi.dptr(buf)))
-        out, off = [], 0
+        views, off = [], 0
         for sh, n in zip(self._shapes, sizes):
-            out.append(buf[off:off + n].reshape(sh))
+            views.append(buf[off:off + n].reshape(sh))
             off += n
-        return out
+        return views
