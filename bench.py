@@ -268,6 +268,7 @@ def run_gpu(args, rank, world):
         batch.solve(**opts)
     stats = batch.kernel_stats()
     batch.set_profiling(False)
+    ring_threads = batch.ring_threads()   # the tuner's pick, from the first CCD solve
     niters = [r["niter"] for r in res]
     fails = sum(r["fail"] for r in res)
     total_ms = float(sum(step_ms))
@@ -323,7 +324,7 @@ def run_gpu(args, rank, world):
     out = {
         "value": value, "ms_per_step": e_max / args.steps, "e2e_value": e2e_value, "h2d": h2d, "d2h": d2h,
         "niter_mean": float(np.mean(niters)), "niter_min": int(min(niters)), "niter_max": int(max(niters)),
-        "fails": int(fails), "rc": rc, "stats": stats, "clocks": clk.summary(),
+        "fails": int(fails), "rc": rc, "stats": stats, "clocks": clk.summary(), "ring_threads": ring_threads,
         "ecorr_first": res[0]["ecorr"], "e2_first": float(e2[0]), "launches_per_step": res[0]["kernel_launches"],
         "systems": systems,
         "replay_niter_mean": float(np.mean([r["niter"] for r in res_r])),
@@ -460,6 +461,7 @@ def main():
     tr = TRAFFIC_PER_SOLVE.get(top)
     roof["traffic"] = tr * nsys if tr else None
     flops_pp = sum(ps["ov2"] * 2 for ps in per_solve) / len(per_solve) * nsys
+    config["ring_cta_threads"] = g["ring_threads"]   # per ring pair class, picked by the launch-shape tuner
     if args.precision == "mixed":
         config["precision"] = "particle-particle ladder FP16 tensor cores (FP32 accumulate), rest FP64"
     line = {"metric": metric, "value": g["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,

@@ -239,6 +239,12 @@ int uegccd_trim_cache(void);
 int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dts, int32_t max_rec,
                          int32_t *n_recorded);
 
+/* CTA sizes of the ring kernel's pair classes (by padded pair size: <= 16, 32, 48 rows,
+ * larger), as the launch-shape tuner picked them on the batch's first CCD solve (timed
+ * on the batch itself, once per batch shape in a process; the CTA size leaves every
+ * result bitwise the same).  Writes at most max values; returns how many. */
+int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max);
+
 /* Live kernel timing: when on, every kernel of a batch solve is bracketed by CUDA
  * events on the batch's stream; stats return per-kernel total ms and launches. */
 int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on);

@@ -101,3 +101,29 @@ def test_all_amplitudes_and_reused_memory(goldens):
         assert e == runs[0][0]
         for a, c in zip(amps, runs[0][1]):
             np.testing.assert_array_equal(a, c)
+
+
+def test_ring_cta_tuning_and_pinned_download(goldens):
+    """The launch-shape tuner leaves a CTA size from its candidate set in every ring pair
+    class, and a page-locked destination receives the same amplitudes as a pageable one."""
+    import ctypes as C
+
+    from uegccd_b200 import Batch
+
+    systems = [_tuple(o) for o in _systems(goldens)]
+    b = Batch(systems)
+    b.solve(max_iter=4)
+    th = b.ring_threads()
+    assert len(th) == 4 and all(t in (32, 64, 128, 256) for t in th)
+    n = b.amplitude_count()
+    rt = C.CDLL("libcudart.so.12")
+    p = C.c_void_p()
+    assert rt.cudaHostAlloc(C.byref(p), C.c_size_t(8 * n), C.c_uint(0)) == 0
+    try:
+        pinned = np.ctypeslib.as_array((C.c_double * n).from_address(p.value))
+        a = [x.copy() for x in b.all_amplitudes(out=pinned)]
+        c = b.all_amplitudes()
+        for x, y in zip(a, c):
+            np.testing.assert_array_equal(x, y)
+    finally:
+        rt.cudaFreeHost(p)

@@ -9,9 +9,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -193,6 +195,7 @@ struct UegccdBatch {
         }
     } gkey{};
     bool have_graph = false;
+    bool rings_tuned = false;        // k_rings CTA sizes picked (before the first graph capture)
     cudaGraphExec_t gexec = nullptr;
     int g_launches = 0;          // kernels per iteration
     // structure factors (on first use): every solve's particle-hole groups {first row, rows},
@@ -697,6 +700,39 @@ int capture_iteration(UegccdBatch &b, const TermFlags &f, double tol, int max_it
     return 0;
 }
 
+// The k_rings CTA sizes of a batch: measured once per batch shape in this process (the
+// shape: pair count and shared memory of every class), on the first CCD solve, before
+// the iteration graph is captured.
+std::mutex g_tune_mu;
+std::map<std::vector<int64_t>, std::array<int, kRingClasses>> g_ring_tuning;
+
+int tune_batch_rings(UegccdBatch &b)
+{
+    DevBatch &d = b.d;
+    std::vector<int64_t> key;
+    for (int c = 0; c <= kRingClasses; c++) {
+        key.push_back(d.nring[c]);
+        key.push_back((int64_t)d.ring_smem[c]);
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_ring_tuning.find(key);
+        if (it != g_ring_tuning.end()) {
+            for (int c = 0; c < kRingClasses; c++) d.ring_threads[c] = it->second[c];
+            b.rings_tuned = true;
+            return 0;
+        }
+    }
+    const int e = tune_rings(d, b.stream);
+    if (e != 0) return fail(UEGCCD_ERR_CUDA, std::string("k_rings tuning: ") + cudaGetErrorString((cudaError_t)e));
+    std::array<int, kRingClasses> th;
+    for (int c = 0; c < kRingClasses; c++) th[c] = d.ring_threads[c];
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_ring_tuning[key] = th;
+    b.rings_tuned = true;
+    return 0;
+}
+
 // Runs the iteration for all solves of the batch from the amplitudes in d.t.
 // Iteration control lives on the device; the host replays a captured iteration
 // graph kPoll times between polls of the number of active solves.  With kernel
@@ -730,6 +766,7 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
         if ((rc = b.alloc(d.tc_err, 1))) return rc;
     }
     if (d.tc_err) CU(cudaMemsetAsync(d.tc_err, 0, sizeof(int), b.stream));
+    if (!b.rings_tuned && !drpa && (f.do_ring || f.do_xring) && (rc = tune_batch_rings(b))) return rc;
     b.launches = 0;
     CU(cudaEventRecord(b.ev0, b.stream));
     // CCEnergy of the start amplitudes and dT = max|T| (CCD.f90:63-64, dRPA.f90:68-69)
@@ -1132,6 +1169,14 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
     CU(cudaEventElapsedTime(&ms, b->ev_solve0, b->ev_solve1));
     for (int s = 0; s < b->d.nsolves; s++) results[s].gpu_ms = ms;
     return st;
+}
+
+int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max)
+{
+    if (!b || !threads || max <= 0) return fail(UEGCCD_ERR_ARG, "bad argument");
+    const int n = std::min<int>(max, kRingClasses);
+    for (int c = 0; c < n; c++) threads[c] = b->d.ring_threads[c];
+    return n;
 }
 
 int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on)

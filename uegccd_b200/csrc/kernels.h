@@ -60,6 +60,7 @@ struct DevBatch {
     // sizes (kRingSmemClass), then k_rings_wide
     int nring[5] = {0, 0, 0, 0, 0};
     size_t ring_smem[5] = {0, 0, 0, 0, 0};
+    int ring_threads[4] = {32, 128, 256, 256};  // CTA size per k_rings class: defaults, then tune_rings
 };
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
@@ -72,12 +73,17 @@ void set_ladder_smem_limit(size_t bytes);
 // dynamic shared memory of k_rings for NOcc = O and groups of n1 and n2 rows
 size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max);
 // k_rings classes by padded pair size N1 + N2 (up to kRingClassRows), each with its
-// CTA size; pairs above the last class, or above kRingSmemMax, go to k_rings_wide
+// CTA size (DevBatch::ring_threads); pairs above the last class, or above kRingSmemMax,
+// go to k_rings_wide
 constexpr int kRingClasses = 4;
 constexpr int kRingClassRows[kRingClasses] = {16, 32, 48, 1 << 30};
-constexpr int kRingClassThreads[kRingClasses] = {32, 64, 128, 256};
 constexpr size_t kRingSmemMax = 200 * 1024;
 void set_rings_smem_limit(int wide, size_t bytes);
+// Launch-shape autotuner: times k_rings of every pair class on the batch's current
+// amplitudes with 32, 64, 128 and 256 threads per CTA and keeps the fastest in
+// d.ring_threads.  The CTA size changes no sum's order: results are bitwise the same.
+// Not inside a stream capture.  Returns a cudaError_t value.
+int tune_rings(DevBatch &d, cudaStream_t st);
 
 constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* use the same bound)
 

@@ -1668,6 +1668,46 @@ const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh"
                                       "k_reduce_solves", "k_rings",
                                       "k_ladder_tc"};
 
+int tune_rings(DevBatch &d, cudaStream_t st)
+{
+    static const int kCand[] = {32, 64, 128, 256};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t err = cudaEventCreate(&e0);
+    if (err == cudaSuccess) err = cudaEventCreate(&e1);
+    int off = 0;
+    for (int c = 0; c < kRingClasses && err == cudaSuccess; c++) {
+        if (d.nring[c] > 0) {
+            float best = 1e30f;
+            int pick = d.ring_threads[c];
+            for (int th : kCand) {
+                auto run = [&]() {
+                    k_rings<<<d.nring[c], th, d.ring_smem[c], st>>>(d.rpairs + off, d.solves, d.ph_i, d.ph_x,
+                                                                    d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, 1, 1,
+                                                                    d.g_rq, d.g_xq, d.active);
+                };
+                run();  // warm
+                cudaEventRecord(e0, st);
+                run();
+                run();
+                cudaEventRecord(e1, st);
+                if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    pick = th;
+                }
+            }
+            d.ring_threads[c] = pick;
+        }
+        off += d.nring[c];
+    }
+    if (err == cudaSuccess) err = cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return (int)err;
+}
+
 int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_out, cudaStream_t st,
                     KernelTimer *kt, const CtlBuffers *diis, int ndiis)
 {
@@ -1720,7 +1760,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         int off = 0;
         for (int c = 0; c < kRingClasses; c++) {
             if (d.nring[c] > 0)
-                k_rings<<<d.nring[c], kRingClassThreads[c], d.ring_smem[c], st>>>(
+                k_rings<<<d.nring[c], d.ring_threads[c], d.ring_smem[c], st>>>(
                     d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, f.do_ring,
                     f.do_xring, d.g_rq, d.g_xq, d.active);
             off += d.nring[c];

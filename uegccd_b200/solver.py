@@ -152,6 +152,14 @@ class Batch:
         """Structure-factor grids of solve s from the amplitudes the batch holds."""
         return _sf_call(self._systems[s], lambda g: capi.lib().uegccd_batch_structure_factor(self._h, s, g))
 
+    def ring_threads(self) -> list:
+        """CTA size of each ring pair class (after the first CCD solve: the tuned ones)."""
+        a = (C.c_int32 * 8)()
+        n = capi.lib().uegccd_batch_ring_threads(self._h, a, 8)
+        if n < 0:
+            capi.check(n)
+        return list(a[:n])
+
     def set_profiling(self, on: bool) -> None:
         capi.check(capi.lib().uegccd_batch_set_profiling(self._h, 1 if on else 0))
 
