@@ -13,8 +13,8 @@ Workload ("ccd-twist-batch", the batched twist-average configuration):
 Metric: CCD solves/s (whole job; N GPUs each solve their own twist batch, weak scaling).
   value  device-timed (CUDA events on the library's stream), inputs resident;
   e2e    the same through the C ABI with host buffers: batch create (plan + uploads),
-         solve, amplitudes copied back to a page-locked host buffer, every step; two steps
-         in flight (the next batch is created while the current one solves).
+         solve, amplitudes copied back to a page-locked host buffer, every step; the next
+         step's create and the previous step's download overlap the current solve.
 --impl reference times the oracle (C restatement of the reference Fortran) on the
 host cores: one process per core, each running CCD iterations of its own twist.
 """
@@ -273,31 +273,40 @@ def run_gpu(args, rank, world):
     fails = sum(r["fail"] for r in res)
     total_ms = float(sum(step_ms))
     # e2e: through the C ABI with host buffers, every step: batch create (plan, uploads),
-    # solve, and every twist's T2 read back into a page-locked host buffer.  Two steps are
-    # in flight: the next step's batch is created on a host thread while this one solves
-    # and downloads (the C calls release the GIL).  The timed run starts before its
-    # first create and ends after its last download, so fill and drain are inside it.
-    out_buf = pinned_buffer(batch.amplitude_count())
+    # solve, and every twist's T2 read back into page-locked host memory.  Three stages
+    # run at once, as a serving host runs them: the next step's batch is created on one
+    # host thread, this step solves, and the previous step's amplitudes are downloaded on
+    # another (the C calls release the GIL; each batch has its own stream).  The timed run
+    # starts before its first create and ends after its last download: the pipeline's fill
+    # and drain are inside it.
+    out_bufs = [pinned_buffer(batch.amplitude_count()) for _ in range(2)]
     xfer = [0, 0]
+
+    def finish(b2, buf):
+        b2.all_amplitudes(out=buf)
+        xfer[0], xfer[1] = b2.transfer_bytes()
+        b2.close()
 
     def e2e_run(nsteps):
         from concurrent.futures import ThreadPoolExecutor
 
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=1) as pool:
-            fut = pool.submit(Batch, systems)
+        with ThreadPoolExecutor(max_workers=1) as creator, ThreadPoolExecutor(max_workers=1) as reader:
+            fut = creator.submit(Batch, systems)
+            done = None
             for k in range(nsteps):
                 b2 = fut.result()
                 if k + 1 < nsteps:
-                    fut = pool.submit(Batch, systems)
+                    fut = creator.submit(Batch, systems)
                 b2.solve(**opts)
-                b2.all_amplitudes(out=out_buf)
-                xfer[0], xfer[1] = b2.transfer_bytes()
-                b2.close()
+                if done is not None:
+                    done.result()
+                done = reader.submit(finish, b2, out_bufs[k % 2])
+            done.result()
         return (time.perf_counter() - t0) * 1e3 / nsteps
 
     e2e_run(max(2, args.warmup))   # warms the device-memory cache and the pinned buffers
-    e2e_ms = [e2e_run(max(3, min(args.steps, 5)))]
+    e2e_ms = [e2e_run(max(5, 2 * args.steps))]
     h2d, d2h = xfer
     # the other precision on the same batch (timed the same way): mixed beside FP64
     other = None
@@ -469,8 +478,8 @@ def main():
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f16/f64", "data": "synthetic", "config": config,
             "e2e": {"value": g["e2e_value"], "unit": "solves/s", "h2d_bytes_per_step": g["h2d"],
                     "d2h_bytes_per_step": g["d2h"],
-                    "note": "batch create + solve + T2 of every twist to page-locked host memory per step; "
-                            "two steps in flight (next create overlaps the current solve)"},
+                    "note": "per step: batch create (plan + uploads), solve, T2 of every twist to page-locked host "
+                            "memory; create of the next step and download of the previous overlap the solve"},
             "gpu_launches": int(g["launches_per_step"]) * args.steps,
             "clocks": g["clocks"], "roofline": roof,
             "kernels": {k: {"ms": v[0], "launches": v[1], **({"roofline": kern[k]} if k in kern else {})}
