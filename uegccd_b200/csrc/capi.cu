@@ -362,12 +362,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             hhoff += (int64_t)B.o * B.o;
             max_o = std::max(max_o, B.o);
             max_v = std::max(max_v, B.v);
-            // row tile NP follows o_K (8, 16, 32); columns in tiles of 128 (4 warps x 32)
-            const int np = B.o <= 8 ? 8 : B.o <= 16 ? 16 : 32;
+            // row tiles of 32 pairs, the last one the remainder rounded up to 8 (8, 16, 24 or 32):
+            // at most 7 padded rows per block; columns in tiles of 128 (4 warps x 32)
+            auto row_tile = [&](int p0) { return std::min(32, (B.o - p0 + 7) & ~7); };
             for (int a0 = 0; a0 < B.v; a0 += 128)
-                for (int p0 = 0; p0 < B.o; p0 += np) tiles.push_back(LadderTile{bi, a0, p0, np});
+                for (int p0 = 0; p0 < B.o; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, row_tile(p0)});
             for (int q0 = 0; q0 < B.o; q0 += 128)
-                for (int p0 = 0; p0 < B.o; p0 += np) htiles.push_back(LadderTile{bi, q0, p0, np});
+                for (int p0 = 0; p0 < B.o; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
             // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows
             const int ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
             auto &tl = ntc == 16 ? tc16 : ntc == 32 ? tc32 : tc64;

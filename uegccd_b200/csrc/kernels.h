@@ -22,7 +22,7 @@ struct DevBatch {
     int64_t namp = 0;
     SolveDev *solves = nullptr;
     BlockDev *blocks = nullptr;
-    LadderTile *tiles = nullptr;     // particle-particle (+hole-hole apply) tiles; pad = row tile NP
+    LadderTile *tiles = nullptr;     // particle-particle (+hole-hole apply) tiles; pad = row tile NP (8/16/24/32)
     LadderTile *htiles = nullptr;    // hole-hole intermediate tiles
     int nhtiles = 0;
     ChunkDev *chunks = nullptr;      // amplitude chunks

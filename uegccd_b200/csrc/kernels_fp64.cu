@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ 
         switch (T.pad) {
         case 8: ladder3_tile<8, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
         case 16: ladder3_tile<16, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+        case 24: ladder3_tile<24, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
         default: ladder3_tile<32, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
         }
         return;
@@ -398,6 +399,7 @@ __global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ 
     switch (T.pad) {
     case 8: ladder3_tile<8, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
     case 16: ladder3_tile<16, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
+    case 24: ladder3_tile<24, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
     default: ladder3_tile<32, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
     }
 }
