@@ -259,6 +259,12 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
 /* Host<->device bytes the batch has moved since its creation (its upload included). */
 int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h);
 
+/* The FP64 tensor-core peak of the current device, measured (TFLOP/s): a register-only
+ * kernel of independent mma.sync.m8n8k4.f64 chains, eight 4-warp CTAs per SM, timed with
+ * CUDA events after one untimed launch (a few ms).  The roofline denominator of the FP64
+ * DMMA kernels. */
+int uegccd_probe_fp64_peak(double *tflops);
+
 const char *uegccd_last_error(void);
 /* Library version string. */
 const char *uegccd_version(void);

@@ -127,3 +127,15 @@ def test_ring_cta_tuning_and_pinned_download(goldens):
             np.testing.assert_array_equal(x, y)
     finally:
         rt.cudaFreeHost(p)
+
+
+def test_fp64_peak_probe():
+    """The register-only FP64 MMA probe (the bench's FP64 roofline denominator) reports a
+    B200-sized figure: its datasheet FP64 tensor peak is about 37-40 TFLOP/s."""
+    import ctypes as C
+
+    from uegccd_b200 import _capi
+
+    v = C.c_double()
+    assert _capi.lib().uegccd_probe_fp64_peak(C.byref(v)) == 0
+    assert 20.0 < v.value < 60.0, v.value

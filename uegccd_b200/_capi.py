@@ -94,6 +94,7 @@ def lib() -> C.CDLL:
         L.uegccd_batch_get_amplitudes.argtypes = [vp, C.c_int32, dp]
         L.uegccd_batch_get_all_amplitudes.argtypes = [vp, dp]
         L.uegccd_batch_mp2.argtypes = [vp, dp]
+        L.uegccd_probe_fp64_peak.argtypes = [dp]
         L.uegccd_diis_create.argtypes = [C.c_int64, C.c_int32, C.c_int32, dp, P(vp)]
         L.uegccd_diis_push.argtypes = [vp, dp, dp]
         L.uegccd_diis_get_t.argtypes = [vp, C.c_int32, dp]

@@ -20,7 +20,7 @@ ZCODE = os.path.join(PKG, "uegccd_zcode")
 OBJDIR = os.path.join(PKG, "_build")
 
 SOURCES = ["capi.cu", "kernels_fp64.cu", "kernels_tc.cu", "plan.cpp", "heg_host.cpp", "zcode.cpp", "mp2_static.cu",
-           "diis_api.cu"]
+           "diis_api.cu", "probe.cu"]
 HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h", "listdir.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
