@@ -786,8 +786,8 @@ size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
 {
     const size_t N1 = round8(n1), N2 = round8(n2), l1 = N1 + 4, l2 = N2 + 4;
     const size_t nsv = q2max < kVtabSmem ? round8(q2max + 1) : 0;
-    const size_t dbl = 2 * N1 * l2 + 3 * N2 * l1 + 3 * N1 * l1 + 3 * N2 * l2 + 3 * (N1 + N2) + nsv;
-    return sizeof(double) * dbl + sizeof(int) * 2 * (N1 + N2) + sizeof(int4) * ((size_t)O + N1 + N2);
+    const size_t dbl = 2 * N1 * l2 + 2 * N2 * l1 + 2 * N1 * l1 + 2 * N2 * l2 + 3 * (N1 + N2) + nsv;
+    return sizeof(double) * dbl + sizeof(int) * 2 * (N1 + N2) + sizeof(int4) * ((size_t)O + 2 * (N1 + N2));
 }
 
 __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ pairs,
@@ -812,16 +812,15 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     const bool vsm = s.q2max < kVtabSmem;
     const int nsv = vsm ? round8(s.q2max + 1) : 0;
     extern __shared__ double smem[];
+    // W and the direct kernels Vs1, Vs2 are table lookups: generated where the DMMA loops
+    // read them (from the rows' n-vectors) instead of stored, for more CTAs per SM
     double *X1 = smem;              // N1 x l2
     double *Y1 = X1 + N1 * l2;      // N1 x l2
     double *X2 = Y1 + N1 * l2;      // N2 x l1
     double *Y2 = X2 + N2 * l1;      // N2 x l1
-    double *W = Y2 + N2 * l1;       // N2 x l1
-    double *Vs1 = W + N2 * l1;      // N1 x l1
-    double *XW1 = Vs1 + N1 * l1;    // N1 x l1
+    double *XW1 = Y2 + N2 * l1;     // N1 x l1
     double *U1 = XW1 + N1 * l1;     // N1 x l1
-    double *Vs2 = U1 + N1 * l1;     // N2 x l2
-    double *XW2 = Vs2 + N2 * l2;    // N2 x l2
+    double *XW2 = U1 + N1 * l1;     // N2 x l2
     double *U2 = XW2 + N2 * l2;     // N2 x l2
     double *Sx = U2 + N2 * l2;      // R: group 1 rows at [0, N1), group 2 rows at [N1, R)
     double *Sy = Sx + R;
@@ -831,6 +830,7 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     int *rw = ri + R;               // R: row * O, the row's offset in the gather-index tables
     int4 *no = (int4 *)(rw + R);    // O
     int4 *nx = no + O;              // R: n-vector of the row's virtual
+    int4 *nr = nx + R;              // R: n-vector of the row's occupied index (0 on padding)
     // the CTA is 1, 2 or 4 warps, by pair size
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, kWarps = nt >> 5;
     auto V = [&](int q2) -> double {
@@ -848,6 +848,7 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     }
     for (int k = tid; k < O; k += nt) no[k] = nv4[s.orb0 + k];
     __syncthreads();
+    for (int r = tid; r < R; r += nt) nr[r] = ri[r] >= 0 ? no[ri[r]] : make_int4(0, 0, 0, 0);
     const int4 q1x = nx[0], q1i = no[ri[0]];
     const int Qx = q1x.x - q1i.x, Qy = q1x.y - q1i.y, Qz = q1x.z - q1i.z;
     const int32_t *gx = ridx_x + s.ph0, *gy = ridx_y + s.ph0;
@@ -884,25 +885,6 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
             }
         }
     }
-    // W[b][a] and the direct kernels Vs1, Vs2 (shared-memory table lookups)
-    for (int e = tid; e < N2 * N1; e += nt) {
-        const int b = e / N1, a = e - b * N1;
-        double w = 0.0;
-        if (b < n2 && a < n1) {
-            const int4 nb = no[ri[N1 + b]], na = no[ri[a]];
-            const int dx = nb.x - na.x - Qx, dy = nb.y - na.y - Qy, dz = nb.z - na.z - Qz;
-            w = V(dx * dx + dy * dy + dz * dz);
-        }
-        W[b * l1 + a] = w;
-    }
-    for (int e = tid; e < N1 * N1; e += nt) {
-        const int a = e / N1, c = e - a * N1;
-        Vs1[a * l1 + c] = (a < n1 && c < n1) ? V(q2_of(no[ri[c]], no[ri[a]])) : 0.0;
-    }
-    for (int e = tid; e < N2 * N2; e += nt) {
-        const int b = e / N2, c = e - b * N2;
-        Vs2[b * l2 + c] = (b < n2 && c < n2) ? V(q2_of(no[ri[N1 + c]], no[ri[N1 + b]])) : 0.0;
-    }
     __syncthreads();
     for (int r = tid; r < R; r += nt) {
         const bool g1 = r < N1;
@@ -919,46 +901,66 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
         Vd[r] = ri[r] >= 0 ? V(q2_of(no[ri[r]], nx[r])) : 0.0;
     }
     const int g = lane >> 2, tg = lane & 3;
-    // phase 1: XW1 = X1 W, U1 = Y1 W - Vs1 (K = N2); XW2 = X2 W^T, U2 = Y2 W^T - Vs2 (K = N1).
-    // Tasks: one 8-row fragment row x up to 4 column fragments.
+    // phase 1: XW1 = X1 W, U1 = Y1 W - Vs1 (K = N2); XW2 = X2 W^T, U2 = Y2 W^T - Vs2 (K = N1),
+    // with W[b][a] = v(n_{i_b} - n_{i_a} - Q) and Vs[c][c'] = v(n_{i_c'} - n_{i_c}) generated from
+    // the rows' n-vectors (0 on padding).  Tasks: one 8-row fragment row x up to 2 column
+    // fragments; X and Y share each generated W fragment.
     {
-        const int ng1 = (N1 + 31) / 32, ng2 = (N2 + 31) / 32;
-        const int t1 = (N1 / 8) * ng1, t2 = (N2 / 8) * ng2;   // per matrix of each group
-        const int ntask = 2 * t1 + 2 * t2;
-        for (int task = warp; task < ntask; task += kWarps) {
-            const bool grp2 = task >= 2 * t1;
-            const int tt = grp2 ? task - 2 * t1 : task, tg1 = grp2 ? t2 : t1, ngr = grp2 ? ng2 : ng1;
-            const int mat = tt / tg1, rem = tt - mat * tg1;
-            const int mf = rem / ngr, ng = rem - mf * ngr;
+        const int ng1 = (N1 + 15) / 16, ng2 = (N2 + 15) / 16;
+        const int t1 = (N1 / 8) * ng1, t2 = (N2 / 8) * ng2;
+        for (int task = warp; task < t1 + t2; task += kWarps) {
+            const bool grp2 = task >= t1;
+            const int tt = grp2 ? task - t1 : task, ngr = grp2 ? ng2 : ng1;
+            const int mf = tt / ngr, ng = tt - mf * ngr;
             const int Ncol = grp2 ? N2 : N1, K = grp2 ? N1 : N2, lda = grp2 ? l1 : l2, ldo = grp2 ? l2 : l1;
-            const double *A = (grp2 ? (mat == 0 ? X2 : Y2) : (mat == 0 ? X1 : Y1)) + (mf * 8 + g) * lda + tg;
-            const int nbase = ng * 32;
-            double acc[4][2];
+            const int nvc = grp2 ? n2 : n1, nvk = grp2 ? n1 : n2;    // valid columns, valid k
+            const int cb = grp2 ? N1 : 0, kb = grp2 ? 0 : N1;         // row slots of columns, of k
+            const double *AX = (grp2 ? X2 : X1) + (mf * 8 + g) * lda + tg;
+            const double *AY = (grp2 ? Y2 : Y1) + (mf * 8 + g) * lda + tg;
+            const int nbase = ng * 16;
+            int4 cn[2];
+            bool cok[2];
 #pragma unroll
-            for (int f = 0; f < 4; f++) acc[f][0] = acc[f][1] = 0.0;
+            for (int f = 0; f < 2; f++) {
+                const int n = nbase + f * 8 + g;
+                cok[f] = n < nvc;
+                cn[f] = cok[f] ? nr[cb + n] : make_int4(0, 0, 0, 0);
+            }
+            double acc[2][2][2];
+#pragma unroll
+            for (int f = 0; f < 2; f++) acc[0][f][0] = acc[0][f][1] = acc[1][f][0] = acc[1][f][1] = 0.0;
             for (int k0 = 0; k0 < K; k0 += 4) {
-                const double av = A[k0];
+                const int k = k0 + tg;
+                const double ax = AX[k0], ay = AY[k0];
+                const bool kok = k < nvk;
+                const int4 kn = nr[kb + k];
 #pragma unroll
-                for (int f = 0; f < 4; f++) {
+                for (int f = 0; f < 2; f++) {
                     if (nbase + f * 8 >= Ncol) break;
-                    const int n = nbase + f * 8 + g;
                     // group 1: B(k=b, n=a') = W[b][a'];  group 2: B(k=a, n=b') = W[b'][a]
-                    const double bv = grp2 ? W[n * l1 + k0 + tg] : W[(k0 + tg) * l1 + n];
-                    dmma_884(acc[f][0], acc[f][1], av, bv);
+                    double bv = 0.0;
+                    if (kok && cok[f]) {
+                        const int4 hb = grp2 ? cn[f] : kn, ha = grp2 ? kn : cn[f];
+                        const int dx = hb.x - ha.x - Qx, dy = hb.y - ha.y - Qy, dz = hb.z - ha.z - Qz;
+                        bv = V(dx * dx + dy * dy + dz * dz);
+                    }
+                    dmma_884(acc[0][f][0], acc[0][f][1], ax, bv);
+                    dmma_884(acc[1][f][0], acc[1][f][1], ay, bv);
                 }
             }
-            double *Out = grp2 ? (mat == 0 ? XW2 : U2) : (mat == 0 ? XW1 : U1);
-            const double *Vsg = grp2 ? Vs2 : Vs1;
+            double *OX = grp2 ? XW2 : XW1, *OU = grp2 ? U2 : U1;
             const int r = mf * 8 + g;
+            const bool rok = r < nvc;
+            const int4 rn = rok ? nr[cb + r] : make_int4(0, 0, 0, 0);
 #pragma unroll
-            for (int f = 0; f < 4; f++) {
+            for (int f = 0; f < 2; f++) {
                 if (nbase + f * 8 >= Ncol) break;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int n = nbase + f * 8 + 2 * tg + h;
-                    double v = acc[f][h];
-                    if (mat == 1) v -= Vsg[r * ldo + n];
-                    Out[r * ldo + n] = v;
+                    const double vs = (rok && n < nvc) ? V(q2_of(nr[cb + n], rn)) : 0.0;
+                    OX[r * ldo + n] = acc[0][f][h];
+                    OU[r * ldo + n] = acc[1][f][h] - vs;
                 }
             }
         }
@@ -975,7 +977,6 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
         const double *AXW = dir ? XW2 : XW1, *AU = dir ? U2 : U1;   // stride K1 + 4
         const double *AX = dir ? X2 : X1, *AY = dir ? Y2 : Y1;      // stride K2 + 4
         const double *BX = dir ? X1 : X2, *BY = dir ? Y1 : Y2;      // stride K1 + 4
-        const double *BV = dir ? Vs1 : Vs2;                         // stride K2 + 4
         const int lk1 = K1 + 4, lk2 = K2 + 4;
         const int nng = (Np + 15) / 16;
         const int mf = tt / nng, ng = tt - mf * nng;
@@ -998,14 +999,26 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
                 dmma_884(xa[f][0], xa[f][1], au, by);
             }
         }
+        // B = -Vs of the B side (dir 0: Vs2[b][b'], dir 1: Vs1[a][a']), generated
+        const int sb = dir ? 0 : N1, nvb = dir ? n1 : n2;
+        int4 bn[2];
+        bool bok[2];
+#pragma unroll
+        for (int f = 0; f < 2; f++) {
+            const int bb = ng * 16 + f * 8 + g;
+            bok[f] = bb < nvb;
+            bn[f] = bok[f] ? nr[sb + bb] : make_int4(0, 0, 0, 0);
+        }
         for (int k0 = 0; k0 < K2; k0 += 4) {
             const int k = k0 + tg;
             const double ax = AX[(m0 + g) * lk2 + k], ay = AY[(m0 + g) * lk2 + k];
+            const bool kok = k < nvb;
+            const int4 kn = nr[sb + k];
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const int n0 = ng * 16 + f * 8;
                 if (n0 >= Np) break;
-                const double bv = -BV[(n0 + g) * lk2 + k];
+                const double bv = (kok && bok[f]) ? -V(q2_of(kn, bn[f])) : -0.0;
                 dmma_884(rb[f][0], rb[f][1], ax, bv);
                 dmma_884(xb[f][0], xb[f][1], ay, bv);
             }
