@@ -304,6 +304,11 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<SolveDev> solves(n);
     std::vector<BlockDev> blocks;
     std::vector<LadderTile> tiles, htiles, tc16, tc32, tc64;
+    std::vector<TcTileDev> tcx16, tcx32, tcx64;   // beside tc16/32/64: FP16 operand offsets
+    std::vector<WSlabDev> wslabs;
+    std::vector<DTileDev> dtiles;
+    int64_t w16_n = 0, d16_n = 0;
+    int nscale = 0;
     std::vector<ChunkDev> chunks, rchunks;
     std::vector<int> chunk_begin(n + 1, 0);
     std::vector<int2> targets;
@@ -369,11 +374,29 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
                 for (int p0 = 0; p0 < B.o; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, row_tile(p0)});
             for (int q0 = 0; q0 < B.o; q0 += 128)
                 for (int p0 = 0; p0 < B.o; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
-            // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows
+            // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows; their FP16 operands: one
+            // Coulomb slab per 128 virtuals, one d tile per row tile, each over all K chunks
             const int ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
             auto &tl = ntc == 16 ? tc16 : ntc == 32 ? tc32 : tc64;
+            auto &tx = ntc == 16 ? tcx16 : ntc == 32 ? tcx32 : tcx64;
+            const int64_t nch = (B.v + 31) / 32;
+            const int64_t w0 = w16_n, d0 = d16_n;
+            const int s0 = nscale;
+            for (int a0 = 0; a0 < B.v; a0 += 128) {
+                wslabs.push_back(WSlabDev{bi, a0, w16_n});
+                w16_n += nch * 128 * 32;
+            }
+            for (int p0 = 0; p0 < B.o; p0 += ntc) {
+                dtiles.push_back(DTileDev{bi, p0, ntc, nscale, d16_n});
+                d16_n += nch * ntc * 32;
+                nscale += ntc;
+            }
             for (int a0 = 0; a0 < B.v; a0 += 128)
-                for (int p0 = 0; p0 < B.o; p0 += ntc) tl.push_back(LadderTile{bi, a0, p0, ntc});
+                for (int p0 = 0; p0 < B.o; p0 += ntc) {
+                    tl.push_back(LadderTile{bi, a0, p0, ntc});
+                    const int it = p0 / ntc;
+                    tx.push_back(TcTileDev{w0 + (a0 / 128) * nch * 128 * 32, d0 + it * nch * ntc * 32, s0 + it * ntc, 0});
+                }
         }
         pair_i.insert(pair_i.end(), P.pair_i.begin(), P.pair_i.end());
         pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
@@ -449,6 +472,15 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     tct.insert(tct.end(), tc16.begin(), tc16.end());
     tct.insert(tct.end(), tc32.begin(), tc32.end());
     tct.insert(tct.end(), tc64.begin(), tc64.end());
+    std::vector<TcTileDev> tcx;
+    tcx.insert(tcx.end(), tcx16.begin(), tcx16.end());
+    tcx.insert(tcx.end(), tcx32.begin(), tcx32.end());
+    tcx.insert(tcx.end(), tcx64.begin(), tcx64.end());
+    d.nwslabs = (int)wslabs.size();
+    d.ndtiles = (int)dtiles.size();
+    d.w16_n = w16_n;
+    d.d16_n = d16_n;
+    d.nscale = nscale;
     d.nchunks = (int)chunks.size();
     d.nrchunks = (int)rchunks.size();
     d.ntargets = (int)targets.size();
@@ -499,6 +531,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.tiles, tiles))) return rc;
     if ((rc = b->upload(d.htiles, htiles))) return rc;
     if ((rc = b->upload(d.tctiles, tct))) return rc;
+    if ((rc = b->upload(d.tcx, tcx))) return rc;
+    if ((rc = b->upload(d.wslabs, wslabs))) return rc;
+    if ((rc = b->upload(d.dtiles, dtiles))) return rc;
     if ((rc = b->upload(d.chunks, chunks))) return rc;
     if ((rc = b->upload(d.rchunks, rchunks))) return rc;
     if ((rc = b->upload(d.chunk_begin, chunk_begin))) return rc;
@@ -631,11 +666,37 @@ int set_integrals(UegccdBatch &b, int core_n, double gapii)
     CU(cudaMemcpyAsync(b.d.solves, b.hsolves.data(), b.hsolves.size() * sizeof(SolveDev), cudaMemcpyHostToDevice,
                        b.stream));
     launch_vcoef(b.d, b.stream);
+    b.d.w16_valid = false;   // the FP16 Coulomb slabs follow the tables
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(b.stream));
     b.h2d_bytes += (int64_t)(vt.size() * sizeof(double) + b.hsolves.size() * sizeof(SolveDev));
     b.core_n = core_n;
     b.gapii = g;
+    return 0;
+}
+
+// Buffers of the mixed-precision ladder, on first use; the FP16 Coulomb slabs are (re)built
+// whenever the integral tables changed since.
+int mixed_alloc(UegccdBatch &b)
+{
+    DevBatch &d = b.d;
+    int rc = 0;
+    if (!d.t_ref) {
+        if ((rc = b.alloc(d.t_ref, d.namp))) return rc;
+        if ((rc = b.alloc(d.g_ref, d.namp))) return rc;
+        if ((rc = b.alloc(d.tc_err, 1))) return rc;
+        uint16_t *w = nullptr, *dd = nullptr;
+        if ((rc = b.alloc(w, (size_t)d.w16_n))) return rc;
+        if ((rc = b.alloc(dd, (size_t)d.d16_n))) return rc;
+        if ((rc = b.alloc(d.dscale, (size_t)d.nscale))) return rc;
+        d.w16 = w;
+        d.d16 = dd;
+    }
+    if (!d.w16_valid) {
+        launch_w16_build(d, b.stream);
+        CU(cudaGetLastError());
+        d.w16_valid = true;
+    }
     return 0;
 }
 
@@ -761,11 +822,7 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     CU(cudaMemcpyAsync(b.ctl.state, st0.data(), n * sizeof(IterState), cudaMemcpyHostToDevice, b.stream));
     CU(cudaMemsetAsync(b.ctl.Bm, 0, (size_t)n * kDiisMax * kDiisMax * sizeof(double), b.stream));
     if ((rc = set_active_all(b, 1))) return rc;
-    if (opt->precision == UEGCCD_MIXED && !d.t_ref) {
-        if ((rc = b.alloc(d.t_ref, d.namp))) return rc;
-        if ((rc = b.alloc(d.g_ref, d.namp))) return rc;
-        if ((rc = b.alloc(d.tc_err, 1))) return rc;
-    }
+    if (opt->precision == UEGCCD_MIXED && (rc = mixed_alloc(b))) return rc;
     if (d.tc_err) CU(cudaMemsetAsync(d.tc_err, 0, sizeof(int), b.stream));
     if (!b.rings_tuned && !drpa && (f.do_ring || f.do_xring) && (rc = tune_batch_rings(b))) return rc;
     b.launches = 0;
@@ -1082,11 +1139,7 @@ int uegccd_ccd_g2_ex(UegccdCtx *c, const double *t_abab, int32_t mask, int32_t p
     DevBatch &d = b.d;
     if (precision == UEGCCD_MIXED) {
         // the tensor-core ladder of t itself: refresh point t_ref = 0, g_ref = 0
-        if (!d.t_ref) {
-            if ((rc = b.alloc(d.t_ref, d.namp))) return rc;
-            if ((rc = b.alloc(d.g_ref, d.namp))) return rc;
-            if ((rc = b.alloc(d.tc_err, 1))) return rc;
-        }
+        if ((rc = mixed_alloc(b))) return rc;
         CU(cudaMemsetAsync(d.t_ref, 0, d.namp * sizeof(double), b.stream));
         CU(cudaMemsetAsync(d.g_ref, 0, d.namp * sizeof(double), b.stream));
         CU(cudaMemsetAsync(d.tc_err, 0, sizeof(int), b.stream));
@@ -1230,7 +1283,14 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     b += O * V * O * 4 * 2;                          // ring gather indices
     b += hh * 8 + nblk * (sizeof(BlockDev) + 8) + M * (16 + 8) + (P.q2max + 1) * 8;
     b += A * (8 + 4) * (int64_t)std::max(0, (int)ndiis);  // DIIS history (t' FP64, e FP32)
-    if (mixed) b += A * 8 * 2;                       // t_ref, g_ref
+    if (mixed) {
+        b += A * 8 * 2;                              // t_ref, g_ref
+        for (const auto &B : P.blocks) {             // FP16 Coulomb slabs and d tiles, row scales
+            const int64_t nch = (B.v + 31) / 32, ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
+            b += ((B.v + 127) / 128) * nch * 128 * 32 * 2;
+            b += ((B.o + ntc - 1) / ntc) * (nch * ntc * 32 * 2 + ntc * 4);
+        }
+    }
     b += (int64_t)O * O * V * 8 * 3;                 // reference-layout staging (one solve)
     *bytes = b;
     if (namp) *namp = A;

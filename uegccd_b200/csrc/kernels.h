@@ -55,6 +55,16 @@ struct DevBatch {
     int ntc16 = 0, ntc32 = 0, ntc64 = 0;
     double *t_ref = nullptr, *g_ref = nullptr;  // refresh point of the defect correction
     int *tc_err = nullptr;
+    // FP16 operands of the tensor-core ladder (allocated and built on first mixed use)
+    TcTileDev *tcx = nullptr;        // beside tctiles
+    WSlabDev *wslabs = nullptr;
+    DTileDev *dtiles = nullptr;
+    int nwslabs = 0, ndtiles = 0;
+    int64_t w16_n = 0, d16_n = 0;    // halves
+    int nscale = 0;
+    void *w16 = nullptr, *d16 = nullptr;   // __half arrays
+    float *dscale = nullptr;
+    bool w16_valid = false;          // built for the current integral tables
     int nrpairs = 0;
     // ring pair classes, rpairs sorted in this order: k_rings in kRingClasses shared-memory
     // sizes (kRingSmemClass), then k_rings_wide
@@ -173,8 +183,11 @@ void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, in
                cudaStream_t st);
 // pos (pre-set to -1), amps, partner, then the ring gather indices, from the block structure
 void launch_block_tables(const DevBatch &d, cudaStream_t st);
-// Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref)
+// Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref); writes the
+// scaled FP16 d tiles first (d.w16 must be built)
 void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st);
+// The static FP16 Coulomb slabs of the tensor-core ladder, from the current |q|^2 tables
+void launch_w16_build(const DevBatch &d, cudaStream_t st);
 // Refresh point: t_ref <- t and g_ref <- FP64 particle-particle ladder of t_ref
 void launch_refresh(const DevBatch &d, cudaStream_t st);
 // Device-side iteration control

@@ -13,6 +13,12 @@
 // so the sum is exact up to the FP16 rounding of d and W, an error that shrinks with
 // |t - t_ref|; FP64 sweeps at the end remove what is left.
 //
+// Both FP16 operands are written to global memory already in the MMA's canonical
+// shared-memory layout, one 32-wide K chunk after another: the Coulomb slabs once per
+// batch (they depend only on the |q|^2 tables; k_w16_build) and the scaled d tiles once
+// per iteration (k_delta16).  The MMA kernel then only streams chunks into shared memory
+// with 16-byte cp.async copies.
+//
 // Shared-memory operands use the canonical K-major layout without swizzle: 8 x 8
 // element core matrices (8 rows of 16 bytes), core matrices adjacent in K 128 bytes
 // apart (LBO) and 8-row groups 512 bytes apart (SBO) for a 32-wide K chunk.
@@ -33,7 +39,7 @@ namespace {
 
 constexpr int kTcM = 128;        // MMA M (virtuals per CTA)
 constexpr int kTcK = 32;         // K chunk staged per pipeline stage
-constexpr int kTcVtab = 1024;    // |q|^2 table entries staged in shared memory
+constexpr int kStages = 3;       // shared-memory stages: two chunk copies in flight beside the MMA
 constexpr long long kWaitLimit = 1LL << 26;  // mbarrier polls before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -122,33 +128,113 @@ __device__ __forceinline__ int q2_of(int4 x, int4 y)
 // SBO = 256 halves (512 B)
 __device__ __forceinline__ int cm_off(int row, int k) { return (row & 7) * 8 + (row >> 3) * 256 + (k & 7) + (k >> 3) * 64; }
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
 }  // namespace
+
+// FP16 Coulomb slab of (block, 128 virtuals a0..): chunk ch holds A[m][k] = v(n_a - n_c),
+// a = a0 + m, c = 32 ch + k, zero outside the block, in the canonical layout.
+__global__ void __launch_bounds__(128) k_w16_build(const WSlabDev *__restrict__ slabs,
+                                                  const BlockDev *__restrict__ blocks,
+                                                  const SolveDev *__restrict__ solves,
+                                                  const int16_t *__restrict__ vir, const int4 *__restrict__ nv4,
+                                                  const double *__restrict__ vtab, __half *__restrict__ w16)
+{
+    __shared__ int4 na[kTcM];
+    const WSlabDev S = slabs[blockIdx.x];
+    const BlockDev B = blocks[S.blk];
+    const SolveDev s = solves[B.solve];
+    const int tid = threadIdx.x, v = B.v;
+    for (int x = tid; x < kTcM; x += blockDim.x) {
+        const int a = S.a0 + x;
+        na[x] = a < v ? nv4[s.orb0 + vir[B.vir0 + a]] : make_int4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    const int nch = (v + kTcK - 1) / kTcK;
+    const int k = tid & (kTcK - 1);
+    for (int ch = 0; ch < nch; ch++) {
+        const int c = ch * kTcK + k;
+        const bool cok = c < v;
+        const int4 nc = cok ? nv4[s.orb0 + vir[B.vir0 + c]] : make_int4(0, 0, 0, 0);
+        __half *dst = w16 + S.woff + (int64_t)ch * kTcM * kTcK;
+        for (int m = tid / kTcK; m < kTcM; m += 128 / kTcK) {
+            float w = 0.f;
+            if (cok && S.a0 + m < v) {
+                const int q2 = q2_of(na[m], nc);
+                w = q2 > s.q2max ? 0.f : (float)vtab[s.vtab0 + q2];
+            }
+            dst[cm_off(m, k)] = __float2half_rn(w);
+        }
+    }
+}
+
+// Scaled FP16 d = t - t_ref of one row tile: the scale of row p is max_c |d[p][c]| (1 if
+// zero); chunk ch holds B[n][k] = d[p0 + n][32 ch + k] / scale, in the canonical layout.
+__global__ void __launch_bounds__(128) k_delta16(const DTileDev *__restrict__ dt,
+                                                const BlockDev *__restrict__ blocks,
+                                                const double *__restrict__ t, const double *__restrict__ t_ref,
+                                                __half *__restrict__ d16, float *__restrict__ dscale,
+                                                const uint8_t *__restrict__ active)
+{
+    __shared__ float rs[64];
+    const DTileDev D = dt[blockIdx.x];
+    const BlockDev B = blocks[D.blk];
+    if (!active[B.solve]) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, v = B.v, o = B.o, np = D.np;
+    for (int pp = warp; pp < np; pp += 4) {
+        const int p = D.p0 + pp;
+        float m = 0.f;
+        if (p < o)
+            for (int c = lane; c < v; c += 32) {
+                const int64_t idx = B.t0 + (int64_t)p * v + c;
+                m = fmaxf(m, fabsf((float)(t[idx] - t_ref[idx])));
+            }
+        for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+        if (lane == 0) {
+            rs[pp] = m > 0.f ? m : 1.f;
+            dscale[D.soff + pp] = rs[pp];
+        }
+    }
+    __syncthreads();
+    const int nch = (v + kTcK - 1) / kTcK;
+    for (int e = tid; e < nch * np * kTcK; e += blockDim.x) {
+        const int ch = e / (np * kTcK), r = e - ch * (np * kTcK);
+        const int pp = r / kTcK, k = r - pp * kTcK;
+        const int p = D.p0 + pp, c = ch * kTcK + k;
+        float x = 0.f;
+        if (p < o && c < v) {
+            const int64_t idx = B.t0 + (int64_t)p * v + c;
+            x = (float)((t[idx] - t_ref[idx]) / (double)rs[pp]);
+        }
+        d16[D.doff + (int64_t)ch * np * kTcK + cm_off(pp, k)] = __float2half_rn(x);
+    }
+}
 
 // One CTA per (block, 128-virtual tile).  g[...] += g_ref[...] + sum_c v(a-c) (t - t_ref)[p][c]
 // for every (p, a) of the tile (g already holds the hole-hole part).
 template <int NP>
 __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict__ tiles,
+                                                  const TcTileDev *__restrict__ tcx,
                                                   const BlockDev *__restrict__ blocks,
-                                                  const SolveDev *__restrict__ solves,
-                                                  const int16_t *__restrict__ vir, const int4 *__restrict__ nv4,
-                                                  const double *__restrict__ vtab, const double *__restrict__ t,
-                                                  const double *__restrict__ t_ref,
+                                                  const __half *__restrict__ w16, const __half *__restrict__ d16,
+                                                  const float *__restrict__ dscale,
                                                   const double *__restrict__ g_ref, double *__restrict__ g,
                                                   const uint8_t *__restrict__ active, int *__restrict__ err)
 {
     constexpr int NCOL = NP < 32 ? 32 : NP;  // tensor-memory columns (power of two, >= 32)
-    __shared__ alignas(1024) __half As[2][kTcM * kTcK];
-    __shared__ alignas(1024) __half Bs[2][NP * kTcK];
-    __shared__ float sv[kTcVtab];
-    __shared__ int4 na[kTcM];
+    __shared__ alignas(1024) __half As[kStages][kTcM * kTcK];
+    __shared__ alignas(1024) __half Bs[kStages][NP * kTcK];
     __shared__ float rscale[NP];
-    __shared__ alignas(8) uint64_t mbar[2];
+    __shared__ alignas(8) uint64_t mbar[kStages];
     __shared__ uint32_t tmem_base;
 
     const LadderTile T = tiles[blockIdx.x];
+    const TcTileDev X = tcx[blockIdx.x];
     const BlockDev B = blocks[T.blk];
     if (!active[B.solve]) return;
-    const SolveDev s = solves[B.solve];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int v = B.v, o = B.o;
 
@@ -158,29 +244,10 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+        for (int b = 0; b < kStages; b++) mbar_init(&mbar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    const bool vsm = s.q2max < kTcVtab;
-    if (vsm)
-        for (int q = tid; q <= s.q2max; q += blockDim.x) sv[q] = (float)vtab[s.vtab0 + q];
-    for (int x = tid; x < kTcM; x += blockDim.x) {
-        const int a = T.a0 + x;
-        na[x] = a < v ? nv4[s.orb0 + vir[B.vir0 + a]] : make_int4(0, 0, 0, 0);
-    }
-    // per-row scale of d = t - t_ref
-    for (int pp = warp; pp < NP; pp += 4) {
-        const int p = T.p0 + pp;
-        float m = 0.f;
-        if (p < o)
-            for (int c = lane; c < v; c += 32) {
-                const int64_t idx = B.t0 + (int64_t)p * v + c;
-                m = fmaxf(m, fabsf((float)(t[idx] - t_ref[idx])));
-            }
-        for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-        if (lane == 0) rscale[pp] = m > 0.f ? m : 1.f;
-    }
+    for (int pp = tid; pp < NP; pp += blockDim.x) rscale[pp] = dscale[X.soff + pp];
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -188,36 +255,26 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
     const uint32_t idesc = idesc_f16(kTcM, NP);
     const int nchunks = (v + kTcK - 1) / kTcK;
     bool ok = true;
+    // chunk c of the Coulomb slab (8 KB) and of the d tile (NP x 64 B), already in the
+    // canonical layout, into stage buffer c % kStages: 16-byte copies, one commit group
+    // per chunk (empty past the last chunk, so the group count stays regular)
+    auto issue = [&](int c) {
+        if (c < nchunks) {
+            const int b = c % kStages;
+            const uint4 *wsrc = reinterpret_cast<const uint4 *>(w16 + X.woff + (int64_t)c * kTcM * kTcK);
+            const uint4 *dsrc = reinterpret_cast<const uint4 *>(d16 + X.doff + (int64_t)c * NP * kTcK);
+            uint4 *wdst = reinterpret_cast<uint4 *>(&As[b][0]);
+            uint4 *ddst = reinterpret_cast<uint4 *>(&Bs[b][0]);
+            for (int e = tid; e < kTcM * kTcK / 8; e += blockDim.x) cp_async16(wdst + e, wsrc + e);
+            for (int e = tid; e < NP * kTcK / 8; e += blockDim.x) cp_async16(ddst + e, dsrc + e);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    for (int c = 0; c < kStages - 1; c++) issue(c);
     for (int ch = 0; ch < nchunks; ch++) {
-        const int st = ch & 1;
-        if (ch >= 2 && !mbar_wait(&mbar[st], ((ch - 2) >> 1) & 1)) ok = false;
-        const int c0 = ch * kTcK;
-        // Coulomb tile A[m][k] = v(n_a - n_c): each thread owns one k and strides over m
-        {
-            const int k = tid & (kTcK - 1);
-            const int c = c0 + k;
-            const bool cok = c < v;
-            const int4 nc = cok ? nv4[s.orb0 + vir[B.vir0 + c]] : make_int4(0, 0, 0, 0);
-            for (int m = tid / kTcK; m < kTcM; m += 128 / kTcK) {
-                float w = 0.f;
-                if (cok && T.a0 + m < v) {
-                    const int q2 = q2_of(na[m], nc);
-                    w = vsm ? sv[q2] : (float)vtab[s.vtab0 + q2];
-                }
-                As[st][cm_off(m, k)] = __float2half_rn(w);
-            }
-        }
-        // d tile B[n][k] = (t - t_ref)[p][c] / scale_p
-        for (int e = tid; e < NP * kTcK; e += blockDim.x) {
-            const int pp = e / kTcK, k = e % kTcK;
-            const int p = T.p0 + pp, c = c0 + k;
-            float x = 0.f;
-            if (p < o && c < v) {
-                const int64_t idx = B.t0 + (int64_t)p * v + c;
-                x = (float)((t[idx] - t_ref[idx]) / (double)rscale[pp]);
-            }
-            Bs[st][cm_off(pp, k)] = __float2half_rn(x);
-        }
+        const int st = ch % kStages;
+        // chunk ch landed (its group and all older ones; kStages - 2 newer may be pending)
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -229,8 +286,14 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
                        (ch > 0 || j > 0) ? 1u : 0u);
             tc_commit(&mbar[st]);
         }
+        // refill the buffer of chunk ch - 1 once its MMA is done, while MMA ch runs
+        const int nx = ch + kStages - 1;
+        if (nx < nchunks && nx >= kStages && !mbar_wait(&mbar[nx % kStages], ((nx - kStages) / kStages) & 1))
+            ok = false;
+        issue(nx);
     }
-    if (!mbar_wait(&mbar[(nchunks - 1) & 1], ((nchunks - 1) >> 1) & 1)) ok = false;
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (!mbar_wait(&mbar[(nchunks - 1) % kStages], ((nchunks - 1) / kStages) & 1)) ok = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
@@ -259,17 +322,28 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(NCOL));
 }
 
+void launch_w16_build(const DevBatch &d, cudaStream_t st)
+{
+    if (d.nwslabs > 0)
+        k_w16_build<<<d.nwslabs, 128, 0, st>>>(d.wslabs, d.blocks, d.solves, d.vir, d.nv4, d.vtab,
+                                               static_cast<__half *>(d.w16));
+}
+
 void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st)
 {
+    const __half *w = static_cast<const __half *>(d.w16), *dd = static_cast<const __half *>(d.d16);
+    if (d.ndtiles > 0)
+        k_delta16<<<d.ndtiles, 128, 0, st>>>(d.dtiles, d.blocks, d.t, t_ref, static_cast<__half *>(d.d16), d.dscale,
+                                             d.active);
     if (d.ntc16)
-        k_ladder_tc<16><<<d.ntc16, 128, 0, st>>>(d.tctiles, d.blocks, d.solves, d.vir, d.nv4, d.vtab, d.t, t_ref,
-                                                  g_ref, d.g, d.active, err);
+        k_ladder_tc<16><<<d.ntc16, 128, 0, st>>>(d.tctiles, d.tcx, d.blocks, w, dd, d.dscale, g_ref, d.g, d.active,
+                                                  err);
     if (d.ntc32)
-        k_ladder_tc<32><<<d.ntc32, 128, 0, st>>>(d.tctiles + d.ntc16, d.blocks, d.solves, d.vir, d.nv4, d.vtab, d.t,
-                                                  t_ref, g_ref, d.g, d.active, err);
+        k_ladder_tc<32><<<d.ntc32, 128, 0, st>>>(d.tctiles + d.ntc16, d.tcx + d.ntc16, d.blocks, w, dd, d.dscale,
+                                                  g_ref, d.g, d.active, err);
     if (d.ntc64)
-        k_ladder_tc<64><<<d.ntc64, 128, 0, st>>>(d.tctiles + d.ntc16 + d.ntc32, d.blocks, d.solves, d.vir, d.nv4,
-                                                  d.vtab, d.t, t_ref, g_ref, d.g, d.active, err);
+        k_ladder_tc<64><<<d.ntc64, 128, 0, st>>>(d.tctiles + d.ntc16 + d.ntc32, d.tcx + d.ntc16 + d.ntc32,
+                                                  d.blocks, w, dd, d.dscale, g_ref, d.g, d.active, err);
 }
 
 }  // namespace uegccd

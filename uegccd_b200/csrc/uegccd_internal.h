@@ -57,6 +57,25 @@ struct LadderTile {
     int blk, a0, p0, pad;
 };
 
+// Mixed precision: where a tensor-core ladder tile finds its FP16 operands, in the MMA's
+// canonical K-major layout (32-wide K chunks): the block's Coulomb slab of its 128 virtuals
+// (static; woff, in halves) and the scaled d = t - t_ref rows of its row tile (each
+// iteration; doff in halves, row scales at soff).
+struct TcTileDev {
+    int64_t woff, doff;
+    int32_t soff, pad;
+};
+// One FP16 Coulomb slab (block blk, virtuals a0 .. a0+127, every K chunk) to build.
+struct WSlabDev {
+    int blk, a0;
+    int64_t woff;
+};
+// One row tile (block blk, rows p0 .. p0+np-1) of scaled FP16 d to write each iteration.
+struct DTileDev {
+    int blk, p0, np, soff;
+    int64_t doff;
+};
+
 // Per-amplitude record: orbital indices local to the solve (a, b absolute, >= O).
 struct AmpInfo {
     int16_t i, j, a, b;
