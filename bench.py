@@ -525,6 +525,7 @@ def main():
             "clocks": g["clocks"], "roofline": roof,
             "kernels": {k: {"ms": v[0], "launches": v[1], **({"roofline": kern[k]} if k in kern else {})}
                         for k, v in stats.items()},
+            "ccd_iterations_per_s": g["value"] * g["niter_mean"],   # solve-iterations of all twists per second
             "check": {"niter_mean": g["niter_mean"], "niter_min": g["niter_min"], "niter_max": g["niter_max"],
                       "not_converged": g["fails"], "ecorr_twist0": g["ecorr_first"], "e2_twist0": g["e2_first"],
                       "pp_ladder_gflop_per_iter": flops_pp / 1e9,
