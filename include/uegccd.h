@@ -228,9 +228,9 @@ int uegccd_mp2_energy_static(const UegccdSystem *sys, void *stream, double *e2);
  * page-locked t_abab (cudaHostAlloc / cudaHostRegister) receives the copy directly;
  * pageable memory goes through a cached pinned buffer. */
 int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab);
-/* A destroyed batch leaves its device memory in a small per-process cache (at most
- * 8 GiB) that the next batch reuses, and large amplitude downloads keep a pinned host
- * staging buffer; this returns both to the driver. */
+/* A destroyed batch leaves its device memory in a per-process cache (at most 32 GiB)
+ * that the next batch reuses, and large amplitude downloads keep a pinned host staging
+ * buffer; this returns both to the driver. */
 int uegccd_trim_cache(void);
 
 /* Solve s's per-iteration energies and biggest changes from the last batch solve (the

@@ -89,7 +89,7 @@ int check_device()
 // bytes) for the next batch; uegccd_trim_cache returns them to the driver.
 namespace {
 constexpr size_t kArenaChunk = 64ull << 20;
-constexpr size_t kPoolCap = 8ull << 30;
+constexpr size_t kPoolCap = 32ull << 30;   // a 100-twist N=54 batch takes ~3 GB; pipelines keep 3-4 alive
 struct DevChunk {
     char *p;
     size_t size;
@@ -566,9 +566,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->alloc(d.g, amp0))) return rc;
     if ((rc = b->alloc(d.jvv, jvv0))) return rc;
     if ((rc = b->alloc(d.joo, joo0))) return rc;
-    if ((rc = b->alloc(d.J1, ph0))) return rc;
-    if ((rc = b->alloc(d.J2, ph0))) return rc;
-    if ((rc = b->alloc(d.J3, ph0))) return rc;
+    d.ph_total = ph0;
     if ((rc = b->alloc(d.hh, hhoff))) return rc;
     if ((rc = b->alloc(d.part_e, chunks.size()))) return rc;
     if ((rc = b->alloc(d.part_dt, chunks.size()))) return rc;
@@ -823,6 +821,7 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     CU(cudaMemsetAsync(b.ctl.Bm, 0, (size_t)n * kDiisMax * kDiisMax * sizeof(double), b.stream));
     if ((rc = set_active_all(b, 1))) return rc;
     if (opt->precision == UEGCCD_MIXED && (rc = mixed_alloc(b))) return rc;
+    if (drpa && !d.J1 && (rc = b.alloc(d.J1, (size_t)d.ph_total))) return rc;
     if (d.tc_err) CU(cudaMemsetAsync(d.tc_err, 0, sizeof(int), b.stream));
     if (!b.rings_tuned && !drpa && (f.do_ring || f.do_xring) && (rc = tune_batch_rings(b))) return rc;
     b.launches = 0;
@@ -1278,7 +1277,7 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     b += A * (8 * 5 + 16 + sizeof(AmpInfo) + 4);     // t, t_new, g, g_rq, g_xq; Coulomb factors; amps; partner
     b += sum_ov * (8 + 4) + (V + O + 1) * (4 + 8);   // mosaic partials and target lists
     b += O * O * V * 4;                              // pos
-    b += O * V * O * 8 * 3;                          // dRPA ring intermediates
+    b += O * V * O * 8;                              // dRPA ring intermediate (allocated for dRPA only)
     b += O * V * 2 * 2;                              // ph rows
     b += O * V * O * 4 * 2;                          // ring gather indices
     b += hh * 8 + nblk * (sizeof(BlockDev) + 8) + M * (16 + 8) + (P.q2max + 1) * 8;

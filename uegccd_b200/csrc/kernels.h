@@ -39,7 +39,8 @@ struct DevBatch {
     double *t = nullptr, *t_new = nullptr, *g = nullptr;
     double2 *vcoef = nullptr;         // per amplitude {v(i-a), v(a-j)} (k_vcoef, once per batch)
     double *jvv = nullptr, *joo = nullptr;
-    double *J1 = nullptr, *J2 = nullptr, *J3 = nullptr;
+    double *J1 = nullptr;             // dRPA ring intermediate (on the first dRPA solve)
+    int64_t ph_total = 0;             // O*V*O entries summed over the solves
     int64_t *hh0 = nullptr;          // per block: offset of H_K in hh
     double *hh = nullptr;
     double *part_e = nullptr, *part_dt = nullptr, *part_r = nullptr;

@@ -533,23 +533,16 @@ void set_mosaic_smem_limit(size_t bytes)
 }
 
 // ----------------------------------------------------------------------------
-// Ring intermediates (quadratic rings CCD.f90:771-797, quadratic crossed rings
-// CCD.f90:899-925), for every (i, x, l) with x virtual:
-//   c = partner of (i,k,x); vd = v(i-x); ve = v(c-l) = v(i+k-x-l)
-//   J1 = sum_k (2t(ik,x) - t(ik,c)) vd - (t(ik,x) - t(ik,c)) ve
-//   J2 = sum_k (2t(ik,x) - t(ik,c)) vd - t(ik,x) ve
-//   J3 = sum_k ve t(ki,x)
-// dRPA (dRPA.f90:517-535): J1 = sum_k 2 t(ik,x) vd.
+// dRPA ring intermediate (dRPA.f90:517-535), for every (i, x, l) with x virtual:
+//   J1 = sum_k 2 t(ik,x) v(i-x).
 // The reference skips (i,x,l) when d = n_l + n_x - n_i is not a virtual; the apply
-// step below makes the same test, so J is formed for every l.
-// Layout: J[ph0 + (i*V + x)*O + l].
+// step in k_update makes the same test, so J1 is formed for every l.
+// Layout: J1[ph0 + (i*V + x)*O + l].  (The CCD rings use k_rings.)
 // ----------------------------------------------------------------------------
 __global__ void k_ring_int(const ChunkDev *__restrict__ rchunks, const SolveDev *__restrict__ solves,
-                           const AmpInfo *__restrict__ amps, const int32_t *__restrict__ partner,
                            const int32_t *__restrict__ pos, const int4 *__restrict__ nv4,
-                           const double *__restrict__ vtab, const double *__restrict__ t, int drpa,
-                           double *__restrict__ J1, double *__restrict__ J2, double *__restrict__ J3,
-                           const uint8_t *__restrict__ active)
+                           const double *__restrict__ vtab, const double *__restrict__ t,
+                           double *__restrict__ J1, const uint8_t *__restrict__ active)
 {
     const ChunkDev ch = rchunks[blockIdx.x];
     if (!active[ch.solve]) return;
@@ -557,32 +550,16 @@ __global__ void k_ring_int(const ChunkDev *__restrict__ rchunks, const SolveDev 
     const int O = s.O, V = s.V;
     const int e = ch.start + threadIdx.x;
     if (e >= O * V * O) return;
-    const int l = e % O;
     const int ix = e / O;
     const int x = ix % V + O;
     const int i = ix / V;
     const double vd = vpq(s, nv4, vtab, i, x);
-    const int4 nl = nv4[s.orb0 + l];
-    double j1 = 0.0, j2 = 0.0, j3 = 0.0;
+    double j1 = 0.0;
     for (int k = 0; k < O; k++) {
-        int p1 = posmap(s, pos, i, k, x);
-        if (p1 < 0) continue;
-        double tx = t[p1];
-        if (drpa) {
-            j1 += 2.0 * tx * vd;
-            continue;
-        }
-        int c = amps[p1].b;
-        double ty = t[partner[p1]];
-        double ve = vtab[s.vtab0 + q2_of(nv4[s.orb0 + c], nl)];
-        j1 += (2.0 * tx - ty) * vd - (tx - ty) * ve;
-        j2 += (2.0 * tx - ty) * vd - tx * ve;
-        int p3 = posmap(s, pos, k, i, x);  // same partner c as (i,k,x): always allowed
-        if (p3 >= 0) j3 += ve * t[p3];
+        const int p1 = posmap(s, pos, i, k, x);
+        if (p1 >= 0) j1 += 2.0 * t[p1] * vd;
     }
-    const int64_t off = s.ph0 + e;
-    J1[off] = j1;
-    if (!drpa) { J2[off] = j2; J3[off] = j3; }
+    J1[s.ph0 + e] = j1;
 }
 
 // ----------------------------------------------------------------------------
@@ -1093,7 +1070,7 @@ struct UpdateArgs {
     double *t_new;
     const double *g_ladder;
     const double *jvv, *joo;
-    const double *J1, *J2, *J3;
+    const double *J1;             // dRPA ring intermediate
     double *part_e, *part_dt, *part_r;
     double *g_out;            // optional: full G per amplitude (term checks)
     const double *g_rq, *g_xq;
@@ -1764,8 +1741,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     }
     if ((f.do_ring || f.do_xring) && f.drpa) {
         kt->begin(KID_RING_INT, st);
-        k_ring_int<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.amps, d.partner, d.pos, d.nv4, d.vtab, d.t,
-                                                  f.drpa, d.J1, d.J2, d.J3, d.active);
+        k_ring_int<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.pos, d.nv4, d.vtab, d.t, d.J1, d.active);
         kt->end(st);
         n++;
     }
@@ -1790,7 +1766,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     UpdateArgs A;
     A.chunks = d.chunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.pos = d.pos;
     A.nv4 = d.nv4; A.eigen = d.eigen; A.vtab = d.vtab; A.t = d.t; A.t_new = d.t_new; A.g_ladder = d.g;
-    A.jvv = d.jvv; A.joo = d.joo; A.J1 = d.J1; A.J2 = d.J2; A.J3 = d.J3;
+    A.jvv = d.jvv; A.joo = d.joo; A.J1 = d.J1;
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
