@@ -217,7 +217,8 @@ def plan_stats(sysl):
         mq = tuple(-q for q in Q)
         if Q < mq and mq in groups:
             n2 = groups[mq]
-            ring += 14 * n1 * n2 * (n1 + n2)
+            a, b = min(n1, n2), max(n1, n2)
+            ring += 10 * a * a * b + 4 * a * b * b
     return {"O": O, "V": M - O, "A": sum(o * v for o, v in ov), "ov2": sum(o * v * v for o, v in ov),
             "o2v": sum(o * o * v for o, v in ov), "ring_flop": ring}
 
@@ -231,8 +232,9 @@ def kernel_units(st):
         "k_ladder_hh": ("flop", 2 * st["o2v"]),
         # pp ladder on the tensor cores (FP16 operands)
         "k_ladder_tc": ("tflop16", 2 * st["ov2"]),
-        # per {Q, -Q} group pair (n1, n2 rows): X W, Y W of both groups, 4 n1 n2 (n1 + n2), and
-        # the ring and crossed-ring products of both directions, 10 n1 n2 (n1 + n2)
+        # per {Q, -Q} group pair, n1 <= n2 rows: X W and Y W of the smaller group, 4 n1^2 n2,
+        # and the ring and crossed-ring products of one direction (the other is its mirror),
+        # 6 n1^2 n2 + 4 n1 n2^2
         "k_rings": ("flop", st["ring_flop"]),
         # reads t once (s is formed in registers; the partial sums are small)
         "k_mosaic_blk": ("byte", 8 * A),

@@ -349,7 +349,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             const auto &G = P.groups[gi];
             if (G.partner < 0 || G.partner < (int)gi) continue;  // each {Q, -Q} once
             const auto &H2 = P.groups[G.partner];
-            rpairs.push_back(RingPairDev{s, G.r0, G.n, H2.r0, H2.n});
+            // the smaller group first: k_rings gathers and multiplies from its side
+            if (G.n <= H2.n) rpairs.push_back(RingPairDev{s, G.r0, G.n, H2.r0, H2.n});
+            else rpairs.push_back(RingPairDev{s, H2.r0, H2.n, G.r0, G.n});
         }
         for (const auto &B : P.blocks) {
             BlockDev bd;

@@ -741,19 +741,27 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
 // t(i_a k, x_a) exists exactly for k in occ2 = {i_b}: its partner is x_b.  So every
 // ph row of one group is dense over the occupied indices of the other group:
 //   X1[a][b] = t(i_a i_b, x_a)   Y1[a][b] = t(i_b i_a, x_a)   (n1 x n2)
-//   X2[b][a] = t(i_b i_a, x_b)   Y2[b][a] = t(i_a i_b, x_b)   (n2 x n1)
-//   W[b][a]  = v(n_{i_b} - n_{i_a} - Q)      (the -Q group uses W^T)
+// The rows of group 2 hold the same amplitudes transposed: by the pair symmetry
+// t(ij, a) = t(ji, b) (T2abab(ij,ab) = T2abab(ji,ba)),
+//   X2[b][a] = t(i_b i_a, x_b) = X1[a][b],   Y2[b][a] = t(i_a i_b, x_b) = Y1[a][b],
+// so only X1 and Y1 are gathered.  With
+//   W[b][a]  = v(n_{i_b} - n_{i_a} - Q)
 //   Vs1[a][a'] = v(n_{i_a'} - n_{i_a}),  Vs2[b][b'] = v(n_{i_b'} - n_{i_b})
-//   XW1 = X1 W,  U1 = Y1 W - Vs1,   XW2 = X2 W^T,  U2 = Y2 W^T - Vs2
-// and the fused ring form above becomes, for the amplitude pair (a, b):
+//   XW1 = X1 W,  U1 = Y1 W - Vs1
+// the fused ring form above becomes, for the amplitude pair (a, b):
 //   ring (i_a, i_b, x_a) = lin + base_a (2 Sx_b - Sy_b)
-//                          + sum_a' [XW1[a][a'] (Y2 - 2 X2)[b][a'] + U1[a][a'] X2[b][a']]
+//                          + sum_a' [XW1[a][a'] (Y1 - 2 X1)[a'][b] + U1[a][a'] X1[a'][b]]
 //                          - sum_b' X1[a][b'] Vs2[b][b']
-//   xring(i_a, i_b, x_b) = sum_a' U1[a][a'] Y2[b][a'] - sum_b' Y1[a][b'] Vs2[b][b']
-// (lin, base as above), and the same with 1 <-> 2 for the amplitudes (i_b, i_a, .).
-// The matrix sides are the group sizes (padded to 8), not NOcc.  Row strides are
-// the padded width + 4 (= 4 or 12 mod 16 doubles): fragment loads without bank
-// conflicts.
+//   xring(i_a, i_b, x_b) = sum_a' U1[a][a'] Y1[a'][b] - sum_b' Y1[a][b'] Vs2[b][b']
+// (lin, base as above; Sx_b, Sy_b are the column sums of X1, Y1).  The residual
+// terms share the pair symmetry (ring and crossed-ring G of (j,i,b) equal those of
+// (i,j,a)), so each value is stored twice: the ring value also at (i_b, i_a, x_b) and
+// the crossed-ring value also at (i_b, i_a, x_a).  The reference forms both halves
+// separately (CCD.f90:716-937); the two agree to rounding.
+// Group 1 is the smaller group (the host orders each pair), which minimises both the
+// shared memory, 2 N1 (N1 + N2 + 8) doubles, and the work, 5 N1^2 N2 + 2 N1 N2^2 DMMA
+// multiply-adds.  Row strides are the padded width + 4 (= 4 or 12 mod 16 doubles):
+// fragment loads without bank conflicts, row-wise and transposed.
 // ----------------------------------------------------------------------------
 constexpr int kRingGather = 8;   // gather elements in flight per thread
 
@@ -763,7 +771,7 @@ size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
 {
     const size_t N1 = round8(n1), N2 = round8(n2), l1 = N1 + 4, l2 = N2 + 4;
     const size_t nsv = q2max < kVtabSmem ? round8(q2max + 1) : 0;
-    const size_t dbl = 2 * N1 * l2 + 2 * N2 * l1 + 2 * N1 * l1 + 2 * N2 * l2 + 3 * (N1 + N2) + nsv;
+    const size_t dbl = 2 * N1 * l2 + 2 * N1 * l1 + 3 * (N1 + N2) + nsv;
     return sizeof(double) * dbl + sizeof(int) * 2 * (N1 + N2) + sizeof(int4) * ((size_t)O + 2 * (N1 + N2));
 }
 
@@ -793,13 +801,9 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     // read them (from the rows' n-vectors) instead of stored, for more CTAs per SM
     double *X1 = smem;              // N1 x l2
     double *Y1 = X1 + N1 * l2;      // N1 x l2
-    double *X2 = Y1 + N1 * l2;      // N2 x l1
-    double *Y2 = X2 + N2 * l1;      // N2 x l1
-    double *XW1 = Y2 + N2 * l1;     // N1 x l1
+    double *XW1 = Y1 + N1 * l2;     // N1 x l1
     double *U1 = XW1 + N1 * l1;     // N1 x l1
-    double *XW2 = U1 + N1 * l1;     // N2 x l2
-    double *U2 = XW2 + N2 * l2;     // N2 x l2
-    double *Sx = U2 + N2 * l2;      // R: group 1 rows at [0, N1), group 2 rows at [N1, R)
+    double *Sx = U1 + N1 * l1;      // R: group 1 rows at [0, N1), group 2 rows at [N1, R)
     double *Sy = Sx + R;
     double *Vd = Sy + R;
     double *sv = Vd + R;            // nsv
@@ -808,7 +812,6 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     int4 *no = (int4 *)(rw + R);    // O
     int4 *nx = no + O;              // R: n-vector of the row's virtual
     int4 *nr = nx + R;              // R: n-vector of the row's occupied index (0 on padding)
-    // the CTA is 1, 2 or 4 warps, by pair size
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, kWarps = nt >> 5;
     auto V = [&](int q2) -> double {
         return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]));
@@ -829,9 +832,9 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     const int4 q1x = nx[0], q1i = no[ri[0]];
     const int Qx = q1x.x - q1i.x, Qy = q1x.y - q1i.y, Qz = q1x.z - q1i.z;
     const int32_t *gx = ridx_x + s.ph0, *gy = ridx_y + s.ph0;
-    // gathers: (X1, Y1) over (a, b), then (X2, Y2) over (b, a), as one flat range; the
-    // index loads of a batch are issued before its amplitude loads
-    const int ne1 = N1 * N2, ne = 2 * ne1;
+    // gather X1, Y1 over (a, b); the index loads of a batch are issued before its
+    // amplitude loads
+    const int ne = N1 * N2;
     for (int e0 = tid; e0 < ne; e0 += nt * kRingGather) {
         int p1[kRingGather], p2[kRingGather];
 #pragma unroll
@@ -839,11 +842,9 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
             const int e = e0 + u * nt;
             p1[u] = p2[u] = -1;
             if (e < ne) {
-                const bool s2 = e >= ne1;
-                const int el = s2 ? e - ne1 : e, nc = s2 ? N1 : N2;
-                const int r = el / nc, c = el - r * nc;
-                if (r < (s2 ? n2 : n1) && c < (s2 ? n1 : n2)) {
-                    const int w = s2 ? rw[N1 + r] + ri[c] : rw[r] + ri[N1 + c];
+                const int r = e / N2, c = e - r * N2;
+                if (r < n1 && c < n2) {
+                    const int w = rw[r] + ri[N1 + c];
                     p1[u] = __ldg(&gx[w]);
                     p2[u] = __ldg(&gy[w]);
                 }
@@ -853,176 +854,165 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
         for (int u = 0; u < kRingGather; u++) {
             const int e = e0 + u * nt;
             if (e < ne) {
-                const bool s2 = e >= ne1;
-                const int el = s2 ? e - ne1 : e, nc = s2 ? N1 : N2;
-                const int r = el / nc, c = el - r * nc;
-                const int o = r * (nc + 4) + c;
-                (s2 ? X2 : X1)[o] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
-                (s2 ? Y2 : Y1)[o] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
+                const int r = e / N2, c = e - r * N2;
+                X1[r * l2 + c] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
+                Y1[r * l2 + c] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
             }
         }
     }
     __syncthreads();
+    // row sums of X1, Y1 for group 1, column sums for group 2 (padding is zero)
     for (int r = tid; r < R; r += nt) {
-        const bool g1 = r < N1;
-        const double *xr = g1 ? X1 + r * l2 : X2 + (r - N1) * l1;
-        const double *yr = g1 ? Y1 + r * l2 : Y2 + (r - N1) * l1;
-        const int nc = g1 ? n2 : n1;
         double sx = 0.0, sy = 0.0;
-        for (int c = 0; c < nc; c++) {
-            sx += xr[c];
-            sy += yr[c];
+        if (r < N1) {
+            for (int c = 0; c < n2; c++) {
+                sx += X1[r * l2 + c];
+                sy += Y1[r * l2 + c];
+            }
+        } else {
+            const int c = r - N1;
+            for (int a = 0; a < n1; a++) {
+                sx += X1[a * l2 + c];
+                sy += Y1[a * l2 + c];
+            }
         }
         Sx[r] = sx;
         Sy[r] = sy;
         Vd[r] = ri[r] >= 0 ? V(q2_of(no[ri[r]], nx[r])) : 0.0;
     }
     const int g = lane >> 2, tg = lane & 3;
-    // phase 1: XW1 = X1 W, U1 = Y1 W - Vs1 (K = N2); XW2 = X2 W^T, U2 = Y2 W^T - Vs2 (K = N1),
-    // with W[b][a] = v(n_{i_b} - n_{i_a} - Q) and Vs[c][c'] = v(n_{i_c'} - n_{i_c}) generated from
-    // the rows' n-vectors (0 on padding).  Tasks: one 8-row fragment row x up to 2 column
-    // fragments; X and Y share each generated W fragment.
+    // phase 1: XW1 = X1 W, U1 = Y1 W - Vs1 (K = N2), with W[b][a] = v(n_{i_b} - n_{i_a} - Q)
+    // and Vs1[a][a'] = v(n_{i_a'} - n_{i_a}) generated from the rows' n-vectors (0 on
+    // padding).  Tasks: one 8-row fragment row x up to 2 column fragments; X and Y share
+    // each generated W fragment.
     {
-        const int ng1 = (N1 + 15) / 16, ng2 = (N2 + 15) / 16;
-        const int t1 = (N1 / 8) * ng1, t2 = (N2 / 8) * ng2;
-        for (int task = warp; task < t1 + t2; task += kWarps) {
-            const bool grp2 = task >= t1;
-            const int tt = grp2 ? task - t1 : task, ngr = grp2 ? ng2 : ng1;
-            const int mf = tt / ngr, ng = tt - mf * ngr;
-            const int Ncol = grp2 ? N2 : N1, K = grp2 ? N1 : N2, lda = grp2 ? l1 : l2, ldo = grp2 ? l2 : l1;
-            const int nvc = grp2 ? n2 : n1, nvk = grp2 ? n1 : n2;    // valid columns, valid k
-            const int cb = grp2 ? N1 : 0, kb = grp2 ? 0 : N1;         // row slots of columns, of k
-            const double *AX = (grp2 ? X2 : X1) + (mf * 8 + g) * lda + tg;
-            const double *AY = (grp2 ? Y2 : Y1) + (mf * 8 + g) * lda + tg;
+        const int ngr = (N1 + 15) / 16, ntask = (N1 / 8) * ngr;
+        for (int task = warp; task < ntask; task += kWarps) {
+            const int mf = task / ngr, ng = task - mf * ngr;
+            const double *AX = X1 + (mf * 8 + g) * l2 + tg;
+            const double *AY = Y1 + (mf * 8 + g) * l2 + tg;
             const int nbase = ng * 16;
             int4 cn[2];
             bool cok[2];
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const int n = nbase + f * 8 + g;
-                cok[f] = n < nvc;
-                cn[f] = cok[f] ? nr[cb + n] : make_int4(0, 0, 0, 0);
+                cok[f] = n < n1;
+                cn[f] = cok[f] ? nr[n] : make_int4(0, 0, 0, 0);
             }
             double acc[2][2][2];
 #pragma unroll
             for (int f = 0; f < 2; f++) acc[0][f][0] = acc[0][f][1] = acc[1][f][0] = acc[1][f][1] = 0.0;
-            for (int k0 = 0; k0 < K; k0 += 4) {
+            for (int k0 = 0; k0 < N2; k0 += 4) {
                 const int k = k0 + tg;
                 const double ax = AX[k0], ay = AY[k0];
-                const bool kok = k < nvk;
-                const int4 kn = nr[kb + k];
+                const bool kok = k < n2;
+                const int4 kn = nr[N1 + k];
 #pragma unroll
                 for (int f = 0; f < 2; f++) {
-                    if (nbase + f * 8 >= Ncol) break;
-                    // group 1: B(k=b, n=a') = W[b][a'];  group 2: B(k=a, n=b') = W[b'][a]
+                    if (nbase + f * 8 >= N1) break;
+                    // B(k = b, n = a') = W[b][a']
                     double bv = 0.0;
                     if (kok && cok[f]) {
-                        const int4 hb = grp2 ? cn[f] : kn, ha = grp2 ? kn : cn[f];
-                        const int dx = hb.x - ha.x - Qx, dy = hb.y - ha.y - Qy, dz = hb.z - ha.z - Qz;
+                        const int dx = kn.x - cn[f].x - Qx, dy = kn.y - cn[f].y - Qy, dz = kn.z - cn[f].z - Qz;
                         bv = V(dx * dx + dy * dy + dz * dz);
                     }
                     dmma_884(acc[0][f][0], acc[0][f][1], ax, bv);
                     dmma_884(acc[1][f][0], acc[1][f][1], ay, bv);
                 }
             }
-            double *OX = grp2 ? XW2 : XW1, *OU = grp2 ? U2 : U1;
             const int r = mf * 8 + g;
-            const bool rok = r < nvc;
-            const int4 rn = rok ? nr[cb + r] : make_int4(0, 0, 0, 0);
+            const bool rok = r < n1;
+            const int4 rn = rok ? nr[r] : make_int4(0, 0, 0, 0);
 #pragma unroll
             for (int f = 0; f < 2; f++) {
-                if (nbase + f * 8 >= Ncol) break;
+                if (nbase + f * 8 >= N1) break;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int n = nbase + f * 8 + 2 * tg + h;
-                    const double vs = (rok && n < nvc) ? V(q2_of(nr[cb + n], rn)) : 0.0;
-                    OX[r * ldo + n] = acc[0][f][h];
-                    OU[r * ldo + n] = acc[1][f][h] - vs;
+                    const double vs = (rok && n < n1) ? V(q2_of(nr[n], rn)) : 0.0;
+                    XW1[r * l1 + n] = acc[0][f][h];
+                    U1[r * l1 + n] = acc[1][f][h] - vs;
                 }
             }
         }
     }
     __syncthreads();
-    // phase 2: dir 0 rows a x columns b, dir 1 rows b x columns a; tasks of 8 x 16
-    const int t1 = (N1 / 8) * ((N2 + 15) / 16), t2 = (N2 / 8) * ((N1 + 15) / 16);
-    for (int task = warp; task < t1 + t2; task += kWarps) {
-        const int dir = task < t1 ? 0 : 1, tt = dir ? task - t1 : task;
-        // dir 0: A side group 1 (XW1, U1 with K1 = N1 over a'; X1, Y1 with K2 = N2 over b'),
-        //        B side group 2 (X2, Y2 rows b over a'; Vs2 rows b over b')
-        const int Mv = dir ? n2 : n1, Nv = dir ? n1 : n2, Np = dir ? N1 : N2;
-        const int K1 = dir ? N2 : N1, K2 = dir ? N1 : N2;
-        const double *AXW = dir ? XW2 : XW1, *AU = dir ? U2 : U1;   // stride K1 + 4
-        const double *AX = dir ? X2 : X1, *AY = dir ? Y2 : Y1;      // stride K2 + 4
-        const double *BX = dir ? X1 : X2, *BY = dir ? Y1 : Y2;      // stride K1 + 4
-        const int lk1 = K1 + 4, lk2 = K2 + 4;
-        const int nng = (Np + 15) / 16;
-        const int mf = tt / nng, ng = tt - mf * nng;
+    // phase 2: rows a x columns b, tasks of 8 x 16
+    const int nng = (N2 + 15) / 16, ntask = (N1 / 8) * nng;
+    for (int task = warp; task < ntask; task += kWarps) {
+        const int mf = task / nng, ng = task - mf * nng;
         const int m0 = mf * 8;
         double ra[2][2], rb[2][2], xa[2][2], xb[2][2];
 #pragma unroll
         for (int f = 0; f < 2; f++)
 #pragma unroll
             for (int h = 0; h < 2; h++) ra[f][h] = rb[f][h] = xa[f][h] = xb[f][h] = 0.0;
-        for (int k0 = 0; k0 < K1; k0 += 4) {
+        // sum over a': A = XW1, U1 rows a; B(k = a', n = b) = X1[a'][b], Y1[a'][b]
+        for (int k0 = 0; k0 < N1; k0 += 4) {
             const int k = k0 + tg;
-            const double axw = AXW[(m0 + g) * lk1 + k], au = AU[(m0 + g) * lk1 + k];
+            const double axw = XW1[(m0 + g) * l1 + k], au = U1[(m0 + g) * l1 + k];
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const int n0 = ng * 16 + f * 8;
-                if (n0 >= Np) break;
-                const double bx = BX[(n0 + g) * lk1 + k], by = BY[(n0 + g) * lk1 + k];
+                if (n0 >= N2) break;
+                const double bx = X1[k * l2 + n0 + g], by = Y1[k * l2 + n0 + g];
                 dmma_884(ra[f][0], ra[f][1], axw, by - 2.0 * bx);
                 dmma_884(rb[f][0], rb[f][1], au, bx);
                 dmma_884(xa[f][0], xa[f][1], au, by);
             }
         }
-        // B = -Vs of the B side (dir 0: Vs2[b][b'], dir 1: Vs1[a][a']), generated
-        const int sb = dir ? 0 : N1, nvb = dir ? n1 : n2;
+        // sum over b': A = X1, Y1 rows a; B = -Vs2[b][b'], generated
         int4 bn[2];
         bool bok[2];
 #pragma unroll
         for (int f = 0; f < 2; f++) {
             const int bb = ng * 16 + f * 8 + g;
-            bok[f] = bb < nvb;
-            bn[f] = bok[f] ? nr[sb + bb] : make_int4(0, 0, 0, 0);
+            bok[f] = bb < n2;
+            bn[f] = bok[f] ? nr[N1 + bb] : make_int4(0, 0, 0, 0);
         }
-        for (int k0 = 0; k0 < K2; k0 += 4) {
+        for (int k0 = 0; k0 < N2; k0 += 4) {
             const int k = k0 + tg;
-            const double ax = AX[(m0 + g) * lk2 + k], ay = AY[(m0 + g) * lk2 + k];
-            const bool kok = k < nvb;
-            const int4 kn = nr[sb + k];
+            const double ax = X1[(m0 + g) * l2 + k], ay = Y1[(m0 + g) * l2 + k];
+            const bool kok = k < n2;
+            const int4 kn = nr[N1 + k];
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const int n0 = ng * 16 + f * 8;
-                if (n0 >= Np) break;
+                if (n0 >= N2) break;
                 const double bv = (kok && bok[f]) ? -V(q2_of(kn, bn[f])) : -0.0;
                 dmma_884(rb[f][0], rb[f][1], ax, bv);
                 dmma_884(xb[f][0], xb[f][1], ay, bv);
             }
         }
-        const int m = m0 + g;
-        if (m >= Mv) continue;
-        const int r1 = dir ? N1 + m : m;                 // this lane's row (slot index)
+        const int r1 = m0 + g;                          // this lane's row (group 1)
+        if (r1 >= n1) continue;
         const double vd = Vd[r1], sx1 = Sx[r1], sy1 = Sy[r1];
         const double base = vd * (2.0 * sx1 - sy1);
+        const int w1 = rw[r1], i1 = ri[r1];
 #pragma unroll
         for (int f = 0; f < 2; f++) {
             const int n0 = ng * 16 + f * 8;
-            if (n0 >= Np) break;
+            if (n0 >= N2) break;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int n = n0 + 2 * tg + h;
-                if (n >= Nv) continue;
-                const int r2 = dir ? n : N1 + n;
-                // ring amplitude (i_r1, i_r2, x_r1) and crossed ring (i_r1, i_r2, x_r2)
+                if (n >= n2) continue;
+                const int r2 = N1 + n, w2 = rw[r2], i2 = ri[r2];
+                // ring amplitude (i_a, i_b, x_a) and its mirror (i_b, i_a, x_b)
                 if (do_ring) {
                     const double lin = 2.0 * vd * (sx1 + Sx[r2]) - vd * (sy1 + Sy[r2]);
-                    const int p = __ldg(&gx[rw[r1] + ri[r2]]);
-                    if (p >= 0) g_rq[p] = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ra[f][h] + rb[f][h];
+                    const double v = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ra[f][h] + rb[f][h];
+                    const int p = __ldg(&gx[w1 + i2]), pm = __ldg(&gx[w2 + i1]);
+                    if (p >= 0) g_rq[p] = v;
+                    if (pm >= 0) g_rq[pm] = v;
                 }
+                // crossed ring (i_a, i_b, x_b) and its mirror (i_b, i_a, x_a)
                 if (do_xring) {
-                    const int p = __ldg(&gy[rw[r2] + ri[r1]]);
-                    if (p >= 0) g_xq[p] = xa[f][h] + xb[f][h];
+                    const double v = xa[f][h] + xb[f][h];
+                    const int p = __ldg(&gy[w2 + i1]), pm = __ldg(&gy[w1 + i2]);
+                    if (p >= 0) g_xq[p] = v;
+                    if (pm >= 0) g_xq[pm] = v;
                 }
             }
         }
