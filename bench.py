@@ -200,14 +200,17 @@ def plan_stats(sysl):
     O = nocc
     M = len(nv)
     idx = {tuple(v): p for p, v in enumerate(nv)}
-    blocks = defaultdict(lambda: [0, None])
+    blocks = defaultdict(lambda: [0, None, 0])   # rows, columns, rows with i <= j
     for i in range(O):
         for j in range(O):
             K = tuple(nv[i] + nv[j])
             blocks[K][0] += 1
+            blocks[K][2] += i <= j
             if blocks[K][1] is None:
                 blocks[K][1] = sum(1 for a in range(O, M) if idx.get(tuple(np.array(K) - nv[a]), -1) >= O)
-    ov = [(o, v) for o, v in blocks.values() if v > 0]
+    ov = [(o, v) for o, v, _ in blocks.values() if v > 0]
+    # the FP64 ladders form the rows i <= j (the mirrors (j,i) follow by the pair symmetry)
+    ocv = [(oc, o, v) for o, v, oc in blocks.values() if v > 0]
     groups = defaultdict(int)
     for i in range(O):
         for x in range(O, M):
@@ -220,7 +223,8 @@ def plan_stats(sysl):
             a, b = min(n1, n2), max(n1, n2)
             ring += 10 * a * a * b + 4 * a * b * b
     return {"O": O, "V": M - O, "A": sum(o * v for o, v in ov), "ov2": sum(o * v * v for o, v in ov),
-            "o2v": sum(o * o * v for o, v in ov), "ring_flop": ring}
+            "ov2_half": sum(oc * v * v for oc, o, v in ocv), "o2v_half": sum(oc * o * v for oc, o, v in ocv),
+            "ring_flop": ring}
 
 
 def kernel_units(st):
@@ -228,8 +232,9 @@ def kernel_units(st):
     A = st["A"]
     ndiis = SOLVE_OPTS["ndiis"]
     return {
-        "k_ladder": ("flop", 2 * (st["ov2"] + st["o2v"])),
-        "k_ladder_hh": ("flop", 2 * st["o2v"]),
+        # rows i <= j: pp ladder sum_c v(a-c) t(p,c) and hole-hole apply sum_q H(p,q) t(q,a)
+        "k_ladder": ("flop", 2 * (st["ov2_half"] + st["o2v_half"])),
+        "k_ladder_hh": ("flop", 2 * st["o2v_half"]),
         # pp ladder on the tensor cores (FP16 operands)
         "k_ladder_tc": ("tflop16", 2 * st["ov2"]),
         # per {Q, -Q} group pair, n1 <= n2 rows: X W and Y W of the smaller group, 4 n1^2 n2,
@@ -512,7 +517,7 @@ def main():
     roof["kernel"] = top
     tr = TRAFFIC_PER_SOLVE.get(top)
     roof["traffic"] = tr * nsys if tr else None
-    flops_pp = sum(ps["ov2"] * 2 for ps in per_solve) / len(per_solve) * nsys
+    flops_pp = sum(ps["ov2_half"] * 2 for ps in per_solve) / len(per_solve) * nsys
     config["ring_cta_threads"] = g["ring_threads"]   # per ring pair class, picked by the launch-shape tuner
     if args.precision == "mixed":
         config["precision"] = "particle-particle ladder FP16 tensor cores (FP32 accumulate), rest FP64"

@@ -359,6 +359,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             bd.pair0 = (int)pair_i.size() + B.pair0;
             bd.vir0 = (int)vir.size() + B.vir0;
             bd.t0 = amp0 + B.t0;
+            bd.nd = B.nd;
+            bd.dg = B.dg;
             bd.row0 = mrows;
             bd.col0 = mcols;   // shifted past all rows below
             mrows += B.o;
@@ -369,13 +371,16 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             hhoff += (int64_t)B.o * B.o;
             max_o = std::max(max_o, B.o);
             max_v = std::max(max_v, B.v);
-            // row tiles of 32 pairs, the last one the remainder rounded up to 8 (8, 16, 24 or 32):
-            // at most 7 padded rows per block; columns in tiles of 128 (4 warps x 32)
-            auto row_tile = [&](int p0) { return std::min(32, (B.o - p0 + 7) & ~7); };
+            // FP64 ladder tiles cover the rows up to the diagonal pair (oc = nd + dg); k_ladder3
+            // writes each mirror row from its pair (i,j) with the pair symmetry.  Row tiles of 32
+            // pairs, the last one the remainder rounded up to 8 (8, 16, 24 or 32): at most 7
+            // padded rows per block; columns in tiles of 128 (4 warps x 32)
+            const int oc = B.nd + B.dg;
+            auto row_tile = [&](int p0) { return std::min(32, (oc - p0 + 7) & ~7); };
             for (int a0 = 0; a0 < B.v; a0 += 128)
-                for (int p0 = 0; p0 < B.o; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, row_tile(p0)});
+                for (int p0 = 0; p0 < oc; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, row_tile(p0)});
             for (int q0 = 0; q0 < B.o; q0 += 128)
-                for (int p0 = 0; p0 < B.o; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
+                for (int p0 = 0; p0 < oc; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
             // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows; their FP16 operands: one
             // Coulomb slab per 128 virtuals, one d tile per row tile, each over all K chunks
             const int ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
@@ -465,6 +470,24 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     DevBatch &d = b->d;
     d.nsolves = n;
     d.nblocks = (int)blocks.size();
+    // ladder tiles by row-tile class (stable: block order within a class)
+    auto by_class = [](std::vector<LadderTile> &v, int *cnt) {
+        std::vector<LadderTile> out;
+        out.reserve(v.size());
+        for (int c = 0; c < kLadderClasses; c++) {
+            cnt[c] = 0;
+            for (const auto &x : v)
+                if (x.pad == 8 * (c + 1)) {
+                    out.push_back(x);
+                    cnt[c]++;
+                }
+        }
+        v.swap(out);
+    };
+    const size_t ntl = tiles.size(), nhtl = htiles.size();
+    by_class(tiles, d.ntile_cls);
+    by_class(htiles, d.nhtile_cls);
+    if (tiles.size() != ntl || htiles.size() != nhtl) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder row tile outside the 8/16/24/32 classes");
     d.ntiles = (int)tiles.size();
     d.nhtiles = (int)htiles.size();
     d.ntc16 = (int)tc16.size();
@@ -488,9 +511,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.ntargets = (int)targets.size();
     d.max_o = max_o;
     d.max_v = max_v;
-    d.ladder_smem = ladder_smem_bytes(max_v);
-    if (d.ladder_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder block exceeds shared memory");
-    set_ladder_smem_limit(d.ladder_smem);
+    if (ladder_smem_bytes(max_v, 32) > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder block exceeds shared memory");
+    set_ladder_smem_limit(max_v);
     d.mosaic_smem = mosaic_smem_bytes(max_v);
     if (d.mosaic_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "mosaic block exceeds shared memory");
     set_mosaic_smem_limit(d.mosaic_smem);

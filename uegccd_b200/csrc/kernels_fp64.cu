@@ -174,7 +174,11 @@ __global__ void k_reduce_solves(const int *__restrict__ chunk_begin, const doubl
 // particle-particle (CCD.f90:660-681): W_K[c][a] = v(c-a) over the block's virtuals;
 // hole-hole (CCD.f90:611-657): H_K[p][q] = v(i_p - k_q) + sum_c t_K[p][c] v(c - k_q),
 // p = (i,j), q = (k,l), after the pair-swap re-indexing t(kl,b) = t(lk,a).
-// k_ladder2 in mode 1 builds H_K; in mode 0 it writes G (overwriting, so it runs first).
+// k_ladder3 in mode 1 builds H_K; in mode 0 it writes G (overwriting, so it runs first).
+// Both run over the rows p = (i,j) with i <= j only: by the pair symmetry
+// t(ij,a) = t(ji,b) (T2abab(ij,ab) = T2abab(ji,ba)) the ladder G of the mirror row (j,i)
+// at column b = K - a equals that of (i,j) at a, and mode 0 stores it there too.  The
+// reference forms both rows (CCD.f90:617-681); the two agree to rounding.
 // ----------------------------------------------------------------------------
 constexpr int kVtabSmem = 1024;  // |q|^2 table entries staged in shared memory
 
@@ -209,14 +213,15 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-size_t ladder_smem_bytes(int max_v)
+size_t ladder_smem_bytes(int max_v, int np)
 {
-    return sizeof(double) * (2 * 32 * kLadLd + kVtabSmem) + sizeof(int4) * (size_t)max_v;
+    return sizeof(double) * (2 * (size_t)np * kLadLd + kVtabSmem) + sizeof(int4) * (size_t)max_v;
 }
 
 template <int NP, bool KS>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
+                                             const int16_t *__restrict__ pcol,
                                              const int4 *__restrict__ nv4, const double *__restrict__ vtab,
                                              const double *__restrict__ t, const double *__restrict__ H, int mode,
                                              int do_pp, int do_hh, double *__restrict__ out, const double *sv,
@@ -226,6 +231,7 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gid = lane >> 2, tig = lane & 3;
     const int v = B.v, o = B.o;
+    const int orow = B.nd + B.dg;   // rows computed: pairs i < j and the diagonal pair
     const int ncol = mode == 0 ? v : o;
     // hole-hole intermediate with at most 32 columns left: the 4 warps share the columns
     // and split the c sum instead (each takes every 4th k step), then reduce
@@ -255,7 +261,7 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
             for (int e = threadIdx.x; e < NP * kLadKC; e += blockDim.x) {
                 const int r = e / kLadKC, c = e - r * kLadKC;
                 const int p = T.p0 + r, cc = c0 + c;
-                if (p < o && cc < v) cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + cc);
+                if (p < orow && cc < v) cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + cc);
                 else dst[r * kLadLd + c] = 0.0;
             }
             cp_async_commit();
@@ -330,7 +336,7 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 #pragma unroll
             for (int n = 0; n < NN; n++) {
                 int p = T.p0 + n * 8 + gid;
-                bf[n] = (qok && p < o) ? H[(int64_t)p * o + q] : 0.0;
+                bf[n] = (qok && p < orow) ? H[(int64_t)p * o + q] : 0.0;
             }
 #pragma unroll
             for (int m = 0; m < 4; m++) {
@@ -350,9 +356,11 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int p = T.p0 + n * 8 + 2 * tig + h;
-                if (p >= o) continue;
+                if (p >= orow) continue;
                 if (mode == 0) {
                     out[B.t0 + (int64_t)p * v + col] = acc[m][n][h];
+                    // the mirror (j,i) at the partner column K - a (none for the diagonal pair)
+                    if (p < B.nd) out[B.t0 + (int64_t)(p + orow) * v + pcol[B.vir0 + col]] = acc[m][n][h];
                 } else {
                     const int4 ni = nv4[s.orb0 + pair_i[B.pair0 + p]];
                     const int q2 = q2_of(ni, na[m]);
@@ -362,22 +370,24 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     }
 }
 
-__global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ tiles,
-                                                const BlockDev *__restrict__ blocks,
-                                                const SolveDev *__restrict__ solves,
-                                                const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
-                                                const int4 *__restrict__ nv4, const double *__restrict__ vtab,
-                                                const double *__restrict__ t, const int64_t *__restrict__ hh0,
-                                                double *__restrict__ hh, int mode, int do_pp, int do_hh,
-                                                double *__restrict__ g, const uint8_t *__restrict__ active)
+// One kernel per row tile NP (8, 16, 24, 32 pairs): the small tiles need fewer registers
+// and less shared memory, so more CTAs fit on an SM to hide the lookup latency.
+template <int NP>
+__global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
+    k_ladder3(const LadderTile *__restrict__ tiles, const BlockDev *__restrict__ blocks,
+              const SolveDev *__restrict__ solves, const int16_t *__restrict__ vir,
+              const int16_t *__restrict__ pair_i, const int16_t *__restrict__ pcol,
+              const int4 *__restrict__ nv4, const double *__restrict__ vtab, const double *__restrict__ t,
+              const int64_t *__restrict__ hh0, double *__restrict__ hh, int mode, int do_pp, int do_hh,
+              double *__restrict__ g, const uint8_t *__restrict__ active)
 {
     const LadderTile T = tiles[blockIdx.x];
     const BlockDev B = blocks[T.blk];
     if (!active[B.solve]) return;
     const SolveDev s = solves[B.solve];
     extern __shared__ double lsm[];
-    double *ts = lsm;                              // 2 x 32 x kLadLd
-    double *sv = ts + 2 * 32 * kLadLd;             // kVtabSmem
+    double *ts = lsm;                              // 2 x NP x kLadLd
+    double *sv = ts + 2 * NP * kLadLd;             // kVtabSmem
     int4 *nvc = (int4 *)(sv + kVtabSmem);          // v_K n-vectors of the block's virtuals
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
@@ -387,35 +397,54 @@ __global__ void __launch_bounds__(128) k_ladder3(const LadderTile *__restrict__ 
     double *H = hh + hh0[T.blk];
     double *out = mode == 0 ? g : H;
     // the hole-hole intermediate (mode 1) may split its c sum across the warps
-    if (mode == 1) {
-        switch (T.pad) {
-        case 8: ladder3_tile<8, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-        case 16: ladder3_tile<16, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-        case 24: ladder3_tile<24, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-        default: ladder3_tile<32, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-        }
-        return;
-    }
-    switch (T.pad) {
-    case 8: ladder3_tile<8, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-    case 16: ladder3_tile<16, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-    case 24: ladder3_tile<24, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-    default: ladder3_tile<32, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc); break;
-    }
+    if (mode == 1)
+        ladder3_tile<NP, true>(T, B, s, vir, pair_i, pcol, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
+    else
+        ladder3_tile<NP, false>(T, B, s, vir, pair_i, pcol, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
 }
 
 // The dynamic shared-memory limits only grow (batches of different sizes coexist), under
 // one lock: batches are created from several host threads while others solve.
 static std::mutex g_smem_limit_mu;
 
-void set_ladder_smem_limit(size_t bytes)
+void set_ladder_smem_limit(int max_v)
 {
     std::lock_guard<std::mutex> lock(g_smem_limit_mu);
-    static size_t current = 48 * 1024;
-    if (bytes > current) {
-        cudaFuncSetAttribute(k_ladder3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        current = bytes;
+    static int current = 0;
+    if (max_v > current) {
+        cudaFuncSetAttribute(k_ladder3<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 8));
+        cudaFuncSetAttribute(k_ladder3<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 16));
+        cudaFuncSetAttribute(k_ladder3<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 24));
+        cudaFuncSetAttribute(k_ladder3<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 32));
+        current = max_v;
     }
+}
+
+// Ladder tiles in row-tile classes (sorted 8, 16, 24, 32 pairs; counts in ncls): one launch
+// per non-empty class.  Returns the launches.
+static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int *ncls, const double *t, int mode,
+                          int do_pp, int do_hh, double *g, cudaStream_t st)
+{
+    int off = 0, n = 0;
+    for (int c = 0; c < kLadderClasses; c++) {
+        const int cnt = ncls[c];
+        if (cnt <= 0) continue;
+        const int np = 8 * (c + 1);
+        const size_t sm = ladder_smem_bytes(d.max_v, np);
+#define UEGCCD_LADDER_ARGS                                                                                  \
+    tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.pcol, d.nv4, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
+        g, d.active
+        switch (np) {
+        case 8: k_ladder3<8><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        case 16: k_ladder3<16><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        case 24: k_ladder3<24><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        default: k_ladder3<32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        }
+#undef UEGCCD_LADDER_ARGS
+        off += cnt;
+        n++;
+    }
+    return n;
 }
 
 // ----------------------------------------------------------------------------
@@ -1426,8 +1455,7 @@ __global__ void k_copy(int64_t n, const double *__restrict__ src, double *__rest
 void launch_refresh(const DevBatch &d, cudaStream_t st)
 {
     k_copy<<<(unsigned)((d.namp + 255) / 256), 256, 0, st>>>(d.namp, d.t, d.t_ref);
-    k_ladder3<<<d.ntiles, 128, d.ladder_smem, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t_ref, d.hh0,
-                                        d.hh, 0, 1, 0, d.g_ref, d.active);
+    launch_ladder3(d, d.tiles, d.ntile_cls, d.t_ref, 0, 1, 0, d.g_ref, st);
 }
 
 void launch_control(const DevBatch &d, const CtlBuffers &c, double tol, int max_iter, int ndiis, int init,
@@ -1699,17 +1727,13 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     if (f.do_ladder && d.nblocks > 0) {
         if (f.do_hh) {
             kt->begin(KID_HH_W, st);
-            k_ladder3<<<d.nhtiles, 128, d.ladder_smem, st>>>(d.htiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t,
-                                                 d.hh0, d.hh, 1, f.do_pp, f.do_hh, d.g, d.active);
+            n += launch_ladder3(d, d.htiles, d.nhtile_cls, d.t, 1, f.do_pp, f.do_hh, d.g, st);
             kt->end(st);
-            n++;
         }
         const int pp64 = (f.do_pp && !f.mixed) ? 1 : 0;
         kt->begin(KID_LADDER, st);
-        k_ladder3<<<d.ntiles, 128, d.ladder_smem, st>>>(d.tiles, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, d.t, d.hh0,
-                                            d.hh, 0, pp64, f.do_hh, d.g, d.active);
+        n += launch_ladder3(d, d.tiles, d.ntile_cls, d.t, 0, pp64, f.do_hh, d.g, st);
         kt->end(st);
-        n++;
         if (f.do_pp && f.mixed) {
             kt->begin(KID_LADDER_TC, st);
             launch_ladder_tc(d, d.t_ref, d.g_ref, d.tc_err, st);

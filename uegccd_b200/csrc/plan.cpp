@@ -116,10 +116,26 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
         blk.pair0 = (int)p.pair_i.size();
         blk.vir0 = (int)p.vir.size();
         blk.t0 = t0;
-        for (auto &pr : kpairs[k]) {
-            p.pair_i.push_back((int16_t)pr.first);
-            p.pair_j.push_back((int16_t)pr.second);
+        // rows: pairs i < j, the diagonal pair, then the mirrors (j,i) in the same order
+        blk.nd = blk.dg = 0;
+        for (auto &pr : kpairs[k])
+            if (pr.first < pr.second) {
+                p.pair_i.push_back((int16_t)pr.first);
+                p.pair_j.push_back((int16_t)pr.second);
+                blk.nd++;
+            }
+        for (auto &pr : kpairs[k])
+            if (pr.first == pr.second) {
+                p.pair_i.push_back((int16_t)pr.first);
+                p.pair_j.push_back((int16_t)pr.second);
+                blk.dg++;
+            }
+        for (int q = 0; q < blk.nd; q++) {
+            const int16_t i = p.pair_i[blk.pair0 + q], j = p.pair_j[blk.pair0 + q];
+            p.pair_i.push_back(j);
+            p.pair_j.push_back(i);
         }
+        if (2 * blk.nd + blk.dg != blk.o || blk.dg > 1) return "pair block without mirror symmetry";
         for (int a : cols) p.vir.push_back((int16_t)a);
         for (int c = 0; c < blk.v; c++) col_of[cols[c]] = c;
         for (int c = 0; c < blk.v; c++) p.pcol.push_back((int16_t)col_of[partner_of_col[c]]);

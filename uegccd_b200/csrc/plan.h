@@ -24,7 +24,10 @@ struct SolvePlan {
     int O = 0, V = 0, M = 0;
     int q2max = 0;
     std::vector<double> vtab;               // V(|q|^2), |q|^2 = 0..q2max
-    struct Block { int o, v, pair0, vir0; int64_t t0; };
+    // rows of a block: nd pairs (i,j) with i < j, then the diagonal pair (i,i) if K = 2 n_i
+    // (dg = 1), then the mirrors (j,i) of the first nd in the same order: row p < nd has its
+    // mirror at p + nd + dg
+    struct Block { int o, v, pair0, vir0; int64_t t0; int nd, dg; };
     std::vector<Block> blocks;
     std::vector<int16_t> pair_i, pair_j;    // concatenated pair lists
     std::vector<int16_t> vir;               // concatenated virtual lists (absolute orbital index)

@@ -50,6 +50,8 @@ struct BlockDev {
     int vir0;               // offset into vir (absolute orbital indices, local to the solve)
     int64_t t0;             // global packed index of element (row 0, col 0)
     int64_t row0, col0;     // offsets of the block's row and column sums in the mosaic partials
+    int nd, dg;             // rows [0, nd) are pairs i < j, row nd the pair (i,i) if dg = 1, and
+                            // row p + nd + dg the mirror (j,i) of row p < nd
 };
 
 // One tile of the particle-particle ladder: rows [p0, p0+P) x columns [a0, a0+A) of block blk.
