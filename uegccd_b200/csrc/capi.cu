@@ -571,6 +571,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.vir, vir))) return rc;
     if ((rc = b->alloc(d.pos, pos0))) return rc;
     if ((rc = b->alloc(d.partner, amp0))) return rc;
+    if ((rc = b->alloc(d.mirror, amp0))) return rc;
     if ((rc = b->alloc(d.amps, amp0))) return rc;
     if ((rc = b->upload(d.nv4, nv4))) return rc;
     if ((rc = b->upload(d.eigen, eigen))) return rc;
@@ -1298,7 +1299,7 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     int64_t b = 0;
     int64_t sum_ov = 0;
     for (const auto &B : P.blocks) sum_ov += B.o + B.v;
-    b += A * (8 * 5 + 16 + sizeof(AmpInfo) + 4);     // t, t_new, g, g_rq, g_xq; Coulomb factors; amps; partner
+    b += A * (8 * 5 + 16 + sizeof(AmpInfo) + 4 + 4); // t, t_new, g, g_rq, g_xq; Coulomb factors; amps; partner, mirror
     b += sum_ov * (8 + 4) + (V + O + 1) * (4 + 8);   // mosaic partials and target lists
     b += O * O * V * 4;                              // pos
     b += O * V * O * 8;                              // dRPA ring intermediate (allocated for dRPA only)

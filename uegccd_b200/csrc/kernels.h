@@ -34,6 +34,7 @@ struct DevBatch {
     int16_t *pcol = nullptr;          // beside vir: column of the partner d = K - c in the same block
     int32_t *pos = nullptr;          // dense (i,j,a) -> global packed index or -1
     int32_t *partner = nullptr;      // packed -> packed index of (i,j,b)
+    int32_t *mirror = nullptr;       // packed (i,j,a): index of (j,i,b) if i < j, -1 if i = j, -2 if i > j
     AmpInfo *amps = nullptr;
     int4 *nv4 = nullptr;
     double *eigen = nullptr, *vtab = nullptr;

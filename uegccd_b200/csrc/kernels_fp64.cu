@@ -177,8 +177,9 @@ __global__ void k_reduce_solves(const int *__restrict__ chunk_begin, const doubl
 // k_ladder3 in mode 1 builds H_K; in mode 0 it writes G (overwriting, so it runs first).
 // Both run over the rows p = (i,j) with i <= j only: by the pair symmetry
 // t(ij,a) = t(ji,b) (T2abab(ij,ab) = T2abab(ji,ba)) the ladder G of the mirror row (j,i)
-// at column b = K - a equals that of (i,j) at a, and mode 0 stores it there too.  The
-// reference forms both rows (CCD.f90:617-681); the two agree to rounding.
+// at column b = K - a equals that of (i,j) at a, and k_update reads G only on the rows
+// i <= j (it updates each mirror from its pair).  The reference forms both rows
+// (CCD.f90:617-681); the two agree to rounding.
 // ----------------------------------------------------------------------------
 constexpr int kVtabSmem = 1024;  // |q|^2 table entries staged in shared memory
 
@@ -221,7 +222,6 @@ size_t ladder_smem_bytes(int max_v, int np)
 template <int NP, bool KS>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
-                                             const int16_t *__restrict__ pcol,
                                              const int4 *__restrict__ nv4, const double *__restrict__ vtab,
                                              const double *__restrict__ t, const double *__restrict__ H, int mode,
                                              int do_pp, int do_hh, double *__restrict__ out, const double *sv,
@@ -359,8 +359,6 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
                 if (p >= orow) continue;
                 if (mode == 0) {
                     out[B.t0 + (int64_t)p * v + col] = acc[m][n][h];
-                    // the mirror (j,i) at the partner column K - a (none for the diagonal pair)
-                    if (p < B.nd) out[B.t0 + (int64_t)(p + orow) * v + pcol[B.vir0 + col]] = acc[m][n][h];
                 } else {
                     const int4 ni = nv4[s.orb0 + pair_i[B.pair0 + p]];
                     const int q2 = q2_of(ni, na[m]);
@@ -376,10 +374,10 @@ template <int NP>
 __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     k_ladder3(const LadderTile *__restrict__ tiles, const BlockDev *__restrict__ blocks,
               const SolveDev *__restrict__ solves, const int16_t *__restrict__ vir,
-              const int16_t *__restrict__ pair_i, const int16_t *__restrict__ pcol,
-              const int4 *__restrict__ nv4, const double *__restrict__ vtab, const double *__restrict__ t,
-              const int64_t *__restrict__ hh0, double *__restrict__ hh, int mode, int do_pp, int do_hh,
-              double *__restrict__ g, const uint8_t *__restrict__ active)
+              const int16_t *__restrict__ pair_i, const int4 *__restrict__ nv4,
+              const double *__restrict__ vtab, const double *__restrict__ t, const int64_t *__restrict__ hh0,
+              double *__restrict__ hh, int mode, int do_pp, int do_hh, double *__restrict__ g,
+              const uint8_t *__restrict__ active)
 {
     const LadderTile T = tiles[blockIdx.x];
     const BlockDev B = blocks[T.blk];
@@ -398,9 +396,9 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     double *out = mode == 0 ? g : H;
     // the hole-hole intermediate (mode 1) may split its c sum across the warps
     if (mode == 1)
-        ladder3_tile<NP, true>(T, B, s, vir, pair_i, pcol, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
+        ladder3_tile<NP, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
     else
-        ladder3_tile<NP, false>(T, B, s, vir, pair_i, pcol, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
+        ladder3_tile<NP, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
 }
 
 // The dynamic shared-memory limits only grow (batches of different sizes coexist), under
@@ -432,7 +430,7 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
         const int np = 8 * (c + 1);
         const size_t sm = ladder_smem_bytes(d.max_v, np);
 #define UEGCCD_LADDER_ARGS                                                                                  \
-    tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.pcol, d.nv4, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
+    tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
         g, d.active
         switch (np) {
         case 8: k_ladder3<8><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
@@ -784,9 +782,10 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
 //   xring(i_a, i_b, x_b) = sum_a' U1[a][a'] Y1[a'][b] - sum_b' Y1[a][b'] Vs2[b][b']
 // (lin, base as above; Sx_b, Sy_b are the column sums of X1, Y1).  The residual
 // terms share the pair symmetry (ring and crossed-ring G of (j,i,b) equal those of
-// (i,j,a)), so each value is stored twice: the ring value also at (i_b, i_a, x_b) and
-// the crossed-ring value also at (i_b, i_a, x_a).  The reference forms both halves
-// separately (CCD.f90:716-937); the two agree to rounding.
+// (i,j,a)), and k_update reads G only where the first occupied index is the smaller
+// one: the ring value goes to (i_a, i_b, x_a) or to its mirror (i_b, i_a, x_b), the
+// crossed-ring value to (i_a, i_b, x_b) or to (i_b, i_a, x_a).  The reference forms
+// both halves separately (CCD.f90:716-937); the two agree to rounding.
 // Group 1 is the smaller group (the host orders each pair), which minimises both the
 // shared memory, 2 N1 (N1 + N2 + 8) doubles, and the work, 5 N1^2 N2 + 2 N1 N2^2 DMMA
 // multiply-adds.  Row strides are the padded width + 4 (= 4 or 12 mod 16 doubles):
@@ -1028,18 +1027,19 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
                 const int n = n0 + 2 * tg + h;
                 if (n >= n2) continue;
                 const int r2 = N1 + n, w2 = rw[r2], i2 = ri[r2];
-                // ring amplitude (i_a, i_b, x_a) and its mirror (i_b, i_a, x_b)
+                // ring amplitude (i_a, i_b, x_a) or its mirror (i_b, i_a, x_b), whichever has
+                // the smaller occupied index first (both on the diagonal pair)
                 if (do_ring) {
                     const double lin = 2.0 * vd * (sx1 + Sx[r2]) - vd * (sy1 + Sy[r2]);
                     const double v = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ra[f][h] + rb[f][h];
-                    const int p = __ldg(&gx[w1 + i2]), pm = __ldg(&gx[w2 + i1]);
+                    const int p = i1 <= i2 ? __ldg(&gx[w1 + i2]) : -1, pm = i2 <= i1 ? __ldg(&gx[w2 + i1]) : -1;
                     if (p >= 0) g_rq[p] = v;
                     if (pm >= 0) g_rq[pm] = v;
                 }
-                // crossed ring (i_a, i_b, x_b) and its mirror (i_b, i_a, x_a)
+                // crossed ring (i_a, i_b, x_b) or its mirror (i_b, i_a, x_a), the same way
                 if (do_xring) {
                     const double v = xa[f][h] + xb[f][h];
-                    const int p = __ldg(&gy[w2 + i1]), pm = __ldg(&gy[w1 + i2]);
+                    const int p = i1 <= i2 ? __ldg(&gy[w2 + i1]) : -1, pm = i2 <= i1 ? __ldg(&gy[w1 + i2]) : -1;
                     if (p >= 0) g_xq[p] = v;
                     if (pm >= 0) g_xq[pm] = v;
                 }
@@ -1081,6 +1081,7 @@ struct UpdateArgs {
     const SolveDev *solves;
     const AmpInfo *amps;
     const int32_t *partner;
+    const int32_t *mirror;
     const int32_t *pos;
     const int4 *nv4;
     const double *eigen;
@@ -1106,12 +1107,15 @@ struct UpdateArgs {
 };
 
 // One CTA per momentum block: for every element (pair r = (i, j), column c = a) the
-// amplitude record (i, j, a, b), the position map entry (i, j, a) -> packed index and
-// the packed index of the partner (i, j, b), b in column pcol[c] of the same block.
+// amplitude record (i, j, a, b), the position map entry (i, j, a) -> packed index, the
+// packed index of the partner (i, j, b), b in column pcol[c] of the same block, and the
+// mirror: (j, i, b) in row r + nd + dg for the rows r < nd (i < j); -1 on the diagonal
+// pair's row, -2 on the mirror rows.
 __global__ void k_block_tables(const BlockDev *__restrict__ blocks, const SolveDev *__restrict__ solves,
                                const int16_t *__restrict__ pair_i, const int16_t *__restrict__ pair_j,
                                const int16_t *__restrict__ vir, const int16_t *__restrict__ pcol,
-                               AmpInfo *__restrict__ amps, int32_t *__restrict__ pos, int32_t *__restrict__ partner)
+                               AmpInfo *__restrict__ amps, int32_t *__restrict__ pos, int32_t *__restrict__ partner,
+                               int32_t *__restrict__ mirror)
 {
     const BlockDev B = blocks[blockIdx.x];
     const SolveDev s = solves[B.solve];
@@ -1124,6 +1128,8 @@ __global__ void k_block_tables(const BlockDev *__restrict__ blocks, const SolveD
         amps[p] = AmpInfo{(int16_t)i, (int16_t)j, (int16_t)a, vir[B.vir0 + pc]};
         pos[s.pos0 + ((int64_t)i * s.O + j) * s.V + (a - s.O)] = (int32_t)p;
         partner[p] = (int32_t)(B.t0 + (int64_t)r * B.v + pc);
+        const int oc = B.nd + B.dg;
+        mirror[p] = r < B.nd ? (int32_t)(B.t0 + (int64_t)(r + oc) * B.v + pc) : r < oc ? -1 : -2;
     }
 }
 
@@ -1147,7 +1153,7 @@ void launch_block_tables(const DevBatch &d, cudaStream_t st)
 {
     if (d.nblocks > 0)
         k_block_tables<<<d.nblocks, 256, 0, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir, d.pcol, d.amps,
-                                                  d.pos, d.partner);
+                                                  d.pos, d.partner, d.mirror);
     if (d.nrchunks > 0)
         k_ring_index<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.ph_i, d.ph_x, d.pos, d.ridx_x,
                                                     d.ridx_y);
@@ -1183,7 +1189,11 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
     const SolveDev s = A.solves[ch.solve];
     const int loc = ch.start + threadIdx.x;
     if (!on && A.mode == 0 && loc < s.namp) A.t_new[s.amp0 + loc] = A.t[s.amp0 + loc];
-    if (on && loc < s.namp) {
+    // By the pair symmetry t(ij,a) = t(ji,b) the amplitudes with i < j also update their
+    // mirrors (j,i,b), whose threads do nothing; every term of G shares the symmetry.
+    const int32_t mir = (on && loc < s.namp) ? A.mirror[s.amp0 + loc] : -2;
+    const double wgt = mir >= 0 ? 2.0 : 1.0;   // energy and DIIS dot weight: this amplitude and its mirror
+    if (mir != -2) {
         const int64_t p = s.amp0 + loc;
         const AmpInfo q = A.amps[p];
         const int i = q.i, j = q.j, a = q.a, b = q.b;
@@ -1223,7 +1233,10 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
             const int cn = __ldg(&A.solves[ch.solve].core_n);
             if (i < cn || j < cn) g = 0.0;
         }
-        if (A.g_out) A.g_out[p] = g;
+        if (A.g_out) {
+            A.g_out[p] = g;
+            if (mir >= 0) A.g_out[mir] = g;
+        }
         const double *ev = A.eigen + s.orb0;
         const double denom = ev[i] + ev[j] - ev[a] - ev[b];
         const double r = -g + denom * told;
@@ -1231,15 +1244,24 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
         if (A.mode == 0) {
             const double f = s.denom_factor;
             const double tn = (g / denom - (1.0 - f) * told) / f;
-            if (A.ndiis == 0) A.t_new[p] = tn;  // with DIIS the history slot holds t'
+            if (A.ndiis == 0) {  // with DIIS the history slot holds t'
+                A.t_new[p] = tn;
+                if (mir >= 0) A.t_new[mir] = tn;
+            }
             dtmax = fabs(tn - told);
             if (A.drpa) esum = via * tn * 2.0;  // SOSEX part added by k_drpa_energy at the end
             else esum = tn * (2.0 * via - vc.y);
+            esum *= wgt;
             if (!(fabs(tn) < 1e300)) dtmax = __longlong_as_double(0x7ff0000000000000LL);  // +Inf marks NaN/Inf
             if (A.ndiis > 0) {
                 const int slot = (A.st[ch.solve].niter - 1) % A.ndiis;
+                const float e = (float)(tn - told);
                 A.hist_t[(int64_t)slot * A.namp + p] = tn;
-                A.hist_e[(int64_t)slot * A.namp + p] = (float)(tn - told);
+                A.hist_e[(int64_t)slot * A.namp + p] = e;
+                if (mir >= 0) {
+                    A.hist_t[(int64_t)slot * A.namp + mir] = tn;
+                    A.hist_e[(int64_t)slot * A.namp + mir] = e;
+                }
             }
         }
     }
@@ -1247,13 +1269,13 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
         // e . e_j of every stored j (the chunk belongs to one solve: the loop is uniform)
         const int nb = A.st[ch.solve].niter;
         const int slot = (nb - 1) % A.ndiis, nvec = min(nb, A.ndiis);
-        const bool mine = loc < s.namp;
+        const bool mine = mir != -2;   // the mirrors count through their pair (weight 2)
         const int64_t p = s.amp0 + loc;
-        const double e = mine ? (double)A.hist_e[(int64_t)slot * A.namp + p] : 0.0;
+        const double e0 = mine ? (double)A.hist_e[(int64_t)slot * A.namp + p] : 0.0, e = wgt * e0;
         __shared__ double sd[kChunk / 32][kDiisMax];
         const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
         for (int jv = 0; jv < nvec; jv++) {
-            double d = mine ? e * (jv == slot ? e : (double)A.hist_e[(int64_t)jv * A.namp + p]) : 0.0;
+            double d = mine ? e * (jv == slot ? e0 : (double)A.hist_e[(int64_t)jv * A.namp + p]) : 0.0;
             for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
             if (l == 0) sd[w][jv] = d;
         }
@@ -1778,7 +1800,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         n++;
     }
     UpdateArgs A;
-    A.chunks = d.chunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.pos = d.pos;
+    A.chunks = d.chunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.mirror = d.mirror; A.pos = d.pos;
     A.nv4 = d.nv4; A.eigen = d.eigen; A.vtab = d.vtab; A.t = d.t; A.t_new = d.t_new; A.g_ladder = d.g;
     A.jvv = d.jvv; A.joo = d.joo; A.J1 = d.J1;
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
