@@ -222,7 +222,8 @@ def plan_stats(sysl):
             n2 = groups[mq]
             a, b = min(n1, n2), max(n1, n2)
             ring += 10 * a * a * b + 4 * a * b * b
-    return {"O": O, "V": M - O, "A": sum(o * v for o, v in ov), "ov2": sum(o * v * v for o, v in ov),
+    return {"O": O, "V": M - O, "A": sum(o * v for o, v in ov), "A_half": sum(oc * v for oc, o, v in ocv),
+            "ov2": sum(o * v * v for o, v in ov),
             "ov2_half": sum(oc * v * v for oc, o, v in ocv), "o2v_half": sum(oc * o * v for oc, o, v in ocv),
             "ring_flop": ring}
 
@@ -241,11 +242,12 @@ def kernel_units(st):
         # and the ring and crossed-ring products of one direction (the other is its mirror),
         # 6 n1^2 n2 + 4 n1 n2^2
         "k_rings": ("flop", st["ring_flop"]),
-        # reads t once (s is formed in registers; the partial sums are small)
-        "k_mosaic_blk": ("byte", 8 * A),
-        # reads t, the ladder G and the two ring G; Pulay push: writes t' (FP64) and e (FP32)
-        # to the history and reads the other ndiis - 1 error vectors (FP32)
-        "k_update": ("byte", (4 * 8 + 8 + 4 + (ndiis - 1) * 4) * A),
+        # reads the rows i <= j of t once (s is formed in registers; the partial sums are small)
+        "k_mosaic_blk": ("byte", 8 * st["A_half"]),
+        # every amplitude: the mirror index (4 B); the amplitudes i <= j: t, the ladder G and the
+        # two ring G, the Pulay push (t' FP64 and e FP32 to the history) and the other ndiis - 1
+        # error vectors (FP32)
+        "k_update": ("byte", 4 * A + (4 * 8 + 8 + 4 + (ndiis - 1) * 4) * st["A_half"]),
     }
 
 

@@ -460,8 +460,8 @@ constexpr int kMosThreads = 128;
 
 size_t mosaic_smem_bytes(int max_v)
 {
-    return sizeof(double) * ((size_t)kVtabSmem + (size_t)(kMosThreads / 32) * max_v) + sizeof(int4) * (size_t)max_v +
-           sizeof(int) * (size_t)max_v;
+    return sizeof(double) * ((size_t)kVtabSmem + (size_t)(kMosThreads / 32 + 1) * max_v) +
+           sizeof(int4) * (size_t)max_v + sizeof(int) * (size_t)max_v;
 }
 
 __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__restrict__ blocks,
@@ -479,13 +479,14 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     const BlockDev B = blocks[blockIdx.x];
     if (!active[B.solve]) return;
     const SolveDev s = solves[B.solve];
-    const int v = B.v, o = B.o;
+    const int v = B.v;
     constexpr int kW = kMosThreads / 32;
     extern __shared__ double msm[];
     double *sv = msm;                          // kVtabSmem
     int4 *nvc = (int4 *)(sv + kVtabSmem);      // v: n-vectors of the block's virtuals
-    double *cacc = (double *)(nvc + v);        // kW x v: per-warp column sums
-    int *pc = (int *)(cacc + kW * v);          // v: column of the partner d = K - c
+    double *cacc = (double *)(nvc + v);        // kW x v: per-warp column sums of the rows i < j
+    double *cdg = cacc + kW * v;               // v: the diagonal pair's row (if any)
+    int *pc = (int *)(cdg + v);                // v: column of the partner d = K - c
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
@@ -494,10 +495,15 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
         nvc[c] = nv4[s.orb0 + vir[B.vir0 + c]];
         pc[c] = pcol[B.vir0 + c];
     }
-    for (int e = tid; e < kW * v; e += kMosThreads) cacc[e] = 0.0;
+    for (int e = tid; e < (kW + 1) * v; e += kMosThreads) cacc[e] = 0.0;
     __syncthreads();
     auto V = [&](int q2) -> double { return vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]); };
-    for (int r = warp; r < o; r += kW) {
+    // Rows i <= j only: by the pair symmetry s(l,k,d) = s(k,l,c) for the mirror (l,k) of a
+    // row (k,l) and d = K - c, so the mirror row has the same row sum (Joo of l) and adds
+    // the column sums of (k,l) with the columns swapped to their partners.
+    const int oc = B.nd + B.dg;
+    for (int r = warp; r < oc; r += kW) {
+        const bool diag = r >= B.nd;
         const int4 nk = nv4[s.orb0 + pair_i[B.pair0 + r]], nl = nv4[s.orb0 + pair_j[B.pair0 + r]];
         const int64_t row = B.t0 + (int64_t)r * v;
         double rs = 0.0;
@@ -513,16 +519,23 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
                 sval = vck * (2.0 * x - y) - vcl * (x - 2.0 * y);
             }
             rs += sval;
-            cacc[warp * v + c] += sval;
+            if (diag) cdg[c] = sval;
+            else cacc[warp * v + c] += sval;
         }
         for (int off = 16; off > 0; off >>= 1) rs += __shfl_down_sync(0xffffffffu, rs, off);
-        if (lane == 0) mpart[B.row0 + r] = rs;
+        if (lane == 0) {
+            mpart[B.row0 + r] = rs;
+            if (!diag) mpart[B.row0 + r + oc] = rs;   // the mirror row
+        }
     }
     __syncthreads();
     for (int c = tid; c < v; c += kMosThreads) {
-        double a = 0.0;
-        for (int w = 0; w < kW; w++) a += cacc[w * v + c];
-        mpart[B.col0 + c] = a;
+        double a = 0.0, m = 0.0;
+        for (int w = 0; w < kW; w++) {
+            a += cacc[w * v + c];
+            m += cacc[w * v + pc[c]];
+        }
+        mpart[B.col0 + c] = a + m + cdg[c];
     }
 }
 
@@ -1256,12 +1269,10 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
             if (A.ndiis > 0) {
                 const int slot = (A.st[ch.solve].niter - 1) % A.ndiis;
                 const float e = (float)(tn - told);
+                // the mirrors' history entries are never read: k_diis_extrap2 and the dot
+                // products go through the amplitudes i <= j
                 A.hist_t[(int64_t)slot * A.namp + p] = tn;
                 A.hist_e[(int64_t)slot * A.namp + p] = e;
-                if (mir >= 0) {
-                    A.hist_t[(int64_t)slot * A.namp + mir] = tn;
-                    A.hist_e[(int64_t)slot * A.namp + mir] = e;
-                }
             }
         }
     }
@@ -1449,9 +1460,11 @@ __global__ void k_diis_rows2(const int *__restrict__ chunk_begin, const IterStat
     }
 }
 
+// t = sum_j c_j t'_j over the amplitudes i <= j, each also written to its mirror (j,i,b)
 __global__ void k_diis_extrap2(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
                                int64_t namp, const double *__restrict__ hist_t, const double *__restrict__ coef,
-                               int ndiis, double *__restrict__ t, const uint8_t *__restrict__ active)
+                               int ndiis, const int32_t *__restrict__ mirror, double *__restrict__ t,
+                               const uint8_t *__restrict__ active)
 {
     const ChunkDev ch = chunks[blockIdx.x];
     if (!active[ch.solve]) return;
@@ -1459,6 +1472,8 @@ __global__ void k_diis_extrap2(const ChunkDev *__restrict__ chunks, const SolveD
     const int loc = ch.start + threadIdx.x;
     if (loc >= s.namp) return;
     const int64_t p = s.amp0 + loc;
+    const int32_t mir = mirror[p];
+    if (mir == -2) return;
     const double *c = coef + ch.solve * kMaxDiis;
     double x = 0.0;
     for (int jv = 0; jv < ndiis; jv++) {
@@ -1466,6 +1481,7 @@ __global__ void k_diis_extrap2(const ChunkDev *__restrict__ chunks, const SolveD
         if (cj != 0.0) x = fma(cj, hist_t[(int64_t)jv * namp + p], x);
     }
     t[p] = x;
+    if (mir >= 0) t[mir] = x;
 }
 
 __global__ void k_copy(int64_t n, const double *__restrict__ src, double *__restrict__ dst)
@@ -1505,8 +1521,8 @@ int launch_iteration(const DevBatch &d, const CtlBuffers &c, const TermFlags &f,
     }
     launch_control(d, c, tol, max_iter, ndiis, 0, st);
     if (ndiis > 0)
-        k_diis_extrap2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, c.hist_t, c.coef, ndiis, d.t,
-                                                     d.active);
+        k_diis_extrap2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, c.hist_t, c.coef, ndiis, d.mirror,
+                                                     d.t, d.active);
     else
         k_commit<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.t_new, d.t, d.active);
     launch_active_swap(d, c, st);
