@@ -361,6 +361,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             bd.t0 = amp0 + B.t0;
             bd.nd = B.nd;
             bd.dg = B.dg;
+            bd.nvd = B.nvd;
+            bd.sd = B.sd;
             bd.row0 = mrows;
             bd.col0 = mcols;   // shifted past all rows below
             mrows += B.o;
@@ -375,12 +377,20 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             // writes each mirror row from its pair (i,j) with the pair symmetry.  Row tiles of 32
             // pairs, the last one the remainder rounded up to 8 (8, 16, 24 or 32): at most 7
             // padded rows per block; columns in tiles of 128 (4 warps x 32)
+            // Blocks with at most kPairedRows such rows run paired tiles (pad 4): each 8-wide
+            // fragment holds the rows and their partner-column images, over the columns
+            // a <= pcol a (mode 0) and the pairs q <= q' (mode 1).
             const int oc = B.nd + B.dg;
             auto row_tile = [&](int p0) { return std::min(32, (oc - p0 + 7) & ~7); };
-            for (int a0 = 0; a0 < B.v; a0 += 128)
-                for (int p0 = 0; p0 < oc; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, row_tile(p0)});
-            for (int q0 = 0; q0 < B.o; q0 += 128)
-                for (int p0 = 0; p0 < oc; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
+            if (oc <= kPairedRows) {
+                for (int a0 = 0; a0 < B.nvd + B.sd; a0 += 128) tiles.push_back(LadderTile{bi, a0, 0, 4});
+                htiles.push_back(LadderTile{bi, 0, 0, 4});
+            } else {
+                for (int a0 = 0; a0 < B.v; a0 += 128)
+                    for (int p0 = 0; p0 < oc; p0 += 32) tiles.push_back(LadderTile{bi, a0, p0, row_tile(p0)});
+                for (int q0 = 0; q0 < B.o; q0 += 128)
+                    for (int p0 = 0; p0 < oc; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
+            }
             // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows; their FP16 operands: one
             // Coulomb slab per 128 virtuals, one d tile per row tile, each over all K chunks
             const int ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
@@ -477,7 +487,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         for (int c = 0; c < kLadderClasses; c++) {
             cnt[c] = 0;
             for (const auto &x : v)
-                if (x.pad == 8 * (c + 1)) {
+                if (x.pad == (c == 0 ? 4 : 8 * c)) {
                     out.push_back(x);
                     cnt[c]++;
                 }
@@ -487,7 +497,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     const size_t ntl = tiles.size(), nhtl = htiles.size();
     by_class(tiles, d.ntile_cls);
     by_class(htiles, d.nhtile_cls);
-    if (tiles.size() != ntl || htiles.size() != nhtl) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder row tile outside the 8/16/24/32 classes");
+    if (tiles.size() != ntl || htiles.size() != nhtl) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder row tile outside the 4/8/16/24/32 classes");
     d.ntiles = (int)tiles.size();
     d.nhtiles = (int)htiles.size();
     d.ntc16 = (int)tc16.size();

@@ -17,8 +17,8 @@ struct DevBatch {
     double *mpart = nullptr;
     int32_t *mt_start = nullptr, *mt_list = nullptr;
     size_t mosaic_smem = 0;
-    int ntile_cls[4] = {0, 0, 0, 0};   // ladder tiles per row-tile class (8, 16, 24, 32 pairs)
-    int nhtile_cls[4] = {0, 0, 0, 0};  // hole-hole intermediate tiles per class
+    int ntile_cls[5] = {0, 0, 0, 0, 0};   // ladder tiles per class: paired 8, then 8, 16, 24, 32 pairs
+    int nhtile_cls[5] = {0, 0, 0, 0, 0};  // hole-hole intermediate tiles per class
     int max_occ = 0;    // largest NOcc
     int64_t namp = 0;
     SolveDev *solves = nullptr;
@@ -81,7 +81,10 @@ size_t rings_smem_bytes(int O, int R);
 size_t mosaic_smem_bytes(int max_v);
 void set_mosaic_smem_limit(size_t bytes);
 // dynamic shared memory of k_ladder3<np> for blocks of at most max_v virtuals
-constexpr int kLadderClasses = 4;   // row tiles of 8, 16, 24 and 32 pairs
+// row-tile classes: paired 8 (blocks with at most kPairedRows rows i <= j, pad = 4 in
+// LadderTile), then 8, 16, 24 and 32 pairs
+constexpr int kLadderClasses = 5;
+constexpr int kPairedRows = 4;
 size_t ladder_smem_bytes(int max_v, int np);
 void set_ladder_smem_limit(int max_v);
 // dynamic shared memory of k_rings for NOcc = O and groups of n1 and n2 rows

@@ -219,7 +219,14 @@ size_t ladder_smem_bytes(int max_v, int np)
     return sizeof(double) * (2 * (size_t)np * kLadLd + kVtabSmem) + sizeof(int4) * (size_t)max_v;
 }
 
-template <int NP, bool KS>
+// PAIRED (blocks with at most 4 rows i <= j, NP = 8): the fragment's 8 columns hold the
+// rows p and, after them, the same rows with the c columns swapped to their partners
+// (t[p][pcol c]).  The block's Coulomb kernel is invariant under (a, c) -> (pcol a, pcol c),
+// so the second half gives G[p][pcol a] from the same Coulomb fragment: the tile runs over
+// the columns a <= pcol a only, half the fragments.  The hole-hole intermediate pairs its
+// columns q with their mirror pairs q' the same way (v(k_q' - pcol c) = v(k_q - c)), and the
+// hole-hole apply reads H[p][q'] for the second half (t[q][pcol a] = t[q'][a]).
+template <int NP, bool KS, bool PAIRED>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
                                              const int4 *__restrict__ nv4, const double *__restrict__ vtab,
@@ -232,7 +239,11 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     const int gid = lane >> 2, tig = lane & 3;
     const int v = B.v, o = B.o;
     const int orow = B.nd + B.dg;   // rows computed: pairs i < j and the diagonal pair
-    const int ncol = mode == 0 ? v : o;
+    const int vc = B.nvd + B.sd;    // columns a <= pcol a
+    const int ncol = mode == 0 ? (PAIRED ? vc : v) : (PAIRED ? orow : o);
+    // partner column of a virtual column, mirror of a pair row (both involutions)
+    auto pcolv = [&](int c) { return c < B.nvd ? c + vc : c < vc ? c : c - vc; };
+    auto mirq = [&](int q) { return q < B.nd ? q + orow : q < orow ? q : q - orow; };
     // hole-hole intermediate with at most 32 columns left: the 4 warps share the columns
     // and split the c sum instead (each takes every 4th k step), then reduce
     const bool ksplit = KS && ncol - T.a0 <= 32;
@@ -260,9 +271,19 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
             const int c0 = j * kLadKC;
             for (int e = threadIdx.x; e < NP * kLadKC; e += blockDim.x) {
                 const int r = e / kLadKC, c = e - r * kLadKC;
-                const int p = T.p0 + r, cc = c0 + c;
-                if (p < orow && cc < v) cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + cc);
-                else dst[r * kLadLd + c] = 0.0;
+                const int cc = c0 + c;
+                if (PAIRED) {
+                    // rows [0, orow): t[p][c]; rows [orow, 2 orow): t[p][pcol c]
+                    const bool second = r >= orow;
+                    const int p = second ? r - orow : r;
+                    if (r < 2 * orow && cc < v)
+                        cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + (second ? pcolv(cc) : cc));
+                    else dst[r * kLadLd + c] = 0.0;
+                } else {
+                    const int p = T.p0 + r;
+                    if (p < orow && cc < v) cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + cc);
+                    else dst[r * kLadLd + c] = 0.0;
+                }
             }
             cp_async_commit();
         };
@@ -335,8 +356,15 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
             double bf[NN];
 #pragma unroll
             for (int n = 0; n < NN; n++) {
-                int p = T.p0 + n * 8 + gid;
-                bf[n] = (qok && p < orow) ? H[(int64_t)p * o + q] : 0.0;
+                if (PAIRED) {
+                    const int nn = n * 8 + gid;
+                    const bool second = nn >= orow;
+                    const int p = second ? nn - orow : nn;
+                    bf[n] = (qok && nn < 2 * orow) ? H[(int64_t)p * o + (second ? mirq(q) : q)] : 0.0;
+                } else {
+                    int p = T.p0 + n * 8 + gid;
+                    bf[n] = (qok && p < orow) ? H[(int64_t)p * o + q] : 0.0;
+                }
             }
 #pragma unroll
             for (int m = 0; m < 4; m++) {
@@ -355,14 +383,26 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
         for (int n = 0; n < NN; n++)
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int p = T.p0 + n * 8 + 2 * tig + h;
+                int p = T.p0 + n * 8 + 2 * tig + h, oc = col;
+                int4 nq = na[m];
+                if (PAIRED) {
+                    const int nn = n * 8 + 2 * tig + h;
+                    if (nn >= 2 * orow) continue;
+                    if (nn >= orow) {
+                        // the partner column (mode 0) or mirror pair (mode 1); once on self-partners
+                        p = nn - orow;
+                        oc = mode == 0 ? pcolv(col) : mirq(col);
+                        if (oc == col) continue;
+                        if (mode == 1) nq = nv4[s.orb0 + pair_i[B.pair0 + oc]];
+                    }
+                }
                 if (p >= orow) continue;
                 if (mode == 0) {
-                    out[B.t0 + (int64_t)p * v + col] = acc[m][n][h];
+                    out[B.t0 + (int64_t)p * v + oc] = acc[m][n][h];
                 } else {
                     const int4 ni = nv4[s.orb0 + pair_i[B.pair0 + p]];
-                    const int q2 = q2_of(ni, na[m]);
-                    out[(int64_t)p * o + col] = (vsm ? sv[q2] : vtab[s.vtab0 + q2]) + acc[m][n][h];
+                    const int q2 = q2_of(ni, nq);
+                    out[(int64_t)p * o + oc] = (vsm ? sv[q2] : vtab[s.vtab0 + q2]) + acc[m][n][h];
                 }
             }
     }
@@ -370,7 +410,7 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 
 // One kernel per row tile NP (8, 16, 24, 32 pairs): the small tiles need fewer registers
 // and less shared memory, so more CTAs fit on an SM to hide the lookup latency.
-template <int NP>
+template <int NP, bool PAIRED>
 __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     k_ladder3(const LadderTile *__restrict__ tiles, const BlockDev *__restrict__ blocks,
               const SolveDev *__restrict__ solves, const int16_t *__restrict__ vir,
@@ -396,9 +436,11 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     double *out = mode == 0 ? g : H;
     // the hole-hole intermediate (mode 1) may split its c sum across the warps
     if (mode == 1)
-        ladder3_tile<NP, true>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
+        ladder3_tile<NP, true, PAIRED>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
+                                       nvc);
     else
-        ladder3_tile<NP, false>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts, nvc);
+        ladder3_tile<NP, false, PAIRED>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
+                                        nvc);
 }
 
 // The dynamic shared-memory limits only grow (batches of different sizes coexist), under
@@ -410,16 +452,21 @@ void set_ladder_smem_limit(int max_v)
     std::lock_guard<std::mutex> lock(g_smem_limit_mu);
     static int current = 0;
     if (max_v > current) {
-        cudaFuncSetAttribute(k_ladder3<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 8));
-        cudaFuncSetAttribute(k_ladder3<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 16));
-        cudaFuncSetAttribute(k_ladder3<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 24));
-        cudaFuncSetAttribute(k_ladder3<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ladder_smem_bytes(max_v, 32));
+        const int b8 = (int)ladder_smem_bytes(max_v, 8);
+        cudaFuncSetAttribute(k_ladder3<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
+        cudaFuncSetAttribute(k_ladder3<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
+        cudaFuncSetAttribute(k_ladder3<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ladder_smem_bytes(max_v, 16));
+        cudaFuncSetAttribute(k_ladder3<24, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ladder_smem_bytes(max_v, 24));
+        cudaFuncSetAttribute(k_ladder3<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ladder_smem_bytes(max_v, 32));
         current = max_v;
     }
 }
 
-// Ladder tiles in row-tile classes (sorted 8, 16, 24, 32 pairs; counts in ncls): one launch
-// per non-empty class.  Returns the launches.
+// Ladder tiles in row-tile classes (sorted: paired 8, then 8, 16, 24, 32 pairs; counts in
+// ncls): one launch per non-empty class.  Returns the launches.
 static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int *ncls, const double *t, int mode,
                           int do_pp, int do_hh, double *g, cudaStream_t st)
 {
@@ -427,16 +474,17 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
     for (int c = 0; c < kLadderClasses; c++) {
         const int cnt = ncls[c];
         if (cnt <= 0) continue;
-        const int np = 8 * (c + 1);
+        const int np = c == 0 ? 8 : 8 * c;
         const size_t sm = ladder_smem_bytes(d.max_v, np);
 #define UEGCCD_LADDER_ARGS                                                                                  \
     tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
         g, d.active
-        switch (np) {
-        case 8: k_ladder3<8><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        case 16: k_ladder3<16><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        case 24: k_ladder3<24><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        default: k_ladder3<32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        switch (c) {
+        case 0: k_ladder3<8, true><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        case 1: k_ladder3<8, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        case 2: k_ladder3<16, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        case 3: k_ladder3<24, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        default: k_ladder3<32, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
         }
 #undef UEGCCD_LADDER_ARGS
         off += cnt;

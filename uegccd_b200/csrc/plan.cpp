@@ -98,24 +98,43 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
     int64_t t0 = 0;
     std::vector<int> cols, partner_of_col, col_of(M, -1);
     for (size_t k = 0; k < kpairs.size(); k++) {
-        // virtual columns of block K: a virtual whose partner b = K - a is a virtual
+        // virtual columns of block K: a virtual whose partner b = K - a is a virtual.  Order:
+        // the columns a < b, the column a = b if K = 2 n_a, then the partners b of the first
+        // ones in the same order, so column c < nvd has its partner at c + nvd + sd
         cols.clear();
         partner_of_col.clear();
         const auto &K = kvecs[k];
+        int nvd = 0, sd = 0;
         for (int a = O; a < M; a++) {
             int b = orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]);
-            if (b >= O) {
+            if (b > a) {
                 cols.push_back(a);
                 partner_of_col.push_back(b);
+                nvd++;
             }
         }
+        for (int a = O; a < M; a++) {
+            int b = orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]);
+            if (b == a) {
+                cols.push_back(a);
+                partner_of_col.push_back(b);
+                sd++;
+            }
+        }
+        for (int c = 0; c < nvd; c++) {
+            cols.push_back(partner_of_col[c]);
+            partner_of_col.push_back(cols[c]);
+        }
         if (cols.empty()) continue;
+        if (sd > 1) return "virtual block without partner symmetry";
         SolvePlan::Block blk;
         blk.o = (int)kpairs[k].size();
         blk.v = (int)cols.size();
         blk.pair0 = (int)p.pair_i.size();
         blk.vir0 = (int)p.vir.size();
         blk.t0 = t0;
+        blk.nvd = nvd;
+        blk.sd = sd;
         // rows: pairs i < j, the diagonal pair, then the mirrors (j,i) in the same order
         blk.nd = blk.dg = 0;
         for (auto &pr : kpairs[k])

@@ -26,8 +26,9 @@ struct SolvePlan {
     std::vector<double> vtab;               // V(|q|^2), |q|^2 = 0..q2max
     // rows of a block: nd pairs (i,j) with i < j, then the diagonal pair (i,i) if K = 2 n_i
     // (dg = 1), then the mirrors (j,i) of the first nd in the same order: row p < nd has its
-    // mirror at p + nd + dg
-    struct Block { int o, v, pair0, vir0; int64_t t0; int nd, dg; };
+    // mirror at p + nd + dg.  Columns likewise: nvd virtuals a < K - a, the virtual a = K - a
+    // if any (sd = 1), then the partners: column c < nvd has its partner at c + nvd + sd.
+    struct Block { int o, v, pair0, vir0; int64_t t0; int nd, dg, nvd, sd; };
     std::vector<Block> blocks;
     std::vector<int16_t> pair_i, pair_j;    // concatenated pair lists
     std::vector<int16_t> vir;               // concatenated virtual lists (absolute orbital index)

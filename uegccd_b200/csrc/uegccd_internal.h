@@ -52,6 +52,8 @@ struct BlockDev {
     int64_t row0, col0;     // offsets of the block's row and column sums in the mosaic partials
     int nd, dg;             // rows [0, nd) are pairs i < j, row nd the pair (i,i) if dg = 1, and
                             // row p + nd + dg the mirror (j,i) of row p < nd
+    int nvd, sd;            // columns likewise: [0, nvd) virtuals a < K - a, column nvd the
+                            // virtual a = K - a if sd = 1, column c + nvd + sd the partner of c < nvd
 };
 
 // One tile of the particle-particle ladder: rows [p0, p0+P) x columns [a0, a0+A) of block blk.
