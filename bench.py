@@ -42,6 +42,7 @@ SEED = 2024
 # checks it every run.  Used to turn the oracle's time per iteration into a time per solve.
 REF_ITERS_PER_SOLVE = 33.16  # measured: replay mode on this workload, 100 twists (min 30, max 35)
 SOLVE_OPTS = dict(scheme=1, ndiis=6, denom_factor=1.0, tol=1e-9)
+E2E_CREATORS = 2   # host threads creating the next batches of the e2e pipeline
 # Nominal FP64 peak of a B200 (datasheet); the bench measures it each run with the library's
 # register-only probe (37.0 TFLOP/s measured on this pool) and uses this only if the probe fails.
 FP64_PEAK_TFLOPS = 37.0
@@ -320,32 +321,48 @@ def run_gpu(args, rank, world):
     fails = sum(r["fail"] for r in res)
     total_ms = float(sum(step_ms))
     # e2e: through the C ABI with host buffers, every step: batch create (plan, uploads),
-    # solve, and every twist's T2 read back into page-locked host memory.  Three stages
-    # run at once, as a serving host runs them: the next step's batch is created on one
-    # host thread, this step solves, and the previous step's amplitudes are downloaded on
-    # another (the C calls release the GIL; each batch has its own stream).  The timed run
-    # starts before its first create and ends after its last download: the pipeline's fill
-    # and drain are inside it.
+    # solve, and every twist's T2 read back into page-locked host memory.  The stages run
+    # at once, as a serving host runs them: the next two steps' batches are created on two
+    # host threads (a create is mostly host work and takes longer than a solve), this step
+    # solves, and the previous step's amplitudes are downloaded on another thread (the C
+    # calls release the GIL; each batch has its own stream).  The timed run starts before
+    # its first create and ends after its last download: the pipeline's fill and drain are
+    # inside it.
     out_bufs = [pinned_buffer(batch.amplitude_count()) for _ in range(2)]
     xfer = [0, 0]
+    stage_ms = {"create": [], "solve": [], "download": []}   # host wall time of each stage
+
+    def create():
+        t = time.perf_counter()
+        b2 = Batch(systems)
+        stage_ms["create"].append((time.perf_counter() - t) * 1e3)
+        return b2
 
     def finish(b2, buf):
+        t = time.perf_counter()
         b2.all_amplitudes(out=buf)
         xfer[0], xfer[1] = b2.transfer_bytes()
         b2.close()
+        stage_ms["download"].append((time.perf_counter() - t) * 1e3)
 
     def e2e_run(nsteps):
         from concurrent.futures import ThreadPoolExecutor
 
+        for v in stage_ms.values():
+            v.clear()
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=1) as creator, ThreadPoolExecutor(max_workers=1) as reader:
-            fut = creator.submit(Batch, systems)
+        with ThreadPoolExecutor(max_workers=E2E_CREATORS) as creator, ThreadPoolExecutor(max_workers=1) as reader:
+            futs = [creator.submit(create)]   # the first create runs alone: nothing to overlap
+            submitted = 1
             done = None
             for k in range(nsteps):
-                b2 = fut.result()
-                if k + 1 < nsteps:
-                    fut = creator.submit(Batch, systems)
+                b2 = futs.pop(0).result()
+                while submitted < nsteps and len(futs) < E2E_CREATORS:
+                    futs.append(creator.submit(create))
+                    submitted += 1
+                ts = time.perf_counter()
                 b2.solve(**opts)
+                stage_ms["solve"].append((time.perf_counter() - ts) * 1e3)
                 if done is not None:
                     done.result()
                 done = reader.submit(finish, b2, out_bufs[k % 2])
@@ -353,7 +370,7 @@ def run_gpu(args, rank, world):
         return (time.perf_counter() - t0) * 1e3 / nsteps
 
     e2e_run(max(2, args.warmup))   # warms the device-memory cache and the pinned buffers
-    e2e_ms = [e2e_run(max(5, 2 * args.steps))]
+    e2e_ms = [e2e_run(max(10, 4 * args.steps))]
     h2d, d2h = xfer
     # the other precision on the same batch (timed the same way): mixed beside FP64
     other = None
@@ -382,6 +399,7 @@ def run_gpu(args, rank, world):
         "niter_mean": float(np.mean(niters)), "niter_min": int(min(niters)), "niter_max": int(max(niters)),
         "fails": int(fails), "rc": rc, "stats": stats, "clocks": clk.summary(), "ring_threads": ring_threads,
         "fp64_peak": fp64_peak,
+        "e2e_stage_ms": {k: round(float(np.median(v)), 2) for k, v in stage_ms.items() if v},
         "ecorr_first": res[0]["ecorr"], "e2_first": float(e2[0]), "launches_per_step": res[0]["kernel_launches"],
         "systems": systems,
         "replay_niter_mean": float(np.mean([r["niter"] for r in res_r])),
@@ -527,9 +545,10 @@ def main():
             "warmup": args.warmup, "ms_per_step": g["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f16/f64", "data": "synthetic", "config": config,
             "e2e": {"value": g["e2e_value"], "unit": "solves/s", "h2d_bytes_per_step": g["h2d"],
-                    "d2h_bytes_per_step": g["d2h"],
+                    "d2h_bytes_per_step": g["d2h"], "stage_ms_median": g["e2e_stage_ms"],
                     "note": "per step: batch create (plan + uploads), solve, T2 of every twist to page-locked host "
-                            "memory; create of the next step and download of the previous overlap the solve"},
+                            "memory; creates of the next two steps (two host threads) and the download of the "
+                            "previous one overlap the solve"},
             "gpu_launches": int(g["launches_per_step"]) * args.steps,
             "clocks": g["clocks"], "roofline": roof,
             "kernels": {k: {"ms": v[0], "launches": v[1], **({"roofline": kern[k]} if k in kern else {})}

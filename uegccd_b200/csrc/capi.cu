@@ -10,8 +10,10 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -275,8 +277,37 @@ int read_system(const UegccdSystem *s, SystemHost &h)
     return 0;
 }
 
+// UEGCCD_TRACE=1 in the environment: batch creation prints its phase times to stderr.
+struct PhaseTrace {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0, last;
+    std::string line;
+    PhaseTrace()
+    {
+        const char *e = std::getenv("UEGCCD_TRACE");
+        on = e && e[0] == '1';
+        t0 = last = std::chrono::steady_clock::now();
+    }
+    void mark(const char *what)
+    {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        char buf[96];
+        std::snprintf(buf, sizeof buf, " %s %.2f", what, std::chrono::duration<double, std::milli>(now - last).count());
+        line += buf;
+        last = now;
+    }
+    ~PhaseTrace()
+    {
+        if (on)
+            std::fprintf(stderr, "uegccd batch create (ms):%s total %.2f\n", line.c_str(),
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
+
 int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch> &out)
 {
+    PhaseTrace trace;
     int rc = check_device();
     if (rc) return rc;
     if (n <= 0) return fail(UEGCCD_ERR_ARG, "empty batch");
@@ -295,11 +326,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         if (!msgs[s].empty()) return fail(UEGCCD_ERR_ARG, "system " + std::to_string(s) + ": " + msgs[s]);
         if (b->plans[s].O > 64) return fail(UEGCCD_ERR_UNSUPPORTED, "NOcc > 64 is outside the hole-hole ladder tiling");
     }
+    trace.mark("plans");
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&b->ev0));
     CU(cudaEventCreate(&b->ev1));
     CU(cudaEventCreate(&b->ev_solve0));
     CU(cudaEventCreate(&b->ev_solve1));
+    trace.mark("stream");
 
     std::vector<SolveDev> solves(n);
     std::vector<BlockDev> blocks;
@@ -438,6 +471,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         if (amp0 >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit packed indices");
     }
     chunk_begin[n] = (int)chunks.size();
+    trace.mark("solve-loop");
     ph_i.resize(phr0);
     ph_x.resize(phr0);
     parallel_for(n, nthreads, [&](int s) {
@@ -476,6 +510,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         }
     });
     if (mrows + mcols >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit mosaic indices");
+    trace.mark("ph+mosaic");
 
     DevBatch &d = b->d;
     d.nsolves = n;
@@ -555,11 +590,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             d.ring_smem[c] = std::max(d.ring_smem[c], b);
         }
     }
+    trace.mark("classes");
     d.nrpairs = (int)rpairs.size();
     if (d.ring_smem[kRingClasses] > 227 * 1024)
         return fail(UEGCCD_ERR_UNSUPPORTED, "ring group pair exceeds shared memory");
     set_rings_smem_limit(0, *std::max_element(d.ring_smem, d.ring_smem + kRingClasses));
     set_rings_smem_limit(1, d.ring_smem[kRingClasses]);
+    trace.mark("host-tables");
     if ((rc = b->upload(d.solves, solves))) return rc;
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;
@@ -613,6 +650,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     b->red.assign(3 * (size_t)n, 0.0);
     b->active.assign(n, 1);
     CU(cudaMemcpyAsync(d.active, b->active.data(), n, cudaMemcpyHostToDevice, b->stream));
+    trace.mark("alloc+upload");
     // position map, amplitude list, partners and ring gather indices, from the blocks
     CU(cudaMemsetAsync(d.pos, 0xff, (size_t)pos0 * sizeof(int32_t), b->stream));   // -1: not allowed
     launch_block_tables(d, b->stream);
@@ -622,7 +660,9 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     b->dense_n = dn;
     for (int k = 0; k < 3; k++)
         if ((rc = b->alloc(b->dense[k], dn))) return rc;
+    trace.mark("device-launch");
     CU(cudaStreamSynchronize(b->stream));
+    trace.mark("device-wait");
     out = std::move(b);
     return 0;
 }

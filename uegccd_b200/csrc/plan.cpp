@@ -32,6 +32,7 @@ struct Lattice {
         idx.assign((size_t)side * side * side, -1);
     }
     bool inside(int x, int y, int z) const { return std::abs(x) <= r && std::abs(y) <= r && std::abs(z) <= r; }
+    int get_inside(int x, int y, int z) const { return idx[((size_t)(x + r) * side + (y + r)) * side + (z + r)]; }
     int &at(int x, int y, int z) { return idx[((size_t)(x + r) * side + (y + r)) * side + (z + r)]; }
     int get(int x, int y, int z) const
     {
@@ -54,8 +55,11 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
         for (int d = 0; d < 3; d++) nmax = std::max(nmax, std::abs(sys.n[q][d]));
     if (nmax > 200) return "plane-wave vectors out of range";
     // orbital lookup: n -> orbital (the basis, as FindIndex's kPointToBasisFn, HEG.f90:306-316)
+    // radius 3 nmax when small: every K - n_a (|K| <= 2 nmax) then lies inside, and the
+    // column scan below needs no bounds test
     Lattice orb;
-    orb.init(nmax);
+    const bool orb_wide = nmax <= 8;
+    orb.init(orb_wide ? 3 * nmax : nmax);
     for (int q = 0; q < M; q++) {
         int &slot = orb.at(sys.n[q][0], sys.n[q][1], sys.n[q][2]);
         if (slot >= 0) return "duplicate plane-wave vector in nVec";
@@ -64,14 +68,22 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
     // |q|^2 range of orbital differences: components of n_x - n_y are within [-2 nmax, 2 nmax]
     int q2max = 0;
     {
-        Lattice diff;
-        diff.init(2 * nmax);
-        std::vector<char> seen(diff.idx.size(), 0);
-        for (int x = 0; x < M; x++)
-            for (int y = 0; y < M; y++) {
-                int d0 = sys.n[x][0] - sys.n[y][0], d1 = sys.n[x][1] - sys.n[y][1], d2 = sys.n[x][2] - sys.n[y][2];
-                q2max = std::max(q2max, d0 * d0 + d1 * d1 + d2 * d2);
+        // component arrays: the inner loop vectorises
+        std::vector<int> nx(M), ny(M), nz(M);
+        for (int q = 0; q < M; q++) {
+            nx[q] = sys.n[q][0];
+            ny[q] = sys.n[q][1];
+            nz[q] = sys.n[q][2];
+        }
+        for (int x = 0; x < M; x++) {
+            const int ax = nx[x], ay = ny[x], az = nz[x];
+            int m = 0;
+            for (int y = x + 1; y < M; y++) {
+                const int d0 = ax - nx[y], d1 = ay - ny[y], d2 = az - nz[y];
+                m = std::max(m, d0 * d0 + d1 * d1 + d2 * d2);
             }
+            q2max = std::max(q2max, m);
+        }
     }
     p.q2max = q2max;
     p.vtab.resize((size_t)q2max + 1);
@@ -105,19 +117,24 @@ std::string build_solve_plan(const SystemHost &sys, SolvePlan &p)
         partner_of_col.clear();
         const auto &K = kvecs[k];
         int nvd = 0, sd = 0;
-        for (int a = O; a < M; a++) {
-            int b = orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]);
-            if (b > a) {
-                cols.push_back(a);
-                partner_of_col.push_back(b);
-                nvd++;
+        auto scan = [&](auto lookup) {
+            for (int a = O; a < M; a++) {
+                const int b = lookup(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]);
+                if (b > a) {
+                    cols.push_back(a);
+                    partner_of_col.push_back(b);
+                    nvd++;
+                }
             }
-        }
-        for (int a = O; a < M; a++) {
-            int b = orb.get(K[0] - sys.n[a][0], K[1] - sys.n[a][1], K[2] - sys.n[a][2]);
-            if (b == a) {
+        };
+        if (orb_wide) scan([&](int x, int y, int z) { return orb.get_inside(x, y, z); });
+        else scan([&](int x, int y, int z) { return orb.get(x, y, z); });
+        // the self-partner a = b has n_a = K / 2
+        if (K[0] % 2 == 0 && K[1] % 2 == 0 && K[2] % 2 == 0) {
+            const int a = orb.get(K[0] / 2, K[1] / 2, K[2] / 2);
+            if (a >= O) {
                 cols.push_back(a);
-                partner_of_col.push_back(b);
+                partner_of_col.push_back(a);
                 sd++;
             }
         }
