@@ -558,7 +558,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.max_v = max_v;
     if (ladder_smem_bytes(max_v, 32) > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder block exceeds shared memory");
     set_ladder_smem_limit(max_v);
-    d.mosaic_smem = mosaic_smem_bytes(max_v);
+    d.mosaic_smem = mosaic_smem_bytes(max_v, max_o);
     if (d.mosaic_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "mosaic block exceeds shared memory");
     set_mosaic_smem_limit(d.mosaic_smem);
     d.max_occ = max_occ;

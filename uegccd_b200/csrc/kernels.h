@@ -78,7 +78,7 @@ struct DevBatch {
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
 // dynamic shared memory of k_mosaic_blk for blocks of at most max_v virtuals
-size_t mosaic_smem_bytes(int max_v);
+size_t mosaic_smem_bytes(int max_v, int max_o);
 void set_mosaic_smem_limit(size_t bytes);
 // dynamic shared memory of k_ladder3<np> for blocks of at most max_v virtuals
 // row-tile classes: paired 8 (blocks with at most kPairedRows rows i <= j, pad = 4 in

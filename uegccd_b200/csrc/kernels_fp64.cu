@@ -506,12 +506,15 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
 // ----------------------------------------------------------------------------
 constexpr int kMosThreads = 128;
 
-size_t mosaic_smem_bytes(int max_v)
+size_t mosaic_smem_bytes(int max_v, int max_o)
 {
-    return sizeof(double) * ((size_t)kVtabSmem + (size_t)(kMosThreads / 32 + 1) * max_v) +
-           sizeof(int4) * (size_t)max_v + sizeof(int) * (size_t)max_v;
+    return sizeof(double) * ((size_t)kVtabSmem + 2 * (size_t)max_v + (size_t)(kMosThreads / 32) * max_o) +
+           sizeof(int4) * ((size_t)max_v + 2 * (size_t)max_o) + sizeof(int) * (size_t)max_v;
 }
 
+// The threads own the columns (c = tid + k * kMosThreads) and walk the rows: all warps stay
+// busy however few rows a block has.  Column sums stay with their thread; row sums are
+// reduced per warp, then over the warps in a fixed order.
 __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__restrict__ blocks,
                                                            const SolveDev *__restrict__ solves,
                                                            const int16_t *__restrict__ pair_i,
@@ -527,14 +530,16 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     const BlockDev B = blocks[blockIdx.x];
     if (!active[B.solve]) return;
     const SolveDev s = solves[B.solve];
-    const int v = B.v;
+    const int v = B.v, oc = B.nd + B.dg;
     constexpr int kW = kMosThreads / 32;
     extern __shared__ double msm[];
     double *sv = msm;                          // kVtabSmem
-    int4 *nvc = (int4 *)(sv + kVtabSmem);      // v: n-vectors of the block's virtuals
-    double *cacc = (double *)(nvc + v);        // kW x v: per-warp column sums of the rows i < j
-    double *cdg = cacc + kW * v;               // v: the diagonal pair's row (if any)
-    int *pc = (int *)(cdg + v);                // v: column of the partner d = K - c
+    double *coff = sv + kVtabSmem;             // v: column sums over the rows i < j
+    double *cdg = coff + v;                    // v: the diagonal pair's row (if any)
+    double *wrs = cdg + v;                     // kW x oc: per-warp row sums
+    int4 *nvc = (int4 *)(wrs + kW * oc);       // v: n-vectors of the block's virtuals
+    int4 *nk = nvc + v, *nl = nk + oc;         // oc: n-vectors of each row's k and l
+    int *pc = (int *)(nl + oc);                // v: column of the partner d = K - c
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
@@ -542,49 +547,49 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     for (int c = tid; c < v; c += kMosThreads) {
         nvc[c] = nv4[s.orb0 + vir[B.vir0 + c]];
         pc[c] = pcol[B.vir0 + c];
+        coff[c] = cdg[c] = 0.0;
     }
-    for (int e = tid; e < (kW + 1) * v; e += kMosThreads) cacc[e] = 0.0;
+    for (int r = tid; r < oc; r += kMosThreads) {
+        nk[r] = nv4[s.orb0 + pair_i[B.pair0 + r]];
+        nl[r] = nv4[s.orb0 + pair_j[B.pair0 + r]];
+    }
     __syncthreads();
     auto V = [&](int q2) -> double { return vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]); };
     // Rows i <= j only: by the pair symmetry s(l,k,d) = s(k,l,c) for the mirror (l,k) of a
     // row (k,l) and d = K - c, so the mirror row has the same row sum (Joo of l) and adds
     // the column sums of (k,l) with the columns swapped to their partners.
-    const int oc = B.nd + B.dg;
-    for (int r = warp; r < oc; r += kW) {
+    for (int r = 0; r < oc; r++) {
         const bool diag = r >= B.nd;
-        const int4 nk = nv4[s.orb0 + pair_i[B.pair0 + r]], nl = nv4[s.orb0 + pair_j[B.pair0 + r]];
-        const int64_t row = B.t0 + (int64_t)r * v;
+        const int4 rk = nk[r], rl = nl[r];
+        const double *row = t + B.t0 + (int64_t)r * v;
         double rs = 0.0;
-        for (int c = lane; c < v; c += 32) {
-            const double x = t[row + c];
-            const double vck = V(q2_of(nvc[c], nk));
+        for (int c = tid; c < v; c += kMosThreads) {
+            const double x = row[c];
+            const int4 ncv = nvc[c];
+            const double vck = V(q2_of(ncv, rk));
             double sval;
             if (drpa) {
                 sval = 2.0 * vck * x;
             } else {
-                const double y = t[row + pc[c]];  // t(kl, d), same row
-                const double vcl = V(q2_of(nvc[c], nl));
+                const double y = row[pc[c]];  // t(kl, d), same row
+                const double vcl = V(q2_of(ncv, rl));
                 sval = vck * (2.0 * x - y) - vcl * (x - 2.0 * y);
             }
             rs += sval;
             if (diag) cdg[c] = sval;
-            else cacc[warp * v + c] += sval;
+            else coff[c] += sval;
         }
         for (int off = 16; off > 0; off >>= 1) rs += __shfl_down_sync(0xffffffffu, rs, off);
-        if (lane == 0) {
-            mpart[B.row0 + r] = rs;
-            if (!diag) mpart[B.row0 + r + oc] = rs;   // the mirror row
-        }
+        if (lane == 0) wrs[warp * oc + r] = rs;
     }
     __syncthreads();
-    for (int c = tid; c < v; c += kMosThreads) {
-        double a = 0.0, m = 0.0;
-        for (int w = 0; w < kW; w++) {
-            a += cacc[w * v + c];
-            m += cacc[w * v + pc[c]];
-        }
-        mpart[B.col0 + c] = a + m + cdg[c];
+    for (int r = tid; r < oc; r += kMosThreads) {
+        double rs = 0.0;
+        for (int w = 0; w < kW; w++) rs += wrs[w * oc + r];
+        mpart[B.row0 + r] = rs;
+        if (r < B.nd) mpart[B.row0 + r + oc] = rs;   // the mirror row
     }
+    for (int c = tid; c < v; c += kMosThreads) mpart[B.col0 + c] = coff[c] + coff[pc[c]] + cdg[c];
 }
 
 // One warp per target: targets (s, y < V) are Jvv(c = O + y), (s, y >= V) are Joo(k = y - V).
