@@ -424,9 +424,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
                 for (int q0 = 0; q0 < B.o; q0 += 128)
                     for (int p0 = 0; p0 < oc; p0 += 32) htiles.push_back(LadderTile{bi, q0, p0, row_tile(p0)});
             }
-            // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows; their FP16 operands: one
-            // Coulomb slab per 128 virtuals, one d tile per row tile, each over all K chunks
-            const int ntc = B.o <= 16 ? 16 : B.o <= 32 ? 32 : 64;
+            // tensor-core tiles: 128 virtuals x (16, 32 or 64) rows over the rows i <= j (the
+            // update reads G there only); their FP16 operands: one Coulomb slab per 128
+            // virtuals, one d tile per row tile, each over all K chunks
+            const int ntc = oc <= 16 ? 16 : oc <= 32 ? 32 : 64;
             auto &tl = ntc == 16 ? tc16 : ntc == 32 ? tc32 : tc64;
             auto &tx = ntc == 16 ? tcx16 : ntc == 32 ? tcx32 : tcx64;
             const int64_t nch = (B.v + 31) / 32;
@@ -436,13 +437,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
                 wslabs.push_back(WSlabDev{bi, a0, w16_n});
                 w16_n += nch * 128 * 32;
             }
-            for (int p0 = 0; p0 < B.o; p0 += ntc) {
+            for (int p0 = 0; p0 < oc; p0 += ntc) {
                 dtiles.push_back(DTileDev{bi, p0, ntc, nscale, d16_n});
                 d16_n += nch * ntc * 32;
                 nscale += ntc;
             }
             for (int a0 = 0; a0 < B.v; a0 += 128)
-                for (int p0 = 0; p0 < B.o; p0 += ntc) {
+                for (int p0 = 0; p0 < oc; p0 += ntc) {
                     tl.push_back(LadderTile{bi, a0, p0, ntc});
                     const int it = p0 / ntc;
                     tx.push_back(TcTileDev{w0 + (a0 / 128) * nch * 128 * 32, d0 + it * nch * ntc * 32, s0 + it * ntc, 0});
