@@ -104,11 +104,11 @@ def _measured_peaks():
 
 
 HBM_PEAK, BF16_PEAK = _measured_peaks()
-# DRAM bytes of one launch per solve (dram__bytes read + write of one ncu capture), scaled by
-# the solves of a launch: k_ladder and k_mosaic_blk from an 8-twist batch, k_rings (its four
-# class launches of one residual) and k_update from the 100-twist batch itself.
-TRAFFIC_PER_SOLVE = {"k_ladder": 15.3e6 / 8, "k_mosaic_blk": 15.3e6 / 8,
-                     "k_rings": 2.317e9 / 100, "k_update": 1.504e9 / 100}
+# DRAM bytes of one launch per solve (dram__bytes.sum.per_second x gpu__time_duration of one ncu
+# capture of the 100-twist batch itself, all class launches of one residual), scaled by the
+# solves of a launch.
+TRAFFIC_PER_SOLVE = {"k_ladder": 201.8e6 / 100, "k_ladder_hh": 104.1e6 / 100, "k_mosaic_blk": 121.3e6 / 100,
+                     "k_rings": 1467.2e6 / 100, "k_update": 871.1e6 / 100}
 
 
 def twists(n: int, seed: int = SEED, rank: int = 0):
@@ -154,7 +154,32 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = None
 
+    def _run_nvml(self):
+        """In-process NVML reads (every 10 ms): enough samples inside a short timed region.
+        Reads only; no setting of the GPU is touched."""
+        import pynvml as N
+
+        N.nvmlInit()
+        try:
+            h = N.nvmlDeviceGetHandleByIndex(self.idx)
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
+            while not self._stop.is_set():
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                pw = N.nvmlDeviceGetPowerUsage(h) / 1000.0
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append([str(sm), str(mx), f"{pw:.1f}"] + ["Active" if r & b else "Not Active" for b in bits])
+                self._stop.wait(0.01)
+        finally:
+            N.nvmlShutdown()
+
     def _run(self):
+        try:
+            self._run_nvml()
+            return
+        except Exception:
+            pass   # no NVML binding: sample through nvidia-smi
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -371,9 +396,13 @@ def run_gpu(args, rank, world):
 
     # warm-up: fills the device-memory cache for the pipeline's four live batches and the
     # pinned buffers; then three timed runs, the median reported
-    e2e_run(max(6, args.warmup))
-    e2e_runs = [e2e_run(max(10, 4 * args.steps)) for _ in range(3)]
-    e2e_ms = [float(np.median(e2e_runs))]
+    if args.no_e2e:
+        e2e_runs = []
+        e2e_ms = [float("nan")]
+    else:
+        e2e_run(max(6, args.warmup))
+        e2e_runs = [e2e_run(max(10, 4 * args.steps)) for _ in range(3)]
+        e2e_ms = [float(np.median(e2e_runs))]
     h2d, d2h = xfer
     # the other precision on the same batch (timed the same way): mixed beside FP64
     other = None
@@ -462,6 +491,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=150,
                     help="requests of the serving stream reported under 'serve' (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=150.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end pipeline (for profiling the timed device solve alone)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="mixed: particle-particle ladder on the tensor cores (FP16/FP32, defect correction)")
     args = ap.parse_args()
