@@ -111,3 +111,49 @@ def test_spin_and_pair_symmetry(goldens, rs, spin_tol):
     scale = np.abs(tb).max()
     assert spin < spin_tol * scale
     assert pair < 1e-14 * scale
+
+
+def _pair_defect(o, g):
+    """max |g(ij,a) - g(ji,b)| over the allowed amplitudes, and max |g|."""
+    O, M = o.nocc, o.nao
+    nv = o.nvec()
+    idx = {tuple(nv[p]): p for p in range(M)}
+    worst = scale = 0.0
+    for i in range(O):
+        for j in range(O):
+            for a in range(O, M):
+                b = idx.get(tuple(nv[i] + nv[j] - nv[a]), -1)
+                if b < O:
+                    continue
+                worst = max(worst, abs(g[a - O, j, i] - g[b - O, i, j]))
+                scale = max(scale, abs(g[a - O, j, i]))
+    return worst, scale
+
+
+@pytest.mark.parametrize("mask", [1, 2, 4, 8, 16, 31])
+def test_every_ccd_term_keeps_the_pair_symmetry(mask):
+    """Each CCD residual term of the reference (drivers, mosaics, ladders, rings, crossed
+    rings) gives G(ij,a) = G(ji,b) for pair-symmetric amplitudes.  The GPU kernels rest on
+    it: they form G on the amplitudes i <= j and copy each value to its mirror (j,i,b)."""
+    o = Oracle(parse_input_text(""))   # N=14, 19 plane waves, rs=1
+    o.change_twist((0.1, 0.2, 0.3))
+    _, ta, tb, tc, _ = o.mp2()
+    o.ccd(ta, tb, tc, max_iter=4)
+    ga, _ = o.ccd_g2(tb, tc, mask)
+    worst, scale = _pair_defect(o, ga)
+    assert scale > 0
+    assert worst <= 1e-14 * scale
+
+
+@pytest.mark.parametrize("mask", [1, 2, 8, 11])
+def test_every_drpa_term_keeps_the_pair_symmetry(mask):
+    """The same for the dRPA terms (drivers, mosaics, direct rings)."""
+    v = parse_input_text("")
+    v["DodRPASOSEX"] = "T"
+    o = Oracle(v)
+    o.change_twist((0.1, 0.2, 0.3))
+    _, ta, _, _, _ = o.mp2()
+    g = o.drpa_g2(ta, mask)
+    worst, scale = _pair_defect(o, g)
+    assert scale > 0
+    assert worst <= 1e-14 * scale
