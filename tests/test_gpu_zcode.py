@@ -127,3 +127,34 @@ def test_ta_program_with_core_and_gap(goldens, tmp_path, monkeypatch):
     ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
     assert abs(ecs[-1] - st.ecorr) < 1e-9
     assert (tmp_path / "fort.61").read_text().split() == ["6", "core", "electrons", "18", "active", "electrons"]
+
+
+def test_range_flags_follow_setpointers(goldens, tmp_path, monkeypatch):
+    """A "... Range" Input value acts only through CasedERI, which SetPointers (Main.f90:
+    299-302) picks under Safe ERI (or with GapII and CoreN both set).  Without it the
+    reference's ERI ignores the flags: the program runs as without them.  Under Safe ERI
+    the range-separated integrals are outside the GPU path and the run fails."""
+    g = goldens["G5"]
+    base = dict(g["keys"])
+    base.update({"Safe ERI": "F", "TACalcN": "2"})
+    outs = []
+    for extra in ({}, {"Rings Range": "1", "Energy Range": "2"}):
+        d = tmp_path / ("r%d" % len(outs))
+        d.mkdir()
+        keys = dict(base)
+        keys.update(extra)
+        (d / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))
+        _write_twists(d / "Twists", g["ta_twists"][:2])
+        monkeypatch.chdir(d)
+        zcode.run("Input", "Twists")
+        outs.append(((d / "Output").read_text(), (d / "fort.59").read_text()))
+    assert outs[0] == outs[1]
+    d = tmp_path / "cased"
+    d.mkdir()
+    keys = dict(base)
+    keys.update({"Safe ERI": "T", "Rings Range": "1"})
+    (d / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))
+    _write_twists(d / "Twists", g["ta_twists"][:2])
+    monkeypatch.chdir(d)
+    with pytest.raises(Exception):
+        zcode.run("Input", "Twists")

@@ -3,7 +3,8 @@
 //
 // Steps of uegccd_zcode (Main.f90 line ranges):
 //   44-48    ReadInput, init_HEG; SetPointers' integrals: CoreN and GapII are
-//            served (CoreERI, GapERI, NoCaseERI), range flags are refused
+//            served (CoreERI, GapERI, NoCaseERI); range flags are refused where
+//            CasedERI would apply them, and ignored where the reference ignores them
 //   78-79    change_rs to rSMin
 //   83-93    DoSingleCalc: MP2, then CCD or dRPA from the MP2 amplitudes
 //   95-97    DoSkipTA: stop after the single calculation
@@ -125,7 +126,11 @@ UegccdOptions options_for(const UegccdInput &in, int32_t scheme)
     o.do_mosaic = in.do_mosaic;
     o.core_n = (int32_t)((in.nelectron / 2) * in.core_factor);
     o.gapii = in.gapii;
-    o.range_flags = in.range_flags;
+    // The range flags act only through CasedERI, which SetPointers (Main.f90:299-302) picks
+    // under Safe ERI, or when range flags, GapII and CoreN are all set; any other ERI routine
+    // ignores them.
+    const bool cased = in.safe_eri || (in.range_flags > 0 && o.gapii > 0.0 && o.core_n > 0);
+    o.range_flags = cased ? in.range_flags : 0;
     if (scheme == UEGCCD_DIIS) {
         o.scheme = UEGCCD_DIIS;
         o.ndiis = 6;
