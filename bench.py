@@ -148,38 +148,34 @@ def build_systems(tw):
 
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock and clock-event reasons while the timed region runs: in-process NVML reads every
+    10 ms (reads only; no setting of the GPU is touched), else nvidia-smi.  NVML is opened before
+    the region starts, and the last sample is taken when it ends, so even a short region has
+    samples."""
+
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+
+    def _nvml_sample(self):
+        N, h, mx, bits = self._nvml
+        sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+        pw = N.nvmlDeviceGetPowerUsage(h) / 1000.0
+        r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append([str(sm), str(mx), f"{pw:.1f}"] + ["Active" if r & b else "Not Active" for b in bits])
 
     def _run_nvml(self):
-        """In-process NVML reads (every 10 ms): enough samples inside a short timed region.
-        Reads only; no setting of the GPU is touched."""
-        import pynvml as N
+        while not self._stop.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            self._stop.wait(0.01)
 
-        N.nvmlInit()
-        try:
-            h = N.nvmlDeviceGetHandleByIndex(self.idx)
-            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
-            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
-                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
-            while not self._stop.is_set():
-                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
-                pw = N.nvmlDeviceGetPowerUsage(h) / 1000.0
-                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append([str(sm), str(mx), f"{pw:.1f}"] + ["Active" if r & b else "Not Active" for b in bits])
-                self._stop.wait(0.01)
-        finally:
-            N.nvmlShutdown()
-
-    def _run(self):
-        try:
-            self._run_nvml()
-            return
-        except Exception:
-            pass   # no NVML binding: sample through nvidia-smi
+    def _run_smi(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -195,13 +191,34 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        try:
+            import pynvml as N
+
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.idx)
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
+            self._nvml = (N, h, mx, bits)
+        except Exception:
+            self._nvml = None
+        self._t = threading.Thread(target=self._run_nvml if self._nvml else self._run_smi, daemon=True)
         self._t.start()
         return self
 
     def __exit__(self, *a):
+        if self._nvml:
+            try:
+                self._nvml_sample()   # the region's end
+            except Exception:
+                pass
         self._stop.set()
         self._t.join(timeout=10)
+        if self._nvml:
+            try:
+                self._nvml[0].nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
