@@ -64,7 +64,8 @@ typedef struct {
     int32_t do_ring, do_xring, do_ladder, do_mosaic;   /* Input "Do Rings" ... (IO.f90:170-180)   */
     int32_t core_n;          /* UEGInfo%CoreN: integrals with an orbital <= CoreN are zero (CAS) */
     double gapii;            /* UEGInfo%GapII: integrals above GapII are zero when GapII > 0     */
-    int32_t range_flags;     /* sum of |"... Range"| Input values; must be 0                    */
+    int32_t range_flags;     /* sum of |"... Range"| Input values where CasedERI applies them;   */
+                             /* non-zero: CCD on the batch's uniform range flag (set_range)      */
     int32_t max_iter;        /* MaxIter, 1000 (CCD.f90:36)                                      */
     double tol;              /* TolMax on max|dT|, 1e-8 (HEG.f90:1078)                          */
     double denom_factor;     /* DenomFactor, 2 (CCD.f90:11)                                     */
@@ -114,6 +115,16 @@ int uegccd_ctx_set_eigen(UegccdCtx *ctx, const double *eigen);
  * Amplitudes of core pairs (i or j <= CoreN) stay zero, as in the reference; amplitudes
  * passed in are read with their core pairs set to zero. */
 int uegccd_ctx_set_integrals(UegccdCtx *ctx, int32_t core_n, double gapii);
+
+/* Range-separated integrals with one flag for every CCD term (CasedERI, HEG.f90:689-774:
+ * 1 short range, 2 long range, 3 none), as the reference computes them when all fifteen
+ * "... Range" Input values equal flag under CasedERI.  The spin adaptation holds in that
+ * case (direct and exchange integrals share the flag).  CCD solves whose options carry
+ * range_flags != 0 then use the flag's integrals for every term and the energy (CCD.f90:
+ * 216-217, 491-492, 555-556, 620-917); the MP2 start keeps the plain integrals
+ * (MP2.f90:61-62).  screening = HEGData%ScreeningDistance (HEG.f90:512).  flag 0 clears.
+ * Terms with different flags, and range-separated dRPA, return UEGCCD_ERR_UNSUPPORTED. */
+int uegccd_ctx_set_range(UegccdCtx *ctx, int32_t flag, double screening);
 
 /* DrvMBPT (MP2.f90:11-157): writes the MP2 amplitudes T2aaaa/T2abab/T2abba (each
  * may be NULL) and E(2).  Its structure factor is uegccd_structure_factor of T2abab. */
@@ -197,6 +208,8 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
 /* uegccd_ctx_set_integrals for every system of the batch (uegccd_batch_solve sets
  * them from its options first). */
 int uegccd_batch_set_integrals(UegccdBatch *b, int32_t core_n, double gapii);
+/* The same for every solve of a batch. */
+int uegccd_batch_set_range(UegccdBatch *b, int32_t flag, double screening);
 /* DrvMBPT for every system: the MP2 amplitudes stay in the batch (what
  * uegccd_batch_structure_factor and uegccd_batch_get_amplitudes then read); e2[n]
  * may be NULL. */

@@ -101,6 +101,8 @@ def lib() -> C.CDLL:
         L.uegccd_diis_destroy.argtypes = [vp]
         L.uegccd_ctx_set_integrals.argtypes = [vp, C.c_int32, C.c_double]
         L.uegccd_batch_set_integrals.argtypes = [vp, C.c_int32, C.c_double]
+        L.uegccd_ctx_set_range.argtypes = [vp, C.c_int32, C.c_double]
+        L.uegccd_batch_set_range.argtypes = [vp, C.c_int32, C.c_double]
         L.uegccd_sf_length.argtypes = [P(System)]
         L.uegccd_sf_length.restype = C.c_int32
         L.uegccd_structure_factor.argtypes = [vp, dp, P(SfGrid)]

@@ -208,6 +208,9 @@ struct UegccdBatch {
     int core_n = 0;
     double gapii = 0.0;
     std::vector<double> vtab_base;
+    // range-separated integrals with one flag for every CCD term (uegccd_*_set_range)
+    int range_flag = 0;
+    double screening = 0.0;
     double *sf_grid = nullptr;
     int *sf_err = nullptr;
 
@@ -724,6 +727,49 @@ int unpack_to_host(UegccdBatch &b, int s, const double *t_dev, double *ab, doubl
 // the |q|^2 tables are filtered; CoreN > 0 zeroes those with an index p <= CoreN
 // (CoreERI, HEG.f90:882-885) -- the kernels hold core pairs at zero.  The per-amplitude
 // Coulomb factors are rebuilt from the filtered tables.
+// The |q|^2 tables of every solve for an ERI flag (CasedERI, HEG.f90:725-774; flag 0 is
+// BaseERI's value), with the reference's "< 0 -> -100" guard and the GapII filter applied in
+// its order.  CoreN is not in the tables: the kernels hold core pairs at zero.
+std::vector<double> integral_tables(const UegccdBatch &b, int flag, double gapii)
+{
+    std::vector<double> vt;
+    vt.reserve(b.vtab_base.size());
+    for (size_t s = 0; s < b.plans.size(); s++) {
+        const double L = b.sys[s].L, mad = b.sys[s].madelung, sd = b.screening;
+        for (int q2 = 0; q2 <= b.plans[s].q2max; q2++) {
+            double v = 0.0;
+            if (flag == 0) {
+                v = coulomb_v(L, mad, q2);
+            } else if (q2 == 0) {
+                if (flag == 1) v = (1.0 / std::pow(L, 3.0)) * 4.0 * kPi / std::pow(sd, 2.0);
+                else if (flag == 2) v = -mad - (1.0 / std::pow(L, 3.0)) * 4.0 * kPi / std::pow(sd, 2.0);
+            } else {
+                const double q2s = (double)q2 * std::pow(2.0 * kPi / L, 2.0);
+                if (flag == 1) v = (1.0 / std::pow(L, 3.0)) * 4.0 * kPi / (std::pow(sd, 2.0) + q2s);
+                else if (flag == 2)
+                    v = (1.0 / std::pow(L, 3.0)) * 4.0 * kPi / (std::pow(sd, 2.0) + q2s) * std::pow(sd, 2.0) / q2s;
+            }
+            if (flag != 0 && v < 0.0) v = -100.0;
+            if (gapii > 0.0 && v > gapii) v = 0.0;
+            vt.push_back(v);
+        }
+    }
+    return vt;
+}
+
+// Uploads the tables of an ERI flag and the Coulomb factors that follow them.
+int load_tables(UegccdBatch &b, int flag)
+{
+    const std::vector<double> vt = integral_tables(b, flag, b.gapii);
+    CU(cudaMemcpyAsync(b.d.vtab, vt.data(), vt.size() * sizeof(double), cudaMemcpyHostToDevice, b.stream));
+    launch_vcoef(b.d, b.stream);
+    b.d.w16_valid = false;   // the FP16 Coulomb slabs follow the tables
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(b.stream));
+    b.h2d_bytes += (int64_t)(vt.size() * sizeof(double));
+    return 0;
+}
+
 int set_integrals(UegccdBatch &b, int core_n, double gapii)
 {
     if (core_n < 0) return fail(UEGCCD_ERR_ARG, "CoreN must be >= 0");
@@ -774,10 +820,15 @@ int mixed_alloc(UegccdBatch &b)
     return 0;
 }
 
-int validate_options(const UegccdOptions *o, int drpa)
+int validate_options(const UegccdOptions *o, int drpa, const UegccdBatch &b)
 {
     if (!o) return fail(UEGCCD_ERR_ARG, "null options");
-    if (o->range_flags != 0) return fail(UEGCCD_ERR_UNSUPPORTED, "range-separated integrals are outside the GPU path");
+    if (o->range_flags != 0 && drpa)
+        return fail(UEGCCD_ERR_UNSUPPORTED, "range-separated dRPA is outside the GPU path");
+    if (o->range_flags != 0 && b.range_flag == 0)
+        return fail(UEGCCD_ERR_UNSUPPORTED,
+                    "range-separated integrals: set one flag for every term with uegccd_*_set_range "
+                    "(terms with different flags are outside the GPU path)");
     if (!drpa && (o->do_ring != 0) != (o->do_xring != 0))
         return fail(UEGCCD_ERR_UNSUPPORTED,
                     "Do Rings and Do XRings must agree: alone, either breaks the spin symmetry the GPU path uses");
@@ -887,6 +938,21 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     f.do_ring = opt->do_ring ? 1 : 0;
     f.do_xring = (!drpa && opt->do_xring) ? 1 : 0;
     const int ndiis = opt->scheme == UEGCCD_DIIS ? opt->ndiis : 0;
+    // range-separated integrals: every CCD term and the energy on the flag's tables (the MP2
+    // start before this used the plain ones); the plain tables back on every exit
+    struct TableGuard {
+        UegccdBatch &b;
+        bool on;
+        ~TableGuard()
+        {
+            if (on) load_tables(b, 0);
+        }
+    } table_guard{b, false};
+    if (opt->range_flags != 0 && b.range_flag != 0) {
+        const int rc0 = load_tables(b, b.range_flag);
+        if (rc0) return rc0;
+        table_guard.on = true;
+    }
     const int max_rec = std::min(opt->max_iter, 1100);
     int rc = ctl_alloc(b, ndiis, max_rec);
     if (rc) return rc;
@@ -1139,6 +1205,27 @@ int uegccd_ctx_set_eigen(UegccdCtx *c, const double *eigen)
     return 0;
 }
 
+int set_range(UegccdBatch &b, int32_t flag, double screening)
+{
+    if (flag < 0 || flag > 3) return fail(UEGCCD_ERR_ARG, "range flag must be 0, 1, 2 or 3");
+    if (flag != 0 && !(screening > 0.0)) return fail(UEGCCD_ERR_ARG, "screening distance must be > 0");
+    b.range_flag = flag;
+    b.screening = flag != 0 ? screening : 0.0;
+    return 0;
+}
+
+int uegccd_ctx_set_range(UegccdCtx *c, int32_t flag, double screening)
+{
+    if (!c) return fail(UEGCCD_ERR_ARG, "null context");
+    return set_range(*c->batch, flag, screening);
+}
+
+int uegccd_batch_set_range(UegccdBatch *b, int32_t flag, double screening)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    return set_range(*b, flag, screening);
+}
+
 int uegccd_ctx_set_integrals(UegccdCtx *c, int32_t core_n, double gapii)
 {
     if (!c) return fail(UEGCCD_ERR_ARG, "null context");
@@ -1172,9 +1259,9 @@ int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t
                UegccdResult *res)
 {
     if (!c || !t_abab || !res) return fail(UEGCCD_ERR_ARG, "null argument");
-    int rc = validate_options(opt, 0);
-    if (rc) return rc;
     UegccdBatch &b = *c->batch;
+    int rc = validate_options(opt, 0, b);
+    if (rc) return rc;
     if ((rc = set_integrals(b, opt->core_n, opt->gapii))) return rc;
     if ((rc = pack_from_host(b, 0, t_abab))) return rc;
     int st = run_solves(b, opt, 0, res);
@@ -1186,9 +1273,9 @@ int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t
 int uegccd_drpa(UegccdCtx *c, const UegccdOptions *opt, double *t2, UegccdResult *res)
 {
     if (!c || !t2 || !res) return fail(UEGCCD_ERR_ARG, "null argument");
-    int rc = validate_options(opt, 1);
-    if (rc) return rc;
     UegccdBatch &b = *c->batch;
+    int rc = validate_options(opt, 1, b);
+    if (rc) return rc;
     if ((rc = set_integrals(b, opt->core_n, opt->gapii))) return rc;
     if ((rc = pack_from_host(b, 0, t2))) return rc;
     int st = run_solves(b, opt, 1, res);
@@ -1274,7 +1361,7 @@ int uegccd_batch_destroy(UegccdBatch *b)
 int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2, UegccdResult *results)
 {
     if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
-    int rc = validate_options(opt, drpa);
+    int rc = validate_options(opt, drpa, *b);
     if (rc) return rc;
     if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
     CU(cudaEventRecord(b->ev_solve0, b->stream));

@@ -64,6 +64,11 @@ class Context:
         """CoreN and GapII of the integrals for the calls that follow (CoreERI/GapERI)."""
         capi.check(capi.lib().uegccd_ctx_set_integrals(self._h, int(core_n), float(gapii)))
 
+    def set_range(self, flag: int, screening: float = 0.0) -> None:
+        """One CasedERI range flag for every CCD term (1 short, 2 long range, 3 none; 0 clears),
+        used by the CCD calls whose options carry range_flags != 0."""
+        capi.check(capi.lib().uegccd_ctx_set_range(self._h, int(flag), float(screening)))
+
     def mp2(self):
         """DrvMBPT: returns (E2, T2aaaa, T2abab, T2abba)."""
         ta, tb, tc = self.zeros_t(), self.zeros_t(), self.zeros_t()
@@ -141,6 +146,10 @@ class Batch:
     def set_integrals(self, core_n: int = 0, gapii: float = 0.0) -> None:
         """CoreN and GapII of the integrals for the calls that follow (CoreERI/GapERI)."""
         capi.check(capi.lib().uegccd_batch_set_integrals(self._h, int(core_n), float(gapii)))
+
+    def set_range(self, flag: int, screening: float = 0.0) -> None:
+        """One CasedERI range flag for every CCD term of every solve (see Context.set_range)."""
+        capi.check(capi.lib().uegccd_batch_set_range(self._h, int(flag), float(screening)))
 
     def mp2(self) -> np.ndarray:
         """DrvMBPT of every system; the MP2 amplitudes stay in the batch.  Returns E(2)."""
