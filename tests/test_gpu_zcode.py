@@ -158,3 +158,30 @@ def test_range_flags_follow_setpointers(goldens, tmp_path, monkeypatch):
     monkeypatch.chdir(d)
     with pytest.raises(Exception):
         zcode.run("Input", "Twists")
+
+
+def test_ta_program_with_one_range_flag(goldens, tmp_path, monkeypatch):
+    """The G5 program on 3 twists with all fifteen "... Range" values 1 under Safe ERI
+    (CasedERI, short range for every CCD term): the per-twist MP2 (plain integrals) in
+    fort.59 and the special-twist Ec(CCD) against the oracle."""
+    from oracle.oracle import Oracle, parse_input_text
+
+    g = goldens["G5"]
+    keys = dict(g["keys"])
+    keys.update({"TACalcN": "3", "Safe ERI": "T"})
+    keys.update({k: "1" for k in ("Rings Range", "XRings Range", "Ladders Range", "Mosaics Range",
+                                  "DriverDir Range", "DriverEx Range", "Energy Range", "LinRings Range",
+                                  "QuadRings Range", "DRings Range", "ExRings Range", "LinLadd Range",
+                                  "QuadLadd Range", "DLadders Range", "ExLadders Range")})
+    (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))
+    _write_twists(tmp_path / "Twists", g["ta_twists"][:3])
+    monkeypatch.chdir(tmp_path)
+    zcode.run("Input", "Twists")
+    rows = np.array([[float(x) for x in l.split()] for l in (tmp_path / "fort.59").read_text().splitlines()[:3]])
+    vals = parse_input_text("")
+    vals.update(keys)
+    per, special, st, _ = Oracle(vals).twist_average(np.array(g["ta_twists"][:3]))
+    np.testing.assert_allclose(rows[:, 3:6], per, rtol=0, atol=1e-12)
+    out = (tmp_path / "Output").read_text()
+    ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
+    assert abs(ecs[-1] - st.ecorr) < 1e-9

@@ -365,6 +365,7 @@ int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
     std::string line;
     int lineno = 0;
     int fcut2ecut = 0;
+    std::map<std::string, int> range;   // the "... Range" values read (the others are 0)
     while (std::getline(f, line)) {
         lineno++;
         size_t c = line.find('!');
@@ -398,6 +399,7 @@ int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
             int r = 0;
             vs >> r;
             in->range_flags += std::abs(r);
+            range[key] = r;
         } else if (key == "NTwist") vs >> in->ntwist[0] >> in->ntwist[1] >> in->ntwist[2];
         else if (key == "CoreFactor") {
             vs >> in->core_factor;
@@ -429,6 +431,18 @@ int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
         }
     }
     in->fcut2ecut = fcut2ecut;
+    {   // one value for all fifteen range flags, or -1
+        int v = 0;
+        bool first = true, same = true;
+        for (int k = 10; k < 25; k++) {   // kNames[10..24]: the "... Range" keys
+            const auto it = range.find(kNames[k]);
+            const int r = it == range.end() ? 0 : it->second;
+            if (first) v = r;
+            else if (r != v) same = false;
+            first = false;
+        }
+        in->range_uniform = same ? v : -1;
+    }
     if (require_all) {
         for (int k = 2; k < nparams; k++)
             if (count[kNames[k]] == 0) return herr(UEGCCD_ERR_ARG, std::string("Error: Parameter ") + kNames[k] + " not set.");

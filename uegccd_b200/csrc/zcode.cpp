@@ -3,8 +3,9 @@
 //
 // Steps of uegccd_zcode (Main.f90 line ranges):
 //   44-48    ReadInput, init_HEG; SetPointers' integrals: CoreN and GapII are
-//            served (CoreERI, GapERI, NoCaseERI); range flags are refused where
-//            CasedERI would apply them, and ignored where the reference ignores them
+//            served (CoreERI, GapERI, NoCaseERI); one range flag shared by all fifteen
+//            "... Range" values is served under CasedERI, different flags are refused,
+//            and the flags are ignored where the reference ignores them
 //   78-79    change_rs to rSMin
 //   83-93    DoSingleCalc: MP2, then CCD or dRPA from the MP2 amplitudes
 //   95-97    DoSkipTA: stop after the single calculation
@@ -107,6 +108,16 @@ void write_cc(FILE *f, const UegccdInput &in, int drpa, const UegccdResult &r, c
     std::snprintf(es, sizeof es, "%.12E", r.max_res);  // ES18.12
     std::fprintf(f, "              * Max CCD Residual is      %18s    *\n", es);
     std::fputs(kStars, f);
+}
+
+constexpr double kPiZ = 3.1415926535897932384626433833;  // Constants.f90:7
+
+// HEGData%ScreeningDistance after change_rs (HEG.f90:509-511)
+static double screening_of(const UegccdInput &in, double L)
+{
+    const double density = in.nelectron / std::pow(L, 3.0);
+    const double kf = std::pow(3.0 * std::pow(kPiZ, 2.0) * density, 1.0 / 3.0);
+    return std::pow(4.0 / kPiZ * kf, 0.5);
 }
 
 // DrvCCD / DrvdRPA options from the Input (FindTol sees rS = 1, HEG.f90:28; the
@@ -225,6 +236,9 @@ int mp2_then_cc(const UegccdInput &in, const UegccdSystem &sys, double ehf, cons
     if (uegccd_ctx_create(&sys, &ctx)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
     double e2 = 0.0;
     int rc = uegccd_ctx_set_integrals(ctx, opt.core_n, opt.gapii);  // the ERI that SetPointers chose
+    // one range flag for every term (otherwise the solve refuses range_flags != 0)
+    if (!rc && opt.range_flags != 0 && in.range_uniform > 0)
+        rc = uegccd_ctx_set_range(ctx, in.range_uniform, screening_of(in, sys.L));
     if (!rc) rc = uegccd_mp2(ctx, x.aaaa.data(), x.abab.data(), x.abba.data(), &e2);
     if (rc) {
         zfail(rc, uegccd_last_error());
@@ -426,6 +440,10 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
     sf.mp2_in_cc = in.do_sf_calc_mp2 != 0;
     sf.ccd = in.do_sf_calc_ccd != 0;
     const UegccdOptions opt = options_for(in, scheme);
+    // CCEnergyAndSF takes its integrals with the energy's range flag (CCD.f90:290-291): the
+    // structure-factor grids are built on the plain integrals only
+    if (opt.range_flags != 0 && (in.do_sf_calc_mp2 || in.do_sf_calc_ccd))
+        return zfail(UEGCCD_ERR_UNSUPPORTED, "structure factors of range-separated integrals are outside the GPU path");
     UegccdHegInfo info;
     UegccdSystem sys;
     UegccdResult res;
@@ -489,6 +507,9 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
     if (uegccd_batch_create(systems.data(), nset, &bg.b)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
     UegccdBatch *b = bg.b;
     if ((rc = uegccd_batch_set_integrals(b, opt.core_n, opt.gapii)) || (rc = uegccd_batch_mp2(b, mp2.data())))
+        return zfail(rc, uegccd_last_error());
+    if (opt.range_flags != 0 && in.range_uniform > 0 &&
+        (rc = uegccd_batch_set_range(b, in.range_uniform, screening_of(in, systems[0].L))))
         return zfail(rc, uegccd_last_error());
     const bool cc_sf = in.do_calc_ta_ccd && !in.do_drpa_sosex;
     std::vector<std::string> mp2_80(nset);   // DrvCCD's DoSFCalcMP2 blocks, written beside the CCD ones
