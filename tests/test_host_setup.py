@@ -69,3 +69,25 @@ def test_find_tol():
     assert heg.find_tol(1.0) == (1e-8, 100.0, 2.0)     # HEG.f90:1078-1079
     assert heg.find_tol(5.5) == (1e-6, 100.0, 5.0)
     assert heg.find_tol(0.5)[1] == 1e6
+
+
+RANGE_KEYS = ["Rings Range", "XRings Range", "Ladders Range", "Mosaics Range", "DriverDir Range",
+              "DriverEx Range", "Energy Range", "LinRings Range", "QuadRings Range", "DRings Range",
+              "ExRings Range", "LinLadd Range", "QuadLadd Range", "DLadders Range", "ExLadders Range"]
+
+
+@pytest.mark.parametrize("flags,total,uniform", [
+    ({}, 0, 0),
+    ({k: "2" for k in RANGE_KEYS}, 30, 2),
+    ({"Rings Range": "1"}, 1, -1),
+    ({**{k: "1" for k in RANGE_KEYS}, "Energy Range": "2"}, 16, -1),
+])
+def test_read_input_range_flags(tmp_path, flags, total, uniform):
+    """ReadInput's "... Range" values: their |sum| (non-zero: CasedERI applies flags) and the
+    one value they share, or -1 (the GPU path serves a shared flag only)."""
+    from uegccd_b200 import heg
+
+    (tmp_path / "Input").write_text("# Electrons: 14\n" + "".join(f"{k}: {v}\n" for k, v in flags.items()))
+    p = heg.read_input(str(tmp_path / "Input"), require_all=False)
+    assert p.range_flags == total
+    assert p.range_uniform == uniform
