@@ -2,9 +2,8 @@
 NOcc=57, 2.1 M allowed amplitudes), Gamma point.
 
 1. Term level: the ring and crossed-ring G2 of the MP2 amplitudes against the oracle
-   at rs=1. The largest {Q,-Q} group pairs of this size go to the FMA form of the
-   ring kernel, the others to the tensor-core form. Tolerance: 1e-12 relative to the
-   largest term.
+   at rs=1, with {Q,-Q} group pairs of up to 57 rows a side on the tensor-core form of
+   the ring kernel. Tolerance: 1e-12 relative to the largest term.
 2. Solve level, per rs in {0.5, 1, 2, 5}: mixed precision (tcgen05 FP16 ladder with
    FP64 refinement) against FP64, both with Pulay DIIS to max|dT| < 1e-11 (tight, so
    that the two stopping points do not differ by their convergence error). The bar is
