@@ -43,8 +43,8 @@ SEED = 2024
 REF_ITERS_PER_SOLVE = 33.16  # measured: replay mode on this workload, 100 twists (min 30, max 35)
 SOLVE_OPTS = dict(scheme=1, ndiis=6, denom_factor=1.0, tol=1e-9)
 E2E_CREATORS = 2   # host threads creating the next batches of the e2e pipeline
-# Nominal FP64 peak of a B200 (datasheet); the bench measures it each run with the library's
-# register-only probe (37.0 TFLOP/s measured on this pool) and uses this only if the probe fails.
+# Nominal FP64 peak of a B200 (datasheet); the bench measures it each run with the register-only
+# probe of bench_peak.cu (37.0 TFLOP/s measured on B200) and uses this only if the probe fails.
 FP64_PEAK_TFLOPS = 37.0
 
 
@@ -71,13 +71,17 @@ def _nvtx():
 
 
 def probe_fp64_peak():
-    """FP64 tensor-core TFLOP/s of this GPU from the library's register-only probe (None on failure)."""
+    """FP64 tensor-core TFLOP/s of this GPU from bench_peak.so's register-only probe (None on failure)."""
     import ctypes as C
 
-    from uegccd_b200 import _capi
-
+    path = os.path.join(ROOT, "bench_peak.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    lib.bench_fp64_peak.argtypes = [C.POINTER(C.c_double), C.c_char_p, C.c_int]
     v = C.c_double()
-    return v.value if _capi.lib().uegccd_probe_fp64_peak(C.byref(v)) == 0 else None
+    msg = C.create_string_buffer(256)
+    return v.value if lib.bench_fp64_peak(C.byref(v), msg, 256) == 0 else None
 
 
 def pinned_buffer(n: int):
@@ -100,7 +104,7 @@ def _measured_peaks():
             d = json.load(f)
         return float(d.get("hbm_gbs", 6650.0)), float(d.get("bf16_tflops", 1590.0))
     except Exception:
-        return 6650.0, 1590.0  # fallback figures of this pool
+        return 6650.0, 1590.0  # fallback figures: an earlier measurement on B200
 
 
 HBM_PEAK, BF16_PEAK = _measured_peaks()
@@ -320,6 +324,16 @@ def ladder_flops(batch_systems):
     return tot
 
 
+def job_rates(args, world: int, device_ms: float, e2e_ms_per_step: float):
+    """Whole-job rates from this rank's times: every rank solves its own args.twists per
+    step, and the job takes as long as its slowest rank (max over ranks).  Returns
+    (solves/s on the device, the max device ms, e2e solves/s)."""
+    e_max, e2e_max = reduce_max([device_ms, e2e_ms_per_step])
+    value = args.twists * world * args.steps / (e_max / 1e3)
+    e2e_value = args.twists * world / (e2e_max / 1e3)
+    return value, e_max, e2e_value
+
+
 def run_gpu(args, rank, world):
     import numpy as np
 
@@ -330,7 +344,8 @@ def run_gpu(args, rank, world):
         opts["precision"] = 1
     tw = twists(args.twists, rank=rank)
     systems = build_systems(tw)
-    batch = Batch(systems)
+    device = int(os.environ.get("LOCAL_RANK", 0))   # one GPU per rank; batches live on it
+    batch = Batch(systems, device=device)
     # the reference's own iteration once (untimed): iteration count and energies
     rc_r, e2_r, res_r = batch.solve()
     # warm-up (untimed)
@@ -376,7 +391,7 @@ def run_gpu(args, rank, world):
 
     def create():
         t = time.perf_counter()
-        b2 = Batch(systems)
+        b2 = Batch(systems, device=device)   # a creator thread starts on device 0: name the rank's
         stage_ms["create"].append((time.perf_counter() - t) * 1e3)
         return b2
 
@@ -437,12 +452,9 @@ def run_gpu(args, rank, world):
         other = {"precision": "mixed" if args.precision != "mixed" else "fp64",
                  "ms": float(sum(oms)), "niter_mean": float(np.mean([r["niter"] for r in reso])),
                  "fails": int(sum(r["fail"] for r in reso)), "max_dE": float(dE)}
-    e_max, e2e_mean = reduce_max([total_ms, float(np.mean(e2e_ms))])
+    value, e_max, e2e_value = job_rates(args, world, total_ms, float(np.mean(e2e_ms)))
     if other is not None:
         other["ms"] = reduce_max([other["ms"]])[0]
-    solves_total = args.twists * world * args.steps
-    value = solves_total / (e_max / 1e3)
-    e2e_value = args.twists * world / (e2e_mean / 1e3)
     out = {
         "value": value, "ms_per_step": e_max / args.steps, "e2e_value": e2e_value, "h2d": h2d, "d2h": d2h,
         "niter_mean": float(np.mean(niters)), "niter_min": int(min(niters)), "niter_max": int(max(niters)),
@@ -493,7 +505,38 @@ def oracle_rate(ncores: int, iters: int, iters_per_solve: float, rank: int = 0):
     return ncores / sec_per_solve, per_iter, wall
 
 
-def main():
+def _rank_entry(target, env, argv):
+    os.environ.update(env)
+    target(argv)
+
+
+def launch_ranks(n: int, target, argv) -> int:
+    """Without torchrun: one process per GPU of this node, ranks 0..n-1 (RANK, LOCAL_RANK,
+    WORLD_SIZE and a 127.0.0.1 rendezvous in each one's environment), each running
+    target(argv).  Returns 0 when every rank exited 0, else the first non-zero exit code."""
+    import multiprocessing as mp
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    procs = []
+    for r in range(n):
+        env = {"RANK": str(r), "LOCAL_RANK": str(r), "WORLD_SIZE": str(n), "LOCAL_WORLD_SIZE": str(n),
+               "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)}
+        p = ctx.Process(target=_rank_entry, args=(target, env, list(argv)))
+        p.start()
+        procs.append(p)
+    rc = 0
+    for p in procs:
+        p.join()
+        if rc == 0 and p.exitcode:
+            rc = p.exitcode if p.exitcode > 0 else 1
+    return rc
+
+
+def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -512,7 +555,10 @@ def main():
                     help="skip the end-to-end pipeline (for profiling the timed device solve alone)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="mixed: particle-particle ladder on the tensor cores (FP16/FP32, defect correction)")
-    args = ap.parse_args()
+    args = ap.parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
+        # not under torchrun: start one rank per GPU here
+        sys.exit(launch_ranks(args.gpus, main, sys.argv[1:] if argv is None else argv))
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     metric = "CCD solves/s (N=54 rs=1 twist batch, FP64)"
@@ -545,10 +591,12 @@ def main():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         from datetime import timedelta
 
-        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        # host-side timing reduction only (the solves exchange nothing): gloo, short timeout
+        dist.init_process_group("gloo", timeout=timedelta(seconds=300))
     g = run_gpu(args, rank, world)
     if rank != 0:
         if world > 1:

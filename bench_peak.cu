@@ -1,17 +1,14 @@
-// probe.cu -- the FP64 tensor-core peak of the current device, measured: the roofline
-// denominator of the FP64 DMMA kernels (the ladders and rings).  A register-only kernel
-// issues independent mma.sync.m8n8k4.f64 chains (eight per warp, eight CTAs of four warps
-// per SM) and is timed with CUDA events after one untimed launch.
+// bench_peak.cu -- bench.py's measurement of the FP64 tensor-core peak of the current
+// device: the roofline denominator of the FP64 DMMA kernels (the ladders and rings), which
+// the measured-peaks record of the machine does not hold.  A register-only kernel issues
+// independent mma.sync.m8n8k4.f64 chains (eight per warp, eight CTAs of four warps per SM)
+// and is timed with CUDA events after one untimed launch.  Built into bench_peak.so beside
+// bench.py; it is measurement tooling, not part of the library's ABI.
+//
+//   int bench_fp64_peak(double *tflops, char *msg, int msg_len);   0 ok, else a CUDA error
 #include <cuda_runtime.h>
 
-#include <string>
-
-#include "../../include/uegccd.h"
-
-namespace uegccd {
-int set_last_error(int code, const char *msg);
-int device_ok();
-}
+#include <cstdio>
 
 namespace {
 
@@ -35,17 +32,20 @@ __global__ void __launch_bounds__(128) k_fp64_mma_probe(double *out, int iters)
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;   // keeps the chains live
 }
 
-int fail(int code, const std::string &m) { return uegccd::set_last_error(code, m.c_str()); }
-
 }  // namespace
 
-extern "C" int uegccd_probe_fp64_peak(double *tflops)
+extern "C" int bench_fp64_peak(double *tflops, char *msg, int msg_len)
 {
-    if (!tflops) return fail(UEGCCD_ERR_ARG, "null argument");
-    if (int rc = uegccd::device_ok()) return rc;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (!tflops) return -1;
+    int dev = 0, sms = 0, major = 0;
+    cudaError_t e0q = cudaGetDevice(&dev);
+    if (e0q == cudaSuccess) e0q = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e0q == cudaSuccess) e0q = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e0q != cudaSuccess || major != 10) {
+        if (msg && msg_len > 0)
+            std::snprintf(msg, (size_t)msg_len, "no sm_100 device: %s", cudaGetErrorString(e0q));
+        return -2;
+    }
     const int threads = 128, blocks = sms * 8, iters = 4096;
     double *out = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -65,8 +65,11 @@ extern "C" int uegccd_probe_fp64_peak(double *tflops)
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (out) cudaFree(out);
-    if (e != cudaSuccess) return fail(UEGCCD_ERR_CUDA, std::string("FP64 probe: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        if (msg && msg_len > 0) std::snprintf(msg, (size_t)msg_len, "FP64 probe: %s", cudaGetErrorString(e));
+        return -2;
+    }
     const double flops = (double)blocks * (threads / 32) * iters * kChains * 512.0;  // 2*8*8*4 per mma
     *tflops = flops / (ms * 1e-3) / 1e12;
-    return UEGCCD_OK;
+    return 0;
 }

@@ -89,6 +89,13 @@ typedef struct {
     int32_t n_recorded;      /* entries written to energies/dts                                 */
     int32_t kernel_launches; /* CUDA kernels this call launched                                 */
     double gpu_ms;           /* device time of the call (CUDA events)                           */
+    int32_t status;          /* this solve's status: UEGCCD_OK, UEGCCD_NOT_CONVERGED (MaxIter or  */
+                             /* MaxRes > FailRatio*TolMax) or UEGCCD_ERR_NUMERIC (NaN/Inf); a     */
+                             /* batch call returns the worst of them                              */
+    int32_t ndiis;           /* DIIS vectors used: opt->ndiis, or fewer (down to 2) when device   */
+                             /* memory or the library's limit held no more, as SetUpDIISCC steps  */
+                             /* its NDIIS down until Allocate succeeds (DIISCC.f90:22-29); 0 for  */
+                             /* UEGCCD_REPLAY                                                     */
 } UegccdResult;
 
 typedef struct UegccdCtx UegccdCtx;
@@ -98,7 +105,9 @@ typedef struct UegccdCtx UegccdCtx;
 void uegccd_default_options(UegccdOptions *opt);
 
 /* Builds the momentum-block plan of one system on the current CUDA device and
- * uploads it.  Replaces the per-call FindIndex lookups (HEG.f90:357-404) and the
+ * uploads it.  The context (like a batch) stays on that device: every later call on it
+ * runs there, from whichever host thread makes it, and leaves the thread's current device
+ * as it found it.  Replaces the per-call FindIndex lookups (HEG.f90:357-404) and the
  * scratch set-up SetUpCCScr (CCScr.f90:9-31). */
 int uegccd_ctx_create(const UegccdSystem *sys, UegccdCtx **out);
 int uegccd_ctx_destroy(UegccdCtx *ctx);
@@ -225,14 +234,15 @@ int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
  * allocate device memory when they call: a host whose device memory already belongs
  * to its own pool allocator, or one running other streams that must not be stalled
  * by the device-wide synchronisation a cudaFree brings.  All device storage is one
- * fixed array of about 1.1 MB inside the library, so the system must have at most
+ * fixed array of 1.05 MB inside the library, so the system must have at most
  * 2048 orbitals and plane-wave components |n_d| <= 31; larger systems return
- * UEGCCD_ERR_ARG.  stream is a cudaStream_t (NULL: the legacy default stream); the
- * call returns when e2 is written.  Every call on a device shares that array:
+ * UEGCCD_ERR_ARG.  stream is a cudaStream_t (NULL: the legacy default stream); every
+ * call synchronises stream and returns when e2 is written.  Every call on a device shares that array:
  * calls must not overlap on one device (from several streams or threads), or
  * their results are wrong.  The first call on a device looks up the array's
  * address (which may load the library's device code): make that first call before
- * any stream capture begins on the device. */
+ * any stream capture begins on the device.  The address is kept until the process
+ * exits: a cudaDeviceReset invalidates it, so do not use this entry point across one. */
 int uegccd_mp2_energy_static(const UegccdSystem *sys, void *stream, double *e2);
 
 /* T2abab of every solve of the batch in the reference layout, solve after solve: solve s
@@ -269,14 +279,21 @@ int32_t uegccd_batch_kernel_stats(UegccdBatch *b, int32_t max, const char **name
  * amplitudes: the admission measure of a serving loop.  Host-only, no device needed. */
 int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int64_t *bytes, int64_t *namp);
 
+/* Device memory.  The library takes its device memory in chunks and keeps the chunks of
+ * destroyed objects in a cache (uegccd_trim_cache).  uegccd_set_memory_limit caps the bytes
+ * it holds on each device -- live batches and contexts plus that cache -- at `bytes` (0: no
+ * cap, the default).  An allocation that would pass the cap first returns the device's cache
+ * to the driver; if it still does not fit, the call fails with UEGCCD_ERR_ALLOC and the
+ * batch keeps what it held before the call.  The reference has no such cap; its one
+ * allocation-failure path is SetUpDIISCC, which steps the DIIS depth down until Allocate
+ * succeeds and Stops when none does (DIISCC.f90:22-33): a DIIS solve here likewise takes
+ * fewer history vectors (UegccdResult.ndiis) when the cap or the device holds no more.
+ * uegccd_memory_info reports, for the current device, the bytes held and the cached part. */
+int uegccd_set_memory_limit(int64_t bytes);
+int uegccd_memory_info(int64_t *held, int64_t *cached);
+
 /* Host<->device bytes the batch has moved since its creation (its upload included). */
 int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h);
-
-/* The FP64 tensor-core peak of the current device, measured (TFLOP/s): a register-only
- * kernel of independent mma.sync.m8n8k4.f64 chains, eight 4-warp CTAs per SM, timed with
- * CUDA events after one untimed launch (a few ms).  The roofline denominator of the FP64
- * DMMA kernels. */
-int uegccd_probe_fp64_peak(double *tflops);
 
 const char *uegccd_last_error(void);
 /* Library version string. */

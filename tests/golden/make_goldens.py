@@ -1,7 +1,7 @@
 """Extract the reference's committed golden outputs into tests/golden/goldens.json.
 
-Run in a container that has the reference checkout (default path below, or
-``--ref DIR``); the GPU box and the test run only read the JSON.  Sources, all
+Run where the reference checkout exists (``--ref DIR``, required); the tests only
+read the JSON.  Sources, all
 relative to the reference checkout:
 
   G1  benchmarks/ZRun-dRPA/{Input,Output}       N=14, 57 plane waves, rs=1, dRPA+SOSEX
@@ -129,7 +129,7 @@ def g3(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference checkout (shepherd-group/uegccd)")
     ap.add_argument("--out", default=os.path.join(HERE, "goldens.json"))
     a = ap.parse_args()
     data = dict(G1=g1(a.ref), G5=g5(a.ref), G3=g3(a.ref))

@@ -130,12 +130,9 @@ def test_ring_cta_tuning_and_pinned_download(goldens):
 
 
 def test_fp64_peak_probe():
-    """The register-only FP64 MMA probe (the bench's FP64 roofline denominator) reports a
-    B200-sized figure: its datasheet FP64 tensor peak is about 37-40 TFLOP/s."""
-    import ctypes as C
+    """The register-only FP64 MMA probe (the bench's FP64 roofline denominator, bench_peak.cu)
+    reports a B200-sized figure: its datasheet FP64 tensor peak is about 37-40 TFLOP/s."""
+    import bench
 
-    from uegccd_b200 import _capi
-
-    v = C.c_double()
-    assert _capi.lib().uegccd_probe_fp64_peak(C.byref(v)) == 0
-    assert 20.0 < v.value < 60.0, v.value
+    v = bench.probe_fp64_peak()
+    assert v is not None and 20.0 < v < 60.0, v

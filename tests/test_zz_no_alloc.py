@@ -84,3 +84,25 @@ def test_static_mp2_refuses_oversize():
     rc, _ = _static_e2((7, 10.0, 1.0, np.linspace(-1, 1, 20), nvec))
     assert rc == ERR_ARG
     assert "31" in _capi.lib().uegccd_last_error().decode()
+
+
+def test_static_mp2_leaves_device_memory_unchanged(goldens):
+    """The entry point's contract is that it allocates nothing: after one warm-up call, the
+    device's free memory (cudaMemGetInfo) stays the same over several more calls, and the
+    library's own device-memory count does not move either."""
+    from uegccd_b200 import _capi
+
+    rt = C.CDLL("libcudart.so.12")
+    free_b, total_b = C.c_size_t(), C.c_size_t()
+    held = C.c_int64()
+    sys_t = _systems(goldens)[2]
+    assert _static_e2(sys_t)[0] == 0   # warm-up: the module and the array are loaded
+    assert rt.cudaMemGetInfo(C.byref(free_b), C.byref(total_b)) == 0
+    _capi.lib().uegccd_memory_info(C.byref(held), None)
+    free0, held0 = free_b.value, held.value
+    for _ in range(4):
+        assert _static_e2(sys_t)[0] == 0
+    assert rt.cudaMemGetInfo(C.byref(free_b), C.byref(total_b)) == 0
+    _capi.lib().uegccd_memory_info(C.byref(held), None)
+    assert free_b.value == free0
+    assert held.value == held0

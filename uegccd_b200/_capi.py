@@ -49,7 +49,7 @@ class Result(C.Structure):
     _fields_ = [
         ("ecorr", C.c_double), ("ecorr_sosex", C.c_double), ("max_res", C.c_double), ("last_dt", C.c_double),
         ("niter", C.c_int32), ("fail", C.c_int32), ("n_recorded", C.c_int32), ("kernel_launches", C.c_int32),
-        ("gpu_ms", C.c_double),
+        ("gpu_ms", C.c_double), ("status", C.c_int32), ("ndiis", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -94,7 +94,6 @@ def lib() -> C.CDLL:
         L.uegccd_batch_get_amplitudes.argtypes = [vp, C.c_int32, dp]
         L.uegccd_batch_get_all_amplitudes.argtypes = [vp, dp]
         L.uegccd_batch_mp2.argtypes = [vp, dp]
-        L.uegccd_probe_fp64_peak.argtypes = [dp]
         L.uegccd_diis_create.argtypes = [C.c_int64, C.c_int32, C.c_int32, dp, P(vp)]
         L.uegccd_diis_push.argtypes = [vp, dp, dp]
         L.uegccd_diis_get_t.argtypes = [vp, C.c_int32, dp]
@@ -113,6 +112,8 @@ def lib() -> C.CDLL:
         L.uegccd_batch_kernel_stats.argtypes = [vp, C.c_int32, P(C.c_char_p), dp, P(C.c_int64)]
         L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
         L.uegccd_footprint.argtypes = [P(System), C.c_int32, C.c_int32, P(C.c_int64), P(C.c_int64)]
+        L.uegccd_set_memory_limit.argtypes = [C.c_int64]
+        L.uegccd_memory_info.argtypes = [P(C.c_int64), P(C.c_int64)]
         L.uegccd_last_error.restype = C.c_char_p
         L.uegccd_version.restype = C.c_char_p
         _lib = L
@@ -157,3 +158,34 @@ def footprint(system_tuple, ndiis: int = 6, mixed: bool = False):
     b, a = C.c_int64(), C.c_int64()
     check(lib().uegccd_footprint(C.byref(s), ndiis, 1 if mixed else 0, C.byref(b), C.byref(a)))
     return b.value, a.value
+
+
+def set_memory_limit(nbytes: int) -> None:
+    """Caps the device memory the library holds per device (0: no cap)."""
+    check(lib().uegccd_set_memory_limit(int(nbytes)))
+
+
+def memory_info():
+    """(bytes held, of which cached) on the calling thread's current device."""
+    h, c = C.c_int64(), C.c_int64()
+    check(lib().uegccd_memory_info(C.byref(h), C.byref(c)))
+    return h.value, c.value
+
+
+def trim_cache() -> None:
+    check(lib().uegccd_trim_cache())
+
+
+_cudart = None
+
+
+def set_device(device: int) -> None:
+    """Makes `device` the calling thread's current CUDA device (the device a batch or
+    context created next on this thread lives on)."""
+    global _cudart
+    lib()   # the library loads the CUDA runtime it uses
+    if _cudart is None:
+        _cudart = C.CDLL("libcudart.so.12")
+    rc = _cudart.cudaSetDevice(C.c_int(int(device)))
+    if rc != 0:
+        raise UegccdError(-2, f"cudaSetDevice({device}) failed ({rc})")

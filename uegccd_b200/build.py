@@ -20,7 +20,10 @@ ZCODE = os.path.join(PKG, "uegccd_zcode")
 OBJDIR = os.path.join(PKG, "_build")
 
 SOURCES = ["capi.cu", "kernels_fp64.cu", "kernels_tc.cu", "plan.cpp", "heg_host.cpp", "zcode.cpp", "mp2_static.cu",
-           "diis_api.cu", "probe.cu"]
+           "diis_api.cu"]
+# bench.py's FP64 tensor-core peak measurement: a library of its own beside bench.py
+BENCH_PEAK_SRC = os.path.join(ROOT, "bench_peak.cu")
+BENCH_PEAK_LIB = os.path.join(ROOT, "bench_peak.so")
 HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h", "listdir.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -59,6 +62,11 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
         subprocess.run(cmd, check=True)
     if _stale(LIB, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if os.path.exists(BENCH_PEAK_SRC) and _stale(BENCH_PEAK_LIB, [BENCH_PEAK_SRC]):
+        cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-shared", BENCH_PEAK_SRC, "-o", BENCH_PEAK_LIB, "-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -97,17 +97,50 @@ struct DevChunk {
     size_t size;
     int dev;
 };
-// pinned staging buffer of the batch-wide amplitude download (grown on demand, kept)
+// pinned staging buffer of the batch-wide amplitude download (grown on demand, kept; portable:
+// page-locked for every device's context)
 constexpr size_t kStageMin = 8ull << 20;
 std::mutex g_stage_mu;
 char *g_stage = nullptr;
 size_t g_stage_bytes = 0;
+// g_pool_mu guards the cache, the per-device byte counts and the limit
 std::mutex g_pool_mu;
 std::vector<DevChunk> g_pool;
 size_t g_pool_bytes = 0;
+int64_t g_dev_bytes[kMaxDevices] = {};   // bytes the library holds from cudaMalloc per device (live + cached)
+int64_t g_mem_limit = 0;                 // uegccd_set_memory_limit; 0: none
 
+// Returns the cache of device dev to the driver (the caller holds no lock; dev is current).
+void drop_cached(int dev)
+{
+    std::vector<DevChunk> drop;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        for (size_t k = 0; k < g_pool.size();)
+            if (g_pool[k].dev == dev) {
+                drop.push_back(g_pool[k]);
+                g_pool_bytes -= g_pool[k].size;
+                g_dev_bytes[dev % kMaxDevices] -= (int64_t)g_pool[k].size;
+                g_pool.erase(g_pool.begin() + k);
+            } else {
+                k++;
+            }
+    }
+    for (auto &c : drop) cudaFree(c.p);
+}
+
+// True when `need` more bytes on dev stay within the limit (under g_pool_mu).
+bool within_limit(int dev, size_t need)
+{
+    return g_mem_limit <= 0 || g_dev_bytes[dev % kMaxDevices] + (int64_t)need <= g_mem_limit;
+}
+
+// A chunk of at least `need` bytes on device dev (current): from the cache, else cudaMalloc.
+// Past the memory limit, or when cudaMalloc fails, the device's cache goes back to the driver
+// and the request is tried once more; then cudaErrorMemoryAllocation.
 cudaError_t chunk_get(size_t need, int dev, DevChunk &out)
 {
+    bool fits = true;
     {
         std::lock_guard<std::mutex> lock(g_pool_mu);
         int best = -1;
@@ -121,31 +154,39 @@ cudaError_t chunk_get(size_t need, int dev, DevChunk &out)
             g_pool.erase(g_pool.begin() + best);
             return cudaSuccess;
         }
+        fits = within_limit(dev, need);
+    }
+    if (!fits) {
+        drop_cached(dev);
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (!within_limit(dev, need)) return cudaErrorMemoryAllocation;
     }
     void *p = nullptr;
     cudaError_t e = cudaMalloc(&p, need);
     if (e != cudaSuccess) {
-        // give the cache of this device back to the driver and try once more
         cudaGetLastError();
-        std::vector<DevChunk> drop;
-        {
-            std::lock_guard<std::mutex> lock(g_pool_mu);
-            for (size_t k = 0; k < g_pool.size();)
-                if (g_pool[k].dev == dev) {
-                    drop.push_back(g_pool[k]);
-                    g_pool_bytes -= g_pool[k].size;
-                    g_pool.erase(g_pool.begin() + k);
-                } else {
-                    k++;
-                }
-        }
-        for (auto &c : drop) cudaFree(c.p);
+        drop_cached(dev);
         e = cudaMalloc(&p, need);
     }
-    if (e == cudaSuccess) out = DevChunk{(char *)p, need, dev};
+    if (e == cudaSuccess) {
+        out = DevChunk{(char *)p, need, dev};
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        g_dev_bytes[dev % kMaxDevices] += (int64_t)need;
+    }
     return e;
 }
 
+// Straight back to the driver; c.dev is current.
+void chunk_free(const DevChunk &c)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        g_dev_bytes[c.dev % kMaxDevices] -= (int64_t)c.size;
+    }
+    cudaFree(c.p);
+}
+
+// Back to the cache, or (past its cap) to the driver; c.dev is current.
 void chunk_put(const DevChunk &c)
 {
     {
@@ -155,19 +196,23 @@ void chunk_put(const DevChunk &c)
             g_pool_bytes += c.size;
             return;
         }
+        g_dev_bytes[c.dev % kMaxDevices] -= (int64_t)c.size;
     }
     cudaFree(c.p);
 }
 }  // namespace
 
 struct UegccdBatch {
+    int dev = -1;                    // the CUDA device the batch lives on (current at creation)
+    bool broken = false;             // restoring the plain integral tables failed: calls are refused
     std::vector<SystemHost> sys;
     std::vector<SolvePlan> plans;
     std::vector<SolveDev> hsolves;
     std::vector<int> chunk_begin;
     DevBatch d;
-    std::vector<DevChunk> chunks;    // device memory of the batch (see chunk_get)
-    size_t chunk_used = 0;           // bytes used in the last chunk
+    std::vector<DevChunk> chunks;    // device memory of the batch (see chunk_get): arena chunks
+    size_t chunk_used = 0;           // bytes used in the last arena chunk
+    std::vector<DevChunk> big;       // chunks of one large array each
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_solve0 = nullptr, ev_solve1 = nullptr;
     std::vector<double> red;         // host copy: 3 per solve
@@ -221,6 +266,7 @@ struct UegccdBatch {
             for (auto &e : kt.ev) cudaEventDestroy(e);
         if (stream) cudaStreamSynchronize(stream);
         for (auto &c : chunks) chunk_put(c);
+        for (auto &c : big) chunk_put(c);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev_solve0) cudaEventDestroy(ev_solve0);
@@ -234,18 +280,49 @@ struct UegccdBatch {
         p = nullptr;
         if (n == 0) n = 1;
         const size_t bytes = (n * sizeof(T) + 255) & ~(size_t)255;
-        if (chunks.empty() || chunk_used + bytes > chunks.back().size) {
-            int dev = 0;
-            cudaGetDevice(&dev);
+        if (bytes >= kArenaChunk / 2) {
+            // large arrays get a chunk of their own, of exactly the size they need
             DevChunk c;
-            cudaError_t e = chunk_get(std::max(bytes, kArenaChunk), dev, c);
-            if (e != cudaSuccess) return fail(UEGCCD_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            cudaError_t e = chunk_get(bytes, dev, c);
+            if (e != cudaSuccess)
+                return fail(UEGCCD_ERR_ALLOC, std::string("device allocation of ") + std::to_string(bytes) +
+                                                  " bytes: " + cudaGetErrorString(e));
+            big.push_back(c);
+            p = reinterpret_cast<T *>(c.p);
+            return 0;
+        }
+        if (chunks.empty() || chunk_used + bytes > chunks.back().size) {
+            DevChunk c;
+            cudaError_t e = chunk_get(kArenaChunk, dev, c);
+            if (e != cudaSuccess)
+                return fail(UEGCCD_ERR_ALLOC, std::string("device allocation of ") + std::to_string(kArenaChunk) +
+                                                  " bytes: " + cudaGetErrorString(e));
             chunks.push_back(c);
             chunk_used = 0;
         }
         p = reinterpret_cast<T *>(chunks.back().p + chunk_used);
         chunk_used += bytes;
         return 0;
+    }
+    // Allocation marks: rollback(mark()) returns every chunk taken since the mark to the driver
+    // (not to the cache: a failed group of allocations means memory is short) and the arena
+    // space carved since -- the batch is left as it was (arena chunks are only ever appended,
+    // so the mark's last one is the last one again).
+    struct Mark {
+        size_t nchunks, nbig, used;
+    };
+    Mark mark() const { return Mark{chunks.size(), big.size(), chunk_used}; }
+    void rollback(const Mark &m)
+    {
+        while (big.size() > m.nbig) {
+            chunk_free(big.back());
+            big.pop_back();
+        }
+        while (chunks.size() > m.nchunks) {
+            chunk_free(chunks.back());
+            chunks.pop_back();
+        }
+        chunk_used = m.used;
     }
     template <class T>
     int upload(T *&p, const std::vector<T> &h)
@@ -315,6 +392,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if (rc) return rc;
     if (n <= 0) return fail(UEGCCD_ERR_ARG, "empty batch");
     auto b = std::make_unique<UegccdBatch>();
+    CU(cudaGetDevice(&b->dev));   // the batch lives on the device current now
     b->sys.resize(n);
     b->plans.resize(n);
     for (int s = 0; s < n; s++) {
@@ -840,28 +918,46 @@ int validate_options(const UegccdOptions *o, int drpa, const UegccdBatch &b)
     return 0;
 }
 
+// Buffers of the device-side iteration control, grown on demand.  Each group of arrays is
+// allocated as a whole: when one of them fails, the group's memory goes back and the batch
+// keeps what it had.
 int ctl_alloc(UegccdBatch &b, int ndiis, int max_rec)
 {
     CtlBuffers &c = b.ctl;
     const int n = b.d.nsolves;
-    int rc;
+    int rc = 0;
     if (!c.state) {
-        if ((rc = b.alloc(c.state, n))) return rc;
-        if ((rc = b.alloc(c.active_next, n))) return rc;
-        if ((rc = b.alloc(c.count, 1))) return rc;
-        if ((rc = b.alloc(c.Bm, (size_t)n * kDiisMax * kDiisMax))) return rc;
-        if ((rc = b.alloc(c.coef, (size_t)n * kDiisMax))) return rc;
-        if ((rc = b.alloc(c.brow, (size_t)n * kDiisMax))) return rc;
-        if ((rc = b.alloc(c.part, (size_t)b.d.nchunks * kDiisMax))) return rc;
+        const UegccdBatch::Mark m = b.mark();
+        CtlBuffers x = c;
+        if ((rc = b.alloc(x.state, n)) || (rc = b.alloc(x.active_next, n)) || (rc = b.alloc(x.count, 1)) ||
+            (rc = b.alloc(x.Bm, (size_t)n * kDiisMax * kDiisMax)) || (rc = b.alloc(x.coef, (size_t)n * kDiisMax)) ||
+            (rc = b.alloc(x.brow, (size_t)n * kDiisMax)) || (rc = b.alloc(x.part, (size_t)b.d.nchunks * kDiisMax))) {
+            b.rollback(m);
+            return rc;
+        }
+        c = x;
     }
     if (max_rec > c.max_rec) {
-        if ((rc = b.alloc(c.rec_e, (size_t)n * max_rec))) return rc;
-        if ((rc = b.alloc(c.rec_dt, (size_t)n * max_rec))) return rc;
+        const UegccdBatch::Mark m = b.mark();
+        double *re = nullptr, *rd = nullptr;
+        if ((rc = b.alloc(re, (size_t)n * max_rec)) || (rc = b.alloc(rd, (size_t)n * max_rec))) {
+            b.rollback(m);
+            return rc;
+        }
+        c.rec_e = re;
+        c.rec_dt = rd;
         c.max_rec = max_rec;
     }
     if (ndiis > b.diis_cap) {
-        if ((rc = b.alloc(c.hist_t, (size_t)ndiis * b.d.namp))) return rc;
-        if ((rc = b.alloc(c.hist_e, (size_t)ndiis * b.d.namp))) return rc;
+        const UegccdBatch::Mark m = b.mark();
+        double *ht = nullptr;
+        float *he = nullptr;
+        if ((rc = b.alloc(ht, (size_t)ndiis * b.d.namp)) || (rc = b.alloc(he, (size_t)ndiis * b.d.namp))) {
+            b.rollback(m);
+            return rc;
+        }
+        c.hist_t = ht;
+        c.hist_e = he;
         b.diis_cap = ndiis;
     }
     return 0;
@@ -937,7 +1033,6 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     f.do_ladder = (!drpa && opt->do_ladder) ? 1 : 0;
     f.do_ring = opt->do_ring ? 1 : 0;
     f.do_xring = (!drpa && opt->do_xring) ? 1 : 0;
-    const int ndiis = opt->scheme == UEGCCD_DIIS ? opt->ndiis : 0;
     // range-separated integrals: every CCD term and the energy on the flag's tables (the MP2
     // start before this used the plain ones); the plain tables back on every exit
     struct TableGuard {
@@ -945,7 +1040,9 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
         bool on;
         ~TableGuard()
         {
-            if (on) load_tables(b, 0);
+            // a batch left on the range-separated tables would give wrong MP2 and CCD results
+            // later: refuse every further call on it instead
+            if (on && load_tables(b, 0) != 0) b.broken = true;
         }
     } table_guard{b, false};
     if (opt->range_flags != 0 && b.range_flag != 0) {
@@ -954,7 +1051,12 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
         table_guard.on = true;
     }
     const int max_rec = std::min(opt->max_iter, 1100);
-    int rc = ctl_alloc(b, ndiis, max_rec);
+    // The DIIS history takes fewer vectors when the device memory (or the library's limit)
+    // does not hold ndiis of them, down to 2, as SetUpDIISCC steps Max_N_DIIS down until its
+    // Allocate succeeds (DIISCC.f90:22-29); the vectors used are reported per solve.
+    int ndiis = opt->scheme == UEGCCD_DIIS ? opt->ndiis : 0;
+    int rc = 0;
+    while ((rc = ctl_alloc(b, ndiis, max_rec)) == UEGCCD_ERR_ALLOC && ndiis > 2) ndiis--;
     if (rc) return rc;
     for (int s = 0; s < n; s++) b.hsolves[s].denom_factor = opt->denom_factor;
     CU(cudaMemcpyAsync(d.solves, b.hsolves.data(), n * sizeof(SolveDev), cudaMemcpyHostToDevice, b.stream));
@@ -1068,8 +1170,11 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
         r.n_recorded = (s == 0) ? nrec : 0;
         r.kernel_launches = b.launches;
         r.gpu_ms = ms;
-        if (st[s].status == 3) status = UEGCCD_ERR_NUMERIC;
-        if (status == 0 && (r.fail || st[s].status == 2)) status = UEGCCD_NOT_CONVERGED;
+        r.status = st[s].status == 3 ? UEGCCD_ERR_NUMERIC
+                   : (r.fail || st[s].status == 2) ? UEGCCD_NOT_CONVERGED : UEGCCD_OK;
+        r.ndiis = ndiis;
+        if (r.status == UEGCCD_ERR_NUMERIC) status = UEGCCD_ERR_NUMERIC;
+        if (status == 0 && r.status == UEGCCD_NOT_CONVERGED) status = UEGCCD_NOT_CONVERGED;
     }
     if (status == UEGCCD_ERR_NUMERIC) fail(status, "non-finite amplitudes or energy");
     return status;
@@ -1156,6 +1261,16 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
     return UEGCCD_OK;
 }
 
+// Every call on a batch or context runs on the device the object was created on (whatever
+// device the calling thread has current), and is refused once the batch is unusable.
+#define ENTER_DEVICE(bp)                                                                               \
+    DeviceScope dev_scope_((bp)->dev);                                                                 \
+    if (dev_scope_.rc != cudaSuccess)                                                                  \
+        return fail(UEGCCD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(dev_scope_.rc))
+#define ENTER(bp)                                                                                      \
+    ENTER_DEVICE(bp);                                                                                  \
+    if ((bp)->broken) return fail(UEGCCD_ERR_CUDA, "batch unusable: restoring its plain integral tables failed")
+
 extern "C" {
 
 const char *uegccd_last_error(void) { return g_last_error.c_str(); }
@@ -1191,6 +1306,8 @@ int uegccd_ctx_create(const UegccdSystem *sys, UegccdCtx **out)
 
 int uegccd_ctx_destroy(UegccdCtx *c)
 {
+    if (!c) return 0;
+    ENTER_DEVICE(c->batch);
     delete c;
     return 0;
 }
@@ -1198,6 +1315,7 @@ int uegccd_ctx_destroy(UegccdCtx *c)
 int uegccd_ctx_set_eigen(UegccdCtx *c, const double *eigen)
 {
     if (!c || !eigen) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(c->batch);
     UegccdBatch &b = *c->batch;
     b.sys[0].eigen.assign(eigen, eigen + b.sys[0].M);
     CU(cudaMemcpyAsync(b.d.eigen, eigen, b.sys[0].M * sizeof(double), cudaMemcpyHostToDevice, b.stream));
@@ -1229,18 +1347,21 @@ int uegccd_batch_set_range(UegccdBatch *b, int32_t flag, double screening)
 int uegccd_ctx_set_integrals(UegccdCtx *c, int32_t core_n, double gapii)
 {
     if (!c) return fail(UEGCCD_ERR_ARG, "null context");
+    ENTER(c->batch);
     return set_integrals(*c->batch, core_n, gapii);
 }
 
 int uegccd_batch_set_integrals(UegccdBatch *b, int32_t core_n, double gapii)
 {
     if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    ENTER(b);
     return set_integrals(*b, core_n, gapii);
 }
 
 int uegccd_mp2(UegccdCtx *c, double *t_aaaa, double *t_abab, double *t_abba, double *e2)
 {
     if (!c) return fail(UEGCCD_ERR_ARG, "null context");
+    ENTER(c->batch);
     UegccdBatch &b = *c->batch;
     launch_mp2(b.d, b.stream);
     launch_reduce(b.d, b.stream);
@@ -1259,6 +1380,7 @@ int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t
                UegccdResult *res)
 {
     if (!c || !t_abab || !res) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(c->batch);
     UegccdBatch &b = *c->batch;
     int rc = validate_options(opt, 0, b);
     if (rc) return rc;
@@ -1273,6 +1395,7 @@ int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t
 int uegccd_drpa(UegccdCtx *c, const UegccdOptions *opt, double *t2, UegccdResult *res)
 {
     if (!c || !t2 || !res) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(c->batch);
     UegccdBatch &b = *c->batch;
     int rc = validate_options(opt, 1, b);
     if (rc) return rc;
@@ -1288,6 +1411,7 @@ int uegccd_ccd_g2_ex(UegccdCtx *c, const double *t_abab, int32_t mask, int32_t p
 {
     if (!c || !t_abab || !g_abab) return fail(UEGCCD_ERR_ARG, "null argument");
     if (precision != UEGCCD_FP64 && precision != UEGCCD_MIXED) return fail(UEGCCD_ERR_ARG, "unknown precision");
+    ENTER(c->batch);
     UegccdBatch &b = *c->batch;
     int rc = pack_from_host(b, 0, t_abab);
     if (rc) return rc;
@@ -1330,6 +1454,7 @@ int32_t uegccd_sf_length(const UegccdSystem *sys)
 int uegccd_structure_factor(UegccdCtx *c, const double *t_abab, const UegccdSfGrid *out)
 {
     if (!c || !t_abab || !out) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(c->batch);
     UegccdBatch &b = *c->batch;
     int rc = pack_from_host(b, 0, t_abab);
     if (rc) return rc;
@@ -1354,6 +1479,8 @@ int uegccd_batch_create(const UegccdSystem *systems, int32_t n, UegccdBatch **ou
 
 int uegccd_batch_destroy(UegccdBatch *b)
 {
+    if (!b) return 0;
+    ENTER_DEVICE(b);
     delete b;
     return 0;
 }
@@ -1361,6 +1488,7 @@ int uegccd_batch_destroy(UegccdBatch *b)
 int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2, UegccdResult *results)
 {
     if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(b);
     int rc = validate_options(opt, drpa, *b);
     if (rc) return rc;
     if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
@@ -1398,6 +1526,7 @@ int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max)
 int uegccd_batch_set_profiling(UegccdBatch *b, int32_t on)
 {
     if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    ENTER(b);
     if (on && !b->kt_events) {
         for (auto &e : b->kt.ev) CU(cudaEventCreate(&e));
         b->kt_events = true;
@@ -1470,12 +1599,14 @@ int uegccd_batch_transfer_bytes(UegccdBatch *b, int64_t *h2d, int64_t *d2h)
 int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab)
 {
     if (!b || !t_abab || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
+    ENTER(b);
     return unpack_to_host(*b, s, b->d.t, t_abab, nullptr, nullptr);
 }
 
 int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab)
 {
     if (!b || !t_abab) return fail(UEGCCD_ERR_ARG, "bad argument");
+    ENTER(b);
     const int n = b->d.nsolves;
     if (!b->dense_all) {
         std::vector<int64_t> off(n + 1, 0);
@@ -1507,7 +1638,7 @@ int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab)
         if (g_stage) cudaFreeHost(g_stage);
         g_stage = nullptr;
         g_stage_bytes = 0;
-        CU(cudaHostAlloc((void **)&g_stage, bytes, cudaHostAllocDefault));
+        CU(cudaHostAlloc((void **)&g_stage, bytes, cudaHostAllocPortable));
         g_stage_bytes = bytes;
     }
     CU(cudaMemcpyAsync(g_stage, b->dense_all, bytes, cudaMemcpyDeviceToHost, b->stream));
@@ -1524,6 +1655,7 @@ int uegccd_batch_get_all_amplitudes(UegccdBatch *b, double *t_abab)
 int uegccd_batch_mp2(UegccdBatch *b, double *e2)
 {
     if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    ENTER(b);
     b->kt.begin(KID_MP2, b->stream);
     launch_mp2(b->d, b->stream);
     b->kt.end(b->stream);
@@ -1542,6 +1674,7 @@ int uegccd_batch_mp2(UegccdBatch *b, double *e2)
 int uegccd_batch_structure_factor(UegccdBatch *b, int32_t s, const UegccdSfGrid *out)
 {
     if (!b || !out || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
+    ENTER(b);
     return structure_factor(*b, s, *out);
 }
 
@@ -1559,7 +1692,34 @@ int uegccd_trim_cache(void)
         drop.swap(g_pool);
         g_pool_bytes = 0;
     }
-    for (auto &c : drop) cudaFree(c.p);
+    for (auto &c : drop) {
+        DeviceScope on(c.dev);
+        cudaFree(c.p);
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        for (auto &c : drop) g_dev_bytes[c.dev % kMaxDevices] -= (int64_t)c.size;
+    }
+    return UEGCCD_OK;
+}
+
+int uegccd_set_memory_limit(int64_t bytes)
+{
+    if (bytes < 0) return fail(UEGCCD_ERR_ARG, "memory limit must be >= 0");
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    g_mem_limit = bytes;
+    return UEGCCD_OK;
+}
+
+int uegccd_memory_info(int64_t *held, int64_t *cached)
+{
+    const int dev = current_device() % kMaxDevices;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    int64_t c = 0;
+    for (const auto &x : g_pool)
+        if (x.dev == dev) c += (int64_t)x.size;
+    if (held) *held = g_dev_bytes[dev];
+    if (cached) *cached = c;
     return UEGCCD_OK;
 }
 
@@ -1568,6 +1728,7 @@ int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dt
 {
     if (!b || s < 0 || s >= b->d.nsolves || max_rec < 0 || !n_recorded)
         return fail(UEGCCD_ERR_ARG, "bad argument");
+    ENTER(b);
     if (b->last_niter.size() != (size_t)b->d.nsolves || !b->ctl.rec_e)
         return fail(UEGCCD_ERR_ARG, "no solve has run on this batch");
     const int n = std::min(b->last_niter[s], max_rec);

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/uegccd.h"
+#include "kernels.h"
 
 namespace uegccd {
 int set_last_error(int code, const char *msg);
@@ -150,6 +151,7 @@ struct UegccdDiis {
     int *slots = nullptr;
     std::vector<double> B;                      // kDiisCap x kDiisCap, by slot
     cudaStream_t stream = nullptr;
+    int dev = -1;                               // the device the history lives on
     ~UegccdDiis()
     {
         if (stream) cudaStreamSynchronize(stream);
@@ -169,6 +171,7 @@ int uegccd_diis_create(int64_t n, int32_t ndiis, int32_t scheme, const double *t
     if (scheme != UEGCCD_REPLAY && scheme != UEGCCD_DIIS) return fail(UEGCCD_ERR_ARG, "unknown scheme");
     if (int rc = uegccd::device_ok()) return rc;
     auto *d = new UegccdDiis;
+    cudaGetDevice(&d->dev);   // the history stays on the device current now
     d->n = n;
     d->ndiis = ndiis;
     d->scheme = scheme;
@@ -202,6 +205,8 @@ int uegccd_diis_create(int64_t n, int32_t ndiis, int32_t scheme, const double *t
 int uegccd_diis_push(UegccdDiis *d, const double *t, const double *r)
 {
     if (!d || !t || !r) return fail(UEGCCD_ERR_ARG, "null argument");
+    uegccd::DeviceScope on_dev(d->dev);
+    if (on_dev.rc != cudaSuccess) return fail(UEGCCD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(on_dev.rc));
     // the start amplitudes (no residual) hold slot 0 until the first push replaces them
     const int slot = d->count == 0 ? 0 : (d->newest + 1) % d->ndiis;
     const size_t bytes = d->n * sizeof(double);
@@ -228,6 +233,8 @@ int uegccd_diis_push(UegccdDiis *d, const double *t, const double *r)
 int uegccd_diis_get_t(UegccdDiis *d, int32_t niter, double *t2)
 {
     if (!d || !t2) return fail(UEGCCD_ERR_ARG, "null argument");
+    uegccd::DeviceScope on_dev(d->dev);
+    if (on_dev.rc != cudaSuccess) return fail(UEGCCD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(on_dev.rc));
     if (d->newest < 0) return fail(UEGCCD_ERR_ARG, "no amplitudes: pass t0 or push a pair first");
     const size_t bytes = d->n * sizeof(double);
     std::vector<double> c;
@@ -258,6 +265,8 @@ int uegccd_diis_get_t(UegccdDiis *d, int32_t niter, double *t2)
 
 int uegccd_diis_destroy(UegccdDiis *d)
 {
+    if (!d) return UEGCCD_OK;
+    uegccd::DeviceScope on_dev(d->dev);
     delete d;
     return UEGCCD_OK;
 }

@@ -206,4 +206,36 @@ int launch_iteration(const DevBatch &d, const CtlBuffers &c, const TermFlags &f,
 void launch_unpack(const DevBatch &d, int s, int namp, const double *t, double *ab, double *ba, double *aa,
                    cudaStream_t st);
 
+// Makes `dev` the calling thread's current CUDA device for the scope's lifetime and puts the
+// previous one back at its end.  Every object of the library (batch, context, DIIS history)
+// records the device it was created on, and every call on it runs under one of these, so a
+// host thread whose current device differs (a fresh thread starts on device 0) still works on
+// the object's own device.  rc is the cudaSetDevice status.
+struct DeviceScope {
+    int prev = -1, dev = -1;
+    cudaError_t rc = cudaSuccess;
+    explicit DeviceScope(int d) : dev(d)
+    {
+        if (d < 0) return;
+        rc = cudaGetDevice(&prev);
+        if (rc == cudaSuccess && prev != d) rc = cudaSetDevice(d);
+        else if (rc == cudaSuccess) prev = -1;   // already current: nothing to restore
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope &) = delete;
+    DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
+// The current device's index, or 0 when the query fails (for per-device caches).
+inline int current_device()
+{
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) d = 0;
+    return d;
+}
+constexpr int kMaxDevices = 64;
+
 }  // namespace uegccd

@@ -444,13 +444,17 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
 }
 
 // The dynamic shared-memory limits only grow (batches of different sizes coexist), under
-// one lock: batches are created from several host threads while others solve.
+// one lock: batches are created from several host threads while others solve.  Kernel
+// attributes belong to a device, so each device keeps its own limits (the caller has made
+// the batch's device current).
 static std::mutex g_smem_limit_mu;
 
 void set_ladder_smem_limit(int max_v)
 {
     std::lock_guard<std::mutex> lock(g_smem_limit_mu);
-    static int current = 0;
+    static int current_by_dev[kMaxDevices] = {};   // attributes are per device
+    const int dev = current_device() % kMaxDevices;
+    int &current = current_by_dev[dev];
     if (max_v > current) {
         const int b8 = (int)ladder_smem_bytes(max_v, 8);
         cudaFuncSetAttribute(k_ladder3<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
@@ -618,7 +622,9 @@ __global__ void __launch_bounds__(256) k_mosaic_sum(const int2 *__restrict__ tar
 void set_mosaic_smem_limit(size_t bytes)
 {
     std::lock_guard<std::mutex> lock(g_smem_limit_mu);
-    static size_t current = 48 * 1024;
+    static size_t current_by_dev[kMaxDevices] = {};   // attributes are per device
+    size_t &current = current_by_dev[current_device() % kMaxDevices];
+    if (current < 48 * 1024) current = 48 * 1024;
     if (bytes > current) {
         cudaFuncSetAttribute(k_mosaic_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         current = bytes;
@@ -1118,7 +1124,8 @@ void set_rings_smem_limit(int wide, size_t bytes)
 {
     // keep the largest limit ever requested per kernel: batches of different sizes coexist
     std::lock_guard<std::mutex> lock(g_smem_limit_mu);
-    static size_t current[2] = {0, 0};
+    static size_t current_by_dev[kMaxDevices][2] = {};   // attributes are per device
+    size_t *current = current_by_dev[current_device() % kMaxDevices];
     if (bytes > current[wide ? 1 : 0]) {
         if (wide) cudaFuncSetAttribute(k_rings_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         else cudaFuncSetAttribute(k_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

@@ -22,8 +22,13 @@
 // own partial sum and the reduction overwrites the result.
 //
 // Set-up: the first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (which may load the module into the context).  Make
-// that first call before any stream capture begins on the device.
+// cudaGetSymbolAddress (which may load the module into the context) and keeps it
+// for the life of the process.  Make that first call before any stream capture
+// begins on the device.  A cudaDeviceReset unloads the module, so the kept address
+// is no longer valid afterwards: do not use this entry point across a reset.
+//
+// Every call copies E(2) back into host memory and synchronises `stream` before
+// it returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -52,7 +57,7 @@ constexpr size_t kOffNvec = kOffEigen + sizeof(double) * kStaticMaxOrb;
 constexpr size_t kOffLattice = kOffNvec + ((sizeof(int32_t) * 3 * kStaticMaxOrb + 255) / 256) * 256;
 constexpr size_t kOffPartial = kOffLattice + ((sizeof(int32_t) * (size_t)kStaticLattice + 255) / 256) * 256;
 constexpr size_t kOffResult = kOffPartial + sizeof(double) * kStaticMaxBlocks;
-constexpr size_t kStaticScratchBytes = kOffResult + 256;  // about 1.1 MB
+constexpr size_t kStaticScratchBytes = kOffResult + 256;  // 1,050,880 bytes (1.05 MB)
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 

@@ -112,8 +112,12 @@ class Context:
 class Batch:
     """uegccd_batch_*: many independent systems solved together."""
 
-    def __init__(self, systems):
-        """systems: iterable of (nocc, L, madelung, eigen, nvec)."""
+    def __init__(self, systems, device: int | None = None):
+        """systems: iterable of (nocc, L, madelung, eigen, nvec).  device: the CUDA device to
+        create the batch on (made current on this thread first); None: the current one.  Every
+        later call on the batch runs on its device, from any thread."""
+        if device is not None:
+            capi.set_device(device)
         self._systems = [capi.make_system(*s) for s in systems]
         arr = (capi.System * len(self._systems))(*self._systems)
         self._arr = arr
@@ -134,13 +138,18 @@ class Batch:
         except Exception:
             pass
 
-    def solve(self, drpa: bool = False, **opts):
+    def solve(self, drpa: bool = False, raise_on_error: bool = True, **opts):
+        """MP2 start + CCD (dRPA) of every system: (status, E(2) per system, result dicts).
+        raise_on_error=False returns a negative status too, with each solve's own status in
+        its result (e.g. UEGCCD_ERR_NUMERIC for the solves that met a NaN)."""
         o = capi.default_options(**opts)
         if drpa and "fail_ratio" not in opts:
             o.fail_ratio = 1.0e4
         e2 = np.zeros(self.n)
         res = (capi.Result * self.n)()
-        rc = capi.check(capi.lib().uegccd_batch_solve(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2), res))
+        rc = capi.lib().uegccd_batch_solve(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2), res)
+        if raise_on_error:
+            capi.check(rc)
         return rc, e2, [r.as_dict() for r in res]
 
     def set_integrals(self, core_n: int = 0, gapii: float = 0.0) -> None:
