@@ -551,6 +551,10 @@ def main(argv=None):
     ap.add_argument("--serve-requests", type=int, default=150,
                     help="requests of the serving stream reported under 'serve' (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=150.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-requests-saturated", type=int, default=600,
+                    help="requests of the saturating serving stream (reported under serve.saturated)")
+    ap.add_argument("--serve-rate-saturated", type=float, default=4000.0,
+                    help="its arrival rate, requests/s: well above what the GPU serves")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end pipeline (for profiling the timed device solve alone)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
@@ -673,14 +677,21 @@ def main(argv=None):
     if world == 1 and args.serve_requests > 0:
         from uegccd_b200 import serve
 
-        reqs = serve.poisson_stream(args.serve_requests, rate=args.serve_rate, seed=SEED)
-        srv = serve.Server(hbm_budget=40 << 30, max_batch=64, tol=1e-8)
-        wall = srv.run(reqs, realtime=True)
-        sv = serve.summarize(reqs, wall)
-        sv.update({"arrival_rate": args.serve_rate, "stream": "Poisson; N in {14,54,66,114}; rs log-uniform "
-                   "[0.5,5]; M/(N/2) in {4,8,12,16,20}; twist U[-0.5,0.5)^3; MP2/dRPA/CCD 0.2/0.2/0.6",
-                   "batches": srv.batches_started, "max_concurrent_batches": srv.max_concurrent,
-                   "hbm_budget_gib": 40})
+        def serve_point(n, rate):
+            reqs = serve.poisson_stream(n, rate=rate, seed=SEED)
+            srv = serve.Server(hbm_budget=40 << 30, max_batch=64, tol=1e-8)
+            wall = srv.run(reqs, realtime=True)
+            sv = serve.summarize(reqs, wall)
+            sv.update({"arrival_rate": rate, "batches": srv.batches_started,
+                       "max_concurrent_batches": srv.max_concurrent})
+            return sv
+
+        # the arrival-bound point, then a saturating stream (arrivals far above the service rate)
+        sv = serve_point(args.serve_requests, args.serve_rate)
+        sv.update({"stream": "Poisson; N in {14,54,66,114}; rs log-uniform [0.5,5]; M/(N/2) in {4,8,12,16,20}; "
+                             "twist U[-0.5,0.5)^3; MP2/dRPA/CCD 0.2/0.2/0.6", "hbm_budget_gib": 40,
+                   "retirement": "per solve, after each round of four iterations (incremental batch solve)"})
+        sv["saturated"] = serve_point(args.serve_requests_saturated, args.serve_rate_saturated)
         line["serve"] = sv
     if world == 1 and not args.no_cpu_baseline:
         ncores = 1

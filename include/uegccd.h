@@ -214,6 +214,20 @@ int uegccd_batch_destroy(UegccdBatch *b);
 /* MP2 start + CCD (or dRPA when drpa != 0) of every system; results[n]. */
 int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2,
                        UegccdResult *results);
+/* An incremental solve, for a serving loop that hands each result back as soon as its solve
+ * stops (the reference has no counterpart: Main.f90:112-168 solves one twist after another).
+ * uegccd_batch_start runs the MP2 start of every system (e2[n] may be NULL) and opens the
+ * iteration with the options of uegccd_batch_solve.  Each uegccd_batch_advance runs up to
+ * `rounds` rounds of four iterations of the solves still iterating, then reports every solve
+ * that stopped since the previous call -- converged, at MaxIter, or on a NaN: its index in
+ * done_ids and its result in done_results (room for n of each), *n_done of them, with its
+ * final residual (MaxRes, CCD.f90:103-107) formed at that point.  *n_active counts the solves
+ * still iterating; 0 closes the solve.  Converged solves cost nothing more: their kernels
+ * return at once.  Each solve's iterations, energy and MaxRes are those of uegccd_batch_solve.
+ * FP64 only: UEGCCD_MIXED and range flags return UEGCCD_ERR_UNSUPPORTED. */
+int uegccd_batch_start(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2);
+int uegccd_batch_advance(UegccdBatch *b, int32_t rounds, int32_t *n_active, int32_t *n_done, int32_t *done_ids,
+                         UegccdResult *done_results);
 /* uegccd_ctx_set_integrals for every system of the batch (uegccd_batch_solve sets
  * them from its options first). */
 int uegccd_batch_set_integrals(UegccdBatch *b, int32_t core_n, double gapii);

@@ -62,6 +62,16 @@ int uegccd_heg_set_eigen(UegccdHeg *h, const double *eigen);
 /* The system view; its arrays stay owned by h (valid until the next change). */
 int uegccd_heg_system(const UegccdHeg *h, UegccdSystem *sys);
 int uegccd_heg_info(const UegccdHeg *h, UegccdHegInfo *info);
+/* ChangeTwist (HEG.f90:551-578) for many twists at once, on the current CUDA device: for
+ * each of the ntwist twists (3 doubles each, units of 2 pi/L) the basis SetupBasis picks
+ * (HEG.f90:150-324: the |n|^2 <= MaxKPoint candidates stably sorted by |n + k_s|^2, cut by
+ * fcut and corefcut), its HF eigenvalues (HEG.f90:581-603) and E_HF (print_HF, as
+ * uegccd_heg_info reports it), at h's current rS.  Writes nvec (ntwist x NAO x 3, each
+ * twist column-major like HEGData%nVec), eigen (ntwist x NAO) and ehf (ntwist, may be NULL);
+ * every value is bit-equal to uegccd_heg_change_twist's.  h is not changed (and writes no
+ * fort.60 lines).  At most 4096 candidates. */
+int uegccd_heg_twists(const UegccdHeg *h, int32_t ntwist, const double *twists, int32_t *nvec, double *eigen,
+                      double *ehf);
 void uegccd_find_tol(double rs, double *tolmax, double *failratio, double *denomfactor);
 /* print_ex_SF (HEG.f90:617-674): pair counts ExSf and ExV = (1/Omega) 4 pi/|k_l1-k_l2|^2
  * over ordered pairs l1 != l2 of occupied orbitals, on the grid of q = n_l1 - n_l2 with

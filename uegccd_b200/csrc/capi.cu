@@ -230,6 +230,15 @@ struct UegccdBatch {
     CtlBuffers ctl;
     int diis_cap = 0;
     std::vector<int> last_niter;     // iterations of each solve in the last solve call
+    // an incremental solve (uegccd_batch_start / _advance): its options and which solves have
+    // had their result released
+    struct Session {
+        bool on = false;
+        UegccdOptions opt{};
+        int drpa = 0, ndiis = 0, max_rec = 0;
+        TermFlags f;
+        std::vector<uint8_t> released;
+    } ses;
     // CUDA graphs of one iteration: plain and with kernel timers, keyed by the options
     struct GraphKey {
         int do_ring, do_xring, do_ladder, do_mosaic, drpa, ndiis, max_iter, mixed;
@@ -406,6 +415,11 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     for (int s = 0; s < n; s++) {
         if (!msgs[s].empty()) return fail(UEGCCD_ERR_ARG, "system " + std::to_string(s) + ": " + msgs[s]);
         if (b->plans[s].O > 64) return fail(UEGCCD_ERR_UNSUPPORTED, "NOcc > 64 is outside the hole-hole ladder tiling");
+        for (const auto &v : b->sys[s].n)
+            if (std::abs(v[0]) > 63 || std::abs(v[1]) > 63 || std::abs(v[2]) > 63)
+                return fail(UEGCCD_ERR_UNSUPPORTED, "system " + std::to_string(s) +
+                                                        ": a plane-wave component beyond +-63 (the kernels take "
+                                                        "momentum differences as signed bytes)");
     }
     trace.mark("plans");
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
@@ -429,6 +443,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int16_t> pair_i, pair_j, vir;
     std::vector<int16_t> pcol;   // beside vir: the partner's column in the same block
     std::vector<int4> nv4;
+    std::vector<int> nvp;   // beside nv4: packed a component per byte
     std::vector<double> eigen, vtab;
     std::vector<int64_t> hh0;
     std::vector<RingPairDev> rpairs;
@@ -464,8 +479,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             if (G.partner < 0 || G.partner < (int)gi) continue;  // each {Q, -Q} once
             const auto &H2 = P.groups[G.partner];
             // the smaller group first: k_rings gathers and multiplies from its side
-            if (G.n <= H2.n) rpairs.push_back(RingPairDev{s, G.r0, G.n, H2.r0, H2.n});
-            else rpairs.push_back(RingPairDev{s, H2.r0, H2.n, G.r0, G.n});
+            if (G.n <= H2.n) rpairs.push_back(RingPairDev{s, G.r0, G.n, H2.r0, H2.n, 0});
+            else rpairs.push_back(RingPairDev{s, H2.r0, H2.n, G.r0, G.n, 0});
         }
         for (const auto &B : P.blocks) {
             BlockDev bd;
@@ -534,7 +549,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         pair_j.insert(pair_j.end(), P.pair_j.begin(), P.pair_j.end());
         vir.insert(vir.end(), P.vir.begin(), P.vir.end());
         pcol.insert(pcol.end(), P.pcol.begin(), P.pcol.end());
-        for (int p = 0; p < P.M; p++) nv4.push_back(make_int4(H.n[p][0], H.n[p][1], H.n[p][2], 0));
+        for (int p = 0; p < P.M; p++) {
+            nv4.push_back(make_int4(H.n[p][0], H.n[p][1], H.n[p][2], 0));
+            nvp.push_back((H.n[p][0] & 0xff) | ((H.n[p][1] & 0xff) << 8) | ((H.n[p][2] & 0xff) << 16));
+        }
         eigen.insert(eigen.end(), H.eigen.begin(), H.eigen.end());
         vtab.insert(vtab.end(), P.vtab.begin(), P.vtab.end());
         chunk_begin[s] = (int)chunks.size();
@@ -553,6 +571,18 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         if (amp0 >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit packed indices");
     }
     chunk_begin[n] = (int)chunks.size();
+    // chunks of the amplitudes i <= j: each block's rows up to its diagonal pair
+    std::vector<HChunkDev> hchunks;
+    std::vector<int> hchunk_begin(n + 1, 0);
+    for (int s = 0; s < n; s++) {
+        hchunk_begin[s] = (int)hchunks.size();
+        for (const auto &B : b->plans[s].blocks) {
+            const int64_t lo = B.t0, hi = B.t0 + (int64_t)(B.nd + B.dg) * B.v;
+            for (int64_t st = lo; st < hi; st += kChunk)
+                hchunks.push_back(HChunkDev{s, (int32_t)st, (int32_t)std::min(st + kChunk, hi), 0});
+        }
+    }
+    hchunk_begin[n] = (int)hchunks.size();
     trace.mark("solve-loop");
     ph_i.resize(phr0);
     ph_x.resize(phr0);
@@ -634,6 +664,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.d16_n = d16_n;
     d.nscale = nscale;
     d.nchunks = (int)chunks.size();
+    d.nhchunks = (int)hchunks.size();
     d.nrchunks = (int)rchunks.size();
     d.ntargets = (int)targets.size();
     d.max_o = max_o;
@@ -663,6 +694,15 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
         std::vector<RingPairDev> sorted(rpairs.size());
         for (size_t k = 0; k < rpairs.size(); k++) sorted[start[cls[k]]++] = rpairs[k];
         rpairs.swap(sorted);
+        // each pair's rows in the particle-hole arrays, in launch order: group-1 row a holds
+        // 2 round8(n2) doubles (a multiple of 16: every row starts 128-byte aligned)
+        int64_t xy_n = 0;
+        for (auto &r : rpairs) {
+            r.xy0 = (int32_t)xy_n;
+            xy_n += (int64_t)r.n1 * 2 * ((r.n2 + 7) & ~7);
+            if (xy_n >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit ring offsets");
+        }
+        d.xy_n = xy_n;
         for (const auto &r : rpairs) {
             const int c = cls_of(r);
             d.nring[c]++;
@@ -690,6 +730,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.chunks, chunks))) return rc;
     if ((rc = b->upload(d.rchunks, rchunks))) return rc;
     if ((rc = b->upload(d.chunk_begin, chunk_begin))) return rc;
+    if ((rc = b->upload(d.hchunks, hchunks))) return rc;
+    if ((rc = b->upload(d.hchunk_begin, hchunk_begin))) return rc;
     if ((rc = b->upload(d.targets, targets))) return rc;
     if ((rc = b->upload(d.pcol, pcol))) return rc;
     if ((rc = b->upload(d.mt_start, mt_start))) return rc;
@@ -703,6 +745,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->alloc(d.mirror, amp0))) return rc;
     if ((rc = b->alloc(d.amps, amp0))) return rc;
     if ((rc = b->upload(d.nv4, nv4))) return rc;
+    if ((rc = b->upload(d.nvp, nvp))) return rc;
     if ((rc = b->upload(d.eigen, eigen))) return rc;
     if ((rc = b->upload(d.vtab, vtab))) return rc;
     b->vtab_base = vtab;
@@ -713,8 +756,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->alloc(d.ridx_x, ph0))) return rc;
     if ((rc = b->alloc(d.ridx_y, ph0))) return rc;
     if ((rc = b->alloc(d.vcoef, amp0))) return rc;
-    if ((rc = b->alloc(d.g_rq, amp0))) return rc;
-    if ((rc = b->alloc(d.g_xq, amp0))) return rc;
+    if ((rc = b->alloc(d.xy, d.xy_n))) return rc;
+    if ((rc = b->alloc(d.rx, d.xy_n))) return rc;
+    if ((rc = b->alloc(d.ph_a, phr0))) return rc;
+    if ((rc = b->alloc(d.ph_b, phr0))) return rc;
     if ((rc = b->alloc(d.t, amp0))) return rc;
     if ((rc = b->alloc(d.t_new, amp0))) return rc;
     if ((rc = b->alloc(d.g, amp0))) return rc;
@@ -722,9 +767,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->alloc(d.joo, joo0))) return rc;
     d.ph_total = ph0;
     if ((rc = b->alloc(d.hh, hhoff))) return rc;
-    if ((rc = b->alloc(d.part_e, chunks.size()))) return rc;
-    if ((rc = b->alloc(d.part_dt, chunks.size()))) return rc;
-    if ((rc = b->alloc(d.part_r, chunks.size()))) return rc;
+    const size_t npart = std::max(chunks.size(), hchunks.size());   // per full or half chunk
+    if ((rc = b->alloc(d.part_e, npart))) return rc;
+    if ((rc = b->alloc(d.part_dt, npart))) return rc;
+    if ((rc = b->alloc(d.part_r, npart))) return rc;
     if ((rc = b->alloc(d.red, 3 * (size_t)n))) return rc;
     if ((rc = b->alloc(d.active, n))) return rc;
     b->hsolves = solves;
@@ -735,6 +781,10 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     trace.mark("alloc+upload");
     // position map, amplitude list, partners and ring gather indices, from the blocks
     CU(cudaMemsetAsync(d.pos, 0xff, (size_t)pos0 * sizeof(int32_t), b->stream));   // -1: not allowed
+    CU(cudaMemsetAsync(d.ph_a, 0xff, (size_t)phr0 * sizeof(int32_t), b->stream));  // -1: no ring pair
+    CU(cudaMemsetAsync(d.ph_b, 0xff, (size_t)phr0 * sizeof(int32_t), b->stream));
+    CU(cudaMemsetAsync(d.xy, 0, (size_t)d.xy_n * sizeof(double), b->stream));      // padding columns stay 0
+
     launch_block_tables(d, b->stream);
     launch_vcoef(d, b->stream);
     size_t dn = 0;
@@ -931,7 +981,7 @@ int ctl_alloc(UegccdBatch &b, int ndiis, int max_rec)
         CtlBuffers x = c;
         if ((rc = b.alloc(x.state, n)) || (rc = b.alloc(x.active_next, n)) || (rc = b.alloc(x.count, 1)) ||
             (rc = b.alloc(x.Bm, (size_t)n * kDiisMax * kDiisMax)) || (rc = b.alloc(x.coef, (size_t)n * kDiisMax)) ||
-            (rc = b.alloc(x.brow, (size_t)n * kDiisMax)) || (rc = b.alloc(x.part, (size_t)b.d.nchunks * kDiisMax))) {
+            (rc = b.alloc(x.brow, (size_t)n * kDiisMax)) || (rc = b.alloc(x.part, (size_t)b.d.nhchunks * kDiisMax))) {
             b.rollback(m);
             return rc;
         }
@@ -1180,6 +1230,126 @@ int run_solves(UegccdBatch &b, const UegccdOptions *opt, int drpa, UegccdResult 
     return status;
 }
 
+// Opens an incremental solve: the set-up of run_solves (control buffers with the DIIS depth
+// step-down, start energy and state, the iteration graph), after the MP2 start.
+int session_start(UegccdBatch &b, const UegccdOptions *opt, int drpa)
+{
+    DevBatch &d = b.d;
+    const int n = d.nsolves;
+    auto &S = b.ses;
+    S = UegccdBatch::Session{};
+    TermFlags &f = S.f;
+    f.drpa = drpa;
+    f.do_driver = 1;
+    f.do_mosaic = opt->do_mosaic ? 1 : 0;
+    f.do_ladder = (!drpa && opt->do_ladder) ? 1 : 0;
+    f.do_ring = opt->do_ring ? 1 : 0;
+    f.do_xring = (!drpa && opt->do_xring) ? 1 : 0;
+    f.mixed = 0;
+    S.max_rec = std::min(opt->max_iter, 1100);
+    int ndiis = opt->scheme == UEGCCD_DIIS ? opt->ndiis : 0;
+    int rc = 0;
+    while ((rc = ctl_alloc(b, ndiis, S.max_rec)) == UEGCCD_ERR_ALLOC && ndiis > 2) ndiis--;
+    if (rc) return rc;
+    for (int s = 0; s < n; s++) b.hsolves[s].denom_factor = opt->denom_factor;
+    CU(cudaMemcpyAsync(d.solves, b.hsolves.data(), n * sizeof(SolveDev), cudaMemcpyHostToDevice, b.stream));
+    std::vector<IterState> st0(n, IterState{1, 0, 0.0, 0.0});
+    CU(cudaMemcpyAsync(b.ctl.state, st0.data(), n * sizeof(IterState), cudaMemcpyHostToDevice, b.stream));
+    CU(cudaMemsetAsync(b.ctl.Bm, 0, (size_t)n * kDiisMax * kDiisMax * sizeof(double), b.stream));
+    if ((rc = set_active_all(b, 1))) return rc;
+    if (drpa && !d.J1 && (rc = b.alloc(d.J1, (size_t)d.ph_total))) return rc;
+    if (!b.rings_tuned && !drpa && (f.do_ring || f.do_xring) && (rc = tune_batch_rings(b))) return rc;
+    launch_energy(d, drpa ? 1 : 0, 0.0, b.stream);
+    launch_reduce(d, b.stream);
+    launch_control(d, b.ctl, opt->tol, opt->max_iter, ndiis, 1, b.stream);
+    launch_active_swap(d, b.ctl, b.stream);
+    b.launches += 4;
+    if ((rc = capture_iteration(b, f, opt->tol, opt->max_iter, ndiis))) return rc;
+    CU(cudaStreamSynchronize(b.stream));
+    S.opt = *opt;
+    S.drpa = drpa;
+    S.ndiis = ndiis;
+    S.released.assign(n, 0);
+    S.on = true;
+    return 0;
+}
+
+// Up to `rounds` poll rounds of the open incremental solve, then the results of every solve
+// that stopped since the last call: their final residual (MaxRes, CCD.f90:103-107) is formed
+// with only them active, after which the still-running solves are active again.
+int session_advance(UegccdBatch &b, int rounds, int *n_active, int *n_done, int *ids, UegccdResult *res)
+{
+    constexpr int kPoll = 4;
+    DevBatch &d = b.d;
+    auto &S = b.ses;
+    const int n = d.nsolves;
+    const UegccdOptions &opt = S.opt;
+    int count = 0;
+    CU(cudaMemcpyAsync(&count, b.ctl.count, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+    for (int r = 0; r < rounds && count > 0; r++) {
+        for (int k = 0; k < kPoll; k++) {
+            CU(cudaGraphLaunch(b.gexec, b.stream));
+            b.launches += b.g_launches;
+        }
+        CU(cudaMemcpyAsync(&count, b.ctl.count, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+        b.d2h_bytes += sizeof(int);
+        CU(cudaStreamSynchronize(b.stream));
+        CU(cudaGetLastError());
+    }
+    std::vector<IterState> st(n);
+    CU(cudaMemcpyAsync(st.data(), b.ctl.state, n * sizeof(IterState), cudaMemcpyDeviceToHost, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+    std::vector<int> fresh;
+    for (int s = 0; s < n; s++)
+        if (st[s].status != 0 && !S.released[s]) fresh.push_back(s);
+    *n_done = (int)fresh.size();
+    int running = 0;
+    for (int s = 0; s < n; s++) running += st[s].status == 0;
+    *n_active = running;
+    if (!fresh.empty()) {
+        std::fill(b.active.begin(), b.active.end(), 0);
+        for (int s : fresh) b.active[s] = 1;
+        CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
+        b.h2d_bytes += n;
+        b.launches += launch_residual(d, S.f, 1, nullptr, b.stream, nullptr);
+        int rc = read_red(b);
+        if (rc) return rc;
+        std::vector<double> rmax(n), esosex(n, 0.0);
+        for (int s = 0; s < n; s++) rmax[s] = b.red[3 * s + 2];
+        if (S.drpa) {
+            launch_energy(d, 1, 1.0, b.stream);
+            launch_reduce(d, b.stream);
+            b.launches += 2;
+            if ((rc = read_red(b))) return rc;
+            for (int s = 0; s < n; s++) esosex[s] = b.red[3 * s];
+        }
+        for (size_t k = 0; k < fresh.size(); k++) {
+            const int s = fresh[k];
+            UegccdResult &r = res[k];
+            std::memset(&r, 0, sizeof r);
+            ids[k] = s;
+            r.ecorr = st[s].e;
+            r.max_res = rmax[s];
+            r.last_dt = st[s].dt;
+            r.niter = st[s].niter;
+            r.fail = rmax[s] > opt.fail_ratio * opt.tol;
+            r.ecorr_sosex = (S.drpa && !r.fail) ? esosex[s] : 0.0;
+            r.kernel_launches = b.launches;
+            r.status = st[s].status == 3 ? UEGCCD_ERR_NUMERIC
+                       : (r.fail || st[s].status == 2) ? UEGCCD_NOT_CONVERGED : UEGCCD_OK;
+            r.ndiis = S.ndiis;
+            S.released[s] = 1;
+        }
+        for (int s = 0; s < n; s++) b.active[s] = st[s].status == 0 ? 1 : 0;
+        CU(cudaMemcpyAsync(d.active, b.active.data(), n, cudaMemcpyHostToDevice, b.stream));
+        b.h2d_bytes += n;
+        CU(cudaStreamSynchronize(b.stream));
+    }
+    if (running == 0) S.on = false;
+    return 0;
+}
+
 }  // namespace
 
 namespace uegccd {
@@ -1220,6 +1390,7 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
         if ((rc = b.upload(b.sf_groups, g))) return rc;
         if ((rc = b.alloc(b.sf_grid, 5 * (size_t)w3max))) return rc;
         if ((rc = b.alloc(b.sf_err, 1))) return rc;
+
     }
     const SystemHost &H = b.sys[s];
     const int S = sf_length(H);
@@ -1489,6 +1660,7 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
 {
     if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
     ENTER(b);
+    b->ses.on = false;   // a full solve ends an open incremental one
     int rc = validate_options(opt, drpa, *b);
     if (rc) return rc;
     if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
@@ -1513,6 +1685,44 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
     CU(cudaEventElapsedTime(&ms, b->ev_solve0, b->ev_solve1));
     for (int s = 0; s < b->d.nsolves; s++) results[s].gpu_ms = ms;
     return st;
+}
+
+int uegccd_batch_start(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2)
+{
+    if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
+    ENTER(b);
+    int rc = validate_options(opt, drpa, *b);
+    if (rc) return rc;
+    if (opt->precision != UEGCCD_FP64)
+        return fail(UEGCCD_ERR_UNSUPPORTED, "an incremental solve runs in FP64 (use uegccd_batch_solve for MIXED)");
+    if (opt->range_flags != 0)
+        return fail(UEGCCD_ERR_UNSUPPORTED, "an incremental solve takes no range flags (use uegccd_batch_solve)");
+    if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
+    b->launches = 0;
+    launch_mp2(b->d, b->stream);
+    launch_reduce(b->d, b->stream);
+    b->launches += 2;
+    if ((rc = read_red(*b))) return rc;
+    if (e2)
+        for (int s = 0; s < b->d.nsolves; s++) e2[s] = b->red[3 * s];
+    if (drpa) {
+        launch_to_aaaa(b->d, b->stream);   // the dRPA start is T2aaaa of the MP2 step (Main.f90:85-91)
+        std::swap(b->d.t, b->d.t_new);
+        b->launches++;
+    }
+    return session_start(*b, opt, drpa);
+}
+
+int uegccd_batch_advance(UegccdBatch *b, int32_t rounds, int32_t *n_active, int32_t *n_done, int32_t *done_ids,
+                         UegccdResult *done_results)
+{
+    if (!b || !n_active || !n_done || !done_ids || !done_results || rounds < 0)
+        return fail(UEGCCD_ERR_ARG, "bad argument");
+    ENTER(b);
+    *n_active = 0;
+    *n_done = 0;
+    if (!b->ses.on) return fail(UEGCCD_ERR_ARG, "no incremental solve is open on this batch (uegccd_batch_start)");
+    return session_advance(*b, rounds, n_active, n_done, done_ids, done_results);
 }
 
 int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max)
@@ -1566,11 +1776,20 @@ int uegccd_footprint(const UegccdSystem *sys, int32_t ndiis, int32_t mixed, int6
     int64_t b = 0;
     int64_t sum_ov = 0;
     for (const auto &B : P.blocks) sum_ov += B.o + B.v;
-    b += A * (8 * 5 + 16 + sizeof(AmpInfo) + 4 + 4); // t, t_new, g, g_rq, g_xq; Coulomb factors; amps; partner, mirror
+    b += A * (8 * 3 + 16 + sizeof(AmpInfo) + 4 + 4); // t, t_new, g; Coulomb factors; amps; partner, mirror
     b += sum_ov * (8 + 4) + (V + O + 1) * (4 + 8);   // mosaic partials and target lists
     b += O * O * V * 4;                              // pos
     b += O * V * O * 8;                              // dRPA ring intermediate (allocated for dRPA only)
     b += O * V * 2 * 2;                              // ph rows
+    int64_t xy = 0;                                  // particle-hole operands and results of the rings
+    for (size_t gi = 0; gi < P.groups.size(); gi++) {
+        const auto &G = P.groups[gi];
+        if (G.partner < 0 || G.partner < (int)gi) continue;
+        const auto &H2 = P.groups[G.partner];
+        const int64_t n1 = std::min(G.n, H2.n), n2 = std::max(G.n, H2.n);
+        xy += n1 * 2 * ((n2 + 7) & ~7);
+    }
+    b += xy * 8 * 2 + O * V * 4 * 2;                 // xy, rx; ph_a, ph_b
     b += O * V * O * 4 * 2;                          // ring gather indices
     b += hh * 8 + nblk * (sizeof(BlockDev) + 8) + M * (16 + 8) + (P.q2max + 1) * 8;
     b += A * (8 + 4) * (int64_t)std::max(0, (int)ndiis);  // DIIS history (t' FP64, e FP32)

@@ -18,6 +18,7 @@
 
 #include "../../include/uegccd.h"
 #include "../../include/uegccd_host.h"
+#include "heg_device.h"
 #include "listdir.h"
 
 namespace {
@@ -320,6 +321,39 @@ bool parse_bool(const std::string &v)
 namespace uegccd {
 void heg_log_to(std::string *sink) { g_log = sink; }
 void heg_sf_log_to(std::string *sink) { g_log82 = sink; }
+}  // namespace uegccd
+
+namespace uegccd {
+// What the device set-up of many twists needs from the host state (heg_device.cu): the
+// untwisted candidates of SetupBasis in its loop order, the basis size after fcut and
+// corefcut, and the scalars of form_eigen / hf_energy at the current rS.
+int heg_twist_setup(const UegccdHeg *h, HegTwistSetup *out)
+{
+    if (!h || !out) return herr(UEGCCD_ERR_ARG, "null argument");
+    const int cell = h->cell;
+    out->cand.clear();
+    for (int l1 = -cell; l1 <= cell; l1++)
+        for (int l2 = -cell; l2 <= cell; l2++)
+            for (int l3 = -cell; l3 <= cell; l3++)
+                if (l1 * l1 + l2 * l2 + l3 * l3 <= h->maxkpoint) out->cand.push_back({l1, l2, l3});
+    const int nbasis0 = (int)out->cand.size();
+    int mfcut = (int)(std::pow(h->in.fcut, 3.0 / 2.0) * h->nel / 2);
+    double mtarget = std::pow(h->in.fcut, 3.0 / 2.0) * h->nel / 2;
+    if (std::fabs(mfcut - mtarget) > std::fabs(mfcut + 1 - mtarget)) mfcut = mfcut + 1;
+    const int nbasis = std::min(mfcut, nbasis0);
+    const int mcore = fcut_to_basis_fn(h->in.corefcut, h->nel);
+    out->nao = nbasis - mcore + h->nel / 2;
+    out->mcore = mcore;
+    out->nel = h->nel;
+    if (out->nao != h->nao) return herr(UEGCCD_ERR_ARG, "basis size differs from the set-up's");
+    out->kscale = 2.0 * kPi / h->L;
+    out->inv_omega = 1.0 / h->omega;
+    out->madelung = h->madelung;
+    out->gap = h->in.gap;
+    out->exchangefactor = h->exchangefactor;
+    out->L = h->L;
+    return 0;
+}
 }  // namespace uegccd
 
 extern "C" {

@@ -29,6 +29,9 @@ struct DevBatch {
     ChunkDev *chunks = nullptr;      // amplitude chunks
     ChunkDev *rchunks = nullptr;     // ring-intermediate chunks over (i, x, l)
     int *chunk_begin = nullptr;      // nsolves+1: first chunk of each solve
+    HChunkDev *hchunks = nullptr;    // chunks of the amplitudes i <= j (k_update, DIIS, commit)
+    int nhchunks = 0;
+    int *hchunk_begin = nullptr;     // nsolves+1: first half chunk of each solve
     int2 *targets = nullptr;         // mosaic targets (solve, id)
     int16_t *pair_i = nullptr, *pair_j = nullptr, *vir = nullptr;
     int16_t *pcol = nullptr;          // beside vir: column of the partner d = K - c in the same block
@@ -37,6 +40,7 @@ struct DevBatch {
     int32_t *mirror = nullptr;       // packed (i,j,a): index of (j,i,b) if i < j, -1 if i = j, -2 if i > j
     AmpInfo *amps = nullptr;
     int4 *nv4 = nullptr;
+    int *nvp = nullptr;              // the same vectors packed a component per byte (q2p in kernels_fp64.cu)
     double *eigen = nullptr, *vtab = nullptr;
     double *t = nullptr, *t_new = nullptr, *g = nullptr;
     double2 *vcoef = nullptr;         // per amplitude {v(i-a), v(a-j)} (k_vcoef, once per batch)
@@ -51,8 +55,16 @@ struct DevBatch {
     // particle-hole form of the ring terms
     int16_t *ph_i = nullptr, *ph_x = nullptr;   // row -> (i, x), rows grouped by Q
     int32_t *ridx_x = nullptr, *ridx_y = nullptr;  // at ph0 + row*O + k: index of t(ik, x), t(ki, x)
-    double *g_rq = nullptr, *g_xq = nullptr;    // per amplitude: ring and crossed-ring G
     RingPairDev *rpairs = nullptr;              // {Q, -Q} group pairs
+    // rings in the particle-hole layout (RingPairDev::xy0): xy holds the amplitudes each pair
+    // multiplies, row by row (k_ring_stage gathers t into it before every ring launch); rx
+    // the ring and crossed-ring G the pair forms, in the same places (k_update reads them).
+    // Per (i, x) at phr0 + i*V + x - O: ph_a = the row's offset in xy/rx when (i, x) is in
+    // its pair's group 1, else -1; ph_b = round8(n2) of its pair in group 1 (where the Y1 /
+    // crossed-ring half of the row starts), its column b in group 2 (-1 without a pair).
+    double *xy = nullptr, *rx = nullptr;
+    int64_t xy_n = 0;
+    int32_t *ph_a = nullptr, *ph_b = nullptr;
     // mixed precision: tensor-core ladder tiles sorted by row tile (16, 32, 64)
     LadderTile *tctiles = nullptr;
     int ntc16 = 0, ntc32 = 0, ntc64 = 0;
@@ -106,7 +118,7 @@ constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* u
 
 // Live per-kernel timing with CUDA events on the launching stream (off unless enabled).
 enum KernelId { KID_MP2 = 0, KID_ENERGY, KID_HH_W, KID_LADDER, KID_MOSAIC_S, KID_MOSAIC_RED, KID_RING_INT,
-                KID_UPDATE, KID_REDUCE, KID_RINGS, KID_LADDER_TC,
+                KID_UPDATE, KID_REDUCE, KID_RINGS, KID_LADDER_TC, KID_RING_STAGE,
                 KID_COUNT };
 struct KernelTimer {
     bool on = false;
@@ -188,7 +200,8 @@ void launch_unpack_all(const DevBatch &d, const int64_t *dense_off, const double
 // zeroed by the caller; *err = 1 if a transfer falls outside.
 void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, int S, double *grid, int *err,
                cudaStream_t st);
-// pos (pre-set to -1), amps, partner, then the ring gather indices, from the block structure
+// pos (pre-set to -1), amps, partner, mirror from the block structure; the particle-hole
+// tables ph_a, ph_b (pre-set to -1) from the ring pairs; the ring gather indices
 void launch_block_tables(const DevBatch &d, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref); writes the
 // scaled FP16 d tiles first (d.w16 must be built)

@@ -23,6 +23,17 @@
 
 namespace uegccd {
 
+// Plane-wave vectors packed one component per byte (x | y << 8 | z << 16, two's complement;
+// DevBatch::nvp): the squared length of the difference of two orbitals' vectors is then one
+// per-byte subtraction and one 4-way byte dot product.  Every |n_d| <= 63 (checked when the
+// batch is made), so each component difference fits a signed byte; modular byte arithmetic
+// keeps a difference of differences exact as long as the final one does.
+__device__ __forceinline__ int q2p(int a, int c)
+{
+    const int d = __vsub4(a, c);
+    return __dp4a(d, d, 0);
+}
+
 __device__ __forceinline__ int q2_of(int4 x, int4 y)
 {
     int d0 = x.x - y.x, d1 = x.y - y.y, d2 = x.z - y.z;
@@ -216,7 +227,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 size_t ladder_smem_bytes(int max_v, int np)
 {
-    return sizeof(double) * (2 * (size_t)np * kLadLd + kVtabSmem) + sizeof(int4) * (size_t)max_v;
+    return sizeof(double) * (2 * (size_t)np * kLadLd + kVtabSmem) + sizeof(int) * (size_t)max_v;
 }
 
 // PAIRED (blocks with at most 4 rows i <= j, NP = 8): the fragment's 8 columns hold the
@@ -229,10 +240,10 @@ size_t ladder_smem_bytes(int max_v, int np)
 template <int NP, bool KS, bool PAIRED>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
-                                             const int4 *__restrict__ nv4, const double *__restrict__ vtab,
+                                             const int *__restrict__ nvp, const double *__restrict__ vtab,
                                              const double *__restrict__ t, const double *__restrict__ H, int mode,
                                              int do_pp, int do_hh, double *__restrict__ out, const double *sv,
-                                             bool vsm, double *ts, const int4 *nvc)
+                                             bool vsm, double *ts, const int *nvc)
 {
     constexpr int NN = NP / 8;  // n fragments
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -249,13 +260,13 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
     const bool ksplit = KS && ncol - T.a0 <= 32;
     const int colbase = ksplit ? T.a0 : T.a0 + warp * 32;
     const bool wact = colbase < ncol;  // warps past the last column only help with the copies
-    // n-vectors of this lane's A-fragment rows (one per m fragment)
-    int4 na[4];
+    // packed n-vectors of this lane's A-fragment rows (one per m fragment)
+    int na[4];
 #pragma unroll
     for (int m = 0; m < 4; m++) {
         int col = colbase + m * 8 + gid;
-        na[m] = make_int4(0, 0, 0, 0);
-        if (col < ncol) na[m] = nv4[s.orb0 + (mode == 0 ? vir[B.vir0 + col] : pair_i[B.pair0 + col])];
+        na[m] = 0;
+        if (col < ncol) na[m] = nvp[s.orb0 + (mode == 0 ? vir[B.vir0 + col] : pair_i[B.pair0 + col])];
     }
     double acc[4][NN][2];
 #pragma unroll
@@ -303,13 +314,13 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 #pragma unroll 2
                 for (int kk = kstart; kk < kLadKC; kk += kstep) {
                     const int c = min(c0 + kk + tig, v - 1);  // beyond v the t column is zero
-                    const int4 nc = nvc[c];
+                    const int nc = nvc[c];
                     double bf[NN];
 #pragma unroll
                     for (int n = 0; n < NN; n++) bf[n] = tb[(n * 8 + gid) * kLadLd + kk + tig];
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
-                        const int q2 = q2_of(na[m], nc);
+                        const int q2 = q2p(na[m], nc);
                         const double af = vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]);
 #pragma unroll
                         for (int n = 0; n < NN; n++) dmma_884(acc[m][n][0], acc[m][n][1], af, bf[n]);
@@ -384,7 +395,7 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 int p = T.p0 + n * 8 + 2 * tig + h, oc = col;
-                int4 nq = na[m];
+                int nq = na[m];
                 if (PAIRED) {
                     const int nn = n * 8 + 2 * tig + h;
                     if (nn >= 2 * orow) continue;
@@ -393,15 +404,15 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
                         p = nn - orow;
                         oc = mode == 0 ? pcolv(col) : mirq(col);
                         if (oc == col) continue;
-                        if (mode == 1) nq = nv4[s.orb0 + pair_i[B.pair0 + oc]];
+                        if (mode == 1) nq = nvp[s.orb0 + pair_i[B.pair0 + oc]];
                     }
                 }
                 if (p >= orow) continue;
                 if (mode == 0) {
                     out[B.t0 + (int64_t)p * v + oc] = acc[m][n][h];
                 } else {
-                    const int4 ni = nv4[s.orb0 + pair_i[B.pair0 + p]];
-                    const int q2 = q2_of(ni, nq);
+                    const int ni = nvp[s.orb0 + pair_i[B.pair0 + p]];
+                    const int q2 = q2p(ni, nq);
                     out[(int64_t)p * o + oc] = (vsm ? sv[q2] : vtab[s.vtab0 + q2]) + acc[m][n][h];
                 }
             }
@@ -414,7 +425,7 @@ template <int NP, bool PAIRED>
 __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     k_ladder3(const LadderTile *__restrict__ tiles, const BlockDev *__restrict__ blocks,
               const SolveDev *__restrict__ solves, const int16_t *__restrict__ vir,
-              const int16_t *__restrict__ pair_i, const int4 *__restrict__ nv4,
+              const int16_t *__restrict__ pair_i, const int *__restrict__ nvp,
               const double *__restrict__ vtab, const double *__restrict__ t, const int64_t *__restrict__ hh0,
               double *__restrict__ hh, int mode, int do_pp, int do_hh, double *__restrict__ g,
               const uint8_t *__restrict__ active)
@@ -426,20 +437,20 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     extern __shared__ double lsm[];
     double *ts = lsm;                              // 2 x NP x kLadLd
     double *sv = ts + 2 * NP * kLadLd;             // kVtabSmem
-    int4 *nvc = (int4 *)(sv + kVtabSmem);          // v_K n-vectors of the block's virtuals
+    int *nvc = (int *)(sv + kVtabSmem);            // v_K packed n-vectors of the block's virtuals
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
         for (int q = threadIdx.x; q <= s.q2max; q += blockDim.x) sv[q] = vtab[s.vtab0 + q];
-    for (int c = threadIdx.x; c < B.v; c += blockDim.x) nvc[c] = nv4[s.orb0 + vir[B.vir0 + c]];
+    for (int c = threadIdx.x; c < B.v; c += blockDim.x) nvc[c] = nvp[s.orb0 + vir[B.vir0 + c]];
     __syncthreads();
     double *H = hh + hh0[T.blk];
     double *out = mode == 0 ? g : H;
     // the hole-hole intermediate (mode 1) may split its c sum across the warps
     if (mode == 1)
-        ladder3_tile<NP, true, PAIRED>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
+        ladder3_tile<NP, true, PAIRED>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
                                        nvc);
     else
-        ladder3_tile<NP, false, PAIRED>(T, B, s, vir, pair_i, nv4, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
+        ladder3_tile<NP, false, PAIRED>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
                                         nvc);
 }
 
@@ -481,7 +492,7 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
         const int np = c == 0 ? 8 : 8 * c;
         const size_t sm = ladder_smem_bytes(d.max_v, np);
 #define UEGCCD_LADDER_ARGS                                                                                  \
-    tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.nv4, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
+    tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.nvp, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
         g, d.active
         switch (c) {
         case 0: k_ladder3<8, true><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
@@ -701,7 +712,7 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
                                                const int32_t *__restrict__ pos, const int32_t *__restrict__ partner,
                                                const int4 *__restrict__ nv4, const double *__restrict__ vtab,
                                                const double *__restrict__ t, int do_ring, int do_xring,
-                                               double *__restrict__ g_rq, double *__restrict__ g_xq,
+                                               double *__restrict__ rx,
                                                const uint8_t *__restrict__ active)
 {
     const RingPairDev P = pairs[blockIdx.x];
@@ -709,6 +720,7 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
     const SolveDev s = solves[P.solve];
     const int O = s.O;
     const int R = P.n1 + P.n2;
+    const int N2 = (P.n2 + 7) & ~7;   // rx row: ring G of the group-2 columns, then crossed-ring G
     // shared-memory strides are odd so that consecutive threads hit distinct banks
     const int ld = O | 1, lr = R | 1;
     extern __shared__ double smem[];
@@ -725,8 +737,8 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
     double *Sy = Sx + R;                                 // R
     double *Vd = Sy + R;                                 // R
     int *ri = (int *)(Vd + R);                           // R
-    int *rx = ri + R;                                    // R
-    int4 *no = (int4 *)(((uintptr_t)(rx + R) + 15) & ~(uintptr_t)15);  // O occupied n-vectors
+    int *rxv = ri + R;                                   // R: the row's virtual
+    int4 *no = (int4 *)(((uintptr_t)(rxv + R) + 15) & ~(uintptr_t)15);  // O occupied n-vectors
     const int tid = threadIdx.x, nt = blockDim.x;
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
@@ -735,12 +747,12 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
     for (int r = tid; r < R; r += nt) {
         const int64_t row = s.phr0 + (r < P.n1 ? P.r1 + r : P.r2 + r - P.n1);
         ri[r] = ph_i[row];
-        rx[r] = ph_x[row];
+        rxv[r] = ph_x[row];
     }
     __syncthreads();
     auto V = [&](int q2) -> double { return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : vtab[s.vtab0 + q2]); };
     // Q of group 1 = n_x - n_i of its first row
-    const int4 qa = nv4[s.orb0 + rx[0]], qb = nv4[s.orb0 + ri[0]];
+    const int4 qa = nv4[s.orb0 + rxv[0]], qb = nv4[s.orb0 + ri[0]];
     const int Qx = qa.x - qb.x, Qy = qa.y - qb.y, Qz = qa.z - qb.z;
     for (int e = tid; e < O * O; e += nt) {
         const int k = e / O, l = e % O;
@@ -755,7 +767,7 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
     // X, Y rows (stored transposed)
     for (int e = tid; e < R * O; e += nt) {
         const int k = e / R, r = e % R;
-        const int p = posmap(s, pos, ri[r], k, rx[r]);
+        const int p = posmap(s, pos, ri[r], k, rxv[r]);
         double xv = 0.0, yv = 0.0;
         if (p >= 0) {
             xv = t[p];
@@ -773,12 +785,14 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
         }
         Sx[r] = sx;
         Sy[r] = sy;
-        const int4 ni = nv4[s.orb0 + ri[r]], nx = nv4[s.orb0 + rx[r]];
+        const int4 ni = nv4[s.orb0 + ri[r]], nx = nv4[s.orb0 + rxv[r]];
         Vd[r] = V(q2_of(ni, nx));
     }
     __syncthreads();
-    // two directions: rows of group 1 against group 2, then the reverse
-    for (int dir = 0; dir < 2; dir++) {
+    // rows of group 1 against group 2: the values at (a, b) are the ring G of (i_a, i_b, x_a)
+    // and the crossed-ring G of (i_a, i_b, x_b), which k_update reads for each amplitude or
+    // its mirror (the reverse direction gives the mirrors' values: not needed)
+    for (int dir = 0; dir < 1; dir++) {
         const int a0 = dir == 0 ? 0 : P.n1, na = dir == 0 ? P.n1 : P.n2;
         const int b0 = dir == 0 ? P.n1 : 0, nb = dir == 0 ? P.n2 : P.n1;
         const double *W = dir == 0 ? W1 : W2;
@@ -816,16 +830,13 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
                     ex21 = fma(vo21, x2, ex21);                // Ex_r2[i1]
                     ey21 = fma(vo21, y2, ey21);                // Ey_r2[i1]
                 }
+                double *out = rx + P.xy0 + (int64_t)r1 * 2 * N2;
                 if (do_ring) {
                     const double vd = Vd[r1];
                     const double lin = 2.0 * vd * (Sx[r1] + Sx[r2]) - vd * (Sy[r1] + Sy[r2]) - ex12 - ex21;
-                    const int p = posmap(s, pos, i1, i2, rx[r1]);
-                    if (p >= 0) g_rq[p] = lin + quad;
+                    out[r2 - P.n1] = lin + quad;
                 }
-                if (do_xring) {
-                    const int p = posmap(s, pos, i1, i2, rx[r2]);
-                    if (p >= 0) g_xq[p] = -ey12 - ey21 + xquad;
-                }
+                if (do_xring) out[N2 + r2 - P.n1] = -ey12 - ey21 + xquad;
             }
             __syncthreads();
         }
@@ -863,8 +874,6 @@ __global__ void __launch_bounds__(256) k_rings_wide(const RingPairDev *__restric
 // multiply-adds.  Row strides are the padded width + 4 (= 4 or 12 mod 16 doubles):
 // fragment loads without bank conflicts, row-wise and transposed.
 // ----------------------------------------------------------------------------
-constexpr int kRingGather = 8;   // gather elements in flight per thread
-
 __host__ __device__ __forceinline__ int round8(int x) { return (x + 7) & ~7; }
 
 size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
@@ -872,19 +881,17 @@ size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
     const size_t N1 = round8(n1), N2 = round8(n2), l1 = N1 + 4, l2 = N2 + 4;
     const size_t nsv = q2max < kVtabSmem ? round8(q2max + 1) : 0;
     const size_t dbl = 2 * N1 * l2 + 2 * N1 * l1 + 3 * (N1 + N2) + nsv;
-    return sizeof(double) * dbl + sizeof(int) * 2 * (N1 + N2) + sizeof(int4) * ((size_t)O + 2 * (N1 + N2));
+    return sizeof(double) * dbl + sizeof(int) * ((size_t)O + 4 * (N1 + N2));
 }
 
 __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ pairs,
                                                         const SolveDev *__restrict__ solves,
                                                         const int16_t *__restrict__ ph_i,
                                                         const int16_t *__restrict__ ph_x,
-                                                        const int32_t *__restrict__ ridx_x,
-                                                        const int32_t *__restrict__ ridx_y,
-                                                        const int4 *__restrict__ nv4,
+                                                        const int *__restrict__ nvp,
                                                         const double *__restrict__ vtab,
-                                                        const double *__restrict__ t, int do_ring, int do_xring,
-                                                        double *__restrict__ g_rq, double *__restrict__ g_xq,
+                                                        const double *__restrict__ xy, int do_ring, int do_xring,
+                                                        double *__restrict__ rx,
                                                         const uint8_t *__restrict__ active)
 {
     const RingPairDev P = pairs[blockIdx.x];
@@ -908,10 +915,9 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
     double *Vd = Sy + R;
     double *sv = Vd + R;            // nsv
     int *ri = (int *)(sv + nsv);    // R: occupied index of the row (-1 on padding)
-    int *rw = ri + R;               // R: row * O, the row's offset in the gather-index tables
-    int4 *no = (int4 *)(rw + R);    // O
-    int4 *nx = no + O;              // R: n-vector of the row's virtual
-    int4 *nr = nx + R;              // R: n-vector of the row's occupied index (0 on padding)
+    int *no = ri + R;               // O: packed n-vectors of the occupied orbitals
+    int *nx = no + O;               // R: packed n-vector of the row's virtual
+    int *nr = nx + R;               // R: packed n-vector of the row's occupied index (0 on padding)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, kWarps = nt >> 5;
     auto V = [&](int q2) -> double {
         return q2 > s.q2max ? 0.0 : (vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]));
@@ -923,41 +929,24 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
         else if (r >= N1 && r - N1 < n2) row = P.r2 + (r - N1);
         const int i = row >= 0 ? ph_i[s.phr0 + row] : -1, x = row >= 0 ? ph_x[s.phr0 + row] : -1;
         ri[r] = i;
-        rw[r] = row >= 0 ? row * O : -1;
-        nx[r] = x >= 0 ? nv4[s.orb0 + x] : make_int4(0, 0, 0, 0);
+        nx[r] = x >= 0 ? nvp[s.orb0 + x] : 0;
     }
-    for (int k = tid; k < O; k += nt) no[k] = nv4[s.orb0 + k];
+    for (int k = tid; k < O; k += nt) no[k] = nvp[s.orb0 + k];
     __syncthreads();
-    for (int r = tid; r < R; r += nt) nr[r] = ri[r] >= 0 ? no[ri[r]] : make_int4(0, 0, 0, 0);
-    const int4 q1x = nx[0], q1i = no[ri[0]];
-    const int Qx = q1x.x - q1i.x, Qy = q1x.y - q1i.y, Qz = q1x.z - q1i.z;
-    const int32_t *gx = ridx_x + s.ph0, *gy = ridx_y + s.ph0;
-    // gather X1, Y1 over (a, b); the index loads of a batch are issued before its
-    // amplitude loads
-    const int ne = N1 * N2;
-    for (int e0 = tid; e0 < ne; e0 += nt * kRingGather) {
-        int p1[kRingGather], p2[kRingGather];
-#pragma unroll
-        for (int u = 0; u < kRingGather; u++) {
-            const int e = e0 + u * nt;
-            p1[u] = p2[u] = -1;
-            if (e < ne) {
-                const int r = e / N2, c = e - r * N2;
-                if (r < n1 && c < n2) {
-                    const int w = rw[r] + ri[N1 + c];
-                    p1[u] = __ldg(&gx[w]);
-                    p2[u] = __ldg(&gy[w]);
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kRingGather; u++) {
-            const int e = e0 + u * nt;
-            if (e < ne) {
-                const int r = e / N2, c = e - r * N2;
-                X1[r * l2 + c] = p1[u] >= 0 ? __ldg(&t[p1[u]]) : 0.0;
-                Y1[r * l2 + c] = p2[u] >= 0 ? __ldg(&t[p2[u]]) : 0.0;
-            }
+    for (int r = tid; r < R; r += nt) nr[r] = ri[r] >= 0 ? no[ri[r]] : 0;
+    const int Qp = __vsub4(nx[0], no[ri[0]]);   // Q = n_x - n_i of group 1, packed
+    // X1 and Y1: the pair's rows in the particle-hole copy of t (k_ring_stage), 2 N2 doubles
+    // a row and 16-byte aligned -- contiguous loads in place of index -> amplitude gathers.
+    // Columns n2..N2-1 are zero in memory; rows n1..N1-1 are padding.
+    {
+        const double2 *src = reinterpret_cast<const double2 *>(xy + P.xy0);
+        const int half = N2 / 2;   // double2 per X1 (or Y1) row
+        for (int e = tid; e < N1 * N2; e += nt) {
+            const int r = e / N2, c2 = e - r * N2;
+            const double2 v = r < n1 ? __ldg(&src[(int64_t)r * N2 + c2]) : make_double2(0.0, 0.0);
+            double *dst = c2 < half ? X1 + r * l2 + 2 * c2 : Y1 + r * l2 + 2 * (c2 - half);
+            dst[0] = v.x;
+            dst[1] = v.y;
         }
     }
     __syncthreads();
@@ -978,7 +967,7 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
         }
         Sx[r] = sx;
         Sy[r] = sy;
-        Vd[r] = ri[r] >= 0 ? V(q2_of(no[ri[r]], nx[r])) : 0.0;
+        Vd[r] = ri[r] >= 0 ? V(q2p(no[ri[r]], nx[r])) : 0.0;
     }
     const int g = lane >> 2, tg = lane & 3;
     // phase 1: XW1 = X1 W, U1 = Y1 W - Vs1 (K = N2), with W[b][a] = v(n_{i_b} - n_{i_a} - Q)
@@ -992,13 +981,13 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
             const double *AX = X1 + (mf * 8 + g) * l2 + tg;
             const double *AY = Y1 + (mf * 8 + g) * l2 + tg;
             const int nbase = ng * 16;
-            int4 cn[2];
+            int cn[2];
             bool cok[2];
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const int n = nbase + f * 8 + g;
                 cok[f] = n < n1;
-                cn[f] = cok[f] ? nr[n] : make_int4(0, 0, 0, 0);
+                cn[f] = cok[f] ? __vadd4(nr[n], Qp) : 0;   // n_{i_a'} + Q
             }
             double acc[2][2][2];
 #pragma unroll
@@ -1007,30 +996,26 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
                 const int k = k0 + tg;
                 const double ax = AX[k0], ay = AY[k0];
                 const bool kok = k < n2;
-                const int4 kn = nr[N1 + k];
+                const int kn = nr[N1 + k];
 #pragma unroll
                 for (int f = 0; f < 2; f++) {
                     if (nbase + f * 8 >= N1) break;
-                    // B(k = b, n = a') = W[b][a']
-                    double bv = 0.0;
-                    if (kok && cok[f]) {
-                        const int dx = kn.x - cn[f].x - Qx, dy = kn.y - cn[f].y - Qy, dz = kn.z - cn[f].z - Qz;
-                        bv = V(dx * dx + dy * dy + dz * dz);
-                    }
+                    // B(k = b, n = a') = W[b][a'] = v(n_{i_b} - n_{i_a'} - Q)
+                    const double bv = (kok && cok[f]) ? V(q2p(kn, cn[f])) : 0.0;
                     dmma_884(acc[0][f][0], acc[0][f][1], ax, bv);
                     dmma_884(acc[1][f][0], acc[1][f][1], ay, bv);
                 }
             }
             const int r = mf * 8 + g;
             const bool rok = r < n1;
-            const int4 rn = rok ? nr[r] : make_int4(0, 0, 0, 0);
+            const int rn = rok ? nr[r] : 0;
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 if (nbase + f * 8 >= N1) break;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int n = nbase + f * 8 + 2 * tg + h;
-                    const double vs = (rok && n < n1) ? V(q2_of(nr[n], rn)) : 0.0;
+                    const double vs = (rok && n < n1) ? V(q2p(nr[n], rn)) : 0.0;
                     XW1[r * l1 + n] = acc[0][f][h];
                     U1[r * l1 + n] = acc[1][f][h] - vs;
                 }
@@ -1063,24 +1048,24 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
             }
         }
         // sum over b': A = X1, Y1 rows a; B = -Vs2[b][b'], generated
-        int4 bn[2];
+        int bn[2];
         bool bok[2];
 #pragma unroll
         for (int f = 0; f < 2; f++) {
             const int bb = ng * 16 + f * 8 + g;
             bok[f] = bb < n2;
-            bn[f] = bok[f] ? nr[N1 + bb] : make_int4(0, 0, 0, 0);
+            bn[f] = bok[f] ? nr[N1 + bb] : 0;
         }
         for (int k0 = 0; k0 < N2; k0 += 4) {
             const int k = k0 + tg;
             const double ax = X1[(m0 + g) * l2 + k], ay = Y1[(m0 + g) * l2 + k];
             const bool kok = k < n2;
-            const int4 kn = nr[N1 + k];
+            const int kn = nr[N1 + k];
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const int n0 = ng * 16 + f * 8;
                 if (n0 >= N2) break;
-                const double bv = (kok && bok[f]) ? -V(q2_of(kn, bn[f])) : -0.0;
+                const double bv = (kok && bok[f]) ? -V(q2p(kn, bn[f])) : -0.0;
                 dmma_884(rb[f][0], rb[f][1], ax, bv);
                 dmma_884(xb[f][0], xb[f][1], ay, bv);
             }
@@ -1089,7 +1074,9 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
         if (r1 >= n1) continue;
         const double vd = Vd[r1], sx1 = Sx[r1], sy1 = Sy[r1];
         const double base = vd * (2.0 * sx1 - sy1);
-        const int w1 = rw[r1], i1 = ri[r1];
+        // the ring G of (i_a, i_b, x_a) and the crossed-ring G of (i_a, i_b, x_b) at (a, b) of
+        // the pair's rows in rx; k_update picks each amplitude's value there (or its mirror's)
+        double *out = rx + P.xy0 + (int64_t)r1 * 2 * N2;
 #pragma unroll
         for (int f = 0; f < 2; f++) {
             const int n0 = ng * 16 + f * 8;
@@ -1098,23 +1085,12 @@ __global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ p
             for (int h = 0; h < 2; h++) {
                 const int n = n0 + 2 * tg + h;
                 if (n >= n2) continue;
-                const int r2 = N1 + n, w2 = rw[r2], i2 = ri[r2];
-                // ring amplitude (i_a, i_b, x_a) or its mirror (i_b, i_a, x_b), whichever has
-                // the smaller occupied index first (both on the diagonal pair)
+                const int r2 = N1 + n;
                 if (do_ring) {
                     const double lin = 2.0 * vd * (sx1 + Sx[r2]) - vd * (sy1 + Sy[r2]);
-                    const double v = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ra[f][h] + rb[f][h];
-                    const int p = i1 <= i2 ? __ldg(&gx[w1 + i2]) : -1, pm = i2 <= i1 ? __ldg(&gx[w2 + i1]) : -1;
-                    if (p >= 0) g_rq[p] = v;
-                    if (pm >= 0) g_rq[pm] = v;
+                    out[n] = lin + base * (2.0 * Sx[r2] - Sy[r2]) + ra[f][h] + rb[f][h];
                 }
-                // crossed ring (i_a, i_b, x_b) or its mirror (i_b, i_a, x_a), the same way
-                if (do_xring) {
-                    const double v = xa[f][h] + xb[f][h];
-                    const int p = i1 <= i2 ? __ldg(&gy[w2 + i1]) : -1, pm = i2 <= i1 ? __ldg(&gy[w1 + i2]) : -1;
-                    if (p >= 0) g_xq[p] = v;
-                    if (pm >= 0) g_xq[pm] = v;
-                }
+                if (do_xring) out[N2 + n] = xa[f][h] + xb[f][h];
             }
         }
     }
@@ -1150,7 +1126,7 @@ size_t rings_smem_bytes(int O, int R)
 // mode 0: update (writes t_new, partials e/dT/|R|); mode 1: residual only (|R|).
 // ----------------------------------------------------------------------------
 struct UpdateArgs {
-    const ChunkDev *chunks;
+    const HChunkDev *chunks;
     const SolveDev *solves;
     const AmpInfo *amps;
     const int32_t *partner;
@@ -1166,7 +1142,8 @@ struct UpdateArgs {
     const double *J1;             // dRPA ring intermediate
     double *part_e, *part_dt, *part_r;
     double *g_out;            // optional: full G per amplitude (term checks)
-    const double *g_rq, *g_xq;
+    const double *rx;                          // ring and crossed-ring G, particle-hole layout
+    const int32_t *ph_a, *ph_b;                // where (i, x) sits in it (DevBatch)
     const uint8_t *active;
     int do_ladder, do_mosaic, do_ring, do_xring, do_driver, drpa, mode;
     // Pulay DIIS push fused into the update (mode 0, ndiis > 0): the new (t', e) pair
@@ -1222,11 +1199,56 @@ __global__ void k_ring_index(const ChunkDev *__restrict__ rchunks, const SolveDe
     ridx_y[s.ph0 + e] = posmap(s, pos, k, i, x);
 }
 
+// One CTA per ring pair: where each of its rows (i, x) sits in the particle-hole arrays.
+// Group-1 row a: ph_a = xy0 + 2 a N2 (its X1 row; Y1 follows at + N2), ph_b = N2.  Group-2
+// row b: ph_a = -1, ph_b = b.  (Rows of groups without a -Q partner keep -1, -1.)
+__global__ void k_ph_tables(const RingPairDev *__restrict__ pairs, const SolveDev *__restrict__ solves,
+                            const int16_t *__restrict__ ph_i, const int16_t *__restrict__ ph_x,
+                            int32_t *__restrict__ ph_a, int32_t *__restrict__ ph_b)
+{
+    const RingPairDev P = pairs[blockIdx.x];
+    const SolveDev s = solves[P.solve];
+    const int N2 = (P.n2 + 7) & ~7;
+    for (int r = threadIdx.x; r < P.n1 + P.n2; r += blockDim.x) {
+        const bool g1 = r < P.n1;
+        const int row = g1 ? P.r1 + r : P.r2 + (r - P.n1);
+        const int i = ph_i[s.phr0 + row], x = ph_x[s.phr0 + row];
+        const int64_t k = s.phr0 + (int64_t)i * s.V + (x - s.O);
+        ph_a[k] = g1 ? P.xy0 + 2 * r * N2 : -1;
+        ph_b[k] = g1 ? N2 : r - P.n1;
+    }
+}
+
+// The particle-hole copy of t that k_rings reads, one CTA per {Q, -Q} pair: row a of group
+// 1 gets X1[a][c] = t(i_a i_c, x_a) and Y1[a][c] = t(i_c i_a, x_a) for the rows c of group 2,
+// through the per-row gather indices (ridx_x, ridx_y).  Each CTA writes its pair's rows
+// contiguously; the indexed reads are all this small kernel does, so many of them are in
+// flight at once (in k_rings, behind its DMMA phases, they were what the kernel waited on).
+__global__ void k_ring_stage(const RingPairDev *__restrict__ pairs, const SolveDev *__restrict__ solves,
+                               const int16_t *__restrict__ ph_i, const int32_t *__restrict__ ridx_x,
+                               const int32_t *__restrict__ ridx_y, const double *__restrict__ t,
+                               double *__restrict__ xy, const uint8_t *__restrict__ active)
+{
+    const RingPairDev P = pairs[blockIdx.x];
+    if (!active[P.solve]) return;
+    const SolveDev s = solves[P.solve];
+    const int N2 = (P.n2 + 7) & ~7, O = s.O;
+    for (int e = threadIdx.x; e < P.n1 * P.n2; e += blockDim.x) {
+        const int a = e / P.n2, c = e - a * P.n2;
+        const int64_t w = s.ph0 + (int64_t)(P.r1 + a) * O + ph_i[s.phr0 + P.r2 + c];
+        const int px = __ldg(&ridx_x[w]), py = __ldg(&ridx_y[w]);
+        double *row = xy + P.xy0 + (int64_t)a * 2 * N2;
+        row[c] = px >= 0 ? __ldg(&t[px]) : 0.0;
+        row[N2 + c] = py >= 0 ? __ldg(&t[py]) : 0.0;
+    }
+}
+
 void launch_block_tables(const DevBatch &d, cudaStream_t st)
 {
     if (d.nblocks > 0)
         k_block_tables<<<d.nblocks, 256, 0, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir, d.pcol, d.amps,
                                                   d.pos, d.partner, d.mirror);
+    if (d.nrpairs > 0) k_ph_tables<<<d.nrpairs, 128, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ph_x, d.ph_a, d.ph_b);
     if (d.nrchunks > 0)
         k_ring_index<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.ph_i, d.ph_x, d.pos, d.ridx_x,
                                                     d.ridx_y);
@@ -1256,15 +1278,21 @@ void launch_vcoef(const DevBatch &d, cudaStream_t st)
 // 100 twists of N=54, against the 64-register form).
 __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
 {
-    const ChunkDev ch = A.chunks[blockIdx.x];
+    const HChunkDev ch = A.chunks[blockIdx.x];
     double esum = 0.0, dtmax = 0.0, rmax = 0.0;
     const bool on = A.active[ch.solve];
     const SolveDev s = A.solves[ch.solve];
     const int loc = ch.start + threadIdx.x;
-    if (!on && A.mode == 0 && loc < s.namp) A.t_new[s.amp0 + loc] = A.t[s.amp0 + loc];
-    // By the pair symmetry t(ij,a) = t(ji,b) the amplitudes with i < j also update their
-    // mirrors (j,i,b), whose threads do nothing; every term of G shares the symmetry.
-    const int32_t mir = (on && loc < s.namp) ? A.mirror[s.amp0 + loc] : -2;
+    // The chunks cover the amplitudes i <= j only: by the pair symmetry t(ij,a) = t(ji,b)
+    // each amplitude with i < j also updates its mirror (j,i,b); every term of G shares the
+    // symmetry.
+    const bool valid = loc < ch.end;
+    const int32_t mirv = valid ? A.mirror[s.amp0 + loc] : -2;
+    if (!on && A.mode == 0 && valid) {
+        A.t_new[s.amp0 + loc] = A.t[s.amp0 + loc];
+        if (mirv >= 0) A.t_new[mirv] = A.t[mirv];
+    }
+    const int32_t mir = on ? mirv : -2;
     const double wgt = mir >= 0 ? 2.0 : 1.0;   // energy and DIIS dot weight: this amplitude and its mirror
     if (mir != -2) {
         const int64_t p = s.amp0 + loc;
@@ -1297,9 +1325,23 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
                     g += 2.0 * Jr[l] * A.t[A.partner[pb]];
                 }
             }
-        } else {
-            if (A.do_ring) g += A.g_rq[p];   // rings, linear + quadratic (CCD.f90:716-811)
-            if (A.do_xring) g += A.g_xq[p];  // crossed rings (CCD.f90:845-937)
+        } else if (A.do_ring || A.do_xring) {
+            // k_rings leaves at (a, b) of a {Q, -Q} pair the ring G of (i_a, i_b, x_a) and the
+            // crossed-ring G of (i_a, i_b, x_b), a in group 1; this amplitude's value sits there
+            // or at its mirror's (j, i, b), whichever has its row in group 1
+            const int32_t *pa = A.ph_a + s.phr0, *pb = A.ph_b + s.phr0;
+            const int V = s.V;
+            if (A.do_ring) {   // rings, linear + quadratic (CCD.f90:716-811)
+                const int ia = i * V + a - O, jb = j * V + b - O;
+                const int ra = __ldg(&pa[ia]);
+                g += ra >= 0 ? A.rx[ra + __ldg(&pb[jb])] : A.rx[__ldg(&pa[jb]) + __ldg(&pb[ia])];
+            }
+            if (A.do_xring) {  // crossed rings (CCD.f90:845-937)
+                const int ib = i * V + b - O, ja = j * V + a - O;
+                const int xa = __ldg(&pa[ib]);
+                g += xa >= 0 ? A.rx[xa + __ldg(&pb[ib]) + __ldg(&pb[ja])]
+                             : A.rx[__ldg(&pa[ja]) + __ldg(&pb[ja]) + __ldg(&pb[ib])];
+            }
         }
         {   // core pair: every term has a zero factor (CoreN read on its own: taken from the
             // solve record above, it costs this kernel registers)
@@ -1492,15 +1534,20 @@ __global__ void k_active_swap(int nsolves, uint8_t *__restrict__ active, const u
 }
 
 // t <- t_new for the solves still iterating this round (replay mode)
-__global__ void k_commit(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
-                         const double *__restrict__ t_new, double *__restrict__ t,
-                         const uint8_t *__restrict__ active)
+__global__ void k_commit(const HChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                         const int32_t *__restrict__ mirror, const double *__restrict__ t_new,
+                         double *__restrict__ t, const uint8_t *__restrict__ active)
 {
-    const ChunkDev ch = chunks[blockIdx.x];
+    const HChunkDev ch = chunks[blockIdx.x];
     if (!active[ch.solve]) return;
     const SolveDev s = solves[ch.solve];
     const int loc = ch.start + threadIdx.x;
-    if (loc < s.namp) t[s.amp0 + loc] = t_new[s.amp0 + loc];
+    if (loc >= ch.end) return;
+    const int64_t p = s.amp0 + loc;
+    const double x = t_new[p];
+    t[p] = x;
+    const int32_t mir = mirror[p];
+    if (mir >= 0) t[mir] = x;
 }
 
 __global__ void k_diis_rows2(const int *__restrict__ chunk_begin, const IterState *__restrict__ st, int ndiis,
@@ -1521,19 +1568,18 @@ __global__ void k_diis_rows2(const int *__restrict__ chunk_begin, const IterStat
 }
 
 // t = sum_j c_j t'_j over the amplitudes i <= j, each also written to its mirror (j,i,b)
-__global__ void k_diis_extrap2(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+__global__ void k_diis_extrap2(const HChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
                                int64_t namp, const double *__restrict__ hist_t, const double *__restrict__ coef,
                                int ndiis, const int32_t *__restrict__ mirror, double *__restrict__ t,
                                const uint8_t *__restrict__ active)
 {
-    const ChunkDev ch = chunks[blockIdx.x];
+    const HChunkDev ch = chunks[blockIdx.x];
     if (!active[ch.solve]) return;
     const SolveDev s = solves[ch.solve];
     const int loc = ch.start + threadIdx.x;
-    if (loc >= s.namp) return;
+    if (loc >= ch.end) return;
     const int64_t p = s.amp0 + loc;
     const int32_t mir = mirror[p];
-    if (mir == -2) return;
     const double *c = coef + ch.solve * kMaxDiis;
     double x = 0.0;
     for (int jv = 0; jv < ndiis; jv++) {
@@ -1576,15 +1622,15 @@ int launch_iteration(const DevBatch &d, const CtlBuffers &c, const TermFlags &f,
     // the DIIS push (history slot and e . e_j partials) happens inside k_update
     int n = launch_residual(d, f, 0, nullptr, st, kt, &c, ndiis);
     if (ndiis > 0) {
-        k_diis_rows2<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, c.state, ndiis, c.part, c.brow, d.active);
+        k_diis_rows2<<<d.nsolves, 256, 0, st>>>(d.hchunk_begin, c.state, ndiis, c.part, c.brow, d.active);
         n += 1;
     }
     launch_control(d, c, tol, max_iter, ndiis, 0, st);
     if (ndiis > 0)
-        k_diis_extrap2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.namp, c.hist_t, c.coef, ndiis, d.mirror,
+        k_diis_extrap2<<<d.nhchunks, kChunk, 0, st>>>(d.hchunks, d.solves, d.namp, c.hist_t, c.coef, ndiis, d.mirror,
                                                      d.t, d.active);
     else
-        k_commit<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.t_new, d.t, d.active);
+        k_commit<<<d.nhchunks, kChunk, 0, st>>>(d.hchunks, d.solves, d.mirror, d.t_new, d.t, d.active);
     launch_active_swap(d, c, st);
     return n + 3;
 }
@@ -1774,7 +1820,7 @@ void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
 const char *kKernelNames[KID_COUNT] = {"k_mp2",      "k_energy",   "k_ladder_hh", "k_ladder",
                                       "k_mosaic_blk", "k_mosaic_sum", "k_ring_int", "k_update",
                                       "k_reduce_solves", "k_rings",
-                                      "k_ladder_tc"};
+                                      "k_ladder_tc", "k_ring_stage"};
 
 int tune_rings(DevBatch &d, cudaStream_t st)
 {
@@ -1790,8 +1836,7 @@ int tune_rings(DevBatch &d, cudaStream_t st)
             for (int th : kCand) {
                 auto run = [&]() {
                     k_rings<<<d.nring[c], th, d.ring_smem[c], st>>>(d.rpairs + off, d.solves, d.ph_i, d.ph_x,
-                                                                    d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, 1, 1,
-                                                                    d.g_rq, d.g_xq, d.active);
+                                                                    d.nvp, d.vtab, d.xy, 1, 1, d.rx, d.active);
                 };
                 run();  // warm
                 cudaEventRecord(e0, st);
@@ -1858,41 +1903,48 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         n++;
     }
     if ((f.do_ring || f.do_xring) && !f.drpa) {
+        kt->begin(KID_RING_STAGE, st);
+        k_ring_stage<<<d.nrpairs, 128, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy, d.active);
+        kt->end(st);
+        n++;
         kt->begin(KID_RINGS, st);
         // pair classes (sorted in this order): DMMA tiles in two shared-memory sizes, then the FMA form
         int off = 0;
         for (int c = 0; c < kRingClasses; c++) {
-            if (d.nring[c] > 0)
+            if (d.nring[c] > 0) {
                 k_rings<<<d.nring[c], d.ring_threads[c], d.ring_smem[c], st>>>(
-                    d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.ridx_x, d.ridx_y, d.nv4, d.vtab, d.t, f.do_ring,
-                    f.do_xring, d.g_rq, d.g_xq, d.active);
+                    d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.nvp, d.vtab, d.xy, f.do_ring, f.do_xring, d.rx,
+                    d.active);
+                n++;
+            }
             off += d.nring[c];
         }
-        if (d.nring[kRingClasses] > 0)
+        if (d.nring[kRingClasses] > 0) {
             k_rings_wide<<<d.nring[kRingClasses], 256, d.ring_smem[kRingClasses], st>>>(d.rpairs + off, d.solves, d.ph_i, d.ph_x, d.pos,
                                                                  d.partner, d.nv4, d.vtab, d.t, f.do_ring,
-                                                                 f.do_xring, d.g_rq, d.g_xq, d.active);
+                                                                 f.do_xring, d.rx, d.active);
+            n++;
+        }
         kt->end(st);
-        n++;
     }
     UpdateArgs A;
-    A.chunks = d.chunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.mirror = d.mirror; A.pos = d.pos;
+    A.chunks = d.hchunks; A.solves = d.solves; A.amps = d.amps; A.partner = d.partner; A.mirror = d.mirror; A.pos = d.pos;
     A.nv4 = d.nv4; A.eigen = d.eigen; A.vtab = d.vtab; A.t = d.t; A.t_new = d.t_new; A.g_ladder = d.g;
     A.jvv = d.jvv; A.joo = d.joo; A.J1 = d.J1;
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
-    A.g_rq = d.g_rq; A.g_xq = d.g_xq;
+    A.rx = d.rx; A.ph_a = d.ph_a; A.ph_b = d.ph_b;
     A.st = diis ? diis->state : nullptr; A.ndiis = (diis && mode == 0) ? ndiis : 0; A.namp = d.namp;
     A.hist_t = diis ? diis->hist_t : nullptr; A.hist_e = diis ? diis->hist_e : nullptr;
     A.dpart = diis ? diis->part : nullptr;
     A.vcoef = d.vcoef;
     kt->begin(KID_UPDATE, st);
-    k_update<<<d.nchunks, kChunk, 0, st>>>(A);
+    k_update<<<d.nhchunks, kChunk, 0, st>>>(A);
     kt->end(st);
     n++;
     kt->begin(KID_REDUCE, st);
-    k_reduce_solves<<<d.nsolves, 256, 0, st>>>(d.chunk_begin, d.part_e, d.part_dt, d.part_r, d.red);
+    k_reduce_solves<<<d.nsolves, 256, 0, st>>>(d.hchunk_begin, d.part_e, d.part_dt, d.part_r, d.red);
     kt->end(st);
     n++;
     return n;

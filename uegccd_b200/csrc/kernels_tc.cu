@@ -16,8 +16,9 @@
 // Both FP16 operands are written to global memory already in the MMA's canonical
 // shared-memory layout, one 32-wide K chunk after another: the Coulomb slabs once per
 // batch (they depend only on the |q|^2 tables; k_w16_build) and the scaled d tiles once
-// per iteration (k_delta16).  The MMA kernel then only streams chunks into shared memory
-// with 16-byte cp.async copies.
+// per iteration (k_delta16).  Each chunk of each operand is then one contiguous range, and
+// the MMA kernel streams it into shared memory with one bulk copy of the TMA engine
+// (cp.async.bulk, completing on the stage's mbarrier).
 //
 // Shared-memory operands use the canonical K-major layout without swizzle: 8 x 8
 // element core matrices (8 rows of 16 bytes), core matrices adjacent in K 128 bytes
@@ -128,9 +129,20 @@ __device__ __forceinline__ int q2_of(int4 x, int4 y)
 // SBO = 256 halves (512 B)
 __device__ __forceinline__ int cm_off(int row, int k) { return (row & 7) * 8 + (row >> 3) * 256 + (k & 7) + (k >> 3) * 64; }
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+// The bulk-copy (TMA) engine: one contiguous global range into this CTA's shared memory,
+// completing `bytes` of the transaction count of an mbarrier.  Addresses 16-byte aligned,
+// sizes multiples of 16; this GPU's own memory only, no multicast.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
 }  // namespace
@@ -228,8 +240,10 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
     __shared__ alignas(1024) __half As[kStages][kTcM * kTcK];
     __shared__ alignas(1024) __half Bs[kStages][NP * kTcK];
     __shared__ float rscale[NP];
-    __shared__ alignas(8) uint64_t mbar[kStages];
+    __shared__ alignas(8) uint64_t mbar[kStages];   // the MMAs of the stage's chunk are done
+    __shared__ alignas(8) uint64_t full[kStages];   // the stage's chunk has landed (bulk copies)
     __shared__ uint32_t tmem_base;
+    __shared__ int ok_all;
 
     const LadderTile T = tiles[blockIdx.x];
     const TcTileDev X = tcx[blockIdx.x];
@@ -244,7 +258,11 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int b = 0; b < kStages; b++) mbar_init(&mbar[b], 1);
+        for (int b = 0; b < kStages; b++) {
+            mbar_init(&mbar[b], 1);
+            mbar_init(&full[b], 1);
+        }
+        ok_all = 1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int pp = tid; pp < NP; pp += blockDim.x) rscale[pp] = dscale[X.soff + pp];
@@ -255,29 +273,26 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
     const uint32_t idesc = idesc_f16(kTcM, NP);
     const int nchunks = (v + kTcK - 1) / kTcK;
     bool ok = true;
-    // chunk c of the Coulomb slab (8 KB) and of the d tile (NP x 64 B), already in the
-    // canonical layout, into stage buffer c % kStages: 16-byte copies, one commit group
-    // per chunk (empty past the last chunk, so the group count stays regular)
-    auto issue = [&](int c) {
-        if (c < nchunks) {
+    if (tid == 0) {
+        // chunk c of the Coulomb slab (8 KB) and of the d tile (NP x 64 B) into stage c % kStages:
+        // one bulk copy each, both completing on full[stage]
+        constexpr uint32_t kWBytes = kTcM * kTcK * 2, kDBytes = NP * kTcK * 2;
+        int issued = 0;
+        auto issue = [&](int c) {
             const int b = c % kStages;
-            const uint4 *wsrc = reinterpret_cast<const uint4 *>(w16 + X.woff + (int64_t)c * kTcM * kTcK);
-            const uint4 *dsrc = reinterpret_cast<const uint4 *>(d16 + X.doff + (int64_t)c * NP * kTcK);
-            uint4 *wdst = reinterpret_cast<uint4 *>(&As[b][0]);
-            uint4 *ddst = reinterpret_cast<uint4 *>(&Bs[b][0]);
-            for (int e = tid; e < kTcM * kTcK / 8; e += blockDim.x) cp_async16(wdst + e, wsrc + e);
-            for (int e = tid; e < NP * kTcK / 8; e += blockDim.x) cp_async16(ddst + e, dsrc + e);
-        }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
-    for (int c = 0; c < kStages - 1; c++) issue(c);
-    for (int ch = 0; ch < nchunks; ch++) {
-        const int st = ch % kStages;
-        // chunk ch landed (its group and all older ones; kStages - 2 newer may be pending)
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+            mbar_expect_tx(&full[b], kWBytes + kDBytes);
+            bulk_g2s(&As[b][0], w16 + X.woff + (int64_t)c * kTcM * kTcK, kWBytes, &full[b]);
+            bulk_g2s(&Bs[b][0], d16 + X.doff + (int64_t)c * NP * kTcK, kDBytes, &full[b]);
+            issued = c + 1;
+        };
+        for (int c = 0; c < kStages && c < nchunks; c++) issue(c);
+        int ch = 0;
+        for (; ch < nchunks && ok; ch++) {
+            const int st = ch % kStages;
+            if (!mbar_wait(&full[st], (ch / kStages) & 1)) {
+                ok = false;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t a0 = smem_u32(&As[st][0]), b0 = smem_u32(&Bs[st][0]);
 #pragma unroll
@@ -285,15 +300,27 @@ __global__ void __launch_bounds__(128) k_ladder_tc(const LadderTile *__restrict_
                 tc_mma(tmem_d, sdesc(a0 + j * 256, 128, 512), sdesc(b0 + j * 256, 128, 512), idesc,
                        (ch > 0 || j > 0) ? 1u : 0u);
             tc_commit(&mbar[st]);
+            // the previous chunk's stage refills once its MMAs are done, while chunk ch's run
+            if (ch >= 1 && ch - 1 + kStages < nchunks) {
+                const int prev = ch - 1;
+                if (!mbar_wait(&mbar[prev % kStages], (prev / kStages) & 1)) {
+                    ok = false;
+                    ch++;
+                    break;
+                }
+                issue(prev + kStages);
+            }
         }
-        // refill the buffer of chunk ch - 1 once its MMA is done, while MMA ch runs
-        const int nx = ch + kStages - 1;
-        if (nx < nchunks && nx >= kStages && !mbar_wait(&mbar[nx % kStages], ((nx - kStages) / kStages) & 1))
-            ok = false;
-        issue(nx);
+        if (!ok) {
+            // let every bulk copy still in flight land before the CTA leaves (bounded)
+            for (int c = ch; c < issued; c++) mbar_wait(&full[c % kStages], (c / kStages) & 1);
+            ok_all = 0;
+        }
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    if (!mbar_wait(&mbar[(nchunks - 1) % kStages], ((nchunks - 1) / kStages) & 1)) ok = false;
+    __syncthreads();
+    if (!ok_all) ok = false;
+    // the last chunk's MMAs (and with them all earlier ones) are done
+    if (ok && !mbar_wait(&mbar[(nchunks - 1) % kStages], ((nchunks - 1) / kStages) & 1)) ok = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);

@@ -86,17 +86,29 @@ struct AmpInfo {
 };
 
 // One pair of particle-hole groups {Q, -Q}: rows [r1, r1+n1) have n_x - n_i = Q,
-// rows [r2, r2+n2) have -Q (rows local to the solve).  All ring and crossed-ring
-// products between the two groups are formed by one CTA.
+// rows [r2, r2+n2) have -Q (rows local to the solve); group 1 is the smaller one.  All
+// ring and crossed-ring products between the two groups are formed by one CTA.
+// xy0: where the pair's operands and results start (in doubles) in the batch's
+// particle-hole arrays: row a < n1 of group 1 holds 2 round8(n2) doubles -- in xy the
+// amplitudes X1[a][b] = t(i_a i_b, x_a) then Y1[a][b] = t(i_b i_a, x_a), in rx the ring G
+// of (i_a, i_b, x_a) then the crossed-ring G of (i_a, i_b, x_b), b over group 2.
 struct RingPairDev {
     int solve;
     int r1, n1;
     int r2, n2;
+    int32_t xy0;
 };
 
 struct ChunkDev {
     int solve;
     int32_t start;          // first amplitude of the chunk, local to the solve
+};
+
+// A chunk of the amplitudes i <= j (the rows a block keeps; each mirror row follows from
+// its pair): [start, end) local to the solve, at most kChunk long, inside one block.
+struct HChunkDev {
+    int solve;
+    int32_t start, end, pad;
 };
 
 }  // namespace uegccd

@@ -58,6 +58,7 @@ def _lib():
         L.uegccd_find_tol.restype = None
         L.uegccd_host_last_error.restype = C.c_char_p
         L.uegccd_heg_exchange_sf.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_double)]
+        L.uegccd_heg_twists.argtypes = [vp, C.c_int32, P(C.c_double), P(C.c_int32), P(C.c_double), P(C.c_double)]
         _bound = True
     return L
 
@@ -140,6 +141,23 @@ class Heg:
         eig = np.ctypeslib.as_array(s.eigen, shape=(s.nao,)).copy()
         nv = np.ctypeslib.as_array(s.nvec, shape=(3, s.nao)).T.copy()
         return s.nocc, s.L, s.madelung, eig, nv
+
+    def twist_systems(self, twists):
+        """The systems (nocc, L, madelung, eigen, nvec) of many twists, set up on the GPU in
+        one launch (uegccd_heg_twists), and their E_HF: bit-equal to change_twist then system()
+        for each twist.  The set-up itself is left unchanged."""
+        tw = np.ascontiguousarray(np.asarray(twists, dtype=np.float64).reshape(-1, 3))
+        info = self.info()
+        T, M = tw.shape[0], info["nao"]
+        nv = np.zeros((T, 3, M), dtype=np.int32)
+        eig = np.zeros((T, M))
+        ehf = np.zeros(T)
+        capi.check(_lib().uegccd_heg_twists(self._h, T, tw.ctypes.data_as(C.POINTER(C.c_double)),
+                                            nv.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            eig.ctypes.data_as(C.POINTER(C.c_double)),
+                                            ehf.ctypes.data_as(C.POINTER(C.c_double))))
+        systems = [(info["nocc"], info["L"], info["madelung"], eig[k], nv[k].T.copy()) for k in range(T)]
+        return systems, ehf
 
     def context(self):
         from .solver import Context

@@ -152,6 +152,26 @@ class Batch:
             capi.check(rc)
         return rc, e2, [r.as_dict() for r in res]
 
+    def start(self, drpa: bool = False, **opts) -> np.ndarray:
+        """Opens an incremental solve (uegccd_batch_start): the MP2 start of every system;
+        returns E(2).  advance() then iterates and hands back the solves that stopped."""
+        o = capi.default_options(**opts)
+        if drpa and "fail_ratio" not in opts:
+            o.fail_ratio = 1.0e4
+        e2 = np.zeros(self.n)
+        capi.check(capi.lib().uegccd_batch_start(self._h, C.byref(o), 1 if drpa else 0, capi.dptr(e2)))
+        self._done_ids = (C.c_int32 * self.n)()
+        self._done_res = (capi.Result * self.n)()
+        return e2
+
+    def advance(self, rounds: int = 1):
+        """Up to `rounds` rounds of four iterations; returns (solves still iterating,
+        [(solve index, result dict) of every solve that stopped since the last call])."""
+        na, nd = C.c_int32(), C.c_int32()
+        capi.check(capi.lib().uegccd_batch_advance(self._h, int(rounds), C.byref(na), C.byref(nd), self._done_ids,
+                                                     self._done_res))
+        return na.value, [(int(self._done_ids[k]), self._done_res[k].as_dict()) for k in range(nd.value)]
+
     def set_integrals(self, core_n: int = 0, gapii: float = 0.0) -> None:
         """CoreN and GapII of the integrals for the calls that follow (CoreERI/GapERI)."""
         capi.check(capi.lib().uegccd_batch_set_integrals(self._h, int(core_n), float(gapii)))
