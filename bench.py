@@ -42,7 +42,7 @@ SEED = 2024
 # checks it every run.  Used to turn the oracle's time per iteration into a time per solve.
 REF_ITERS_PER_SOLVE = 33.16  # measured: replay mode on this workload, 100 twists (min 30, max 35)
 SOLVE_OPTS = dict(scheme=1, ndiis=6, denom_factor=1.0, tol=1e-9)
-E2E_CREATORS = 2   # host threads creating the next batches of the e2e pipeline
+E2E_CREATORS = 1   # host threads creating the next batches of the e2e pipeline
 # Nominal FP64 peak of a B200 (datasheet); the bench measures it each run with the register-only
 # probe of bench_peak.cu (37.0 TFLOP/s measured on B200) and uses this only if the probe fails.
 FP64_PEAK_TFLOPS = 37.0
@@ -379,12 +379,11 @@ def run_gpu(args, rank, world):
     total_ms = float(sum(step_ms))
     # e2e: through the C ABI with host buffers, every step: batch create (plan, uploads),
     # solve, and every twist's T2 read back into page-locked host memory.  The stages run
-    # at once, as a serving host runs them: the next two steps' batches are created on two
-    # host threads (a create is mostly host work and takes longer than a solve), this step
-    # solves, and the previous step's amplitudes are downloaded on another thread (the C
-    # calls release the GIL; each batch has its own stream).  The timed run starts before
-    # its first create and ends after its last download: the pipeline's fill and drain are
-    # inside it.
+    # at once, as a serving host runs them: the next step's batch is created on a host
+    # thread (E2E_CREATORS), this step solves, and the previous step's amplitudes are
+    # downloaded on another thread (the C calls release the GIL; each batch has its own
+    # stream).  The timed run starts before its first create and ends after its last
+    # download: the pipeline's fill and drain are inside it.
     out_bufs = [pinned_buffer(batch.amplitude_count()) for _ in range(2)]
     xfer = [0, 0]
     stage_ms = {"create": [], "solve": [], "download": []}   # host wall time of each stage
@@ -652,8 +651,8 @@ def main(argv=None):
                     "d2h_bytes_per_step": g["d2h"], "stage_ms_median": g["e2e_stage_ms"],
                     "ms_per_step_runs": g["e2e_runs_ms"],
                     "note": "per step: batch create (plan + uploads), solve, T2 of every twist to page-locked host "
-                            "memory; creates of the next two steps (two host threads) and the download of the "
-                            "previous one overlap the solve"},
+                            f"memory; the create of the next step ({E2E_CREATORS} host thread(s)) and the download of "
+                            "the previous one overlap the solve"},
             "gpu_launches": int(g["launches_per_step"]) * args.steps,
             "clocks": g["clocks"], "roofline": roof,
             "kernels": {k: {"ms": v[0], "launches": v[1], **({"roofline": kern[k]} if k in kern else {})}

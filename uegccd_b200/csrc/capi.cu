@@ -9,6 +9,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
+#include <deque>
+#include <condition_variable>
+#include <atomic>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -33,7 +37,62 @@ namespace {
 
 thread_local std::string g_last_error;
 
-// Runs f(0..n-1) on up to nthreads host threads (static interleaved split).
+// A persistent pool of host threads (one per core) for the parallel parts of batch creation
+// and downloads: starting threads per call cost more than the work of a small batch.  Several
+// callers (the creator threads of a pipelined host) share it.
+class HostPool {
+public:
+    explicit HostPool(int n)
+    {
+        for (int k = 0; k < n; k++)
+            th_.emplace_back([this]() {
+                for (;;) {
+                    std::function<void()> job;
+                    {
+                        std::unique_lock<std::mutex> lock(mu_);
+                        cv_.wait(lock, [this]() { return stop_ || !q_.empty(); });
+                        if (stop_ && q_.empty()) return;
+                        job = std::move(q_.front());
+                        q_.pop_front();
+                    }
+                    job();
+                }
+            });
+    }
+    ~HostPool()
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void post(std::function<void()> job)
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            q_.push_back(std::move(job));
+        }
+        cv_.notify_one();
+    }
+
+private:
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> q_;
+    std::vector<std::thread> th_;
+    bool stop_ = false;
+};
+
+HostPool &host_pool()
+{
+    static HostPool pool(std::max(1, (int)std::thread::hardware_concurrency()));
+    return pool;
+}
+
+// Runs f(0..n-1) on the calling thread and up to nthreads - 1 pool threads; items are taken
+// in turn from a shared counter, and each f(i) writes only its own outputs.
 template <class F>
 void parallel_for(int n, int nthreads, F f)
 {
@@ -41,12 +100,25 @@ void parallel_for(int n, int nthreads, F f)
         for (int i = 0; i < n; i++) f(i);
         return;
     }
-    std::vector<std::thread> th;
-    for (int t = 0; t < nthreads; t++)
-        th.emplace_back([&, t]() {
-            for (int i = t; i < n; i += nthreads) f(i);
+    struct Shared {
+        std::atomic<int> next{0};
+        std::mutex mu;
+        std::condition_variable cv;
+        int finished = 0;
+    } sh;
+    const int helpers = std::min(nthreads, n) - 1;
+    auto body = [&]() {
+        for (int i; (i = sh.next.fetch_add(1)) < n;) f(i);
+    };
+    for (int k = 0; k < helpers; k++)
+        host_pool().post([&]() {
+            body();
+            std::lock_guard<std::mutex> lock(sh.mu);
+            if (++sh.finished == helpers) sh.cv.notify_one();
         });
-    for (auto &x : th) x.join();
+    body();
+    std::unique_lock<std::mutex> lock(sh.mu);
+    sh.cv.wait(lock, [&]() { return sh.finished == helpers; });
 }
 
 int fail(int code, const std::string &msg)
@@ -437,17 +509,35 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<DTileDev> dtiles;
     int64_t w16_n = 0, d16_n = 0;
     int nscale = 0;
-    std::vector<ChunkDev> chunks, rchunks;
+    // the large host tables live in vectors kept per creating thread between creates: a
+    // fresh allocation would page-fault on first touch, which cost more than filling them
+    struct HostTables {
+        std::vector<ChunkDev> chunks, rchunks;
+        std::vector<int2> targets;
+        std::vector<int16_t> pair_i, pair_j, vir, pcol, ph_i, ph_x;
+        std::vector<int4> nv4;
+        std::vector<int> nvp;
+        std::vector<double> eigen;
+    };
+    static thread_local HostTables ht;
+    auto &chunks = ht.chunks, &rchunks = ht.rchunks;
+    auto &targets = ht.targets;
+    auto &pair_i = ht.pair_i, &pair_j = ht.pair_j, &vir = ht.vir;
+    auto &pcol = ht.pcol;   // beside vir: the partner's column in the same block
+    auto &nv4 = ht.nv4;
+    auto &nvp = ht.nvp;     // beside nv4: packed a component per byte
+    auto &eigen = ht.eigen;
+    auto &ph_i = ht.ph_i, &ph_x = ht.ph_x;
+    for (auto *v : {&chunks, &rchunks}) v->clear();
+    targets.clear();
+    for (auto *v : {&pair_i, &pair_j, &vir, &pcol, &ph_i, &ph_x}) v->clear();
+    nv4.clear();
+    nvp.clear();
+    eigen.clear();
     std::vector<int> chunk_begin(n + 1, 0);
-    std::vector<int2> targets;
-    std::vector<int16_t> pair_i, pair_j, vir;
-    std::vector<int16_t> pcol;   // beside vir: the partner's column in the same block
-    std::vector<int4> nv4;
-    std::vector<int> nvp;   // beside nv4: packed a component per byte
-    std::vector<double> eigen, vtab;
+    std::vector<double> vtab;
     std::vector<int64_t> hh0;
     std::vector<RingPairDev> rpairs;
-    std::vector<int16_t> ph_i, ph_x;
     int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0, mrows = 0, mcols = 0;
     std::vector<int> s_t0(n);   // first mosaic target of each solve
     int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_v = 0, max_occ = 0;
@@ -595,32 +685,18 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     // mosaic targets: Jvv(c) adds the column sums of c over the blocks holding it, Joo(k)
     // the row sums of the pairs (k, l); both in block order
     for (auto &bd : blocks) bd.col0 += mrows;
-    std::vector<int32_t> mt_start(targets.size() + 1, 0);
-    parallel_for(n, nthreads, [&](int s) {
-        const SolvePlan &P = b->plans[s];
-        for (const auto &B : P.blocks) {
-            for (int c = 0; c < B.v; c++) mt_start[s_t0[s] + (P.vir[B.vir0 + c] - P.O) + 1]++;
-            for (int r = 0; r < B.o; r++) mt_start[s_t0[s] + P.V + P.pair_i[B.pair0 + r] + 1]++;
-        }
-    });
-    for (size_t k = 0; k + 1 < mt_start.size(); k++) mt_start[k + 1] += mt_start[k];
-    std::vector<int32_t> mt_list(mt_start.back());
-    parallel_for(n, nthreads, [&](int s) {
-        const SolvePlan &P = b->plans[s];
-        std::vector<int> fill(P.V + P.O, 0);
-        for (size_t bi = 0; bi < P.blocks.size(); bi++) {
-            const auto &B = P.blocks[bi];
-            const BlockDev &bd = blocks[solves[s].blk0 + bi];
-            for (int c = 0; c < B.v; c++) {
-                const int y = P.vir[B.vir0 + c] - P.O;
-                mt_list[mt_start[s_t0[s] + y] + fill[y]++] = (int32_t)(bd.col0 + c);
-            }
-            for (int r = 0; r < B.o; r++) {
-                const int y = P.V + P.pair_i[B.pair0 + r];
-                mt_list[mt_start[s_t0[s] + y] + fill[y]++] = (int32_t)(bd.row0 + r);
-            }
-        }
-    });
+    // the lists themselves are built on the device (k_mosaic_targets); here only each solve's
+    // first target and first list entry
+    std::vector<int64_t> mt_lbase(n + 1, 0);
+    int max_vo = 0;
+    for (int s = 0; s < n; s++) {
+        int64_t e = 0;
+        for (const auto &B : b->plans[s].blocks) e += (int64_t)B.o + B.v;
+        mt_lbase[s + 1] = mt_lbase[s] + e;
+        max_vo = std::max(max_vo, b->plans[s].V + b->plans[s].O);
+    }
+    if (mt_lbase[n] >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit mosaic lists");
+    if ((size_t)max_vo * sizeof(int) > 200 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "NAO too large for the mosaic lists");
     if (mrows + mcols >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit mosaic indices");
     trace.mark("ph+mosaic");
 
@@ -734,8 +810,12 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.hchunk_begin, hchunk_begin))) return rc;
     if ((rc = b->upload(d.targets, targets))) return rc;
     if ((rc = b->upload(d.pcol, pcol))) return rc;
-    if ((rc = b->upload(d.mt_start, mt_start))) return rc;
-    if ((rc = b->upload(d.mt_list, mt_list))) return rc;
+    int *d_tbase = nullptr;
+    int64_t *d_lbase = nullptr;
+    if ((rc = b->upload(d_tbase, s_t0))) return rc;
+    if ((rc = b->upload(d_lbase, mt_lbase))) return rc;
+    if ((rc = b->alloc(d.mt_start, targets.size() + 1))) return rc;
+    if ((rc = b->alloc(d.mt_list, (size_t)mt_lbase[n]))) return rc;
     if ((rc = b->alloc(d.mpart, mrows + mcols))) return rc;
     if ((rc = b->upload(d.pair_i, pair_i))) return rc;
     if ((rc = b->upload(d.pair_j, pair_j))) return rc;
@@ -786,6 +866,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     CU(cudaMemsetAsync(d.xy, 0, (size_t)d.xy_n * sizeof(double), b->stream));      // padding columns stay 0
 
     launch_block_tables(d, b->stream);
+    launch_mosaic_targets(d, d_tbase, d_lbase, (size_t)max_vo * sizeof(int), b->stream);
     launch_vcoef(d, b->stream);
     size_t dn = 0;
     for (int s = 0; s < n; s++) dn = std::max(dn, (size_t)b->plans[s].O * b->plans[s].O * b->plans[s].V);

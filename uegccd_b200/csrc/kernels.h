@@ -203,6 +203,9 @@ void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, in
 // pos (pre-set to -1), amps, partner, mirror from the block structure; the particle-hole
 // tables ph_a, ph_b (pre-set to -1) from the ring pairs; the ring gather indices
 void launch_block_tables(const DevBatch &d, cudaStream_t st);
+// mt_start / mt_list of the mosaic sums from the blocks (tbase: each solve's first target;
+// lbase: its first list entry; smem: (max V + O) ints)
+void launch_mosaic_targets(const DevBatch &d, const int *tbase, const int64_t *lbase, size_t smem, cudaStream_t st);
 // Mixed precision: FP16 tcgen05 ladder of t - t_ref added to g (plus g_ref); writes the
 // scaled FP16 d tiles first (d.w16 must be built)
 void launch_ladder_tc(const DevBatch &d, const double *t_ref, const double *g_ref, int *err, cudaStream_t st);

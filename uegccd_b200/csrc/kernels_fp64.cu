@@ -608,6 +608,62 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
 }
 
 // One warp per target: targets (s, y < V) are Jvv(c = O + y), (s, y >= V) are Joo(k = y - V).
+// The per-target lists k_mosaic_sum adds, built once per batch, one CTA per solve: target y
+// < V (the virtual O + y) lists the column partials of every block holding that virtual,
+// target V + k the row partials of the pair rows (k, l); both in block order, the order
+// k_mosaic_sum then adds them in.  A virtual is one column of a block at most, and an
+// occupied k the first index of one row at most (l = K - k), so within a block the targets
+// are distinct and the block's entries go in at once.  mt_start[tbase[s] + y] is the first
+// entry of target y of solve s (entries from lbase[s] on); the last solve also writes the
+// end sentinel.  cnt: V + O ints of dynamic shared memory.
+__global__ void k_mosaic_targets(const SolveDev *__restrict__ solves, const BlockDev *__restrict__ blocks,
+                                 const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
+                                 const int *__restrict__ tbase, const int64_t *__restrict__ lbase,
+                                 int32_t *__restrict__ mt_start, int32_t *__restrict__ mt_list)
+{
+    extern __shared__ int cnt[];
+    const int sv = blockIdx.x;
+    const SolveDev S = solves[sv];
+    const int nt = S.V + S.O, t0 = tbase[sv];
+    for (int y = threadIdx.x; y < nt; y += blockDim.x) cnt[y] = 0;
+    __syncthreads();
+    for (int bi = 0; bi < S.nblk; bi++) {
+        const BlockDev B = blocks[S.blk0 + bi];
+        for (int c = threadIdx.x; c < B.v; c += blockDim.x) atomicAdd(&cnt[vir[B.vir0 + c] - S.O], 1);
+        for (int r = threadIdx.x; r < B.o; r += blockDim.x) atomicAdd(&cnt[S.V + pair_i[B.pair0 + r]], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t run = lbase[sv];
+        for (int y = 0; y < nt; y++) {
+            mt_start[t0 + y] = (int32_t)run;
+            run += cnt[y];
+            cnt[y] = 0;
+        }
+        mt_start[t0 + nt] = (int32_t)run;   // the next solve's first entry, or the end sentinel
+    }
+    __syncthreads();
+    for (int bi = 0; bi < S.nblk; bi++) {
+        const BlockDev B = blocks[S.blk0 + bi];
+        for (int c = threadIdx.x; c < B.v; c += blockDim.x) {
+            const int y = vir[B.vir0 + c] - S.O;
+            mt_list[mt_start[t0 + y] + cnt[y]++] = (int32_t)(B.col0 + c);
+        }
+        for (int r = threadIdx.x; r < B.o; r += blockDim.x) {
+            const int y = S.V + pair_i[B.pair0 + r];
+            mt_list[mt_start[t0 + y] + cnt[y]++] = (int32_t)(B.row0 + r);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_mosaic_targets(const DevBatch &d, const int *tbase, const int64_t *lbase, size_t smem, cudaStream_t st)
+{
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_mosaic_targets, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_mosaic_targets<<<d.nsolves, 256, smem, st>>>(d.solves, d.blocks, d.vir, d.pair_i, tbase, lbase, d.mt_start,
+                                                   d.mt_list);
+}
+
 __global__ void __launch_bounds__(256) k_mosaic_sum(const int2 *__restrict__ targets, int ntargets,
                                                    const SolveDev *__restrict__ solves,
                                                    const int32_t *__restrict__ mt_start,

@@ -10,8 +10,11 @@ Requests (N, rs, basis ratio M/(N/2), twist, method) arrive over time.
   part of the budget, groups them by method and starts each group as a cohort: one batch
   on its own CUDA stream, driven by its own host thread.  With a batching window
   (batch_window seconds, default 0) it first lets requests gather: it admits once the
-  oldest waiting request has waited that long, or when no other request is on its way.  Cohorts that start while others
-  run overlap with them on the device (the ctypes calls release the GIL).
+  oldest waiting request has waited that long, or when no other request is on its way.
+  At most max_cohorts cohorts run at a time (default 4): under light load every request
+  starts at once, under heavy load arrivals gather while the cohorts run and start
+  together in larger cohorts.  Cohorts that run at the same time overlap on the device
+  (the ctypes calls release the GIL).
 * Iteration-level retirement: a cohort runs the incremental solve of the library
   (uegccd_batch_start / uegccd_batch_advance): after every round of four iterations, each
   solve that stopped -- converged, or at MaxIter -- is retired at once, with its final
@@ -120,7 +123,7 @@ class Server:
 
     def __init__(self, hbm_budget: int = 40 << 30, max_batch: int = 64, ndiis: int = 6, tol: float = 1e-8,
                  max_iter: int = 200, setup_threads: int = 8, rounds: int = 1, device: int = 0,
-                 batch_window: float = 0.0):
+                 batch_window: float = 0.0, max_cohorts: int = 4):
         self.budget = hbm_budget
         self.max_batch = max_batch
         self.opts = dict(scheme=1, ndiis=ndiis, denom_factor=1.0, tol=tol, max_iter=max_iter)
@@ -129,6 +132,7 @@ class Server:
         self.rounds = rounds
         self.device = device
         self.batch_window = batch_window
+        self.max_cohorts = max_cohorts
         self.lock = threading.Lock()
         self.in_use = 0
         self.batches_started = 0
@@ -217,6 +221,8 @@ class Server:
                     group = []
                     with self.lock:
                         free = self.budget - self.in_use
+                        if self._live >= self.max_cohorts:
+                            free = -1   # wait for a running cohort to finish
                         for r in [w for w in waiting if w.method == method]:
                             if len(group) >= self.max_batch:
                                 break
