@@ -42,7 +42,7 @@ SEED = 2024
 # checks it every run.  Used to turn the oracle's time per iteration into a time per solve.
 REF_ITERS_PER_SOLVE = 33.16  # measured: replay mode on this workload, 100 twists (min 30, max 35)
 SOLVE_OPTS = dict(scheme=1, ndiis=6, denom_factor=1.0, tol=1e-9)
-E2E_CREATORS = 1   # host threads creating the next batches of the e2e pipeline
+E2E_CREATORS = 2   # host threads creating the next batches of the e2e pipeline
 # Nominal FP64 peak of a B200 (datasheet); the bench measures it each run with the register-only
 # probe of bench_peak.cu (37.0 TFLOP/s measured on B200) and uses this only if the probe fails.
 FP64_PEAK_TFLOPS = 37.0
@@ -108,11 +108,11 @@ def _measured_peaks():
 
 
 HBM_PEAK, BF16_PEAK = _measured_peaks()
-# DRAM bytes of one launch per solve (dram__bytes.sum.per_second x gpu__time_duration of one ncu
-# capture of the 100-twist batch itself, all class launches of one residual), scaled by the
-# solves of a launch.
-TRAFFIC_PER_SOLVE = {"k_ladder": 201.8e6 / 100, "k_ladder_hh": 104.1e6 / 100, "k_mosaic_blk": 121.3e6 / 100,
-                     "k_rings": 1467.2e6 / 100, "k_update": 871.1e6 / 100}
+# DRAM bytes of one launch per solve: dram__bytes_read.sum + dram__bytes_write.sum of every class
+# launch of one residual, from one ncu capture of the 100-twist batch itself (a one-pass
+# metric set), divided by the 100 solves of a launch.
+TRAFFIC_PER_SOLVE = {"k_ladder": 194.1e6 / 100, "k_ladder_hh": 101.5e6 / 100, "k_mosaic_blk": 117.8e6 / 100,
+                     "k_rings": 307.2e6 / 100, "k_ring_stage": 829.8e6 / 100, "k_update": 880.0e6 / 100}
 
 
 def twists(n: int, seed: int = SEED, rank: int = 0):
@@ -291,6 +291,9 @@ def kernel_units(st):
         "k_rings": ("flop", st["ring_flop"]),
         # reads the rows i <= j of t once (s is formed in registers; the partial sums are small)
         "k_mosaic_blk": ("byte", 8 * st["A_half"]),
+        # the particle-hole copy: every amplitude read once through a 4-byte index and written
+        # once (the pairs' X1 and Y1 hold A entries between them)
+        "k_ring_stage": ("byte", (8 + 4 + 8) * A),
         # every amplitude: the mirror index (4 B); the amplitudes i <= j: t, the ladder G and the
         # two ring G, the Pulay push (t' FP64 and e FP32 to the history) and the other ndiis - 1
         # error vectors (FP32)
@@ -372,7 +375,7 @@ def run_gpu(args, rank, world):
         batch.solve(**opts)
     stats = batch.kernel_stats()
     batch.set_profiling(False)
-    ring_threads = batch.ring_threads()   # the tuner's pick, from the first CCD solve
+    ring_threads = batch.launch_shapes()  # the tuner's picks, from the first CCD solve
     fp64_peak = probe_fp64_peak()           # the FP64 tensor-core roofline denominator, measured
     niters = [r["niter"] for r in res]
     fails = sum(r["fail"] for r in res)
@@ -472,8 +475,11 @@ def run_gpu(args, rank, world):
 
 # ------------------------------------------------------------------- oracle arm
 def _oracle_iter_worker(q):
-    """Runs `iters` CCD iterations of one twist in the oracle; returns seconds per iteration."""
-    tw, iters = q
+    """Runs `iters` CCD iterations of one twist in the oracle, pinned to one host core (the
+    reference is serial); returns seconds per iteration."""
+    tw, iters, core = q
+    if core is not None and hasattr(os, "sched_setaffinity"):
+        os.sched_setaffinity(0, {core})
     sys.path.insert(0, ROOT)
     import numpy as np  # noqa: F401
 
@@ -495,10 +501,12 @@ def oracle_rate(ncores: int, iters: int, iters_per_solve: float, rank: int = 0):
     import multiprocessing as mp
 
     tw = twists(max(ncores, 1), rank=rank)
+    cores = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else []
+    pin = [cores[k] if k < len(cores) else None for k in range(ncores)]   # one worker per core
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(ncores) as pool:
-        per_iter = pool.map(_oracle_iter_worker, [(tuple(t), iters) for t in tw[:ncores]])
+        per_iter = pool.map(_oracle_iter_worker, [(tuple(t), iters, pin[k]) for k, t in enumerate(tw[:ncores])])
     wall = time.perf_counter() - t0
     sec_per_solve = statistics.mean(per_iter) * iters_per_solve
     return ncores / sec_per_solve, per_iter, wall
@@ -584,8 +592,8 @@ def main(argv=None):
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": v, "unit": "solves/s", "cores": ncores, "kind": "port",
-                                 "sample": f"{args.cpu_iters} CCD iteration(s) of one twist per core, "
-                                           f"x {ips} iterations per solve"},
+                                 "sample": f"{args.cpu_iters} CCD iteration(s) of one twist per core (one "
+                                           f"process pinned to each), x {ips} iterations per solve"},
                 "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -641,7 +649,7 @@ def main(argv=None):
     tr = TRAFFIC_PER_SOLVE.get(top)
     roof["traffic"] = tr * nsys if tr else None
     flops_pp = sum(ps["ov2_half"] * 2 for ps in per_solve) / len(per_solve) * nsys
-    config["ring_cta_threads"] = g["ring_threads"]   # per ring pair class, picked by the launch-shape tuner
+    config["launch_shapes"] = g["ring_threads"]   # picked by the launch-shape tuner on the batch
     if args.precision == "mixed":
         config["precision"] = "particle-particle ladder FP16 tensor cores (FP32 accumulate), rest FP64"
     line = {"metric": metric, "value": g["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -697,8 +705,9 @@ def main(argv=None):
         r, per_iter, wall = oracle_rate(ncores, args.cpu_iters, g["replay_niter_mean"])
         line["cpu_baseline"] = {"value": r, "unit": "solves/s", "cores": ncores, "kind": "port",
                                 "sample": f"{args.cpu_iters} CCD iteration(s) of twist 0 in the oracle (the "
-                                          f"reference's iteration), x {g['replay_niter_mean']:.2f} mean iterations "
-                                          f"per solve ({per_iter[0]:.2f} s/iter)"}
+                                          f"reference's iteration) on one pinned core, x "
+                                          f"{g['replay_niter_mean']:.2f} mean iterations per solve "
+                                          f"({per_iter[0]:.2f} s/iter); host cores: {os.cpu_count()}"}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -115,6 +115,9 @@ def test_ring_cta_tuning_and_pinned_download(goldens):
     b.solve(max_iter=4)
     th = b.ring_threads()
     assert len(th) == 4 and all(t in (32, 64, 128, 256) for t in th)
+    shapes = b.launch_shapes()
+    assert shapes["ring_threads"] == th and shapes["stage_threads"] in (64, 128, 256)
+    assert shapes["ladder_order"] in ("block", "longest first")
     n = b.amplitude_count()
     rt = C.CDLL("libcudart.so.12")
     p = C.c_void_p()
@@ -136,3 +139,4 @@ def test_fp64_peak_probe():
 
     v = bench.probe_fp64_peak()
     assert v is not None and 20.0 < v < 60.0, v
+

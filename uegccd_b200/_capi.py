@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
         L.uegccd_batch_set_profiling.argtypes = [vp, C.c_int32]
         L.uegccd_batch_ring_threads.argtypes = [vp, P(C.c_int32), C.c_int32]
         L.uegccd_batch_ring_threads.restype = C.c_int32
+        L.uegccd_batch_launch_shapes.argtypes = [vp, P(C.c_int32), C.c_int32]
+        L.uegccd_batch_launch_shapes.restype = C.c_int32
         L.uegccd_batch_kernel_stats.argtypes = [vp, C.c_int32, P(C.c_char_p), dp, P(C.c_int64)]
         L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
         L.uegccd_footprint.argtypes = [P(System), C.c_int32, C.c_int32, P(C.c_int64), P(C.c_int64)]

@@ -723,6 +723,21 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if (tiles.size() != ntl || htiles.size() != nhtl) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder row tile outside the 4/8/16/24/32 classes");
     d.ntiles = (int)tiles.size();
     d.nhtiles = (int)htiles.size();
+    // the second tile order the launch-shape tuner may pick: within each class, the tiles of
+    // the blocks with the most virtuals (the longest c loops) first
+    auto longest_first = [&](const std::vector<LadderTile> &v, const int *cnt) {
+        std::vector<LadderTile> out(v);
+        size_t off = 0;
+        for (int c = 0; c < kLadderClasses; c++) {
+            std::stable_sort(out.begin() + off, out.begin() + off + cnt[c], [&](const LadderTile &x, const LadderTile &y) {
+                return blocks[x.blk].v > blocks[y.blk].v;
+            });
+            off += cnt[c];
+        }
+        return out;
+    };
+    const std::vector<LadderTile> tiles_lpt = longest_first(tiles, d.ntile_cls),
+                                  htiles_lpt = longest_first(htiles, d.nhtile_cls);
     d.ntc16 = (int)tc16.size();
     d.ntc32 = (int)tc32.size();
     d.ntc64 = (int)tc64.size();
@@ -799,6 +814,8 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->upload(d.blocks, blocks))) return rc;
     if ((rc = b->upload(d.tiles, tiles))) return rc;
     if ((rc = b->upload(d.htiles, htiles))) return rc;
+    if ((rc = b->upload(d.tiles_lpt, tiles_lpt))) return rc;
+    if ((rc = b->upload(d.htiles_lpt, htiles_lpt))) return rc;
     if ((rc = b->upload(d.tctiles, tct))) return rc;
     if ((rc = b->upload(d.tcx, tcx))) return rc;
     if ((rc = b->upload(d.wslabs, wslabs))) return rc;
@@ -1114,11 +1131,12 @@ int capture_iteration(UegccdBatch &b, const TermFlags &f, double tol, int max_it
     return 0;
 }
 
-// The k_rings CTA sizes of a batch: measured once per batch shape in this process (the
-// shape: pair count and shared memory of every class), on the first CCD solve, before
-// the iteration graph is captured.
+// The launch shapes of a batch (k_rings CTA sizes, k_ring_stage CTA size, ladder tile
+// order): measured once per batch shape in this process (the shape: pair count and shared
+// memory of every ring class, ladder tiles per class, largest block), on the first CCD
+// solve, before the iteration graph is captured.
 std::mutex g_tune_mu;
-std::map<std::vector<int64_t>, std::array<int, kRingClasses>> g_ring_tuning;
+std::map<std::vector<int64_t>, std::array<int, kRingClasses + 2>> g_ring_tuning;
 
 int tune_batch_rings(UegccdBatch &b)
 {
@@ -1128,19 +1146,28 @@ int tune_batch_rings(UegccdBatch &b)
         key.push_back(d.nring[c]);
         key.push_back((int64_t)d.ring_smem[c]);
     }
+    for (int c = 0; c < kLadderClasses; c++) {
+        key.push_back(d.ntile_cls[c]);
+        key.push_back(d.nhtile_cls[c]);
+    }
+    key.push_back(d.max_v);
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_ring_tuning.find(key);
         if (it != g_ring_tuning.end()) {
             for (int c = 0; c < kRingClasses; c++) d.ring_threads[c] = it->second[c];
+            d.stage_threads = it->second[kRingClasses];
+            d.ladder_sched = it->second[kRingClasses + 1];
             b.rings_tuned = true;
             return 0;
         }
     }
     const int e = tune_rings(d, b.stream);
-    if (e != 0) return fail(UEGCCD_ERR_CUDA, std::string("k_rings tuning: ") + cudaGetErrorString((cudaError_t)e));
-    std::array<int, kRingClasses> th;
+    if (e != 0) return fail(UEGCCD_ERR_CUDA, std::string("launch-shape tuning: ") + cudaGetErrorString((cudaError_t)e));
+    std::array<int, kRingClasses + 2> th;
     for (int c = 0; c < kRingClasses; c++) th[c] = d.ring_threads[c];
+    th[kRingClasses] = d.stage_threads;
+    th[kRingClasses + 1] = d.ladder_sched;
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_ring_tuning[key] = th;
     b.rings_tuned = true;
@@ -1811,6 +1838,18 @@ int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max)
     if (!b || !threads || max <= 0) return fail(UEGCCD_ERR_ARG, "bad argument");
     const int n = std::min<int>(max, kRingClasses);
     for (int c = 0; c < n; c++) threads[c] = b->d.ring_threads[c];
+    return n;
+}
+
+int32_t uegccd_batch_launch_shapes(UegccdBatch *b, int32_t *vals, int32_t max)
+{
+    if (!b || !vals || max <= 0) return fail(UEGCCD_ERR_ARG, "bad argument");
+    int32_t v[kRingClasses + 2];
+    for (int c = 0; c < kRingClasses; c++) v[c] = b->d.ring_threads[c];
+    v[kRingClasses] = b->d.stage_threads;
+    v[kRingClasses + 1] = b->d.ladder_sched;
+    const int n = std::min<int>(max, kRingClasses + 2);
+    for (int k = 0; k < n; k++) vals[k] = v[k];
     return n;
 }
 

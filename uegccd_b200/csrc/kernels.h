@@ -86,6 +86,11 @@ struct DevBatch {
     int nring[5] = {0, 0, 0, 0, 0};
     size_t ring_smem[5] = {0, 0, 0, 0, 0};
     int ring_threads[4] = {32, 128, 256, 256};  // CTA size per k_rings class: defaults, then tune_rings
+    int stage_threads = 128;                    // CTA size of k_ring_stage (tune_rings)
+    // ladder tiles in a second order: within each row-tile class the blocks with the most
+    // virtuals (the longest c loops) first; ladder_sched picks the order the launches use
+    LadderTile *tiles_lpt = nullptr, *htiles_lpt = nullptr;
+    int ladder_sched = 0;                       // 0: block order, 1: longest first (tune_rings)
 };
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
@@ -108,10 +113,12 @@ constexpr int kRingClasses = 4;
 constexpr int kRingClassRows[kRingClasses] = {16, 32, 48, 1 << 30};
 constexpr size_t kRingSmemMax = 200 * 1024;
 void set_rings_smem_limit(int wide, size_t bytes);
-// Launch-shape autotuner: times k_rings of every pair class on the batch's current
-// amplitudes with 32, 64, 128 and 256 threads per CTA and keeps the fastest in
-// d.ring_threads.  The CTA size changes no sum's order: results are bitwise the same.
-// Not inside a stream capture.  Returns a cudaError_t value.
+// Launch-shape autotuner, on the batch's current amplitudes: times k_rings of every pair
+// class with 32, 64, 128 and 256 threads per CTA (d.ring_threads), k_ring_stage with 64,
+// 128 and 256 (d.stage_threads), and the particle-particle ladder with its tiles in block
+// order and longest first (d.ladder_sched); keeps the fastest of each.  None of these
+// changes a sum's order: results are bitwise the same.  Not inside a stream capture.
+// Returns a cudaError_t value.
 int tune_rings(DevBatch &d, cudaStream_t st);
 
 constexpr int kDiisMax = 16;   // DIIS history capacity (k_update and k_diis_* use the same bound)

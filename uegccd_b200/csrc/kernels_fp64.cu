@@ -1911,6 +1911,47 @@ int tune_rings(DevBatch &d, cudaStream_t st)
         }
         off += d.nring[c];
     }
+    // the staging kernel's CTA size
+    if (err == cudaSuccess && d.nrpairs > 0) {
+        float best = 1e30f;
+        for (int th : {64, 128, 256}) {
+            auto run = [&]() {
+                k_ring_stage<<<d.nrpairs, th, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy,
+                                                       d.active);
+            };
+            run();
+            cudaEventRecord(e0, st);
+            run();
+            run();
+            cudaEventRecord(e1, st);
+            if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                d.stage_threads = th;
+            }
+        }
+    }
+    // the ladder tiles' order (particle-particle part alone; it writes only d.g)
+    if (err == cudaSuccess && d.nblocks > 0 && d.tiles_lpt) {
+        float best = 1e30f;
+        for (int sched = 0; sched < 2 && err == cudaSuccess; sched++) {
+            const LadderTile *tl = sched ? d.tiles_lpt : d.tiles;
+            launch_ladder3(d, tl, d.ntile_cls, d.t, 0, 1, 0, d.g, st);
+            cudaEventRecord(e0, st);
+            launch_ladder3(d, tl, d.ntile_cls, d.t, 0, 1, 0, d.g, st);
+            launch_ladder3(d, tl, d.ntile_cls, d.t, 0, 1, 0, d.g, st);
+            cudaEventRecord(e1, st);
+            if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                d.ladder_sched = sched;
+            }
+        }
+    }
     if (err == cudaSuccess) err = cudaGetLastError();
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -1926,12 +1967,13 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     if (f.do_ladder && d.nblocks > 0) {
         if (f.do_hh) {
             kt->begin(KID_HH_W, st);
-            n += launch_ladder3(d, d.htiles, d.nhtile_cls, d.t, 1, f.do_pp, f.do_hh, d.g, st);
+            n += launch_ladder3(d, d.ladder_sched ? d.htiles_lpt : d.htiles, d.nhtile_cls, d.t, 1, f.do_pp, f.do_hh,
+                                d.g, st);
             kt->end(st);
         }
         const int pp64 = (f.do_pp && !f.mixed) ? 1 : 0;
         kt->begin(KID_LADDER, st);
-        n += launch_ladder3(d, d.tiles, d.ntile_cls, d.t, 0, pp64, f.do_hh, d.g, st);
+        n += launch_ladder3(d, d.ladder_sched ? d.tiles_lpt : d.tiles, d.ntile_cls, d.t, 0, pp64, f.do_hh, d.g, st);
         kt->end(st);
         if (f.do_pp && f.mixed) {
             kt->begin(KID_LADDER_TC, st);
@@ -1960,7 +2002,8 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     }
     if ((f.do_ring || f.do_xring) && !f.drpa) {
         kt->begin(KID_RING_STAGE, st);
-        k_ring_stage<<<d.nrpairs, 128, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy, d.active);
+        k_ring_stage<<<d.nrpairs, d.stage_threads, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy,
+                                                            d.active);
         kt->end(st);
         n++;
         kt->begin(KID_RINGS, st);
