@@ -537,7 +537,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     std::vector<int> chunk_begin(n + 1, 0);
     std::vector<double> vtab;
     std::vector<int64_t> hh0;
-    std::vector<RingPairDev> rpairs;
+    std::vector<RingPairDev> rpairs, spairs;
     int64_t amp0 = 0, pos0 = 0, ph0 = 0, hhoff = 0, phr0 = 0, mrows = 0, mcols = 0;
     std::vector<int> s_t0(n);   // first mosaic target of each solve
     int orb0 = 0, vtab0 = 0, jvv0 = 0, joo0 = 0, max_o = 0, max_v = 0, max_occ = 0;
@@ -794,6 +794,11 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
             if (xy_n >= ((int64_t)1 << 31)) return fail(UEGCCD_ERR_ARG, "batch too large for 32-bit ring offsets");
         }
         d.xy_n = xy_n;
+        // the staging kernel walks the pairs solve by solve (the class sort is stable, so a
+        // stable sort by solve restores that order)
+        spairs.assign(rpairs.begin(), rpairs.end());
+        std::stable_sort(spairs.begin(), spairs.end(),
+                         [](const RingPairDev &x, const RingPairDev &y) { return x.solve < y.solve; });
         for (const auto &r : rpairs) {
             const int c = cls_of(r);
             d.nring[c]++;
@@ -848,6 +853,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     b->vtab_base = vtab;
     if ((rc = b->upload(d.hh0, hh0))) return rc;
     if ((rc = b->upload(d.rpairs, rpairs))) return rc;
+    if ((rc = b->upload(d.spairs, spairs))) return rc;
     if ((rc = b->upload(d.ph_i, ph_i))) return rc;
     if ((rc = b->upload(d.ph_x, ph_x))) return rc;
     if ((rc = b->alloc(d.ridx_x, ph0))) return rc;

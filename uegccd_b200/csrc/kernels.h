@@ -55,7 +55,9 @@ struct DevBatch {
     // particle-hole form of the ring terms
     int16_t *ph_i = nullptr, *ph_x = nullptr;   // row -> (i, x), rows grouped by Q
     int32_t *ridx_x = nullptr, *ridx_y = nullptr;  // at ph0 + row*O + k: index of t(ik, x), t(ki, x)
-    RingPairDev *rpairs = nullptr;              // {Q, -Q} group pairs
+    RingPairDev *rpairs = nullptr;              // {Q, -Q} group pairs, by k_rings class
+    RingPairDev *spairs = nullptr;              // the same pairs in solve order (k_ring_stage: each
+                                                // solve's amplitudes are gathered while in L2)
     // rings in the particle-hole layout (RingPairDev::xy0): xy holds the amplitudes each pair
     // multiplies, row by row (k_ring_stage gathers t into it before every ring launch); rx
     // the ring and crossed-ring G the pair forms, in the same places (k_update reads them).

@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
                                                            const int16_t *__restrict__ pair_i,
                                                            const int16_t *__restrict__ pair_j,
                                                            const int16_t *__restrict__ vir,
-                                                           const int4 *__restrict__ nv4,
+                                                           const int *__restrict__ nvp,
                                                            const double *__restrict__ vtab,
                                                            const double *__restrict__ t,
                                                            const int16_t *__restrict__ pcol, int drpa,
@@ -552,21 +552,21 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     double *coff = sv + kVtabSmem;             // v: column sums over the rows i < j
     double *cdg = coff + v;                    // v: the diagonal pair's row (if any)
     double *wrs = cdg + v;                     // kW x oc: per-warp row sums
-    int4 *nvc = (int4 *)(wrs + kW * oc);       // v: n-vectors of the block's virtuals
-    int4 *nk = nvc + v, *nl = nk + oc;         // oc: n-vectors of each row's k and l
-    int *pc = (int *)(nl + oc);                // v: column of the partner d = K - c
+    int *nvc = (int *)(wrs + kW * oc);         // v: packed n-vectors of the block's virtuals
+    int *nk = nvc + v, *nl = nk + oc;          // oc: packed n-vectors of each row's k and l
+    int *pc = nl + oc;                         // v: column of the partner d = K - c
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
         for (int q = tid; q <= s.q2max; q += kMosThreads) sv[q] = vtab[s.vtab0 + q];
     for (int c = tid; c < v; c += kMosThreads) {
-        nvc[c] = nv4[s.orb0 + vir[B.vir0 + c]];
+        nvc[c] = nvp[s.orb0 + vir[B.vir0 + c]];
         pc[c] = pcol[B.vir0 + c];
         coff[c] = cdg[c] = 0.0;
     }
     for (int r = tid; r < oc; r += kMosThreads) {
-        nk[r] = nv4[s.orb0 + pair_i[B.pair0 + r]];
-        nl[r] = nv4[s.orb0 + pair_j[B.pair0 + r]];
+        nk[r] = nvp[s.orb0 + pair_i[B.pair0 + r]];
+        nl[r] = nvp[s.orb0 + pair_j[B.pair0 + r]];
     }
     __syncthreads();
     auto V = [&](int q2) -> double { return vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]); };
@@ -575,19 +575,19 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     // the column sums of (k,l) with the columns swapped to their partners.
     for (int r = 0; r < oc; r++) {
         const bool diag = r >= B.nd;
-        const int4 rk = nk[r], rl = nl[r];
+        const int rk = nk[r], rl = nl[r];
         const double *row = t + B.t0 + (int64_t)r * v;
         double rs = 0.0;
         for (int c = tid; c < v; c += kMosThreads) {
             const double x = row[c];
-            const int4 ncv = nvc[c];
-            const double vck = V(q2_of(ncv, rk));
+            const int ncv = nvc[c];
+            const double vck = V(q2p(ncv, rk));
             double sval;
             if (drpa) {
                 sval = 2.0 * vck * x;
             } else {
                 const double y = row[pc[c]];  // t(kl, d), same row
-                const double vcl = V(q2_of(ncv, rl));
+                const double vcl = V(q2p(ncv, rl));
                 sval = vck * (2.0 * x - y) - vcl * (x - 2.0 * y);
             }
             rs += sval;
@@ -1916,7 +1916,7 @@ int tune_rings(DevBatch &d, cudaStream_t st)
         float best = 1e30f;
         for (int th : {64, 128, 256}) {
             auto run = [&]() {
-                k_ring_stage<<<d.nrpairs, th, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy,
+                k_ring_stage<<<d.nrpairs, th, 0, st>>>(d.spairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy,
                                                        d.active);
             };
             run();
@@ -1985,7 +1985,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     if (f.do_mosaic) {
         kt->begin(KID_MOSAIC_S, st);
         k_mosaic_blk<<<d.nblocks, kMosThreads, d.mosaic_smem, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir,
-                                                                   d.nv4, d.vtab, d.t, d.pcol, f.drpa, d.mpart,
+                                                                   d.nvp, d.vtab, d.t, d.pcol, f.drpa, d.mpart,
                                                                    d.active);
         kt->end(st);
         kt->begin(KID_MOSAIC_RED, st);
@@ -2002,7 +2002,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     }
     if ((f.do_ring || f.do_xring) && !f.drpa) {
         kt->begin(KID_RING_STAGE, st);
-        k_ring_stage<<<d.nrpairs, d.stage_threads, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy,
+        k_ring_stage<<<d.nrpairs, d.stage_threads, 0, st>>>(d.spairs, d.solves, d.ph_i, d.ridx_x, d.ridx_y, d.t, d.xy,
                                                             d.active);
         kt->end(st);
         n++;
