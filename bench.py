@@ -670,7 +670,12 @@ def main(argv=None):
                       "not_converged": g["fails"], "ecorr_twist0": g["ecorr_first"], "e2_twist0": g["e2_first"],
                       "pp_ladder_gflop_per_iter": flops_pp / 1e9,
                       "replay_niter_mean": g["replay_niter_mean"],
-                      "replay_vs_diis_max_dE": g["replay_vs_diis_max_dE"]}}
+                      "replay_vs_diis_max_dE": g["replay_vs_diis_max_dE"],
+                      # how much of a solves/s ratio against the reference's iteration is the
+                      # iteration count (Pulay DIIS here, 1/2-damped Jacobi there) and how much
+                      # the rate of iterations
+                      "iterations_ratio_replay_over_diis": g["replay_niter_mean"] / g["niter_mean"],
+                      "solve_iterations_per_s": g["value"] * g["niter_mean"]}}
     if g.get("other"):
         o = g["other"]
         line[o["precision"]] = {

@@ -100,9 +100,11 @@ __device__ __forceinline__ double block_sum(double v)
 // E(2) = 1/2 sum [T2aaaa (V_ijab - V_ijba) + T2abab V_ijab - T2abba V_ijba]
 //      = sum t(ij,a) (2 v(i-a) - v(i-b))   after the a <-> b re-indexing.
 // ----------------------------------------------------------------------------
+// The integrals come from the per-amplitude Coulomb factors {v(i-a), v(a-j)} (k_vcoef; the
+// same table entries): v(i-b) = v(a-j), since n_i - n_b = n_a - n_j.
 __global__ void k_mp2(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
-                      const AmpInfo *__restrict__ amps, const int4 *__restrict__ nv4,
-                      const double *__restrict__ eigen, const double *__restrict__ vtab, double *__restrict__ t,
+                      const AmpInfo *__restrict__ amps, const double2 *__restrict__ vcoef,
+                      const double *__restrict__ eigen, double *__restrict__ t,
                       double *__restrict__ part_e, double *__restrict__ part_a, double *__restrict__ part_b)
 {
     const ChunkDev ch = chunks[blockIdx.x];
@@ -114,8 +116,9 @@ __global__ void k_mp2(const ChunkDev *__restrict__ chunks, const SolveDev *__res
         const AmpInfo q = amps[p];
         const double *ev = eigen + s.orb0;
         double denom = ev[q.i] + ev[q.j] - ev[q.a] - ev[q.b];
-        double via = vpq(s, nv4, vtab, q.i, q.a);
-        double vib = vpq(s, nv4, vtab, q.i, q.b);
+        const double2 vc = vcoef[p];
+        double via = vc.x;
+        double vib = vc.y;
         // a core pair's integrals are zero (CoreERI), so is its amplitude
         double x = (q.i < s.core_n || q.j < s.core_n) ? 0.0 : via / denom;
         t[p] = x;
@@ -130,9 +133,10 @@ __global__ void k_mp2(const ChunkDev *__restrict__ chunks, const SolveDev *__res
 // Energy of the current amplitudes and max|t| (the dT before the first iteration).
 // kind 0, CCEnergy (CCD.f90:225-227): E = sum t(ij,a) (2 v(i-a) - v(a-j)) after re-indexing;
 // kind 1, dRPA CCEnergy (dRPA.f90:206-210): E = sum t (2 v(a-i) - csosex v(b-i)).
+// The integrals come from the per-amplitude Coulomb factors {v(i-a), v(a-j)} (k_vcoef):
+// v(a-i) = v(i-a), and v(b-i) = v(a-j) since n_b - n_i = n_j - n_a.
 __global__ void k_energy(const ChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
-                         const AmpInfo *__restrict__ amps, const int4 *__restrict__ nv4,
-                         const double *__restrict__ vtab, const double *__restrict__ t, int kind, double csosex,
+                         const double2 *__restrict__ vcoef, const double *__restrict__ t, int kind, double csosex,
                          double *__restrict__ part_e, double *__restrict__ part_a, double *__restrict__ part_b)
 {
     const ChunkDev ch = chunks[blockIdx.x];
@@ -141,11 +145,11 @@ __global__ void k_energy(const ChunkDev *__restrict__ chunks, const SolveDev *__
     double e = 0.0, mx = 0.0;
     if (loc < s.namp) {
         const int64_t p = s.amp0 + loc;
-        const AmpInfo q = amps[p];
         double x = t[p];
-        double via = vpq(s, nv4, vtab, q.a, q.i);
-        if (kind == 0) e = x * (2.0 * via - vpq(s, nv4, vtab, q.a, q.j));
-        else e = via * x * 2.0 - vpq(s, nv4, vtab, q.b, q.i) * x * csosex;
+        const double2 vc = vcoef[p];
+        double via = vc.x;
+        if (kind == 0) e = x * (2.0 * via - vc.y);
+        else e = via * x * 2.0 - vc.y * x * csosex;
         mx = fabs(x);
     }
     double dummy = 0.0;
@@ -940,7 +944,9 @@ size_t rings_dmma_smem_bytes(int O, int n1, int n2, int q2max)
     return sizeof(double) * dbl + sizeof(int) * ((size_t)O + 4 * (N1 + N2));
 }
 
-__global__ void __launch_bounds__(256) k_rings(const RingPairDev *__restrict__ pairs,
+// Capped at 64 registers (four 256-thread CTAs an SM): a few spill slots, more CTAs resident
+// (0.396 -> 0.362 ms per residual on the 100-twist batch, against the 78 registers uncapped).
+__global__ void __launch_bounds__(256, 4) k_rings(const RingPairDev *__restrict__ pairs,
                                                         const SolveDev *__restrict__ solves,
                                                         const int16_t *__restrict__ ph_i,
                                                         const int16_t *__restrict__ ph_x,
@@ -1853,8 +1859,8 @@ void launch_sf(const DevBatch &d, const int2 *groups, int ngroups, int solve, in
 // ----------------------------------------------------------------------------
 void launch_mp2(const DevBatch &d, cudaStream_t st)
 {
-    k_mp2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.amps, d.nv4, d.eigen, d.vtab, d.t, d.part_e,
-                                        d.part_dt, d.part_r);
+    k_mp2<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.amps, d.vcoef, d.eigen, d.t, d.part_e, d.part_dt,
+                                        d.part_r);
 }
 
 void launch_reduce(const DevBatch &d, cudaStream_t st)
@@ -1864,8 +1870,8 @@ void launch_reduce(const DevBatch &d, cudaStream_t st)
 
 void launch_energy(const DevBatch &d, int kind, double csosex, cudaStream_t st)
 {
-    k_energy<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.amps, d.nv4, d.vtab, d.t, kind, csosex, d.part_e,
-                                           d.part_dt, d.part_r);
+    k_energy<<<d.nchunks, kChunk, 0, st>>>(d.chunks, d.solves, d.vcoef, d.t, kind, csosex, d.part_e, d.part_dt,
+                                           d.part_r);
 }
 
 void launch_to_aaaa(const DevBatch &d, cudaStream_t st)
