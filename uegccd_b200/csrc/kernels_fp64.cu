@@ -217,8 +217,12 @@ __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, doubl
 // The t rows of the tile pass through shared memory in chunks of kLadKC columns,
 // double-buffered with cp.async (8-byte copies: rows of odd length are not 16-byte
 // aligned); the block's virtual n-vectors and the |q|^2 table are staged once.
-constexpr int kLadKC = 32;            // c columns per chunk
+constexpr int kLadKC = 32;            // c columns per chunk (mode 0)
 constexpr int kLadLd = kLadKC + 4;    // chunk row stride: = 4 mod 16 doubles, conflict-free fragments
+// The hole-hole intermediate (mode 1) has little work per column: wider chunks, fewer of the
+// round trips that bound it
+constexpr int kLadKC1 = 64;
+constexpr int kLadLd1 = kLadKC1 + 4;
 
 __device__ __forceinline__ void cp_async8(double *dst, const double *src)
 {
@@ -233,6 +237,10 @@ size_t ladder_smem_bytes(int max_v, int np)
 {
     return sizeof(double) * (2 * (size_t)np * kLadLd + kVtabSmem) + sizeof(int) * (size_t)max_v;
 }
+size_t ladder1_smem_bytes(int max_v, int np)
+{
+    return sizeof(double) * (2 * (size_t)np * kLadLd1 + kVtabSmem) + sizeof(int) * (size_t)max_v;
+}
 
 // PAIRED (blocks with at most 4 rows i <= j, NP = 8): the fragment's 8 columns hold the
 // rows p and, after them, the same rows with the c columns swapped to their partners
@@ -241,7 +249,7 @@ size_t ladder_smem_bytes(int max_v, int np)
 // the columns a <= pcol a only, half the fragments.  The hole-hole intermediate pairs its
 // columns q with their mirror pairs q' the same way (v(k_q' - pcol c) = v(k_q - c)), and the
 // hole-hole apply reads H[p][q'] for the second half (t[q][pcol a] = t[q'][a]).
-template <int NP, bool KS, bool PAIRED>
+template <int NP, bool KS, bool PAIRED, int KC = kLadKC>
 __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev &B, const SolveDev &s,
                                              const int16_t *__restrict__ vir, const int16_t *__restrict__ pair_i,
                                              const int *__restrict__ nvp, const double *__restrict__ vtab,
@@ -278,26 +286,27 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 #pragma unroll
         for (int n = 0; n < NN; n++) acc[m][n][0] = acc[m][n][1] = 0.0;
     if (do_pp || mode == 1) {
-        const int nchunk = (v + kLadKC - 1) / kLadKC;
+        constexpr int LD = KC + 4;
+        const int nchunk = (v + KC - 1) / KC;
         const double *trow0 = t + B.t0;
         // chunk j of the tile's t rows -> buffer b
         auto issue = [&](int j, int b) {
-            double *dst = ts + b * (NP * kLadLd);
-            const int c0 = j * kLadKC;
-            for (int e = threadIdx.x; e < NP * kLadKC; e += blockDim.x) {
-                const int r = e / kLadKC, c = e - r * kLadKC;
+            double *dst = ts + b * (NP * LD);
+            const int c0 = j * KC;
+            for (int e = threadIdx.x; e < NP * KC; e += blockDim.x) {
+                const int r = e / KC, c = e - r * KC;
                 const int cc = c0 + c;
                 if (PAIRED) {
                     // rows [0, orow): t[p][c]; rows [orow, 2 orow): t[p][pcol c]
                     const bool second = r >= orow;
                     const int p = second ? r - orow : r;
                     if (r < 2 * orow && cc < v)
-                        cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + (second ? pcolv(cc) : cc));
-                    else dst[r * kLadLd + c] = 0.0;
+                        cp_async8(dst + r * LD + c, trow0 + (int64_t)p * v + (second ? pcolv(cc) : cc));
+                    else dst[r * LD + c] = 0.0;
                 } else {
                     const int p = T.p0 + r;
-                    if (p < orow && cc < v) cp_async8(dst + r * kLadLd + c, trow0 + (int64_t)p * v + cc);
-                    else dst[r * kLadLd + c] = 0.0;
+                    if (p < orow && cc < v) cp_async8(dst + r * LD + c, trow0 + (int64_t)p * v + cc);
+                    else dst[r * LD + c] = 0.0;
                 }
             }
             cp_async_commit();
@@ -312,16 +321,16 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
             }
             __syncthreads();
             if (wact) {
-                const double *tb = ts + (j & 1) * (NP * kLadLd);
-                const int c0 = j * kLadKC;
+                const double *tb = ts + (j & 1) * (NP * LD);
+                const int c0 = j * KC;
                 const int kstart = KS && ksplit ? 4 * warp : 0, kstep = KS && ksplit ? 16 : 4;
 #pragma unroll 2
-                for (int kk = kstart; kk < kLadKC; kk += kstep) {
+                for (int kk = kstart; kk < KC; kk += kstep) {
                     const int c = min(c0 + kk + tig, v - 1);  // beyond v the t column is zero
                     const int nc = nvc[c];
                     double bf[NN];
 #pragma unroll
-                    for (int n = 0; n < NN; n++) bf[n] = tb[(n * 8 + gid) * kLadLd + kk + tig];
+                    for (int n = 0; n < NN; n++) bf[n] = tb[(n * 8 + gid) * LD + kk + tig];
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         const int q2 = q2p(na[m], nc);
@@ -439,8 +448,8 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     if (!active[B.solve]) return;
     const SolveDev s = solves[B.solve];
     extern __shared__ double lsm[];
-    double *ts = lsm;                              // 2 x NP x kLadLd
-    double *sv = ts + 2 * NP * kLadLd;             // kVtabSmem
+    double *ts = lsm;                              // 2 x NP x (chunk width + 4)
+    double *sv = ts + 2 * NP * (mode == 1 ? kLadLd1 : kLadLd);   // kVtabSmem
     int *nvc = (int *)(sv + kVtabSmem);            // v_K packed n-vectors of the block's virtuals
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
@@ -451,8 +460,8 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     double *out = mode == 0 ? g : H;
     // the hole-hole intermediate (mode 1) may split its c sum across the warps
     if (mode == 1)
-        ladder3_tile<NP, true, PAIRED>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
-                                       nvc);
+        ladder3_tile<NP, true, PAIRED, kLadKC1>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv,
+                                                vsm, ts, nvc);
     else
         ladder3_tile<NP, false, PAIRED>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
                                         nvc);
@@ -471,15 +480,13 @@ void set_ladder_smem_limit(int max_v)
     const int dev = current_device() % kMaxDevices;
     int &current = current_by_dev[dev];
     if (max_v > current) {
-        const int b8 = (int)ladder_smem_bytes(max_v, 8);
+        auto lb = [&](int np) { return (int)std::max(ladder_smem_bytes(max_v, np), ladder1_smem_bytes(max_v, np)); };
+        const int b8 = lb(8);
         cudaFuncSetAttribute(k_ladder3<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
         cudaFuncSetAttribute(k_ladder3<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
-        cudaFuncSetAttribute(k_ladder3<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ladder_smem_bytes(max_v, 16));
-        cudaFuncSetAttribute(k_ladder3<24, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ladder_smem_bytes(max_v, 24));
-        cudaFuncSetAttribute(k_ladder3<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ladder_smem_bytes(max_v, 32));
+        cudaFuncSetAttribute(k_ladder3<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(16));
+        cudaFuncSetAttribute(k_ladder3<24, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(24));
+        cudaFuncSetAttribute(k_ladder3<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(32));
         current = max_v;
     }
 }
@@ -494,7 +501,7 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
         const int cnt = ncls[c];
         if (cnt <= 0) continue;
         const int np = c == 0 ? 8 : 8 * c;
-        const size_t sm = ladder_smem_bytes(d.max_v, np);
+        const size_t sm = mode == 1 ? ladder1_smem_bytes(d.max_v, np) : ladder_smem_bytes(d.max_v, np);
 #define UEGCCD_LADDER_ARGS                                                                                  \
     tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.nvp, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
         g, d.active
