@@ -863,6 +863,7 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     if ((rc = b->alloc(d.rx, d.xy_n))) return rc;
     if ((rc = b->alloc(d.ph_a, phr0))) return rc;
     if ((rc = b->alloc(d.ph_b, phr0))) return rc;
+    if ((rc = b->alloc(d.rpos, amp0))) return rc;
     if ((rc = b->alloc(d.t, amp0))) return rc;
     if ((rc = b->alloc(d.t_new, amp0))) return rc;
     if ((rc = b->alloc(d.g, amp0))) return rc;

@@ -67,6 +67,7 @@ struct DevBatch {
     double *xy = nullptr, *rx = nullptr;
     int64_t xy_n = 0;
     int32_t *ph_a = nullptr, *ph_b = nullptr;
+    int2 *rpos = nullptr;            // per amplitude i <= j: its ring G and crossed-ring G in rx
     // mixed precision: tensor-core ladder tiles sorted by row tile (16, 32, 64)
     LadderTile *tctiles = nullptr;
     int ntc16 = 0, ntc32 = 0, ntc64 = 0;

@@ -1212,7 +1212,7 @@ struct UpdateArgs {
     double *part_e, *part_dt, *part_r;
     double *g_out;            // optional: full G per amplitude (term checks)
     const double *rx;                          // ring and crossed-ring G, particle-hole layout
-    const int32_t *ph_a, *ph_b;                // where (i, x) sits in it (DevBatch)
+    const int2 *rpos;                          // where each amplitude's two values sit in it
     const uint8_t *active;
     int do_ladder, do_mosaic, do_ring, do_xring, do_driver, drpa, mode;
     // Pulay DIIS push fused into the update (mode 0, ndiis > 0): the new (t', e) pair
@@ -1312,12 +1312,38 @@ __global__ void k_ring_stage(const RingPairDev *__restrict__ pairs, const SolveD
     }
 }
 
+// Where k_update finds each amplitude's ring values in rx, once per batch: k_rings leaves at
+// (a, b) of a {Q, -Q} pair the ring G of (i_a, i_b, x_a) and the crossed-ring G of
+// (i_a, i_b, x_b), a in group 1.  Amplitude (i,j,a) (partner b, i <= j) finds its ring G at
+// row (i,a), column (j,b) when (i,a) is in group 1, else at row (j,b), column (i,a) (its
+// mirror's place); its crossed-ring G in the second half of row (i,b) at column (j,a), or of
+// row (j,a) at column (i,b).
+__global__ void k_rx_pos(const HChunkDev *__restrict__ chunks, const SolveDev *__restrict__ solves,
+                         const AmpInfo *__restrict__ amps, const int32_t *__restrict__ ph_a,
+                         const int32_t *__restrict__ ph_b, int2 *__restrict__ rpos)
+{
+    const HChunkDev ch = chunks[blockIdx.x];
+    const SolveDev s = solves[ch.solve];
+    const int loc = ch.start + threadIdx.x;
+    if (loc >= ch.end) return;
+    const int64_t p = s.amp0 + loc;
+    const AmpInfo q = amps[p];
+    const int V = s.V, O = s.O;
+    const int32_t *pa = ph_a + s.phr0, *pb = ph_b + s.phr0;
+    const int ia = q.i * V + q.a - O, jb = q.j * V + q.b - O, ib = q.i * V + q.b - O, ja = q.j * V + q.a - O;
+    const int r = pa[ia] >= 0 ? pa[ia] + pb[jb] : pa[jb] + pb[ia];
+    const int x = pa[ib] >= 0 ? pa[ib] + pb[ib] + pb[ja] : pa[ja] + pb[ja] + pb[ib];
+    rpos[p] = make_int2(r, x);
+}
+
 void launch_block_tables(const DevBatch &d, cudaStream_t st)
 {
     if (d.nblocks > 0)
         k_block_tables<<<d.nblocks, 256, 0, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir, d.pcol, d.amps,
                                                   d.pos, d.partner, d.mirror);
     if (d.nrpairs > 0) k_ph_tables<<<d.nrpairs, 128, 0, st>>>(d.rpairs, d.solves, d.ph_i, d.ph_x, d.ph_a, d.ph_b);
+    if (d.nrpairs > 0 && d.nhchunks > 0)
+        k_rx_pos<<<d.nhchunks, kChunk, 0, st>>>(d.hchunks, d.solves, d.amps, d.ph_a, d.ph_b, d.rpos);
     if (d.nrchunks > 0)
         k_ring_index<<<d.nrchunks, kChunk, 0, st>>>(d.rchunks, d.solves, d.ph_i, d.ph_x, d.pos, d.ridx_x,
                                                     d.ridx_y);
@@ -1395,22 +1421,11 @@ __global__ void __launch_bounds__(kChunk, 8) k_update(UpdateArgs A)
                 }
             }
         } else if (A.do_ring || A.do_xring) {
-            // k_rings leaves at (a, b) of a {Q, -Q} pair the ring G of (i_a, i_b, x_a) and the
-            // crossed-ring G of (i_a, i_b, x_b), a in group 1; this amplitude's value sits there
-            // or at its mirror's (j, i, b), whichever has its row in group 1
-            const int32_t *pa = A.ph_a + s.phr0, *pb = A.ph_b + s.phr0;
-            const int V = s.V;
-            if (A.do_ring) {   // rings, linear + quadratic (CCD.f90:716-811)
-                const int ia = i * V + a - O, jb = j * V + b - O;
-                const int ra = __ldg(&pa[ia]);
-                g += ra >= 0 ? A.rx[ra + __ldg(&pb[jb])] : A.rx[__ldg(&pa[jb]) + __ldg(&pb[ia])];
-            }
-            if (A.do_xring) {  // crossed rings (CCD.f90:845-937)
-                const int ib = i * V + b - O, ja = j * V + a - O;
-                const int xa = __ldg(&pa[ib]);
-                g += xa >= 0 ? A.rx[xa + __ldg(&pb[ib]) + __ldg(&pb[ja])]
-                             : A.rx[__ldg(&pa[ja]) + __ldg(&pb[ja]) + __ldg(&pb[ib])];
-            }
+            // the ring G (rings, linear + quadratic, CCD.f90:716-811) and the crossed-ring G
+            // (CCD.f90:845-937) of this amplitude, where k_rings left them (k_rx_pos)
+            const int2 ro = A.rpos[p];
+            if (A.do_ring) g += A.rx[ro.x];
+            if (A.do_xring) g += A.rx[ro.y];
         }
         {   // core pair: every term has a zero factor (CoreN read on its own: taken from the
             // solve record above, it costs this kernel registers)
@@ -2046,7 +2061,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
     A.part_e = d.part_e; A.part_dt = d.part_dt; A.part_r = d.part_r; A.g_out = g_out; A.active = d.active;
     A.do_ladder = f.do_ladder; A.do_mosaic = f.do_mosaic; A.do_ring = f.do_ring; A.do_xring = f.do_xring;
     A.do_driver = f.do_driver; A.drpa = f.drpa; A.mode = mode;
-    A.rx = d.rx; A.ph_a = d.ph_a; A.ph_b = d.ph_b;
+    A.rx = d.rx; A.rpos = d.rpos;
     A.st = diis ? diis->state : nullptr; A.ndiis = (diis && mode == 0) ? ndiis : 0; A.namp = d.namp;
     A.hist_t = diis ? diis->hist_t : nullptr; A.hist_e = diis ? diis->hist_e : nullptr;
     A.dpart = diis ? diis->part : nullptr;
