@@ -111,8 +111,8 @@ HBM_PEAK, BF16_PEAK = _measured_peaks()
 # DRAM bytes of one launch per solve: dram__bytes_read.sum + dram__bytes_write.sum of every class
 # launch of one residual, from one ncu capture of the 100-twist batch itself (a one-pass
 # metric set), divided by the 100 solves of a launch.
-TRAFFIC_PER_SOLVE = {"k_ladder": 194.1e6 / 100, "k_ladder_hh": 101.5e6 / 100, "k_mosaic_blk": 117.8e6 / 100,
-                     "k_rings": 307.2e6 / 100, "k_ring_stage": 829.8e6 / 100, "k_update": 880.0e6 / 100}
+TRAFFIC_PER_SOLVE = {"k_ladder": 193.4e6 / 100, "k_ladder_hh": 101.5e6 / 100, "k_mosaic_blk": 116.7e6 / 100,
+                     "k_rings": 310.0e6 / 100, "k_ring_stage": 496.8e6 / 100, "k_update": 968.7e6 / 100}
 
 
 def twists(n: int, seed: int = SEED, rank: int = 0):
@@ -386,7 +386,8 @@ def run_gpu(args, rank, world):
     # thread (E2E_CREATORS), this step solves, and the previous step's amplitudes are
     # downloaded on another thread (the C calls release the GIL; each batch has its own
     # stream).  The timed run starts before its first create and ends after its last
-    # download: the pipeline's fill and drain are inside it.
+    # download: the pipeline's fill and drain (one create and one download that overlap
+    # nothing) are inside it, spread over at least 32 steps.
     out_bufs = [pinned_buffer(batch.amplitude_count()) for _ in range(2)]
     xfer = [0, 0]
     stage_ms = {"create": [], "solve": [], "download": []}   # host wall time of each stage
@@ -435,7 +436,7 @@ def run_gpu(args, rank, world):
         e2e_ms = [float("nan")]
     else:
         e2e_run(max(6, args.warmup))
-        e2e_runs = [e2e_run(max(10, 4 * args.steps)) for _ in range(3)]
+        e2e_runs = [e2e_run(max(32, 4 * args.steps)) for _ in range(3)]
         e2e_ms = [float(np.median(e2e_runs))]
     h2d, d2h = xfer
     # the other precision on the same batch (timed the same way): mixed beside FP64

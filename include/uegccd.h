@@ -132,23 +132,60 @@ int uegccd_ctx_set_integrals(UegccdCtx *ctx, int32_t core_n, double gapii);
  * range_flags != 0 then use the flag's integrals for every term and the energy (CCD.f90:
  * 216-217, 491-492, 555-556, 620-917); the MP2 start keeps the plain integrals
  * (MP2.f90:61-62).  screening = HEGData%ScreeningDistance (HEG.f90:512).  flag 0 clears.
- * Terms with different flags, and range-separated dRPA, return UEGCCD_ERR_UNSUPPORTED. */
+ * Terms with different flags, and range-separated dRPA, take uegccd_ctx_set_eri below. */
 int uegccd_ctx_set_range(UegccdCtx *ctx, int32_t flag, double screening);
+
+/* ---- the two-channel form: per-term integral flags, Do Rings without Do XRings ----------
+ * The reference iterates T2abab and T2abba (CCD.f90:18-183) and gives each integral of each
+ * CCD term its own range flag, the Max(...) of the term's flags (CCD.f90:620-937).  Once a
+ * term's direct and exchange integrals differ, or only one of Do Rings / Do XRings is on,
+ * T2abba(i,j,a) = -T2abab(i,j,b) no longer holds.  The two-channel form keeps both arrays as
+ * the reference does, in its layout, with per-integral flag tables.
+ *
+ * The fifteen "... Range" Input values (UEGInfo%IRange*, read in IO.f90), as CasedERI
+ * applies them (HEG.f90:689-774): 0 Coulomb, 1 short range, 2 long range, 3 none. */
+typedef struct {
+    int32_t ring, xring, ladder, mosaic, driver_direct, driver_exchange, energy;
+    int32_t lin_rings, quad_rings, direct_rings, exchange_rings;
+    int32_t lin_ladders, quad_ladders, direct_ladders, exchange_ladders;
+} UegccdRangeTerms;
+
+/* SetPointers in full (Main.f90:274-318): with the options' core_n and gapii, the flags and
+ * Safe ERI pick CasedERI (Safe ERI, or flags, GapII and CoreN all set), NoCaseERI, CoreERI,
+ * GapERI or BaseERI, and every later uegccd_ccd, uegccd_drpa, uegccd_ccd_g2_2ch and
+ * uegccd_drpa_g2 on the context runs the two-channel (dRPA: general-flag) form with them.
+ * screening = HEGData%ScreeningDistance (HEG.f90:512), > 0 when a flag is 1 or 2.  Flags
+ * outside 0..3 return UEGCCD_ERR_ARG; flags == NULL returns the context to the spin-adapted
+ * kernels.  Without this call, uegccd_ccd takes the two-channel form by itself when
+ * do_ring != do_xring (with the integrals of core_n and gapii). */
+int uegccd_ctx_set_eri(UegccdCtx *ctx, const UegccdRangeTerms *flags, int32_t safe_eri, double screening);
+
+/* TermsWrapper (CCD.f90:146-181) on both channels in the two-channel form, with the
+ * integrals of the last uegccd_ctx_set_eri (none: the context's core_n / gapii integrals):
+ * G2abab and G2abba of the terms in term_mask (as uegccd_ccd_g2), reference layout. */
+int uegccd_ccd_g2_2ch(UegccdCtx *ctx, const double *t_abab, const double *t_abba, int32_t term_mask,
+                      double *g_abab, double *g_abba);
+/* The dRPA residual G2 (dRPA.f90:339-551: bit0 drivers, bit1 mosaics, bit3 rings) of one
+ * amplitude array, with the same integrals. */
+int uegccd_drpa_g2(UegccdCtx *ctx, const double *t2, int32_t term_mask, double *g2);
 
 /* DrvMBPT (MP2.f90:11-157): writes the MP2 amplitudes T2aaaa/T2abab/T2abba (each
  * may be NULL) and E(2).  Its structure factor is uegccd_structure_factor of T2abab. */
 int uegccd_mp2(UegccdCtx *ctx, double *t_aaaa, double *t_abab, double *t_abba, double *e2);
 
 /* DrvCCD (CCD.f90:18-183): iterates from the amplitudes given (the MP2 guess in
- * Main.f90:85-89) and writes the converged amplitudes back in place.  Requires
- * do_ring == do_xring: the library stores the spin-adapted amplitude T2abab alone,
- * with T2abba(i,j,a) = -T2abab(i,j,b) and T2aaaa = T2abab + T2abba, which the
- * reference's equations keep only when rings and crossed rings are both on or both off. */
+ * Main.f90:85-89) and writes the converged amplitudes back in place.  With do_ring ==
+ * do_xring and no uegccd_ctx_set_eri, the library stores the spin-adapted amplitude T2abab
+ * alone, with T2abba(i,j,a) = -T2abab(i,j,b) and T2aaaa = T2abab + T2abba, which the
+ * reference's equations keep only when rings and crossed rings are both on or both off.
+ * Otherwise it runs the two-channel form: t_abba is read as given (NULL: from t_abab by the
+ * MP2 relation) and all three arrays are written back. */
 int uegccd_ccd(UegccdCtx *ctx, const UegccdOptions *opt, double *t_aaaa, double *t_abab,
                double *t_abba, UegccdResult *res);
 
 /* DrvdRPA (dRPA.f90:23-174) on one amplitude array (the caller passes T2aaaa of
- * the MP2 step, Main.f90:91); returns Ec(dRPA) and Ec(SOSEX). */
+ * the MP2 step, Main.f90:91); returns Ec(dRPA) and Ec(SOSEX).  After uegccd_ctx_set_eri
+ * each term takes its own flag; the energy keeps flag 0 (dRPA.f90:206-207). */
 int uegccd_drpa(UegccdCtx *ctx, const UegccdOptions *opt, double *t2, UegccdResult *res);
 
 /* One CCD residual G2 of the selected terms (TermsWrapper, CCD.f90:146-181; bit0

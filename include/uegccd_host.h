@@ -40,6 +40,7 @@ typedef struct {
     int32_t do_only_mp2_grid;        /* DoOnlyMP2Grid: stop after the first DrvMBPT (MP2.f90:152-154) */
     int32_t core_factor_set;         /* the Input sets CoreFactor (ReadInput then writes fort.61)    */
     int32_t range_uniform;           /* the value of all fifteen "... Range" flags, -1 if they differ */
+    UegccdRangeTerms range_terms;    /* the fifteen "... Range" values themselves                     */
 } UegccdInput;
 
 typedef struct {

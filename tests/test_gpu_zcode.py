@@ -133,7 +133,7 @@ def test_range_flags_follow_setpointers(goldens, tmp_path, monkeypatch):
     """A "... Range" Input value acts only through CasedERI, which SetPointers (Main.f90:
     299-302) picks under Safe ERI (or with GapII and CoreN both set).  Without it the
     reference's ERI ignores the flags: the program runs as without them.  Under Safe ERI
-    the range-separated integrals are outside the GPU path and the run fails."""
+    the flags act, and the program's answer changes."""
     g = goldens["G5"]
     base = dict(g["keys"])
     base.update({"Safe ERI": "F", "TACalcN": "2"})
@@ -152,12 +152,12 @@ def test_range_flags_follow_setpointers(goldens, tmp_path, monkeypatch):
     d = tmp_path / "cased"
     d.mkdir()
     keys = dict(base)
-    keys.update({"Safe ERI": "T", "Rings Range": "1"})
+    keys.update({"Safe ERI": "T", "Rings Range": "1", "Energy Range": "2"})
     (d / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))
     _write_twists(d / "Twists", g["ta_twists"][:2])
     monkeypatch.chdir(d)
-    with pytest.raises(Exception):
-        zcode.run("Input", "Twists")
+    zcode.run("Input", "Twists")
+    assert (d / "Output").read_text() != outs[0][0]
 
 
 def test_ta_program_with_one_range_flag(goldens, tmp_path, monkeypatch):
@@ -182,6 +182,37 @@ def test_ta_program_with_one_range_flag(goldens, tmp_path, monkeypatch):
     vals.update(keys)
     per, special, st, _ = Oracle(vals).twist_average(np.array(g["ta_twists"][:3]))
     np.testing.assert_allclose(rows[:, 3:6], per, rtol=0, atol=1e-12)
+    out = (tmp_path / "Output").read_text()
+    ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
+    assert abs(ecs[-1] - st.ecorr) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["per-term flags", "rings without crossed rings"])
+def test_ta_program_two_channel(goldens, tmp_path, monkeypatch, case):
+    """The G5 program on 3 twists, with CCD at every twist (DoCalcTACCD), in the two-channel
+    form: "... Range" values that differ between terms under Safe ERI (direct and exchange
+    integrals of a term on different flags), or Do XRings F.  Every twist's CCD runs in its
+    own context; fort.59 (E_HF, E_MP2, Ec(CCD) per twist) and the special-twist Ec(CCD)
+    against the oracle's twist average."""
+    from oracle.oracle import Oracle, parse_input_text
+
+    g = goldens["G5"]
+    keys = dict(g["keys"])
+    keys.update({"TACalcN": "3", "DoCalcTACCD": "T"})
+    if case == "per-term flags":
+        keys.update({"Safe ERI": "T", "Rings Range": "1", "ExRings Range": "2", "Ladders Range": "1",
+                     "DriverEx Range": "3", "Energy Range": "2"})
+    else:
+        keys.update({"Do XRings": "F"})
+    (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))
+    _write_twists(tmp_path / "Twists", g["ta_twists"][:3])
+    monkeypatch.chdir(tmp_path)
+    zcode.run("Input", "Twists")
+    rows = np.array([[float(x) for x in l.split()] for l in (tmp_path / "fort.59").read_text().splitlines()[:3]])
+    vals = parse_input_text("")
+    vals.update(keys)
+    per, special, st, _ = Oracle(vals).twist_average(np.array(g["ta_twists"][:3]))
+    np.testing.assert_allclose(rows[:, 3:6], per, rtol=0, atol=1e-10)
     out = (tmp_path / "Output").read_text()
     ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
     assert abs(ecs[-1] - st.ecorr) < 1e-9

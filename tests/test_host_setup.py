@@ -91,3 +91,6 @@ def test_read_input_range_flags(tmp_path, flags, total, uniform):
     p = heg.read_input(str(tmp_path / "Input"), require_all=False)
     assert p.range_flags == total
     assert p.range_uniform == uniform
+    # the values themselves, in the order of UegccdRangeTerms (the Input's order)
+    terms = [getattr(p.range_terms, name) for name in _capi.RANGE_TERMS]
+    assert terms == [int(flags.get(k, 0)) for k in RANGE_KEYS]

@@ -71,6 +71,16 @@ class SfGrid(C.Structure):
     _fields_ = [(k, C.POINTER(C.c_double)) for k in ("sum", "dsum", "xsum", "g", "v")]
 
 
+RANGE_TERMS = ("ring", "xring", "ladder", "mosaic", "driver_direct", "driver_exchange", "energy", "lin_rings",
+               "quad_rings", "direct_rings", "exchange_rings", "lin_ladders", "quad_ladders", "direct_ladders",
+               "exchange_ladders")
+
+
+class RangeTerms(C.Structure):
+    """UegccdRangeTerms: the fifteen "... Range" Input values, in the Input file's order."""
+    _fields_ = [(k, C.c_int32) for k in RANGE_TERMS]
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
@@ -101,6 +111,9 @@ def lib() -> C.CDLL:
         L.uegccd_ctx_set_integrals.argtypes = [vp, C.c_int32, C.c_double]
         L.uegccd_batch_set_integrals.argtypes = [vp, C.c_int32, C.c_double]
         L.uegccd_ctx_set_range.argtypes = [vp, C.c_int32, C.c_double]
+        L.uegccd_ctx_set_eri.argtypes = [vp, P(RangeTerms), C.c_int32, C.c_double]
+        L.uegccd_ccd_g2_2ch.argtypes = [vp, dp, dp, C.c_int32, dp, dp]
+        L.uegccd_drpa_g2.argtypes = [vp, dp, C.c_int32, dp]
         L.uegccd_batch_set_range.argtypes = [vp, C.c_int32, C.c_double]
         L.uegccd_sf_length.argtypes = [P(System)]
         L.uegccd_sf_length.restype = C.c_int32

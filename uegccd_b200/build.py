@@ -20,11 +20,11 @@ ZCODE = os.path.join(PKG, "uegccd_zcode")
 OBJDIR = os.path.join(PKG, "_build")
 
 SOURCES = ["capi.cu", "kernels_fp64.cu", "kernels_tc.cu", "plan.cpp", "heg_host.cpp", "zcode.cpp", "mp2_static.cu",
-           "diis_api.cu", "heg_device.cu"]
+           "diis_api.cu", "heg_device.cu", "two_channel.cu"]
 # bench.py's FP64 tensor-core peak measurement: a library of its own beside bench.py
 BENCH_PEAK_SRC = os.path.join(ROOT, "bench_peak.cu")
 BENCH_PEAK_LIB = os.path.join(ROOT, "bench_peak.so")
-HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h", "listdir.h", "heg_device.h"]
+HEADERS = ["kernels.h", "plan.h", "uegccd_internal.h", "listdir.h", "heg_device.h", "two_channel.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 

@@ -29,6 +29,7 @@
 #include "../../include/uegccd.h"
 #include "kernels.h"
 #include "plan.h"
+#include "two_channel.h"
 #include "uegccd_internal.h"
 
 using namespace uegccd;
@@ -418,6 +419,13 @@ struct UegccdBatch {
 
 struct UegccdCtx {
     std::unique_ptr<UegccdBatch> batch;
+    // the two-channel form (two_channel.cu), made on first use, and the integral selection of
+    // uegccd_ctx_set_eri
+    std::unique_ptr<uegccd::TwoChannel> tc;
+    bool eri_set = false;
+    UegccdRangeTerms flags{};
+    int safe_eri = 0;
+    double screening = 0.0;
 };
 
 namespace {
@@ -1053,18 +1061,25 @@ int mixed_alloc(UegccdBatch &b)
     return 0;
 }
 
-int validate_options(const UegccdOptions *o, int drpa, const UegccdBatch &b)
+int validate_options(const UegccdOptions *o, int drpa, const UegccdBatch &b, bool two_channel = false)
 {
     if (!o) return fail(UEGCCD_ERR_ARG, "null options");
-    if (o->range_flags != 0 && drpa)
-        return fail(UEGCCD_ERR_UNSUPPORTED, "range-separated dRPA is outside the GPU path");
-    if (o->range_flags != 0 && b.range_flag == 0)
-        return fail(UEGCCD_ERR_UNSUPPORTED,
-                    "range-separated integrals: set one flag for every term with uegccd_*_set_range "
-                    "(terms with different flags are outside the GPU path)");
-    if (!drpa && (o->do_ring != 0) != (o->do_xring != 0))
-        return fail(UEGCCD_ERR_UNSUPPORTED,
-                    "Do Rings and Do XRings must agree: alone, either breaks the spin symmetry the GPU path uses");
+    if (two_channel) {
+        // the two-channel form takes its integrals from uegccd_ctx_set_eri, not range_flags
+        if (o->precision != UEGCCD_FP64) return fail(UEGCCD_ERR_UNSUPPORTED, "the two-channel form runs in FP64");
+    } else {
+        if (o->range_flags != 0 && drpa)
+            return fail(UEGCCD_ERR_UNSUPPORTED,
+                        "range-separated dRPA takes per-term flags: uegccd_ctx_set_eri on a context");
+        if (o->range_flags != 0 && b.range_flag == 0)
+            return fail(UEGCCD_ERR_UNSUPPORTED,
+                        "range-separated integrals: set one flag for every term with uegccd_*_set_range, or "
+                        "per-term flags with uegccd_ctx_set_eri on a context");
+        if (!drpa && (o->do_ring != 0) != (o->do_xring != 0))
+            return fail(UEGCCD_ERR_UNSUPPORTED,
+                        "Do Rings and Do XRings must agree in a batch solve: alone, either breaks the spin "
+                        "symmetry of the batched kernels (a context's uegccd_ccd runs the two-channel form)");
+    }
     if (o->max_iter <= 0 || !(o->tol > 0) || !(o->denom_factor != 0)) return fail(UEGCCD_ERR_ARG, "bad iteration options");
     if (o->scheme != UEGCCD_REPLAY && o->scheme != UEGCCD_DIIS) return fail(UEGCCD_ERR_ARG, "unknown scheme");
     if (o->scheme == UEGCCD_DIIS && (o->ndiis < 2 || o->ndiis > kDiisMax))
@@ -1549,6 +1564,39 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
 
 // Every call on a batch or context runs on the device the object was created on (whatever
 // device the calling thread has current), and is refused once the batch is unusable.
+// The two-channel state of a context, made on first use in the context's batch memory, with
+// the integrals of the context's selection (uegccd_ctx_set_eri; none: SetPointers without
+// range flags) for CoreN and GapII.
+int two_channel_ready(UegccdCtx &c, int core_n, double gapii)
+{
+    UegccdBatch &b = *c.batch;
+    if (!c.tc) {
+        struct Arena {
+            UegccdBatch *b;
+            UegccdBatch::Mark m;
+        };
+        auto ar = std::make_shared<Arena>(Arena{&b, b.mark()});
+        uegccd::TcAlloc al;
+        al.get = [ar](void **p, size_t bytes) {
+            char *q = nullptr;
+            const int rc = ar->b->alloc(q, bytes);
+            *p = q;
+            return rc;
+        };
+        al.begin = [ar]() { ar->m = ar->b->mark(); };
+        al.rollback = [ar]() { ar->b->rollback(ar->m); };
+        auto tc = std::make_unique<uegccd::TwoChannel>();
+        const int rc = tc->init(b.sys[0], b.stream, al);
+        if (rc) return rc;
+        c.tc = std::move(tc);
+    }
+    UegccdRangeTerms none{};
+    const UegccdRangeTerms &fl = c.eri_set ? c.flags : none;
+    const int safe = c.eri_set ? c.safe_eri : 0;
+    const int routine = uegccd::tc_pick_routine(fl, safe, core_n, gapii);
+    return c.tc->set_integrals(routine, fl, core_n, gapii, c.screening);
+}
+
 #define ENTER_DEVICE(bp)                                                                               \
     DeviceScope dev_scope_((bp)->dev);                                                                 \
     if (dev_scope_.rc != cudaSuccess)                                                                  \
@@ -1668,9 +1716,14 @@ int uegccd_ccd(UegccdCtx *c, const UegccdOptions *opt, double *t_aaaa, double *t
     if (!c || !t_abab || !res) return fail(UEGCCD_ERR_ARG, "null argument");
     ENTER(c->batch);
     UegccdBatch &b = *c->batch;
-    int rc = validate_options(opt, 0, b);
+    const bool two = opt && (c->eri_set || (opt->do_ring != 0) != (opt->do_xring != 0));
+    int rc = validate_options(opt, 0, b, two);
     if (rc) return rc;
     if ((rc = set_integrals(b, opt->core_n, opt->gapii))) return rc;
+    if (two) {
+        if ((rc = two_channel_ready(*c, opt->core_n, opt->gapii))) return rc;
+        return c->tc->solve(*opt, false, b.sys[0].eigen, t_aaaa, t_abab, t_abba, *res);
+    }
     if ((rc = pack_from_host(b, 0, t_abab))) return rc;
     int st = run_solves(b, opt, 0, res);
     if (st < 0) return st;
@@ -1683,9 +1736,13 @@ int uegccd_drpa(UegccdCtx *c, const UegccdOptions *opt, double *t2, UegccdResult
     if (!c || !t2 || !res) return fail(UEGCCD_ERR_ARG, "null argument");
     ENTER(c->batch);
     UegccdBatch &b = *c->batch;
-    int rc = validate_options(opt, 1, b);
+    int rc = validate_options(opt, 1, b, c->eri_set);
     if (rc) return rc;
     if ((rc = set_integrals(b, opt->core_n, opt->gapii))) return rc;
+    if (c->eri_set) {
+        if ((rc = two_channel_ready(*c, opt->core_n, opt->gapii))) return rc;
+        return c->tc->solve(*opt, true, b.sys[0].eigen, nullptr, t2, nullptr, *res);
+    }
     if ((rc = pack_from_host(b, 0, t2))) return rc;
     int st = run_solves(b, opt, 1, res);
     if (st < 0) return st;
@@ -1750,6 +1807,46 @@ int uegccd_structure_factor(UegccdCtx *c, const double *t_abab, const UegccdSfGr
 int uegccd_ccd_g2(UegccdCtx *c, const double *t_abab, int32_t mask, double *g_abab)
 {
     return uegccd_ccd_g2_ex(c, t_abab, mask, UEGCCD_FP64, g_abab);
+}
+
+int uegccd_ctx_set_eri(UegccdCtx *c, const UegccdRangeTerms *flags, int32_t safe_eri, double screening)
+{
+    if (!c) return fail(UEGCCD_ERR_ARG, "null context");
+    if (!flags) {
+        c->eri_set = false;
+        return 0;
+    }
+    const int32_t *p = &flags->ring;
+    bool screened = false;
+    for (int k = 0; k < 15; k++) {
+        if (p[k] < 0 || p[k] > 3) return fail(UEGCCD_ERR_ARG, "range flags must be 0, 1, 2 or 3");
+        screened = screened || p[k] == 1 || p[k] == 2;
+    }
+    if (screened && !(screening > 0.0)) return fail(UEGCCD_ERR_ARG, "screening distance must be > 0");
+    c->flags = *flags;
+    c->safe_eri = safe_eri ? 1 : 0;
+    c->screening = screening;
+    c->eri_set = true;
+    return 0;
+}
+
+int uegccd_ccd_g2_2ch(UegccdCtx *c, const double *t_abab, const double *t_abba, int32_t mask, double *g_abab,
+                      double *g_abba)
+{
+    if (!c || !t_abab || !t_abba || !g_abab || !g_abba) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(c->batch);
+    int rc = two_channel_ready(*c, c->batch->core_n, c->batch->gapii);
+    if (rc) return rc;
+    return c->tc->ccd_g2(t_abab, t_abba, mask, g_abab, g_abba);
+}
+
+int uegccd_drpa_g2(UegccdCtx *c, const double *t2, int32_t mask, double *g2)
+{
+    if (!c || !t2 || !g2) return fail(UEGCCD_ERR_ARG, "null argument");
+    ENTER(c->batch);
+    int rc = two_channel_ready(*c, c->batch->core_n, c->batch->gapii);
+    if (rc) return rc;
+    return c->tc->drpa_g2(t2, mask, g2);
 }
 
 int uegccd_batch_create(const UegccdSystem *systems, int32_t n, UegccdBatch **out)

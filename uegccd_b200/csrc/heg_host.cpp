@@ -465,12 +465,15 @@ int uegccd_read_input(const char *path, int32_t require_all, UegccdInput *in)
         }
     }
     in->fcut2ecut = fcut2ecut;
-    {   // one value for all fifteen range flags, or -1
+    {   // the fifteen range flags (UegccdRangeTerms keeps the Input's order), and one value for
+        // all of them, or -1
         int v = 0;
         bool first = true, same = true;
+        int32_t *terms = &in->range_terms.ring;
         for (int k = 10; k < 25; k++) {   // kNames[10..24]: the "... Range" keys
             const auto it = range.find(kNames[k]);
             const int r = it == range.end() ? 0 : it->second;
+            terms[k - 10] = r;
             if (first) v = r;
             else if (r != v) same = false;
             first = false;

@@ -150,6 +150,17 @@ UegccdOptions options_for(const UegccdInput &in, int32_t scheme)
     return o;
 }
 
+// The two-channel form (uegccd_ctx_set_eri): CCD with only one of rings / crossed rings, or
+// with range flags that differ between terms under CasedERI; dRPA with range flags under
+// CasedERI.  *eri: CasedERI applies the flags, so the context takes them with set_eri.
+bool two_channel_of(const UegccdInput &in, const UegccdOptions &opt, bool *eri)
+{
+    const bool cased = in.safe_eri || (in.range_flags > 0 && opt.gapii > 0.0 && opt.core_n > 0);
+    *eri = cased;
+    if (in.do_drpa_sosex) return cased && in.range_flags > 0;
+    return in.do_ring != in.do_xring || (cased && in.range_uniform < 0);
+}
+
 // ---- structure-factor files (fort.80, fort.81), opened on their first block
 
 struct SfGrids {
@@ -239,6 +250,10 @@ int mp2_then_cc(const UegccdInput &in, const UegccdSystem &sys, double ehf, cons
     // one range flag for every term (otherwise the solve refuses range_flags != 0)
     if (!rc && opt.range_flags != 0 && in.range_uniform > 0)
         rc = uegccd_ctx_set_range(ctx, in.range_uniform, screening_of(in, sys.L));
+    // the two-channel form: the fifteen flags themselves under CasedERI
+    bool eri = false;
+    if (!rc && two_channel_of(in, opt, &eri) && eri)
+        rc = uegccd_ctx_set_eri(ctx, &in.range_terms, in.safe_eri, screening_of(in, sys.L));
     if (!rc) rc = uegccd_mp2(ctx, x.aaaa.data(), x.abab.data(), x.abba.data(), &e2);
     if (rc) {
         zfail(rc, uegccd_last_error());
@@ -444,6 +459,11 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
     // structure-factor grids are built on the plain integrals only
     if (opt.range_flags != 0 && (in.do_sf_calc_mp2 || in.do_sf_calc_ccd))
         return zfail(UEGCCD_ERR_UNSUPPORTED, "structure factors of range-separated integrals are outside the GPU path");
+    bool two_eri = false;
+    const bool two = two_channel_of(in, opt, &two_eri);
+    // the structure-factor grids read spin-adapted amplitudes
+    if (two && in.do_sf_calc_ccd && !in.do_drpa_sosex)
+        return zfail(UEGCCD_ERR_UNSUPPORTED, "structure factors of two-channel CCD amplitudes are outside the GPU path");
     UegccdHegInfo info;
     UegccdSystem sys;
     UegccdResult res;
@@ -521,9 +541,37 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
         if (cc_sf && sf.mp2_in_cc) mp2_80[t] = sf_block(g, true);
     }
     std::vector<UegccdResult> br(nset);
+    std::vector<std::vector<double>> two_en, two_dt;   // the two-channel solves' iteration tables
     if (in.do_calc_ta_ccd && !in.do_only_mp2_grid) {
-        rc = uegccd_batch_solve(b, &opt, in.do_drpa_sosex, mp2.data(), br.data());
-        if (rc < 0) return zfail(rc, uegccd_last_error());
+        if (two) {
+            // one context per twist: the two-channel form runs one system at a time
+            two_en.assign(nset, std::vector<double>(1100));
+            two_dt.assign(nset, std::vector<double>(1100));
+            for (int t = 0; t < nset; t++) {
+                Amps x(systems[t]);
+                UegccdOptions o = opt;
+                o.energies = two_en[t].data();
+                o.dts = two_dt[t].data();
+                o.max_rec = 1100;
+                UegccdCtx *ctx = nullptr;
+                if (uegccd_ctx_create(&systems[t], &ctx)) return zfail(UEGCCD_ERR_CUDA, uegccd_last_error());
+                double e2 = 0.0;
+                rc = uegccd_ctx_set_integrals(ctx, opt.core_n, opt.gapii);
+                if (!rc && two_eri)
+                    rc = uegccd_ctx_set_eri(ctx, &in.range_terms, in.safe_eri, screening_of(in, systems[t].L));
+                if (!rc) rc = uegccd_mp2(ctx, x.aaaa.data(), x.abab.data(), x.abba.data(), &e2);
+                if (!rc)
+                    rc = in.do_drpa_sosex ? uegccd_drpa(ctx, &o, x.aaaa.data(), &br[t])
+                                          : uegccd_ccd(ctx, &o, x.aaaa.data(), x.abab.data(), x.abba.data(), &br[t]);
+                if (rc < 0) zfail(rc, uegccd_last_error());
+                uegccd_ctx_destroy(ctx);
+                if (rc < 0) return rc;
+                rc = 0;
+            }
+        } else {
+            rc = uegccd_batch_solve(b, &opt, in.do_drpa_sosex, mp2.data(), br.data());
+            if (rc < 0) return zfail(rc, uegccd_last_error());
+        }
     }
     FILE *out = std::fopen("Output", "a");
     if (!out) return zfail(UEGCCD_ERR_ARG, "cannot append to Output");
@@ -546,8 +594,13 @@ static int run_zcode(const char *input_path, const char *twists_path, int32_t sc
                 return rc;
             }
             int32_t nrec = 0;
-            uegccd_batch_history(b, t, en.data(), dt.data(), 1100, &nrec);
-            write_cc(out, in, in.do_drpa_sosex, br[t], en.data(), dt.data(), nrec, hf[t]);
+            if (two) {
+                nrec = br[t].n_recorded;
+                write_cc(out, in, in.do_drpa_sosex, br[t], two_en[t].data(), two_dt[t].data(), nrec, hf[t]);
+            } else {
+                uegccd_batch_history(b, t, en.data(), dt.data(), 1100, &nrec);
+                write_cc(out, in, in.do_drpa_sosex, br[t], en.data(), dt.data(), nrec, hf[t]);
+            }
             // HEGData%ECorr after the driver: Ec(SOSEX) for a converged dRPA, else the last energy
             cc[t] = (in.do_drpa_sosex && !br[t].fail) ? br[t].ecorr_sosex : br[t].ecorr;
         }

@@ -24,7 +24,7 @@ class Input(C.Structure):
         ("fcut", C.c_double), ("corefcut", C.c_double), ("fcut2ecut", C.c_int32), ("gapii", C.c_double),
         ("do_skip_ta", C.c_int32), ("do_sf_calc_mp2", C.c_int32),
         ("do_sf_calc_ccd", C.c_int32), ("do_only_mp2_grid", C.c_int32), ("core_factor_set", C.c_int32),
-        ("range_uniform", C.c_int32),
+        ("range_uniform", C.c_int32), ("range_terms", capi.RangeTerms),
     ]
 
 

@@ -69,6 +69,36 @@ class Context:
         used by the CCD calls whose options carry range_flags != 0."""
         capi.check(capi.lib().uegccd_ctx_set_range(self._h, int(flag), float(screening)))
 
+    def set_eri(self, flags=None, safe_eri: bool = False, screening: float = 0.0) -> None:
+        """SetPointers in full for the two-channel form: flags maps the names of
+        capi.RANGE_TERMS to the "... Range" Input values (missing: 0).  Every later ccd, drpa,
+        ccd_g2_2ch and drpa_g2 takes per-term integral flags; None returns to the spin-adapted
+        kernels."""
+        if flags is None:
+            capi.check(capi.lib().uegccd_ctx_set_eri(self._h, None, 0, 0.0))
+            return
+        unknown = set(flags) - set(capi.RANGE_TERMS)
+        if unknown:
+            raise ValueError(f"unknown range terms: {sorted(unknown)}")
+        rt = capi.RangeTerms(*[int(flags.get(k, 0)) for k in capi.RANGE_TERMS])
+        capi.check(capi.lib().uegccd_ctx_set_eri(self._h, C.byref(rt), 1 if safe_eri else 0, float(screening)))
+
+    def ccd_g2_2ch(self, t_abab, t_abba, mask: int = 31):
+        """TermsWrapper on both channels: (G2abab, G2abba) of the selected terms."""
+        ga, gb = self.zeros_t(), self.zeros_t()
+        ta = np.ascontiguousarray(t_abab, dtype=np.float64)
+        tb = np.ascontiguousarray(t_abba, dtype=np.float64)
+        capi.check(capi.lib().uegccd_ccd_g2_2ch(self._h, capi.dptr(ta), capi.dptr(tb), mask, capi.dptr(ga),
+                                                 capi.dptr(gb)))
+        return ga, gb
+
+    def drpa_g2(self, t2, mask: int = 11) -> np.ndarray:
+        """The dRPA residual G2 of one amplitude array (bit0 drivers, bit1 mosaics, bit3 rings)."""
+        g = self.zeros_t()
+        t = np.ascontiguousarray(t2, dtype=np.float64)
+        capi.check(capi.lib().uegccd_drpa_g2(self._h, capi.dptr(t), mask, capi.dptr(g)))
+        return g
+
     def mp2(self):
         """DrvMBPT: returns (E2, T2aaaa, T2abab, T2abba)."""
         ta, tb, tc = self.zeros_t(), self.zeros_t(), self.zeros_t()
