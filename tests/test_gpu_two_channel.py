@@ -82,13 +82,15 @@ def test_two_channel_terms_match_oracle(case):
         ga, gb = o.ccd_g2(tb, tc, mask)
         ha, hb = ctx.ccd_g2_2ch(tb, tc, mask)
         scale = max(np.abs(ga).max(), np.abs(gb).max())
-        assert scale > 0
+        # flag 3 ("none") zeroes whole terms: the rings of "flags 3" vanish
+        assert scale > 0 or (case == "flags 3" and mask == 8)
         assert np.abs(ha - ga).max() <= 1e-12 * scale, (case, mask, "abab")
         assert np.abs(hb - gb).max() <= 1e-12 * scale, (case, mask, "abba")
     for mask in (1, 2, 8, 11):
         g = o.drpa_g2(tb, mask)
         h = ctx.drpa_g2(tb, mask)
         assert np.abs(h - g).max() <= 1e-12 * np.abs(g).max(), (case, mask, "dRPA")
+        assert np.abs(g).max() > 0 or (case == "flags 3" and mask == 8)
 
 
 @pytest.mark.parametrize("rings", [(1, 0), (0, 1)])
@@ -163,6 +165,10 @@ def test_two_channel_diis_reaches_the_replay_answer():
     assert r_diis["ndiis"] == 6
     assert r_diis["niter"] < r_rep["niter"]
     assert abs(r_diis["ecorr"] - r_rep["ecorr"]) < 1e-9
+    # again on the same context: the history left by the first solve changes nothing
+    args = [x.copy() for x in (ta, tb, tc)]
+    rc3, r_again, _, _ = ctx.ccd(*args, do_ring=1, do_xring=0, tol=1e-10, scheme=1, ndiis=6)
+    assert rc3 == 0 and r_again["niter"] == r_diis["niter"] and r_again["ecorr"] == r_diis["ecorr"]
 
 
 def test_two_channel_refusals():
@@ -199,3 +205,33 @@ def test_two_channel_n54_iterations_match_oracle():
     assert np.abs(tb - tb2).max() < 1e-13 and np.abs(tc - tc2).max() < 1e-13
     print(f"two-channel N=54: {r['gpu_ms'] / 4:.3f} ms per iteration (4 residuals + start), "
           f"{r['kernel_launches']} launches")
+
+
+def test_batch_two_channel_matches_oracle():
+    """A batch CCD solve with Do XRings F runs each system in the two-channel form: the
+    oracle's iteration count and energies per twist, T2abab back from the batch, each solve's
+    iteration table; the structure factor (spin-adapted amplitudes only) is refused."""
+    from uegccd_b200 import Batch
+
+    systems, refs = [], []
+    for tw in ((0.1, 0.2, 0.3), (-0.2, 0.05, 0.4)):
+        o, _ = _setup(extra={"Do XRings": "F"}, twist=tw)
+        sc = o.scalars()
+        systems.append((o.nocc, sc["L"], sc["madelung"], o.eigen(), o.nvec()))
+        _, ta2, tb2, tc2, _ = o.mp2()
+        st, en_o, _ = o.ccd(ta2, tb2, tc2)
+        refs.append((st, en_o, tb2))
+    b = Batch(systems)
+    rc, e2, res = b.solve(do_ring=1, do_xring=0)
+    assert rc == 0
+    for s, (st, en_o, tb2) in enumerate(refs):
+        assert res[s]["niter"] == st.niter
+        assert abs(res[s]["ecorr"] - st.ecorr) < 1e-11
+        en, _ = b.history(s)
+        np.testing.assert_allclose(en, en_o, atol=1e-11, rtol=0)
+        assert np.abs(b.amplitudes(s) - tb2).max() < 1e-10
+    with pytest.raises(capi.UegccdError):
+        b.structure_factor(0)
+    # an incremental solve stays spin-adapted: refused
+    with pytest.raises(capi.UegccdError):
+        b.start(do_ring=1, do_xring=0)

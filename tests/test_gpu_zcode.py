@@ -200,8 +200,9 @@ def test_ta_program_two_channel(goldens, tmp_path, monkeypatch, case):
     keys = dict(g["keys"])
     keys.update({"TACalcN": "3", "DoCalcTACCD": "T"})
     if case == "per-term flags":
-        keys.update({"Safe ERI": "T", "Rings Range": "1", "ExRings Range": "2", "Ladders Range": "1",
-                     "DriverEx Range": "3", "Energy Range": "2"})
+        # (many flag sets make the reference's own iteration diverge; this one converges)
+        keys.update({"Safe ERI": "T", "Rings Range": "2", "XRings Range": "1", "Ladders Range": "2",
+                     "DriverEx Range": "1", "Energy Range": "2"})
     else:
         keys.update({"Do XRings": "F"})
     (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in keys.items()))

@@ -128,6 +128,7 @@ def lib() -> C.CDLL:
         L.uegccd_batch_transfer_bytes.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
         L.uegccd_footprint.argtypes = [P(System), C.c_int32, C.c_int32, P(C.c_int64), P(C.c_int64)]
         L.uegccd_batch_start.argtypes = [vp, P(Options), C.c_int32, dp]
+        L.uegccd_batch_history.argtypes = [vp, C.c_int32, dp, dp, C.c_int32, P(C.c_int32)]
         L.uegccd_batch_advance.argtypes = [vp, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Result)]
         L.uegccd_set_memory_limit.argtypes = [C.c_int64]
         L.uegccd_memory_info.argtypes = [P(C.c_int64), P(C.c_int64)]

@@ -338,6 +338,12 @@ struct UegccdBatch {
     // range-separated integrals with one flag for every CCD term (uegccd_*_set_range)
     int range_flag = 0;
     double screening = 0.0;
+    // batch solves in the two-channel form (do_ring != do_xring): one two_channel.cu state per
+    // system, made on first use; each solve's iteration table; two_channel_amps: the batch's
+    // amplitudes hold T2abab of such a solve (the spin relation does not give T2abba)
+    std::vector<std::unique_ptr<uegccd::TwoChannel>> tcs;
+    std::vector<std::vector<double>> tc_en, tc_dt;
+    bool two_channel_amps = false;
     double *sf_grid = nullptr;
     int *sf_err = nullptr;
 
@@ -1567,34 +1573,96 @@ int structure_factor(UegccdBatch &b, int s, const UegccdSfGrid &out)
 // The two-channel state of a context, made on first use in the context's batch memory, with
 // the integrals of the context's selection (uegccd_ctx_set_eri; none: SetPointers without
 // range flags) for CoreN and GapII.
+// A two-channel state for system s of a batch, its device memory carved from the batch's.
+int make_two_channel(UegccdBatch &b, int s, std::unique_ptr<uegccd::TwoChannel> &out)
+{
+    struct Arena {
+        UegccdBatch *b;
+        UegccdBatch::Mark m;
+    };
+    auto ar = std::make_shared<Arena>(Arena{&b, b.mark()});
+    uegccd::TcAlloc al;
+    al.get = [ar](void **p, size_t bytes) {
+        char *q = nullptr;
+        const int rc = ar->b->alloc(q, bytes);
+        *p = q;
+        return rc;
+    };
+    al.begin = [ar]() { ar->m = ar->b->mark(); };
+    al.rollback = [ar]() { ar->b->rollback(ar->m); };
+    auto tc = std::make_unique<uegccd::TwoChannel>();
+    const int rc = tc->init(b.sys[s], b.stream, al);
+    if (rc) return rc;
+    out = std::move(tc);
+    return 0;
+}
+
 int two_channel_ready(UegccdCtx &c, int core_n, double gapii)
 {
-    UegccdBatch &b = *c.batch;
     if (!c.tc) {
-        struct Arena {
-            UegccdBatch *b;
-            UegccdBatch::Mark m;
-        };
-        auto ar = std::make_shared<Arena>(Arena{&b, b.mark()});
-        uegccd::TcAlloc al;
-        al.get = [ar](void **p, size_t bytes) {
-            char *q = nullptr;
-            const int rc = ar->b->alloc(q, bytes);
-            *p = q;
-            return rc;
-        };
-        al.begin = [ar]() { ar->m = ar->b->mark(); };
-        al.rollback = [ar]() { ar->b->rollback(ar->m); };
-        auto tc = std::make_unique<uegccd::TwoChannel>();
-        const int rc = tc->init(b.sys[0], b.stream, al);
+        const int rc = make_two_channel(*c.batch, 0, c.tc);
         if (rc) return rc;
-        c.tc = std::move(tc);
     }
     UegccdRangeTerms none{};
     const UegccdRangeTerms &fl = c.eri_set ? c.flags : none;
     const int safe = c.eri_set ? c.safe_eri : 0;
     const int routine = uegccd::tc_pick_routine(fl, safe, core_n, gapii);
     return c.tc->set_integrals(routine, fl, core_n, gapii, c.screening);
+}
+
+// A batch CCD solve in the two-channel form (do_ring != do_xring): every system in turn from its
+// MP2 amplitudes, on a two-channel state of its own; the integrals of the batch's options (and
+// its uniform range flag, as CasedERI applies it).  The batch keeps each solve's T2abab (what
+// uegccd_batch_get_amplitudes reads) and its iteration table (uegccd_batch_history).
+int run_two_channel_solves(UegccdBatch &b, const UegccdOptions *opt, UegccdResult *res)
+{
+    const int n = b.d.nsolves;
+    if (b.tcs.size() != (size_t)n) b.tcs.resize(n);
+    b.tc_en.assign(n, {});
+    b.tc_dt.assign(n, {});
+    UegccdRangeTerms flags{};
+    int routine = uegccd::tc_pick_routine(flags, 0, opt->core_n, opt->gapii);
+    if (opt->range_flags != 0) {
+        int32_t *p = &flags.ring;
+        for (int k = 0; k < 15; k++) p[k] = b.range_flag;
+        routine = uegccd::TC_CASED;
+    }
+    const int max_rec = std::min(opt->max_iter, 1100);
+    int status = 0;
+    for (int s = 0; s < n; s++) {
+        const SystemHost &H = b.sys[s];
+        const size_t na = (size_t)H.O * H.O * (H.M - H.O);
+        std::vector<double> aa(na), ab(na), ba(na);
+        int rc = unpack_to_host(b, s, b.d.t, ab.data(), ba.data(), aa.data());
+        if (rc) return rc;
+        if (!b.tcs[s] && (rc = make_two_channel(b, s, b.tcs[s]))) return rc;
+        if ((rc = b.tcs[s]->set_integrals(routine, flags, opt->core_n, opt->gapii, b.screening))) return rc;
+        UegccdOptions o = *opt;
+        b.tc_en[s].assign(max_rec, 0.0);
+        b.tc_dt[s].assign(max_rec, 0.0);
+        o.energies = b.tc_en[s].data();
+        o.dts = b.tc_dt[s].data();
+        o.max_rec = max_rec;
+        rc = b.tcs[s]->solve(o, false, H.eigen, aa.data(), ab.data(), ba.data(), res[s]);
+        if (rc < 0 && rc != UEGCCD_ERR_NUMERIC) return rc;
+        b.tc_en[s].resize(res[s].n_recorded);
+        b.tc_dt[s].resize(res[s].n_recorded);
+        // the caller's arrays receive solve 0's table, as run_solves gives them
+        if (s == 0 && opt->max_rec > 0) {
+            const int k = std::min(res[s].n_recorded, opt->max_rec);
+            if (opt->energies) std::copy(b.tc_en[s].begin(), b.tc_en[s].begin() + k, opt->energies);
+            if (opt->dts) std::copy(b.tc_dt[s].begin(), b.tc_dt[s].begin() + k, opt->dts);
+            res[s].n_recorded = k;
+        } else {
+            res[s].n_recorded = 0;
+        }
+        if ((rc = pack_from_host(b, s, ab.data()))) return rc;
+        if (res[s].status == UEGCCD_ERR_NUMERIC) status = UEGCCD_ERR_NUMERIC;
+        if (status == 0 && res[s].status == UEGCCD_NOT_CONVERGED) status = UEGCCD_NOT_CONVERGED;
+    }
+    b.two_channel_amps = true;
+    if (status == UEGCCD_ERR_NUMERIC) fail(status, "non-finite amplitudes or energy");
+    return status;
 }
 
 #define ENTER_DEVICE(bp)                                                                               \
@@ -1873,9 +1941,13 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
     if (!b || !results) return fail(UEGCCD_ERR_ARG, "null argument");
     ENTER(b);
     b->ses.on = false;   // a full solve ends an open incremental one
-    int rc = validate_options(opt, drpa, *b);
+    const bool two = opt && !drpa && (opt->do_ring != 0) != (opt->do_xring != 0);
+    if (two && opt->range_flags != 0 && b->range_flag == 0)
+        return fail(UEGCCD_ERR_UNSUPPORTED, "range-separated integrals: set one flag with uegccd_batch_set_range");
+    int rc = validate_options(opt, drpa, *b, two);
     if (rc) return rc;
     if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
+    b->two_channel_amps = false;
     CU(cudaEventRecord(b->ev_solve0, b->stream));
     b->kt.begin(KID_MP2, b->stream);
     launch_mp2(b->d, b->stream);
@@ -1889,7 +1961,7 @@ int uegccd_batch_solve(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
         launch_to_aaaa(b->d, b->stream);
         std::swap(b->d.t, b->d.t_new);
     }
-    int st = run_solves(*b, opt, drpa, results);
+    int st = two ? run_two_channel_solves(*b, opt, results) : run_solves(*b, opt, drpa, results);
     if (st < 0) return st;
     CU(cudaEventRecord(b->ev_solve1, b->stream));
     CU(cudaEventSynchronize(b->ev_solve1));
@@ -1910,6 +1982,7 @@ int uegccd_batch_start(UegccdBatch *b, const UegccdOptions *opt, int32_t drpa, d
     if (opt->range_flags != 0)
         return fail(UEGCCD_ERR_UNSUPPORTED, "an incremental solve takes no range flags (use uegccd_batch_solve)");
     if ((rc = set_integrals(*b, opt->core_n, opt->gapii))) return rc;
+    b->two_channel_amps = false;
     b->launches = 0;
     launch_mp2(b->d, b->stream);
     launch_reduce(b->d, b->stream);
@@ -2099,6 +2172,7 @@ int uegccd_batch_mp2(UegccdBatch *b, double *e2)
 {
     if (!b) return fail(UEGCCD_ERR_ARG, "null batch");
     ENTER(b);
+    b->two_channel_amps = false;
     b->kt.begin(KID_MP2, b->stream);
     launch_mp2(b->d, b->stream);
     b->kt.end(b->stream);
@@ -2118,6 +2192,8 @@ int uegccd_batch_structure_factor(UegccdBatch *b, int32_t s, const UegccdSfGrid 
 {
     if (!b || !out || s < 0 || s >= b->d.nsolves) return fail(UEGCCD_ERR_ARG, "bad argument");
     ENTER(b);
+    if (b->two_channel_amps)
+        return fail(UEGCCD_ERR_UNSUPPORTED, "structure factors of two-channel amplitudes are outside the GPU path");
     return structure_factor(*b, s, *out);
 }
 
@@ -2172,6 +2248,14 @@ int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dt
     if (!b || s < 0 || s >= b->d.nsolves || max_rec < 0 || !n_recorded)
         return fail(UEGCCD_ERR_ARG, "bad argument");
     ENTER(b);
+    if (b->two_channel_amps) {
+        const auto &e = b->tc_en[s], &d = b->tc_dt[s];
+        const int n = std::min((int)e.size(), max_rec);
+        if (energies) std::copy(e.begin(), e.begin() + n, energies);
+        if (dts) std::copy(d.begin(), d.begin() + n, dts);
+        *n_recorded = n;
+        return UEGCCD_OK;
+    }
     if (b->last_niter.size() != (size_t)b->d.nsolves || !b->ctl.rec_e)
         return fail(UEGCCD_ERR_ARG, "no solve has run on this batch");
     const int n = std::min(b->last_niter[s], max_rec);

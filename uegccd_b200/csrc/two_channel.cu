@@ -431,7 +431,17 @@ __global__ void __launch_bounds__(kThreads) k2_update(View2 D, double df, double
         const int O = D.O;
         const int i = x % O, j = (x / O) % O, a = O + x / (O * O);
         const int b = fnd(D, i, j, a);
-        if (b >= O) {
+        if (b < O) {
+            // no virtual partner: the amplitude stays as it is, and its history entries are
+            // that value and a zero residual, so that the dot products and the extrapolation
+            // read defined values everywhere
+            if (rab) rab[x] = 0.0;
+            if (hab) hab[x] = tab[x];
+            if (!DRPA) {
+                if (rba) rba[x] = 0.0;
+                if (hba) hba[x] = tba[x];
+            }
+        } else {
             const double denom = D.eig[i] + D.eig[j] - D.eig[a] - D.eig[b];
             const double o1 = tab[x], q1 = gab[x];
             if (rab) rab[x] = -q1 + denom * o1;

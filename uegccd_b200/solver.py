@@ -139,17 +139,29 @@ class Context:
         return _sf_call(self._sys, lambda g: capi.lib().uegccd_structure_factor(self._h, capi.dptr(t), g))
 
 
+class SystemSet:
+    """The UegccdSystem structs of many systems, built once.  A host that creates batch after
+    batch of the same systems (a pipeline) passes this to Batch instead of the tuples: the
+    conversion holds the interpreter lock, which the other pipeline threads then wait on."""
+
+    def __init__(self, systems):
+        self.systems = [capi.make_system(*s) for s in systems]
+        self.arr = (capi.System * len(self.systems))(*self.systems)
+
+
 class Batch:
     """uegccd_batch_*: many independent systems solved together."""
 
     def __init__(self, systems, device: int | None = None):
-        """systems: iterable of (nocc, L, madelung, eigen, nvec).  device: the CUDA device to
-        create the batch on (made current on this thread first); None: the current one.  Every
-        later call on the batch runs on its device, from any thread."""
+        """systems: iterable of (nocc, L, madelung, eigen, nvec), or a SystemSet.  device: the
+        CUDA device to create the batch on (made current on this thread first); None: the
+        current one.  Every later call on the batch runs on its device, from any thread."""
         if device is not None:
             capi.set_device(device)
-        self._systems = [capi.make_system(*s) for s in systems]
-        arr = (capi.System * len(self._systems))(*self._systems)
+        sset = systems if isinstance(systems, SystemSet) else SystemSet(systems)
+        self._sset = sset
+        self._systems = sset.systems
+        arr = sset.arr
         self._arr = arr
         h = C.c_void_p()
         capi.check(capi.lib().uegccd_batch_create(arr, len(self._systems), C.byref(h)))
@@ -259,6 +271,14 @@ class Batch:
         t = np.zeros(self._shapes[s])
         capi.check(capi.lib().uegccd_batch_get_amplitudes(self._h, s, capi.dptr(t)))
         return t
+
+    def history(self, s: int, max_rec: int = 1100):
+        """Solve s's per-iteration energies and max|dT| from the last batch solve."""
+        en, dt = np.zeros(max_rec), np.zeros(max_rec)
+        n = C.c_int32()
+        capi.check(capi.lib().uegccd_batch_history(self._h, int(s), capi.dptr(en), capi.dptr(dt), int(max_rec),
+                                                    C.byref(n)))
+        return en[: n.value].copy(), dt[: n.value].copy()
 
     def amplitude_count(self) -> int:
         """Doubles that all_amplitudes fills (every solve's NOcc^2 (NAO - NOcc))."""
