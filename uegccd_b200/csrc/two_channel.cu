@@ -331,12 +331,26 @@ __global__ void __launch_bounds__(kThreads) k2_assemble(View2 D, int mask, const
             g1 += 0.5 * (h2 * tab[y] + h3 * tba[y]);
             g2 += 0.5 * (h2 * tba[y] + h3 * tab[y]);
         }
+        // the particle-particle sum over c, the largest loop of the form: ERI(c,d,a,b) and
+        // ERI(c,d,b,a) (momentum transfers n_c - n_a and n_c - n_b) with the vectors of a and b,
+        // the table rows of both flags and the row (i,j) of FindIndex taken out of the loop
+        const int4 na = __ldg(D.nv + a), nb = __ldg(D.nv + b);
+        const bool core_ab = min(a, b) < D.core_n;
+        const double *vd0 = D.vt + f.lad_lin_d * D.nq, *vd1 = vd0 + 4 * D.nq;
+        const double *vx0 = D.vt + f.lad_lin_x * D.nq, *vx1 = vx0 + 4 * D.nq;
+        const int OO = O * O, x0 = i + O * j;
+        const int *Fij = D.F + x0;
         for (int c = O; c < D.M; c++) {
-            const int d = fnd(D, i, j, c);
+            const int d = __ldg(Fij + OO * c) - 1;
             if (d < O) continue;
-            const double v1 = eri(D, c, d, a, b, f.lad_lin_d), v2 = eri(D, c, d, b, a, f.lad_lin_x);
+            const int4 nc = __ldg(D.nv + c);
+            const int ax = nc.x - na.x, ay = nc.y - na.y, az = nc.z - na.z;
+            const int bx = nc.x - nb.x, by = nc.y - nb.y, bz = nc.z - nb.z;
+            const bool core = core_ab || min(c, d) < D.core_n;
+            const double v1 = __ldg((core ? vd1 : vd0) + (ax * ax + ay * ay + az * az));
+            const double v2 = __ldg((core ? vx1 : vx0) + (bx * bx + by * by + bz * bz));
             if (excluded(v1, v2)) continue;
-            const int y = i + O * (j + O * (c - O));
+            const int y = x0 + OO * (c - O);
             g1 += 0.5 * (v1 * tab[y] - v2 * tba[y]);
             g2 += 0.5 * (v1 * tba[y] - v2 * tab[y]);
         }
