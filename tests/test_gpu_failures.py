@@ -9,6 +9,7 @@
   return UEGCCD_ERR_ALLOC and leaves the library's memory as it was; a cap that holds only
   part of the DIIS history makes the solve take fewer vectors, as SetUpDIISCC steps its
   depth down until Allocate succeeds (DIISCC.f90:22-29).
+* The two-channel form: a NaN ends its solve with UEGCCD_ERR_NUMERIC too.
 * Devices: a batch created on one host thread and solved from another gives the same
   energies, and every call leaves the calling thread's current device as it was.
 """
@@ -145,3 +146,23 @@ def test_batch_created_on_one_thread_solves_on_another():
     assert box["dev_before"] == box["dev_after"]
     for a, c in zip(box["res"], ref):
         assert abs(a["ecorr"] - c["ecorr"]) < 1e-12 and a["niter"] == c["niter"]
+
+
+def test_nan_in_a_two_channel_solve_is_reported():
+    """The two-channel form (Do XRings F) with a NaN planted in the eigenvalues: the solve
+    stops with UEGCCD_ERR_NUMERIC instead of iterating to MaxIter, and the context stays
+    usable: the same solve on clean eigenvalues then converges."""
+    from uegccd_b200 import Context, _capi
+
+    nocc, L, mad, eig, nvec = _sys()
+    ctx = Context(nocc, L, mad, eig, nvec)
+    _, ta, tb, tc = ctx.mp2()
+    bad = eig.copy()
+    bad[nocc + 2] = np.nan
+    ctx.set_eigen(bad)
+    with pytest.raises(_capi.UegccdError) as err:
+        ctx.ccd(ta.copy(), tb.copy(), tc.copy(), do_ring=1, do_xring=0)
+    assert err.value.code == ERR_NUMERIC
+    ctx.set_eigen(eig)
+    rc, r, _, _ = ctx.ccd(ta.copy(), tb.copy(), tc.copy(), do_ring=1, do_xring=0)
+    assert rc == 0 and r["status"] == 0 and np.isfinite(r["ecorr"])
