@@ -583,30 +583,54 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     auto V = [&](int q2) -> double { return vsm ? sv[q2] : __ldg(&vtab[s.vtab0 + q2]); };
     // Rows i <= j only: by the pair symmetry s(l,k,d) = s(k,l,c) for the mirror (l,k) of a
     // row (k,l) and d = K - c, so the mirror row has the same row sum (Joo of l) and adds
-    // the column sums of (k,l) with the columns swapped to their partners.
-    for (int r = 0; r < oc; r++) {
-        const bool diag = r >= B.nd;
-        const int rk = nk[r], rl = nl[r];
-        const double *row = t + B.t0 + (int64_t)r * v;
-        double rs = 0.0;
-        for (int c = tid; c < v; c += kMosThreads) {
-            const double x = row[c];
-            const int ncv = nvc[c];
-            const double vck = V(q2p(ncv, rk));
-            double sval;
-            if (drpa) {
-                sval = 2.0 * vck * x;
-            } else {
-                const double y = row[pc[c]];  // t(kl, d), same row
-                const double vcl = V(q2p(ncv, rl));
-                sval = vck * (2.0 * x - y) - vcl * (x - 2.0 * y);
-            }
-            rs += sval;
-            if (diag) cdg[c] = sval;
-            else coff[c] += sval;
+    // the column sums of (k,l) with the columns swapped to their partners.  Four rows at a
+    // time: their loads go out together (most blocks have at most four rows), and each column
+    // sum still takes the rows in order.
+    constexpr int kR = 4;
+    for (int r0 = 0; r0 < oc; r0 += kR) {
+        const int nr = min(kR, oc - r0);
+        const double *row[kR];
+        int rk[kR], rl[kR];
+        double rs[kR];
+#pragma unroll
+        for (int q = 0; q < kR; q++) {
+            const int r = min(r0 + q, oc - 1);
+            row[q] = t + B.t0 + (int64_t)r * v;
+            rk[q] = nk[r];
+            rl[q] = nl[r];
+            rs[q] = 0.0;
         }
-        for (int off = 16; off > 0; off >>= 1) rs += __shfl_down_sync(0xffffffffu, rs, off);
-        if (lane == 0) wrs[warp * oc + r] = rs;
+        for (int c = tid; c < v; c += kMosThreads) {
+            const int ncv = nvc[c];
+            const int pcc = drpa ? c : pc[c];
+            double x[kR], y[kR];
+#pragma unroll
+            for (int q = 0; q < kR; q++) {
+                x[q] = q < nr ? row[q][c] : 0.0;
+                y[q] = (q < nr && !drpa) ? row[q][pcc] : 0.0;   // t(kl, d), same row
+            }
+#pragma unroll
+            for (int q = 0; q < kR; q++) {
+                if (q >= nr) continue;
+                const double vck = V(q2p(ncv, rk[q]));
+                double sval;
+                if (drpa) {
+                    sval = 2.0 * vck * x[q];
+                } else {
+                    const double vcl = V(q2p(ncv, rl[q]));
+                    sval = vck * (2.0 * x[q] - y[q]) - vcl * (x[q] - 2.0 * y[q]);
+                }
+                rs[q] += sval;
+                if (r0 + q >= B.nd) cdg[c] = sval;
+                else coff[c] += sval;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kR; q++) {
+            double v0 = rs[q];
+            for (int off = 16; off > 0; off >>= 1) v0 += __shfl_down_sync(0xffffffffu, v0, off);
+            if (lane == 0 && q < nr) wrs[warp * oc + r0 + q] = v0;
+        }
     }
     __syncthreads();
     for (int r = tid; r < oc; r += kMosThreads) {
