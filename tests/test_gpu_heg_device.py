@@ -50,3 +50,22 @@ def test_benchmark_twists():
     h = heg.Heg(heg.default_input(nelectron=bench.N_ELECTRONS, maxkpoint=bench.MAXK, rsmin=bench.RS,
                                   rsmax=bench.RS, fcut=bench.FCUT))
     _compare(h, bench.twists(100))
+
+
+@pytest.mark.parametrize("gap, ks", [(0.3, 0), (-0.2, 1)])
+def test_device_twists_with_gap_and_kohn_sham(gap, ks):
+    """uegccd_heg_twists with Gap and DoKS set (HEG.f90:298, 523-525): bitwise against the host
+    set-up of the same twists."""
+    from uegccd_b200 import heg
+
+    tws = np.random.default_rng(11).random((8, 3)) - 0.5
+    inp = heg.default_input(gap=gap, do_ks=ks)
+    dev_sys, dev_ehf = heg.Heg(inp).twist_systems(tws)
+    h = heg.Heg(heg.default_input(gap=gap, do_ks=ks))
+    for k, tw in enumerate(tws):
+        h.change_twist(tw)
+        nocc, L, mad, eig, nv = h.system()
+        assert dev_sys[k][0] == nocc
+        np.testing.assert_array_equal(dev_sys[k][3], eig)
+        np.testing.assert_array_equal(dev_sys[k][4], nv)
+        assert dev_ehf[k] == h.info()["ehf"]

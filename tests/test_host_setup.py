@@ -94,3 +94,23 @@ def test_read_input_range_flags(tmp_path, flags, total, uniform):
     # the values themselves, in the order of UegccdRangeTerms (the Input's order)
     terms = [getattr(p.range_terms, name) for name in _capi.RANGE_TERMS]
     assert terms == [int(flags.get(k, 0)) for k in RANGE_KEYS]
+
+
+@pytest.mark.parametrize("gap, ks", [(0.3, 0), (0.0, 1), (-0.2, 1)])
+def test_setup_with_gap_and_kohn_sham_matches_oracle(gap, ks):
+    """Gap (the occupied eigenvalues take + Madelung - Gap, HEG.f90:525) and DoKS (ExchangeFactor
+    0 drops the exchange term, HEG.f90:298, 523; read at IO.f90:253-254) in the HF set-up, bitwise
+    against the oracle, at the Gamma point and at a twist."""
+    vals = parse_input_text("")
+    vals.update({"Gap": str(gap), "DoKS": "T" if ks else "F"})
+    o = Oracle(vals)
+    h = heg.Heg(heg.default_input(gap=gap, do_ks=ks))
+    for tw in (None, (0.1, -0.2, 0.35)):
+        if tw is not None:
+            h.change_twist(tw)
+            o.change_twist(tw)
+        nocc, L, mad, eig, nv = h.system()
+        assert nocc == o.nocc
+        np.testing.assert_array_equal(eig, o.eigen())
+        np.testing.assert_array_equal(nv, o.nvec())
+        assert h.info()["ehf"] == o.scalars()["ehf"]

@@ -131,7 +131,7 @@ __device__ __forceinline__ int cm_off(int row, int k) { return (row & 7) * 8 + (
 
 // The bulk-copy (TMA) engine: one contiguous global range into this CTA's shared memory,
 // completing `bytes` of the transaction count of an mbarrier.  Addresses 16-byte aligned,
-// sizes multiples of 16; this GPU's own memory only, no multicast.
+// sizes multiples of 16; this GPU's own memory only, each CTA fetching its own copy.
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
