@@ -322,9 +322,10 @@ int uegccd_batch_history(UegccdBatch *b, int32_t s, double *energies, double *dt
 int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max);
 /* Every launch shape the tuner picked on the batch's first CCD solve (new; the reference has
  * no launches): the four ring CTA sizes above, the CTA size of the ring staging kernel (64,
- * 128 or 256), and the ladder tile order (0: block order, 1: the blocks with the most
- * virtuals first, within each row-tile class).  None changes a result.  Writes at most max
- * values; returns how many. */
+ * 128 or 256), the ladder tile order (0: block order, 1: the blocks with the most virtuals
+ * first, within each row-tile class), and the column chunk of the hole-hole intermediate (64
+ * or 32 virtuals per shared-memory stage).  None changes a result.  Writes at most max values;
+ * returns how many. */
 int32_t uegccd_batch_launch_shapes(UegccdBatch *b, int32_t *vals, int32_t max);
 
 /* Live kernel timing: when on, every kernel of a batch solve is bracketed by CUDA

@@ -117,7 +117,7 @@ def test_ring_cta_tuning_and_pinned_download(goldens):
     assert len(th) == 4 and all(t in (32, 64, 128, 256) for t in th)
     shapes = b.launch_shapes()
     assert shapes["ring_threads"] == th and shapes["stage_threads"] in (64, 128, 256)
-    assert shapes["ladder_order"] in ("block", "longest first")
+    assert shapes["ladder_order"] in ("block", "longest first") and shapes["hh_chunk"] in (32, 64)
     n = b.amplitude_count()
     rt = C.CDLL("libcudart.so.12")
     p = C.c_void_p()

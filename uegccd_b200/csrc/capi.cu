@@ -1164,7 +1164,7 @@ int capture_iteration(UegccdBatch &b, const TermFlags &f, double tol, int max_it
 // memory of every ring class, ladder tiles per class, largest block), on the first CCD
 // solve, before the iteration graph is captured.
 std::mutex g_tune_mu;
-std::map<std::vector<int64_t>, std::array<int, kRingClasses + 2>> g_ring_tuning;
+std::map<std::vector<int64_t>, std::array<int, kRingClasses + 3>> g_ring_tuning;
 
 int tune_batch_rings(UegccdBatch &b)
 {
@@ -1186,16 +1186,18 @@ int tune_batch_rings(UegccdBatch &b)
             for (int c = 0; c < kRingClasses; c++) d.ring_threads[c] = it->second[c];
             d.stage_threads = it->second[kRingClasses];
             d.ladder_sched = it->second[kRingClasses + 1];
+            d.hh_kc = it->second[kRingClasses + 2];
             b.rings_tuned = true;
             return 0;
         }
     }
     const int e = tune_rings(d, b.stream);
     if (e != 0) return fail(UEGCCD_ERR_CUDA, std::string("launch-shape tuning: ") + cudaGetErrorString((cudaError_t)e));
-    std::array<int, kRingClasses + 2> th;
+    std::array<int, kRingClasses + 3> th;
     for (int c = 0; c < kRingClasses; c++) th[c] = d.ring_threads[c];
     th[kRingClasses] = d.stage_threads;
     th[kRingClasses + 1] = d.ladder_sched;
+    th[kRingClasses + 2] = d.hh_kc;
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_ring_tuning[key] = th;
     b.rings_tuned = true;
@@ -2021,11 +2023,12 @@ int32_t uegccd_batch_ring_threads(UegccdBatch *b, int32_t *threads, int32_t max)
 int32_t uegccd_batch_launch_shapes(UegccdBatch *b, int32_t *vals, int32_t max)
 {
     if (!b || !vals || max <= 0) return fail(UEGCCD_ERR_ARG, "bad argument");
-    int32_t v[kRingClasses + 2];
+    int32_t v[kRingClasses + 3];
     for (int c = 0; c < kRingClasses; c++) v[c] = b->d.ring_threads[c];
     v[kRingClasses] = b->d.stage_threads;
     v[kRingClasses + 1] = b->d.ladder_sched;
-    const int n = std::min<int>(max, kRingClasses + 2);
+    v[kRingClasses + 2] = b->d.hh_kc;
+    const int n = std::min<int>(max, kRingClasses + 3);
     for (int k = 0; k < n; k++) vals[k] = v[k];
     return n;
 }

@@ -94,6 +94,7 @@ struct DevBatch {
     // virtuals (the longest c loops) first; ladder_sched picks the order the launches use
     LadderTile *tiles_lpt = nullptr, *htiles_lpt = nullptr;
     int ladder_sched = 0;                       // 0: block order, 1: longest first (tune_rings)
+    int hh_kc = 64;                             // the hole-hole intermediate's column chunk: 64 or 32 (tune_rings)
 };
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);

@@ -221,8 +221,7 @@ constexpr int kLadKC = 32;            // c columns per chunk (mode 0)
 constexpr int kLadLd = kLadKC + 4;    // chunk row stride: = 4 mod 16 doubles, conflict-free fragments
 // The hole-hole intermediate (mode 1) has little work per column: wider chunks, fewer of the
 // round trips that bound it
-constexpr int kLadKC1 = 64;
-constexpr int kLadLd1 = kLadKC1 + 4;
+constexpr int kLadKC1 = 64;   // the default; the launch-shape tuner may pick 32 (DevBatch::hh_kc)
 
 __device__ __forceinline__ void cp_async8(double *dst, const double *src)
 {
@@ -237,9 +236,9 @@ size_t ladder_smem_bytes(int max_v, int np)
 {
     return sizeof(double) * (2 * (size_t)np * kLadLd + kVtabSmem) + sizeof(int) * (size_t)max_v;
 }
-size_t ladder1_smem_bytes(int max_v, int np)
+size_t ladder1_smem_bytes(int max_v, int np, int kc)
 {
-    return sizeof(double) * (2 * (size_t)np * kLadLd1 + kVtabSmem) + sizeof(int) * (size_t)max_v;
+    return sizeof(double) * (2 * (size_t)np * (kc + 4) + kVtabSmem) + sizeof(int) * (size_t)max_v;
 }
 
 // PAIRED (blocks with at most 4 rows i <= j, NP = 8): the fragment's 8 columns hold the
@@ -434,7 +433,8 @@ __device__ __forceinline__ void ladder3_tile(const LadderTile &T, const BlockDev
 
 // One kernel per row tile NP (8, 16, 24, 32 pairs): the small tiles need fewer registers
 // and less shared memory, so more CTAs fit on an SM to hide the lookup latency.
-template <int NP, bool PAIRED>
+// KC1: the hole-hole intermediate's column chunk (mode 1), 64 or 32 (the launch-shape tuner's pick)
+template <int NP, bool PAIRED, int KC1 = kLadKC1>
 __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     k_ladder3(const LadderTile *__restrict__ tiles, const BlockDev *__restrict__ blocks,
               const SolveDev *__restrict__ solves, const int16_t *__restrict__ vir,
@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     const SolveDev s = solves[B.solve];
     extern __shared__ double lsm[];
     double *ts = lsm;                              // 2 x NP x (chunk width + 4)
-    double *sv = ts + 2 * NP * (mode == 1 ? kLadLd1 : kLadLd);   // kVtabSmem
+    double *sv = ts + 2 * NP * (mode == 1 ? KC1 + 4 : kLadLd);   // kVtabSmem
     int *nvc = (int *)(sv + kVtabSmem);            // v_K packed n-vectors of the block's virtuals
     const bool vsm = s.q2max < kVtabSmem;
     if (vsm)
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(128, NP <= 8 ? 8 : NP <= 16 ? 6 : 4)
     double *out = mode == 0 ? g : H;
     // the hole-hole intermediate (mode 1) may split its c sum across the warps
     if (mode == 1)
-        ladder3_tile<NP, true, PAIRED, kLadKC1>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv,
+        ladder3_tile<NP, true, PAIRED, KC1>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv,
                                                 vsm, ts, nvc);
     else
         ladder3_tile<NP, false, PAIRED>(T, B, s, vir, pair_i, nvp, vtab, t, H, mode, do_pp, do_hh, out, sv, vsm, ts,
@@ -480,13 +480,20 @@ void set_ladder_smem_limit(int max_v)
     const int dev = current_device() % kMaxDevices;
     int &current = current_by_dev[dev];
     if (max_v > current) {
-        auto lb = [&](int np) { return (int)std::max(ladder_smem_bytes(max_v, np), ladder1_smem_bytes(max_v, np)); };
+        auto lb = [&](int np) {
+            return (int)std::max(ladder_smem_bytes(max_v, np), ladder1_smem_bytes(max_v, np, kLadKC1));
+        };
         const int b8 = lb(8);
         cudaFuncSetAttribute(k_ladder3<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
         cudaFuncSetAttribute(k_ladder3<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
         cudaFuncSetAttribute(k_ladder3<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(16));
         cudaFuncSetAttribute(k_ladder3<24, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(24));
         cudaFuncSetAttribute(k_ladder3<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(32));
+        cudaFuncSetAttribute(k_ladder3<8, true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
+        cudaFuncSetAttribute(k_ladder3<8, false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b8);
+        cudaFuncSetAttribute(k_ladder3<16, false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(16));
+        cudaFuncSetAttribute(k_ladder3<24, false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(24));
+        cudaFuncSetAttribute(k_ladder3<32, false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lb(32));
         current = max_v;
     }
 }
@@ -501,16 +508,27 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
         const int cnt = ncls[c];
         if (cnt <= 0) continue;
         const int np = c == 0 ? 8 : 8 * c;
-        const size_t sm = mode == 1 ? ladder1_smem_bytes(d.max_v, np) : ladder_smem_bytes(d.max_v, np);
+        const bool kc32 = mode == 1 && d.hh_kc == 32;
+        const size_t sm = mode == 1 ? ladder1_smem_bytes(d.max_v, np, kc32 ? 32 : kLadKC1) : ladder_smem_bytes(d.max_v, np);
 #define UEGCCD_LADDER_ARGS                                                                                  \
     tiles + off, d.blocks, d.solves, d.vir, d.pair_i, d.nvp, d.vtab, t, d.hh0, d.hh, mode, do_pp, do_hh, \
         g, d.active
-        switch (c) {
-        case 0: k_ladder3<8, true><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        case 1: k_ladder3<8, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        case 2: k_ladder3<16, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        case 3: k_ladder3<24, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
-        default: k_ladder3<32, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+        if (kc32) {
+            switch (c) {
+            case 0: k_ladder3<8, true, 32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            case 1: k_ladder3<8, false, 32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            case 2: k_ladder3<16, false, 32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            case 3: k_ladder3<24, false, 32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            default: k_ladder3<32, false, 32><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            }
+        } else {
+            switch (c) {
+            case 0: k_ladder3<8, true><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            case 1: k_ladder3<8, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            case 2: k_ladder3<16, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            case 3: k_ladder3<24, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            default: k_ladder3<32, false><<<cnt, 128, sm, st>>>(UEGCCD_LADDER_ARGS); break;
+            }
         }
 #undef UEGCCD_LADDER_ARGS
         off += cnt;
@@ -2003,6 +2021,28 @@ int tune_rings(DevBatch &d, cudaStream_t st)
                 d.ladder_sched = sched;
             }
         }
+    }
+    // the hole-hole intermediate's column chunk (mode 1 alone; it writes only d.hh)
+    if (err == cudaSuccess && d.nblocks > 0) {
+        float best = 1e30f;
+        int pick = 64;
+        const LadderTile *tl = d.ladder_sched ? d.htiles_lpt : d.htiles;
+        for (int kc : {64, 32}) {
+            d.hh_kc = kc;
+            launch_ladder3(d, tl, d.nhtile_cls, d.t, 1, 1, 1, d.g, st);
+            cudaEventRecord(e0, st);
+            launch_ladder3(d, tl, d.nhtile_cls, d.t, 1, 1, 1, d.g, st);
+            launch_ladder3(d, tl, d.nhtile_cls, d.t, 1, 1, 1, d.g, st);
+            cudaEventRecord(e1, st);
+            if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                pick = kc;
+            }
+        }
+        d.hh_kc = pick;
     }
     if (err == cudaSuccess) err = cudaGetLastError();
     if (e0) cudaEventDestroy(e0);

@@ -242,13 +242,15 @@ class Batch:
 
     def launch_shapes(self) -> dict:
         """The tuner's picks (after the first CCD solve): ring CTA sizes per class, the ring
-        staging CTA size, the ladder tile order (0 block order, 1 longest first)."""
+        staging CTA size, the ladder tile order (0 block order, 1 longest first), the hole-hole
+        intermediate's column chunk."""
         a = (C.c_int32 * 8)()
         n = capi.lib().uegccd_batch_launch_shapes(self._h, a, 8)
         if n < 0:
             capi.check(n)
         v = list(a[:n])
-        return {"ring_threads": v[:4], "stage_threads": v[4], "ladder_order": "longest first" if v[5] else "block"}
+        return {"ring_threads": v[:4], "stage_threads": v[4], "ladder_order": "longest first" if v[5] else "block",
+                "hh_chunk": v[6]}
 
     def set_profiling(self, on: bool) -> None:
         capi.check(capi.lib().uegccd_batch_set_profiling(self._h, 1 if on else 0))
