@@ -776,7 +776,13 @@ int build_batch(const UegccdSystem *systems, int n, std::unique_ptr<UegccdBatch>
     d.max_v = max_v;
     if (ladder_smem_bytes(max_v, 32) > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "ladder block exceeds shared memory");
     set_ladder_smem_limit(max_v);
-    d.mosaic_smem = mosaic_smem_bytes(max_v, max_o);
+    {   // the |q|^2 table the mosaic kernel stages: the batch's largest (tables beyond 1024
+        // entries stay in global memory)
+        int q2m = 0;
+        for (const auto &P : b->plans) q2m = std::max(q2m, P.q2max);
+        d.mosaic_vt = std::min(q2m + 1, kVtabSmemEntries);
+    }
+    d.mosaic_smem = mosaic_smem_bytes(max_v, max_o, d.mosaic_vt);
     if (d.mosaic_smem > 227 * 1024) return fail(UEGCCD_ERR_UNSUPPORTED, "mosaic block exceeds shared memory");
     set_mosaic_smem_limit(d.mosaic_smem);
     d.max_occ = max_occ;

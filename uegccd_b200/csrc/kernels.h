@@ -9,6 +9,8 @@
 namespace uegccd {
 
 // Raw device pointers of one batch (owned by the Batch object in capi.cu).
+constexpr int kVtabSmemEntries = 1024;   // |q|^2 table entries a kernel stages in shared memory at most
+
 struct DevBatch {
     int nsolves = 0, nblocks = 0, ntiles = 0, nchunks = 0, nrchunks = 0, ntargets = 0;
     int max_o = 0;      // largest o_K
@@ -17,6 +19,7 @@ struct DevBatch {
     double *mpart = nullptr;
     int32_t *mt_start = nullptr, *mt_list = nullptr;
     size_t mosaic_smem = 0;
+    int mosaic_vt = 0;  // |q|^2 table entries k_mosaic_blk stages: the batch's largest, at most kVtabSmemEntries
     int ntile_cls[5] = {0, 0, 0, 0, 0};   // ladder tiles per class: paired 8, then 8, 16, 24, 32 pairs
     int nhtile_cls[5] = {0, 0, 0, 0, 0};  // hole-hole intermediate tiles per class
     int max_occ = 0;    // largest NOcc
@@ -99,7 +102,7 @@ struct DevBatch {
 // dynamic shared memory of k_rings_wide for NOcc = O and R rows of a group pair
 size_t rings_smem_bytes(int O, int R);
 // dynamic shared memory of k_mosaic_blk for blocks of at most max_v virtuals
-size_t mosaic_smem_bytes(int max_v, int max_o);
+size_t mosaic_smem_bytes(int max_v, int max_o, int vt_n);
 void set_mosaic_smem_limit(size_t bytes);
 // dynamic shared memory of k_ladder3<np> for blocks of at most max_v virtuals
 // row-tile classes: paired 8 (blocks with at most kPairedRows rows i <= j, pad = 4 in

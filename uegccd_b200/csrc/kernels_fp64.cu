@@ -196,7 +196,7 @@ __global__ void k_reduce_solves(const int *__restrict__ chunk_begin, const doubl
 // i <= j (it updates each mirror from its pair).  The reference forms both rows
 // (CCD.f90:617-681); the two agree to rounding.
 // ----------------------------------------------------------------------------
-constexpr int kVtabSmem = 1024;  // |q|^2 table entries staged in shared memory
+constexpr int kVtabSmem = kVtabSmemEntries;  // |q|^2 table entries staged in shared memory
 
 // Ladder tiles v3: FP64 tensor-core MMA (mma.sync m8n8k4 f64; tcgen05 has no f64
 // kind).  One warp owns a 32 (a) x NP (p) output tile as 4 x NP/8 fragments of 8x8;
@@ -550,10 +550,10 @@ static int launch_ladder3(const DevBatch &d, const LadderTile *tiles, const int 
 // ----------------------------------------------------------------------------
 constexpr int kMosThreads = 128;
 
-size_t mosaic_smem_bytes(int max_v, int max_o)
+size_t mosaic_smem_bytes(int max_v, int max_o, int vt_n)
 {
-    return sizeof(double) * ((size_t)kVtabSmem + 2 * (size_t)max_v + (size_t)(kMosThreads / 32) * max_o) +
-           sizeof(int4) * ((size_t)max_v + 2 * (size_t)max_o) + sizeof(int) * (size_t)max_v;
+    return sizeof(double) * ((size_t)vt_n + 2 * (size_t)max_v + (size_t)(kMosThreads / 32) * max_o) +
+           sizeof(int) * (2 * (size_t)max_v + 2 * (size_t)max_o);
 }
 
 // The threads own the columns (c = tid + k * kMosThreads) and walk the rows: all warps stay
@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
                                                            const double *__restrict__ t,
                                                            const int16_t *__restrict__ pcol, int drpa,
                                                            double *__restrict__ mpart,
-                                                           const uint8_t *__restrict__ active)
+                                                           const uint8_t *__restrict__ active, int vt_n)
 {
     const BlockDev B = blocks[blockIdx.x];
     if (!active[B.solve]) return;
@@ -577,15 +577,15 @@ __global__ void __launch_bounds__(kMosThreads) k_mosaic_blk(const BlockDev *__re
     const int v = B.v, oc = B.nd + B.dg;
     constexpr int kW = kMosThreads / 32;
     extern __shared__ double msm[];
-    double *sv = msm;                          // kVtabSmem
-    double *coff = sv + kVtabSmem;             // v: column sums over the rows i < j
+    double *sv = msm;                          // vt_n: the batch's largest |q|^2 table (at most kVtabSmem)
+    double *coff = sv + vt_n;                  // v: column sums over the rows i < j
     double *cdg = coff + v;                    // v: the diagonal pair's row (if any)
     double *wrs = cdg + v;                     // kW x oc: per-warp row sums
     int *nvc = (int *)(wrs + kW * oc);         // v: packed n-vectors of the block's virtuals
     int *nk = nvc + v, *nl = nk + oc;          // oc: packed n-vectors of each row's k and l
     int *pc = nl + oc;                         // v: column of the partner d = K - c
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const bool vsm = s.q2max < kVtabSmem;
+    const bool vsm = s.q2max < vt_n;
     if (vsm)
         for (int q = tid; q <= s.q2max; q += kMosThreads) sv[q] = vtab[s.vtab0 + q];
     for (int c = tid; c < v; c += kMosThreads) {
@@ -2078,7 +2078,7 @@ int launch_residual(const DevBatch &d, const TermFlags &f, int mode, double *g_o
         kt->begin(KID_MOSAIC_S, st);
         k_mosaic_blk<<<d.nblocks, kMosThreads, d.mosaic_smem, st>>>(d.blocks, d.solves, d.pair_i, d.pair_j, d.vir,
                                                                    d.nvp, d.vtab, d.t, d.pcol, f.drpa, d.mpart,
-                                                                   d.active);
+                                                                   d.active, d.mosaic_vt);
         kt->end(st);
         kt->begin(KID_MOSAIC_RED, st);
         k_mosaic_sum<<<(d.ntargets + 7) / 8, 256, 0, st>>>(d.targets, d.ntargets, d.solves, d.mt_start, d.mt_list,
