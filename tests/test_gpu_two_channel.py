@@ -235,3 +235,23 @@ def test_batch_two_channel_matches_oracle():
     # an incremental solve stays spin-adapted: refused
     with pytest.raises(capi.UegccdError):
         b.start(do_ring=1, do_xring=0)
+
+
+def test_batch_two_channel_with_a_uniform_range_flag():
+    """A batch solve with Do XRings F on the batch's uniform range flag (uegccd_batch_set_range,
+    every term on flag 1 under Safe ERI) in the two-channel form, against the oracle."""
+    from uegccd_b200 import Batch
+
+    flags = {name: 1 for name in capi.RANGE_TERMS}
+    o, _ = _setup(flags, safe=True, extra={"Do XRings": "F"})
+    sc = o.scalars()
+    b = Batch([(o.nocc, sc["L"], sc["madelung"], o.eigen(), o.nvec())])
+    b.set_range(1, _screening(2 * o.nocc, sc["L"]))
+    rc, e2, res = b.solve(do_ring=1, do_xring=0, range_flags=len(KEYS))
+    _, ta2, tb2, tc2, _ = o.mp2()
+    st, en_o, _ = o.ccd(ta2, tb2, tc2)
+    assert rc == 0
+    assert res[0]["niter"] == st.niter
+    assert abs(res[0]["ecorr"] - st.ecorr) < 1e-11
+    en, _ = b.history(0)
+    np.testing.assert_allclose(en, en_o, atol=1e-11, rtol=0)

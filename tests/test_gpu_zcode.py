@@ -217,3 +217,27 @@ def test_ta_program_two_channel(goldens, tmp_path, monkeypatch, case):
     out = (tmp_path / "Output").read_text()
     ecs = [float(x) for x in re.findall(r"Ec\(CCD\) is\s+(-?\d+\.\d+)", out)]
     assert abs(ecs[-1] - st.ecorr) < 1e-9
+
+
+def test_g1_drpa_program_with_range_flags(goldens, tmp_path, monkeypatch):
+    """The G1 dRPA program under Safe ERI with per-term flags (Rings Range 2, DriverDir Range 1):
+    the general-flag dRPA (the terms on their flags, the energy on flag 0, dRPA.f90:206-207,
+    363-529) against the oracle's DrvdRPA on the same Input."""
+    from oracle.oracle import Oracle, parse_input_text
+
+    g = goldens["G1"]
+    vals = parse_input_text(g["input_text"])
+    vals.update({"Safe ERI": "T", "Rings Range": "2", "DriverDir Range": "1"})
+    (tmp_path / "Input").write_text("".join(f"{k}: {v}\n" for k, v in vals.items()))
+    monkeypatch.chdir(tmp_path)
+    zcode.run("Input")
+    out = (tmp_path / "Output").read_text()
+    ec = float(re.search(r"Ec\(dRPA\) is\s+(-?\d+\.\d+)", out).group(1))
+    es = float(re.search(r"Ec\(SOSEX\) is\s+(-?\d+\.\d+)", out).group(1))
+    niter = int(re.search(r"dRPA has converged in\s+(\d+)", out).group(1))
+    o = Oracle(vals)
+    _, ta, _, _, _ = o.mp2()
+    st, _, _ = o.drpa(ta.copy())
+    assert niter == st.niter
+    assert abs(ec - st.ecorr) < 5e-12 and abs(es - st.ecorr_sosex) < 5e-12
+    assert abs(ec - g["ec_drpa"]) > 1e-3   # the flags act
