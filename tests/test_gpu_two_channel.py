@@ -255,3 +255,32 @@ def test_batch_two_channel_with_a_uniform_range_flag():
     assert abs(res[0]["ecorr"] - st.ecorr) < 1e-11
     en, _ = b.history(0)
     np.testing.assert_allclose(en, en_o, atol=1e-11, rtol=0)
+
+
+def test_two_channel_solve_with_core_and_gap():
+    """Do XRings F with CoreN and GapII (NoCaseERI, HEG.f90:776-833): the replay solve of both
+    channels against the oracle; the core pairs stay zero in both channels."""
+    o, ctx = _setup(extra={"Do XRings": "F", "CoreFactor": "0.3", "GapII": "0.05"})
+    core = int(o.nocc * 0.3)
+    ctx.set_integrals(core_n=core, gapii=0.05)
+    _, ta, tb, tc = ctx.mp2()
+    rc, r, en, _ = ctx.ccd(ta, tb, tc, do_ring=1, do_xring=0, core_n=core, gapii=0.05)
+    _, ta2, tb2, tc2, _ = o.mp2()
+    st, en_o, _ = o.ccd(ta2, tb2, tc2)
+    assert rc == 0 and r["niter"] == st.niter
+    np.testing.assert_allclose(en, en_o, atol=1e-11, rtol=0)
+    assert np.abs(tb - tb2).max() < 1e-10 and np.abs(tc - tc2).max() < 1e-10
+    assert np.all(tb[:, :core, :] == 0) and np.all(tc[:, :, :core] == 0)
+
+
+def test_general_drpa_diis_reaches_the_replay_answer():
+    """dRPA with per-term flags under the Pulay scheme converges to the replay energy."""
+    flags = dict(ring=1, driver_direct=1)
+    o, ctx = _setup(flags, safe=True)
+    _, ta, _, _ = ctx.mp2()
+    rc, r_rep, _, _ = ctx.drpa(ta.copy(), tol=1e-10)
+    rc2, r_diis, _, _ = ctx.drpa(ta.copy(), tol=1e-10, scheme=1, ndiis=6)
+    assert rc == 0 and rc2 == 0 and r_diis["ndiis"] == 6
+    assert r_diis["niter"] <= r_rep["niter"]
+    assert abs(r_diis["ecorr"] - r_rep["ecorr"]) < 1e-9
+    assert abs(r_diis["ecorr_sosex"] - r_rep["ecorr_sosex"]) < 1e-9
