@@ -293,9 +293,8 @@ int uegccd_batch_get_amplitudes(UegccdBatch *b, int32_t s, double *t_abab);
  * call synchronises stream and returns when e2 is written.  Every call on a device shares that array:
  * calls must not overlap on one device (from several streams or threads), or
  * their results are wrong.  The first call on a device looks up the array's
- * address (which may load the library's device code): make that first call before
- * any stream capture begins on the device.  The address is kept until the process
- * exits: a cudaDeviceReset invalidates it, so do not use this entry point across one. */
+ * address (which may load the library's device code).  The address is kept until the
+ * process exits: a cudaDeviceReset invalidates it, so do not use this entry point across one. */
 int uegccd_mp2_energy_static(const UegccdSystem *sys, void *stream, double *e2);
 
 /* T2abab of every solve of the batch in the reference layout, solve after solve: solve s

@@ -23,8 +23,7 @@
 //
 // Set-up: the first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (which may load the module into the context) and keeps it
-// for the life of the process.  Make that first call before any stream capture
-// begins on the device.  A cudaDeviceReset unloads the module, so the kept address
+// for the life of the process.  A cudaDeviceReset unloads the module, so the kept address
 // is no longer valid afterwards: do not use this entry point across a reset.
 //
 // Every call copies E(2) back into host memory and synchronises `stream` before
